@@ -1,0 +1,158 @@
+/*
+ * sors_b200.h -- C ABI of the B200 implicit-Euler FEM step (libsors_b200.so).
+ *
+ * Plain C: opaque handle, caller-owned buffers, int32 status codes.  All
+ * vectors are FP64, 3*N long, in the reference's DOF order (3*vertex +
+ * component, cpp/src/energy.cpp:217-222).  Host pointers unless a name says
+ * "_device".
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the SORS project root).  The reference's Python module py_sors
+ * (cpp/py_sors.cpp) binds the C++ classes Energy<3,E> and Solver<3,E>; a
+ * maintainer binds these functions instead.
+ */
+#ifndef SORS_B200_H
+#define SORS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference throws std::runtime_error; the shim above this
+ * ABI rethrows with the same messages (see sors_last_error). */
+#define SORS_OK 0
+#define SORS_ERR_ARG 1            /* bad argument / unknown option            */
+#define SORS_ERR_INVERTED 2       /* "Inverted Elements" neoHookean.cpp:98-101 */
+#define SORS_ERR_NOT_CONVERGED 3  /* "Newton's method did not converge" solver.cpp:100-103 */
+#define SORS_ERR_PCG_BREAKDOWN 4  /* non-positive curvature in the linear solve */
+#define SORS_ERR_CUDA 5           /* CUDA runtime error                        */
+#define SORS_ERR_OOM 6            /* device allocation failed                  */
+#define SORS_ERR_LINESEARCH 7     /* Armijo backtracking exhausted             */
+#define SORS_ERR_UNSUPPORTED 8    /* option not built for this mesh type       */
+
+/* SimulationSettings (cpp/headers/simulationSettings.h:18-71) plus the
+ * device-solver options that have no reference counterpart. */
+typedef struct SorsSettings {
+    int32_t time_stepping;   /* 0 "backward_euler", 1 "crank_nicolson"           */
+    int32_t solver_method;   /* 0 "minimize_newton", 1 "minimize_newton_linesearch",
+                                2 "minimize_frozenhessian"                        */
+    double dt;               /* settings.dt, used when a call passes dt == 0      */
+    int32_t substeps;        /* settings.substeps                                */
+    int32_t cfl;             /* settings.CFLtimeSteppingFlag                     */
+    double grav[3];          /* gravAcceleration                                 */
+    double damping_alpha;    /* dampingAlpha                                     */
+    int32_t precision;       /* 0: FP64 everywhere; 1: FP32 Hessian + PCG, FP64
+                                residual, energy, dots and log(J)                */
+    int32_t project_spd;     /* 1: clamp negative eigenvalues of dP/dF per
+                                quadrature point before assembly                  */
+    int32_t material;        /* 0 "neohookean"; 1 the reference's quartic test
+                                element (cpp/src/_test.cpp:8-66)                 */
+    double newton_dx_tol;    /* ||dx|| stop, reference DX_TOL = 1e-9              */
+    double newton_res_tol;   /* ||gradient|| stop (absolute); <= 0 disables       */
+    int32_t newton_max_iter; /* reference MAX_ITER = 100                          */
+    double pcg_rel_tol;      /* smallest PCG forcing term                         */
+    int32_t pcg_max_iter;
+    int32_t device;          /* CUDA device ordinal                              */
+} SorsSettings;
+
+typedef struct SorsStepStats {
+    int32_t newton_iters;    /* summed over substeps                             */
+    int32_t pcg_iters;       /* summed over Newton iterations                    */
+    int32_t substeps;
+    double residual_norm;    /* ||gradient|| at the last evaluation              */
+    double dx_norm;          /* ||dx|| of the last Newton update                 */
+} SorsStepStats;
+
+typedef struct SorsHandle SorsHandle;
+
+/* Fills the defaults listed above. */
+void sors_default_settings(SorsSettings* s);
+
+/* Replaces Energy<3,E>::Energy (cpp/src/energy.cpp:4-204) for Neo-Hookean
+ * elements and the py_sors factory Energy(...) (cpp/py_sors.cpp:30-62).
+ * X: N x 3 undeformed vertices; conn: E x nodes_per_elem (4 tets, 8 hexes);
+ * density/youngs/poisson: per element.  Copies everything to the device,
+ * builds the fixed block-CSR Hessian pattern and the row-owner slot maps. */
+int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n_elems,
+                int32_t nodes_per_elem, const double* density, const double* youngs,
+                const double* poisson, const SorsSettings* settings, SorsHandle** out);
+
+/* Frees the handle and all its device memory. */
+void sors_destroy(SorsHandle* h);
+
+/* Message of the last failed call on this thread (reference exception text). */
+int sors_last_error(char* buf, size_t n);
+
+/* NeumannBC constraint parameters neumannBCmask / neumannBCvalue
+ * (cpp/src/energy.cpp:61-68, cpp/src/constraints/neumannBC.cpp). 3N each. */
+int sors_set_neumann(SorsHandle* h, const int32_t* mask, const double* value);
+
+/* PressureForce(surfaceVertexIdx, surfaceGroups)
+ * (cpp/src/forces/pressureForce.cpp:4-10): faces F x {3|4}, group per face. */
+int sors_set_pressure_faces(SorsHandle* h, const int32_t* faces, int32_t n_faces,
+                            int32_t verts_per_face, const int32_t* groups, int32_t n_groups);
+
+/* VertexForce (cpp/src/forces/vertexForce.cpp): enables the "vertexForce" actuation. */
+int sors_enable_vertex_force(SorsHandle* h, int32_t enable);
+
+/* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values)
+ * or "vertexForce" (3N values, row-major N x 3). */
+int sors_set_actuation(SorsHandle* h, const char* name, const double* values, int64_t n);
+
+/* Energy::set_initial_deformation / set_initial_velocity (cpp/headers/energy.h:203-204). */
+int sors_set_initial_deformation(SorsHandle* h, const double* q);
+int sors_set_initial_velocity(SorsHandle* h, const double* v);
+
+/* TimeIntegrator::get_qPrev / get_vPrev (cpp/headers/integrator.h:100-101). */
+int sors_get_state(SorsHandle* h, double* q_prev, double* v_prev);
+
+/* Energy::compute_energy (cpp/src/energy.cpp:208-248). */
+int sors_energy(SorsHandle* h, const double* q, double dt, double* out);
+
+/* Energy::compute_gradient (cpp/src/energy.cpp:252-308). */
+int sors_gradient(SorsHandle* h, const double* q, double dt, double* g);
+
+/* Energy::compute_hessian (cpp/src/energy.cpp:312-390) as 3x3 block CSR.
+ * Call with NULL outputs to get nnzb; row_ptr has N+1 entries, val 9*nnzb
+ * (row-major blocks).  The pattern is fixed at sors_create. */
+int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr, int32_t* col,
+                     double* val, int64_t* nnzb);
+
+/* Per-element Tetrahedron/Hexahedron::compute_{energy,gradient,hessian}
+ * (cpp/src/geometries/tetrahedron.cpp:99-134, hexahedron.cpp:68-103),
+ * scaled by the undeformed volume.  psi: E; grad: E x 3nv; hess: E x (3nv)^2.
+ * Any output may be NULL. */
+int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi, double* grad,
+                   double* hess);
+
+/* Solver<3,E>::step (cpp/src/solver.cpp:5-44): substeps of the configured
+ * minimiser followed by Energy::update_state.  dt == 0 / substeps == 0 take
+ * the settings.  q_in and q_out may alias. */
+int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps,
+              SorsStepStats* stats);
+
+/* Same step on a device-resident FP64 solution vector (in place). */
+int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substeps,
+                     SorsStepStats* stats);
+
+/* Energy::update_state (cpp/src/energy.cpp:539-557). */
+int sors_update_state(SorsHandle* h, const double* q, double dt);
+
+/* Device memory held by the handle, in bytes (admission by HBM footprint). */
+int64_t sors_device_bytes(const SorsHandle* h);
+
+/* Sizes of the fixed pattern: N, E, nnz blocks. */
+int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t* nnzb);
+
+/* CUDA stream of the handle (cudaStream_t as void*), for callers that order
+ * their own work after a step. */
+void* sors_stream(SorsHandle* h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SORS_B200_H */

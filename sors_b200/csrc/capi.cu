@@ -1,0 +1,850 @@
+// capi.cu -- C ABI, mesh-load set-up and the Newton / PCG driver.
+//
+// One handle = one mesh resident on one GPU with one CUDA stream.  Set-up
+// builds, once, the 3x3-block CSR pattern of the Hessian, the node -> (element,
+// local vertex) pair lists and the slot-item lists that map every pair block
+// to its CSR slot.  A step then runs, per Newton iteration: the row-owner
+// assembly (gradient rows + Hessian block-rows), the follower-load rows, the
+// gradient finalisation (integrator + Neumann rows), the block-Jacobi
+// inverses, PCG in CUDA-graph chunks, and the update.  One host
+// synchronisation per Newton iteration and one per PCG chunk.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/sors_b200.h"
+#include "sors_internal.h"
+
+using namespace sors;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CK(expr)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (expr);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return fail(SORS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) +     \
+                                           " at " #expr);                                         \
+    } while (0)
+
+constexpr int kPcgChunk = 16;  // PCG iterations per captured graph (even)
+
+}  // namespace
+
+struct SorsHandle {
+    SorsSettings s{};
+    int N = 0, E = 0, nv = 0, ndof = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int64_t nnzb = 0;
+    int max_pairs = 0;
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    // mesh + state
+    double *X = nullptr, *q = nullptr, *q0 = nullptr, *qPrev = nullptr, *vPrev = nullptr, *gPrev = nullptr,
+           *gPrevTmp = nullptr, *g = nullptr, *g_int = nullptr, *f_ext = nullptr, *mass = nullptr, *mval = nullptr,
+           *vforce = nullptr;
+    int* conn = nullptr;
+    double2* mat = nullptr;
+    int *row_ptr = nullptr, *col = nullptr, *diag_slot = nullptr, *pair_ptr = nullptr, *pair_ev = nullptr,
+        *slot_item_ptr = nullptr;
+    uint16_t* slot_items = nullptr;
+    uint8_t* node_mask = nullptr;
+    std::vector<uint8_t> mask_h;
+    std::vector<int> row_ptr_h, col_h;
+
+    // linear system
+    void* H = nullptr;
+    void* Minv = nullptr;
+    void *x = nullptr, *r = nullptr, *z = nullptr, *p0 = nullptr, *p1 = nullptr, *qv = nullptr;
+    double* partials = nullptr;
+    DevScalars* sc = nullptr;
+    DevScalars* sc_host = nullptr;  // pinned
+    int* status = nullptr;          // points into sc
+
+    // follower load
+    bool has_pressure = false, has_vforce = false, has_neumann = false;
+    int n_faces = 0, fnv = 0, n_groups = 0, nsurf = 0;
+    int *faces = nullptr, *face_group = nullptr, *surf_nodes = nullptr, *sface_ptr = nullptr, *sface_fl = nullptr;
+    double* pressure_d = nullptr;
+
+    // PCG chunk graph
+    cudaGraphExec_t pcg_exec = nullptr;
+    bool graph_failed = false;
+
+    double prev_gnorm = -1.0;
+};
+
+namespace {
+
+bool mixed(const SorsHandle* h) { return h->s.precision == 1; }
+size_t hsize(const SorsHandle* h) { return mixed(h) ? sizeof(float) : sizeof(double); }
+
+int dalloc(SorsHandle* h, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return fail(SORS_ERR_OOM, std::string("device allocation of ") + std::to_string(bytes) +
+                                      " bytes failed: " + cudaGetErrorString(e));
+    }
+    h->allocs.push_back(*p);
+    h->bytes += bytes;
+    return SORS_OK;
+}
+
+template <typename T>
+int dalloc_t(SorsHandle* h, T** p, size_t count) {
+    return dalloc(h, (void**)p, count * sizeof(T));
+}
+
+template <typename T>
+int upload(SorsHandle* h, T** p, const T* src, size_t count) {
+    int st = dalloc_t(h, p, count);
+    if (st) return st;
+    if (count) CK(cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    return SORS_OK;
+}
+
+double tet_vol_h(const double* a, const double* b, const double* c, const double* d) {
+    double ab[3], ac[3], ad[3];
+    for (int k = 0; k < 3; k++) { ab[k] = b[k] - a[k]; ac[k] = c[k] - a[k]; ad[k] = d[k] - a[k]; }
+    double cx = ac[1] * ad[2] - ac[2] * ad[1], cy = ac[2] * ad[0] - ac[0] * ad[2], cz = ac[0] * ad[1] - ac[1] * ad[0];
+    return fabs(ab[0] * cx + ab[1] * cy + ab[2] * cz) / 6.0;
+}
+
+// undeformed volume: tet (tetrahedron.cpp:137-149), hex 5-tet split (hexahedron.cpp:106-130)
+double elem_volume(const double* X, const int* en, int nv) {
+    if (nv == 4) return tet_vol_h(X + 3 * en[0], X + 3 * en[1], X + 3 * en[2], X + 3 * en[3]);
+    static const int T5[5][4] = {{0, 1, 3, 4}, {1, 2, 3, 6}, {1, 4, 5, 6}, {3, 4, 6, 7}, {1, 3, 4, 6}};
+    double v = 0;
+    for (int t = 0; t < 5; t++)
+        v += tet_vol_h(X + 3 * en[T5[t][0]], X + 3 * en[T5[t][1]], X + 3 * en[T5[t][2]], X + 3 * en[T5[t][3]]);
+    return v;
+}
+
+template <typename F>
+void parallel_for(int n, F&& f) {
+    int nt = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    if (n < 4096 || nt == 1) {
+        f(0, n);
+        return;
+    }
+    std::vector<std::thread> ts;
+    int chunk = (n + nt - 1) / nt;
+    for (int t = 0; t < nt; t++) {
+        int a = t * chunk, b = std::min(n, a + chunk);
+        if (a >= b) break;
+        ts.emplace_back([&f, a, b]() { f(a, b); });
+    }
+    for (auto& t : ts) t.join();
+}
+
+// Builds pattern, pair lists and slot-item lists (host), then uploads.
+int build_pattern(SorsHandle* h, const int32_t* conn) {
+    const int N = h->N, E = h->E, nv = h->nv;
+    std::vector<int> pair_ptr(N + 1, 0);
+    for (long long t = 0; t < (long long)E * nv; t++) pair_ptr[conn[t] + 1]++;
+    for (int i = 0; i < N; i++) pair_ptr[i + 1] += pair_ptr[i];
+    std::vector<int> pair_ev((size_t)E * nv);
+    {
+        std::vector<int> pos(pair_ptr.begin(), pair_ptr.end() - 1);
+        for (int e = 0; e < E; e++)
+            for (int v = 0; v < nv; v++) pair_ev[pos[conn[(size_t)e * nv + v]]++] = e * 8 + v;
+    }
+    int max_pairs = 0;
+    for (int i = 0; i < N; i++) max_pairs = std::max(max_pairs, pair_ptr[i + 1] - pair_ptr[i]);
+    if ((long long)max_pairs * nv > 65535)
+        return fail(SORS_ERR_UNSUPPORTED, "a node has too many incident elements for the slot maps");
+    h->max_pairs = max_pairs;
+
+    // block pattern: row i = sorted unique nodes of incident elements
+    std::vector<int> row_len(N, 0);
+    std::vector<std::vector<int>> rows_tmp;  // filled per chunk
+    std::vector<int> row_ptr(N + 1, 0);
+    std::vector<int> cols_all;
+    {
+        std::vector<std::vector<int>> per(N);
+        parallel_for(N, [&](int a, int b) {
+            std::vector<int> buf;
+            for (int i = a; i < b; i++) {
+                buf.clear();
+                for (int t = pair_ptr[i]; t < pair_ptr[i + 1]; t++) {
+                    int e = pair_ev[t] >> 3;
+                    for (int w = 0; w < nv; w++) buf.push_back(conn[(size_t)e * nv + w]);
+                }
+                if (buf.empty()) buf.push_back(i);  // isolated node keeps a diagonal block
+                std::sort(buf.begin(), buf.end());
+                buf.erase(std::unique(buf.begin(), buf.end()), buf.end());
+                per[i] = buf;
+            }
+        });
+        for (int i = 0; i < N; i++) row_ptr[i + 1] = row_ptr[i] + (int)per[i].size();
+        if ((long long)row_ptr[N] > 0x7fffffffLL / 9)
+            return fail(SORS_ERR_UNSUPPORTED, "Hessian pattern exceeds the 32-bit index range");
+        cols_all.resize(row_ptr[N]);
+        for (int i = 0; i < N; i++) std::copy(per[i].begin(), per[i].end(), cols_all.begin() + row_ptr[i]);
+    }
+    const int nnzb = row_ptr[N];
+    h->nnzb = nnzb;
+    for (int i = 0; i < N; i++) {
+        int nb = row_ptr[i + 1] - row_ptr[i];
+        if (nb > 255 * 9) return fail(SORS_ERR_UNSUPPORTED, "Hessian row too long");
+    }
+    std::vector<int> diag(N);
+    for (int i = 0; i < N; i++) {
+        auto b = cols_all.begin() + row_ptr[i], e = cols_all.begin() + row_ptr[i + 1];
+        diag[i] = (int)(std::lower_bound(b, e, i) - cols_all.begin());
+    }
+    // slot-item lists: items of slot b = (k*nv + w) for pairs k of row i whose vertex w is col[b]
+    std::vector<int> slot_cnt(nnzb + 1, 0);
+    std::vector<int> item_slot((size_t)E * nv * nv);
+    parallel_for(N, [&](int a, int b) {
+        for (int i = a; i < b; i++) {
+            auto cb = cols_all.begin() + row_ptr[i], ce = cols_all.begin() + row_ptr[i + 1];
+            for (int t = pair_ptr[i]; t < pair_ptr[i + 1]; t++) {
+                int e = pair_ev[t] >> 3;
+                for (int w = 0; w < nv; w++) {
+                    int j = conn[(size_t)e * nv + w];
+                    item_slot[(size_t)t * nv + w] = (int)(std::lower_bound(cb, ce, j) - cols_all.begin());
+                }
+            }
+        }
+    });
+    for (size_t t = 0; t < item_slot.size() && t < (size_t)pair_ptr[N] * nv; t++) slot_cnt[item_slot[t] + 1]++;
+    for (int b = 0; b < nnzb; b++) slot_cnt[b + 1] += slot_cnt[b];
+    std::vector<uint16_t> items((size_t)pair_ptr[N] * nv);
+    {
+        std::vector<int> pos(slot_cnt.begin(), slot_cnt.end() - 1);
+        for (int i = 0; i < N; i++)
+            for (int t = pair_ptr[i]; t < pair_ptr[i + 1]; t++) {
+                int k = t - pair_ptr[i];
+                for (int w = 0; w < nv; w++) items[pos[item_slot[(size_t)t * nv + w]]++] = (uint16_t)(k * nv + w);
+            }
+    }
+    int st;
+    if ((st = upload(h, &h->pair_ptr, pair_ptr.data(), pair_ptr.size()))) return st;
+    if ((st = upload(h, &h->pair_ev, pair_ev.data(), pair_ev.size()))) return st;
+    if ((st = upload(h, &h->row_ptr, row_ptr.data(), row_ptr.size()))) return st;
+    if ((st = upload(h, &h->col, cols_all.data(), cols_all.size()))) return st;
+    if ((st = upload(h, &h->diag_slot, diag.data(), diag.size()))) return st;
+    if ((st = upload(h, &h->slot_item_ptr, slot_cnt.data(), slot_cnt.size()))) return st;
+    if ((st = upload(h, &h->slot_items, items.data(), items.size()))) return st;
+    h->row_ptr_h = std::move(row_ptr);
+    h->col_h = std::move(cols_all);
+    return SORS_OK;
+}
+
+double inertia_coef(const SorsHandle* h, double dt) {
+    if (dt == 0.0) return 0.0;
+    double a = h->s.damping_alpha;
+    if (h->s.time_stepping == 0) return 1.0 / (dt * dt) + a / dt;
+    return 2.0 / (dt * dt) + 2.0 * a / dt;
+}
+
+int method(const SorsHandle* h) { return h->s.solver_method; }
+
+// f_ext = vertexForce + pressure forces at h->q
+int compute_external(SorsHandle* h) {
+    if (!(h->has_vforce || h->has_pressure)) return SORS_OK;
+    if (h->has_vforce)
+        CK(cudaMemcpyAsync(h->f_ext, h->vforce, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+    else
+        CK(cudaMemsetAsync(h->f_ext, 0, sizeof(double) * h->ndof, h->stream));
+    if (h->has_pressure) {
+        PressureArgs p;
+        p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
+        p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
+        p.f_ext = h->f_ext;
+        launch_pressure_force(p, h->stream);
+    }
+    return SORS_OK;
+}
+
+// Gradient (and Hessian when want_hess) at h->q.  Leaves gnorm2 in sc.
+template <typename HT>
+int eval_system(SorsHandle* h, double dt, bool want_hess) {
+    int st = compute_external(h);
+    if (st) return st;
+    AsmArgs<HT> a;
+    a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat;
+    a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
+    a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
+    a.H = (HT*)h->H; a.g_int = h->g_int; a.status = h->status;
+    a.stage_per_warp = h->max_pairs * h->nv * 9;
+    a.material = h->s.material; a.project = h->s.project_spd; a.apply_mask = 1;
+    a.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0;
+    a.want_hess = want_hess ? 1 : 0;
+    a.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0;
+    a.inertia_coef = inertia_coef(h, dt);
+    launch_assemble<HT>(a, h->max_pairs, h->stream);
+    if (want_hess && h->has_pressure && method(h) == 0) {
+        PressureArgs p;
+        p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
+        p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
+        p.f_ext = h->f_ext;
+        launch_pressure_jac<HT>(p, h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->stream);
+    }
+    launch_finalize_grad(h->N, h->g_int, h->f_ext, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, h->mass,
+                         h->node_mask, h->mval, dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav,
+                         a.neumann_override, (h->has_vforce || h->has_pressure) ? 1 : 0, h->g, h->partials, h->sc,
+                         h->stream);
+    CK(cudaGetLastError());
+    return SORS_OK;
+}
+
+int eval_energy(SorsHandle* h, double dt, double* out) {
+    int st = compute_external(h);
+    if (st) return st;
+    launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, h->partials, h->sc, h->stream);
+    launch_dof_energy(h->N, h->q, h->qPrev, h->vPrev, h->mass, h->f_ext, (h->has_vforce || h->has_pressure) ? 1 : 0,
+                      dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav, h->partials, h->sc, h->stream);
+    CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    *out = h->sc_host->e_elem + h->sc_host->e_dof;
+    return SORS_OK;
+}
+
+template <typename HT, typename VT>
+void pcg_iter_pair(SorsHandle* h) {
+    VT* z = (VT*)h->z;
+    launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
+                            h->partials, h->sc, h->stream);
+    launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
+                          h->stream);
+    launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
+                            h->partials, h->sc, h->stream);
+    launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
+                          h->stream);
+}
+
+template <typename HT, typename VT>
+int pcg_chunk(SorsHandle* h) {
+    if (!h->pcg_exec && !h->graph_failed) {
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
+            e = cudaStreamEndCapture(h->stream, &graph);
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pcg_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            h->graph_failed = true;
+            h->pcg_exec = nullptr;
+            cudaGetLastError();
+        }
+    }
+    if (h->pcg_exec) {
+        CK(cudaGraphLaunch(h->pcg_exec, h->stream));
+    } else {
+        for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
+        CK(cudaGetLastError());
+    }
+    return SORS_OK;
+}
+
+// Solves H dx = -g (dx in h->x).  Returns PCG iterations in *iters.
+template <typename HT, typename VT>
+int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters) {
+    launch_block_jacobi<HT, VT>(h->N, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, eta * eta,
+                            abs_tol * abs_tol, h->s.pcg_max_iter, h->partials, h->sc, h->stream);
+    CK(cudaGetLastError());
+    int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
+    for (int c = 0; c < maxchunks; c++) {
+        int st = pcg_chunk<HT, VT>(h);
+        if (st) return st;
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->sc_host->done) break;
+    }
+    *iters = h->sc_host->it;
+    if (h->sc_host->breakdown && h->sc_host->it == 0)
+        return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
+    return SORS_OK;
+}
+
+template <typename HT, typename VT>
+int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
+    const int n = h->ndof;
+    const int m = method(h);
+    const double dx_tol = h->s.newton_dx_tol;
+    const double res_tol = h->s.newton_res_tol;
+    bool converged = false;
+    int st = SORS_OK;
+    double prev_g = -1.0;
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    bool have_hess = false;
+    for (int it = 0; it < h->s.newton_max_iter; it++) {
+        bool want_hess = (m != 2) || !have_hess;  // frozen Hessian: assemble once
+        if ((st = eval_system<HT>(h, dt, want_hess))) return st;
+        if (want_hess) have_hess = true;
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->sc_host->status & kFlagInverted)
+            return fail(SORS_ERR_INVERTED, "Inverted Elements");
+        double gn = sqrt(h->sc_host->gnorm2);
+        if (stats) { stats->newton_iters++; stats->residual_norm = gn; }
+        if (!(gn == gn)) break;  // NaN gradient: diverged
+        if (res_tol > 0.0 && gn < res_tol) { converged = true; break; }
+        // forcing term (Eisenstat-Walker choice 2), floor pcg_rel_tol
+        double eta = 0.5;
+        if (prev_g > 0.0) {
+            double ratio = gn / prev_g;
+            eta = std::min(0.5, 0.9 * ratio * ratio);
+        }
+        eta = std::max(eta, h->s.pcg_rel_tol);
+        prev_g = gn;
+        int pit = 0;
+        if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
+        if (stats) stats->pcg_iters += pit;
+        if (m == 1) {
+            // Armijo backtracking (solver.cpp:201-264): c = 0.1, beta = 0.5
+            CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+            launch_dot_gdx<VT>(n, h->g, (const VT*)h->x, h->partials, h->sc, h->stream);
+            double e0;
+            if ((st = eval_energy(h, dt, &e0))) return st;
+            double gdx = h->sc_host->gdx;
+            double alpha = 1.0;
+            bool accepted = false;
+            for (int ls = 0; ls < 64; ls++) {
+                launch_newton_update<VT>(n, (const VT*)h->x, alpha, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+                double e1;
+                if ((st = eval_energy(h, dt, &e1))) return st;
+                if (e1 <= e0 + 0.1 * alpha * gdx) { accepted = true; break; }
+                alpha *= 0.5;
+            }
+            if (!accepted) return fail(SORS_ERR_LINESEARCH, "line search did not find a decrease");
+        } else {
+            CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+            launch_newton_update<VT>(n, (const VT*)h->x, 1.0, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+        }
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        double dxn = sqrt(h->sc_host->dxnorm2);
+        if (stats) stats->dx_norm = dxn;
+        if (!(dxn == dxn)) break;  // "Newton's method diverged"
+        if (dxn < dx_tol) { converged = true; break; }
+    }
+    if (!converged && m != 2) return fail(SORS_ERR_NOT_CONVERGED, "Newton's method did not converge");
+    return SORS_OK;
+}
+
+int run_minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
+    if (mixed(h)) return minimize<float, float>(h, dt, stats);
+    return minimize<double, double>(h, dt, stats);
+}
+
+// CFL time step (solver.cpp:300-331), host side
+int cfl_dt(SorsHandle* h, double dt, double* out) {
+    std::vector<double> q(h->ndof), v(h->ndof);
+    std::vector<int> conn((size_t)h->E * h->nv);
+    CK(cudaMemcpyAsync(q.data(), h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(v.data(), h->vPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(conn.data(), h->conn, sizeof(int) * conn.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double vmax = 0;
+    for (double a : v) vmax = std::max(vmax, fabs(a));
+    double lmin = -1;
+    for (int e = 0; e < h->E; e++)
+        for (int i = 0; i < h->nv; i++)
+            for (int j = i + 1; j < h->nv; j++) {
+                const double* a = &q[3 * conn[(size_t)e * h->nv + i]];
+                const double* b = &q[3 * conn[(size_t)e * h->nv + j]];
+                double l = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+                if (lmin < 0 || l < lmin) lmin = l;
+            }
+    double dtc = lmin / vmax;
+    *out = dtc < dt ? dtc : dt;
+    return SORS_OK;
+}
+
+int step_resident(SorsHandle* h, double dt, int substeps, SorsStepStats* stats) {
+    if (dt == 0.0) dt = h->s.dt;
+    if (substeps == 0) substeps = h->s.substeps;
+    if (h->s.cfl) {
+        double dtc;
+        int st = cfl_dt(h, dt, &dtc);
+        if (st) return st;
+        substeps = (int)ceil(dt / dtc);
+    }
+    if (substeps < 1) return fail(SORS_ERR_ARG, "substeps must be >= 1");
+    double dts = dt / substeps;
+    if (stats) memset(stats, 0, sizeof(*stats));
+    for (int j = 0; j < substeps; j++) {
+        int st = run_minimize(h, dts, stats);
+        if (st) return st;
+        launch_update_state(h->ndof, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, dts, h->s.time_stepping,
+                            h->stream);
+        if (stats) stats->substeps++;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaGetLastError());
+    return SORS_OK;
+}
+
+int set_device(SorsHandle* h) {
+    CK(cudaSetDevice(h->device));
+    return SORS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+void sors_default_settings(SorsSettings* s) {
+    memset(s, 0, sizeof(*s));
+    s->time_stepping = 1;  // SimulationSettings default "crank_nicolson"
+    s->solver_method = 0;
+    s->dt = 0.0;
+    s->substeps = 1;
+    s->cfl = 0;
+    s->damping_alpha = 0.0;
+    s->precision = 0;
+    s->project_spd = 1;
+    s->material = 0;
+    s->newton_dx_tol = 1e-9;
+    s->newton_res_tol = 0.0;
+    s->newton_max_iter = 100;
+    s->pcg_rel_tol = 1e-10;
+    s->pcg_max_iter = 20000;
+    s->device = 0;
+}
+
+int sors_last_error(char* buf, size_t n) {
+    if (!buf || n == 0) return (int)g_last_error.size();
+    size_t k = std::min(n - 1, g_last_error.size());
+    memcpy(buf, g_last_error.data(), k);
+    buf[k] = 0;
+    return (int)k;
+}
+
+int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n_elems, int32_t nodes_per_elem,
+                const double* density, const double* youngs, const double* poisson, const SorsSettings* settings,
+                SorsHandle** out) {
+    if (!out) return fail(SORS_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (nodes_per_elem != 4 && nodes_per_elem != 8) return fail(SORS_ERR_ARG, "nodes_per_elem must be 4 or 8");
+    if (n_nodes <= 0 || n_elems < 0 || !X || (n_elems > 0 && (!conn || !density || !youngs || !poisson)))
+        return fail(SORS_ERR_ARG, "empty mesh or NULL input");
+    for (long long t = 0; t < (long long)n_elems * nodes_per_elem; t++)
+        if (conn[t] < 0 || conn[t] >= n_nodes) return fail(SORS_ERR_ARG, "element index out of range");
+    SorsHandle* h = new (std::nothrow) SorsHandle();
+    if (!h) return fail(SORS_ERR_OOM, "host allocation failed");
+    if (settings) h->s = *settings; else sors_default_settings(&h->s);
+    h->N = n_nodes; h->E = n_elems; h->nv = nodes_per_elem; h->ndof = 3 * n_nodes;
+    h->device = h->s.device;
+    int st;
+    auto bail = [&](int code) { sors_destroy(h); return code; };
+    if ((st = set_device(h))) return bail(st);
+    if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return bail(fail(SORS_ERR_CUDA, "stream creation failed"));
+    const int N = n_nodes, E = n_elems, nv = nodes_per_elem;
+    // per-element Lame parameters (neoHookean.cpp:10-11) and lumped mass (energy.cpp:176-189)
+    std::vector<double2> mat(E > 0 ? E : 1);
+    std::vector<double> mass(N, 0.0);
+    for (int e = 0; e < E; e++) {
+        double Ey = youngs[e], nu = poisson[e];
+        mat[e].y = (Ey * nu) / ((1 + nu) * (1 - 2 * nu));
+        mat[e].x = Ey / (2 * (1 + nu));
+        double m = density[e] * elem_volume(X, conn + (size_t)e * nv, nv);
+        for (int v = 0; v < nv; v++) mass[conn[(size_t)e * nv + v]] += m / nv;
+    }
+    if ((st = upload(h, &h->X, X, (size_t)3 * N))) return bail(st);
+    if ((st = upload(h, &h->conn, conn, (size_t)E * nv))) return bail(st);
+    if ((st = upload(h, &h->mat, mat.data(), (size_t)E))) return bail(st);
+    if ((st = upload(h, &h->mass, mass.data(), (size_t)N))) return bail(st);
+    if ((st = build_pattern(h, conn))) return bail(st);
+    const size_t nd = (size_t)3 * N;
+    double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,
+                       &h->mval, &h->vforce};
+    for (double** p : vecs) {
+        if ((st = dalloc_t(h, p, nd))) return bail(st);
+        CK(cudaMemset(*p, 0, nd * sizeof(double)));
+    }
+    // TimeIntegrator(settings, undeformed vertices): qPrev = X (integrator.h:155-161)
+    CK(cudaMemcpy(h->qPrev, X, nd * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->q, X, nd * sizeof(double), cudaMemcpyHostToDevice));
+    h->mask_h.assign(N, 0);
+    if ((st = upload(h, &h->node_mask, h->mask_h.data(), (size_t)N))) return bail(st);
+    size_t hs = hsize(h);
+    if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs))) return bail(st);
+    if ((st = dalloc(h, &h->Minv, (size_t)N * 9 * hs))) return bail(st);
+    void** vv[] = {&h->x, &h->r, &h->z, &h->p0, &h->p1, &h->qv};
+    for (void** p : vv) {
+        if ((st = dalloc(h, p, nd * hs))) return bail(st);
+        CK(cudaMemset(*p, 0, nd * hs));
+    }
+    if ((st = dalloc_t(h, &h->partials, (size_t)kRedBlocks * kMaxScalars))) return bail(st);
+    if ((st = dalloc_t(h, &h->sc, 1))) return bail(st);
+    CK(cudaMemset(h->sc, 0, sizeof(DevScalars)));
+    h->status = &h->sc->status;
+    if (cudaMallocHost((void**)&h->sc_host, sizeof(DevScalars)) != cudaSuccess)
+        return bail(fail(SORS_ERR_OOM, "pinned allocation failed"));
+    if ((st = dalloc_t(h, &h->pressure_d, 1))) return bail(st);
+    CK(cudaDeviceSynchronize());
+    *out = h;
+    return SORS_OK;
+}
+
+void sors_destroy(SorsHandle* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->pcg_exec) cudaGraphExecDestroy(h->pcg_exec);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->sc_host) cudaFreeHost(h->sc_host);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+int sors_set_neumann(SorsHandle* h, const int32_t* mask, const double* value) {
+    if (!h || !mask || !value) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    for (int i = 0; i < h->N; i++) {
+        uint8_t m = 0;
+        for (int k = 0; k < 3; k++)
+            if (mask[3 * i + k] == 1) m |= (uint8_t)(1u << k);
+        h->mask_h[i] = m;
+    }
+    CK(cudaMemcpy(h->node_mask, h->mask_h.data(), h->N, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->mval, value, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    h->has_neumann = true;
+    return SORS_OK;
+}
+
+int sors_set_pressure_faces(SorsHandle* h, const int32_t* faces, int32_t n_faces, int32_t verts_per_face,
+                            const int32_t* groups, int32_t n_groups) {
+    if (!h || (n_faces > 0 && (!faces || !groups))) return fail(SORS_ERR_ARG, "NULL argument");
+    if (verts_per_face != 3 && verts_per_face != 4) return fail(SORS_ERR_ARG, "faces must have 3 or 4 vertices");
+    if ((h->nv == 4) != (verts_per_face == 3))
+        return fail(SORS_ERR_ARG, "tet meshes take triangles, hex meshes take quads");
+    int st;
+    if ((st = set_device(h))) return st;
+    for (long long t = 0; t < (long long)n_faces * verts_per_face; t++)
+        if (faces[t] < 0 || faces[t] >= h->N) return fail(SORS_ERR_ARG, "face vertex out of range");
+    for (int f = 0; f < n_faces; f++)
+        if (groups[f] < 0 || groups[f] >= n_groups) return fail(SORS_ERR_ARG, "face group out of range");
+    // surface rows: node -> (face, local index)
+    std::vector<std::vector<int>> inc(h->N);
+    for (int f = 0; f < n_faces; f++)
+        for (int k = 0; k < verts_per_face; k++) inc[faces[(size_t)f * verts_per_face + k]].push_back(f * 4 + k);
+    std::vector<int> surf, ptr(1, 0), fl;
+    for (int i = 0; i < h->N; i++)
+        if (!inc[i].empty()) {
+            surf.push_back(i);
+            fl.insert(fl.end(), inc[i].begin(), inc[i].end());
+            ptr.push_back((int)fl.size());
+        }
+    h->n_faces = n_faces; h->fnv = verts_per_face; h->n_groups = n_groups; h->nsurf = (int)surf.size();
+    if ((st = upload(h, &h->faces, faces, (size_t)n_faces * verts_per_face))) return st;
+    if ((st = upload(h, &h->face_group, groups, (size_t)n_faces))) return st;
+    if ((st = upload(h, &h->surf_nodes, surf.data(), surf.size()))) return st;
+    if ((st = upload(h, &h->sface_ptr, ptr.data(), ptr.size()))) return st;
+    if ((st = upload(h, &h->sface_fl, fl.data(), fl.size()))) return st;
+    if ((st = dalloc_t(h, &h->pressure_d, (size_t)std::max(1, n_groups)))) return st;
+    CK(cudaMemset(h->pressure_d, 0, sizeof(double) * std::max(1, n_groups)));
+    h->has_pressure = true;
+    return SORS_OK;
+}
+
+int sors_enable_vertex_force(SorsHandle* h, int32_t enable) {
+    if (!h) return fail(SORS_ERR_ARG, "NULL handle");
+    h->has_vforce = enable != 0;
+    return SORS_OK;
+}
+
+int sors_set_actuation(SorsHandle* h, const char* name, const double* values, int64_t n) {
+    if (!h || !name || (n > 0 && !values)) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    std::string nm(name);
+    if (nm == "pressure") {
+        if (!h->has_pressure) return SORS_OK;  // unused actuation entries are ignored
+        if (n < h->n_groups) return fail(SORS_ERR_ARG, "pressure actuation has fewer entries than surface groups");
+        CK(cudaMemcpy(h->pressure_d, values, sizeof(double) * h->n_groups, cudaMemcpyHostToDevice));
+        return SORS_OK;
+    }
+    if (nm == "vertexForce") {
+        if (n != h->ndof) return fail(SORS_ERR_ARG, "vertexForce actuation must have 3N entries");
+        CK(cudaMemcpy(h->vforce, values, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+        return SORS_OK;
+    }
+    return SORS_OK;  // other Params keys (e.g. softconMuscle) are not used by Neo-Hookean elements
+}
+
+int sors_set_initial_deformation(SorsHandle* h, const double* q) {
+    if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpy(h->qPrev, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    return SORS_OK;
+}
+
+int sors_set_initial_velocity(SorsHandle* h, const double* v) {
+    if (!h || !v) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpy(h->vPrev, v, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    return SORS_OK;
+}
+
+int sors_get_state(SorsHandle* h, double* q_prev, double* v_prev) {
+    if (!h) return fail(SORS_ERR_ARG, "NULL handle");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    if (q_prev) CK(cudaMemcpy(q_prev, h->qPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost));
+    if (v_prev) CK(cudaMemcpy(v_prev, h->vPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost));
+    return SORS_OK;
+}
+
+int sors_energy(SorsHandle* h, const double* q, double dt, double* out) {
+    if (!h || !q || !out) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    return eval_energy(h, dt, out);
+}
+
+int sors_gradient(SorsHandle* h, const double* q, double dt, double* g) {
+    if (!h || !q || !g) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    st = mixed(h) ? eval_system<float>(h, dt, false) : eval_system<double>(h, dt, false);
+    if (st) return st;
+    CK(cudaMemcpyAsync(g, h->g, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
+
+int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr, int32_t* col, double* val,
+                     int64_t* nnzb) {
+    if (!h) return fail(SORS_ERR_ARG, "NULL handle");
+    if (nnzb) *nnzb = h->nnzb;
+    if (!row_ptr && !col && !val) return SORS_OK;
+    int st;
+    if ((st = set_device(h))) return st;
+    if (row_ptr) memcpy(row_ptr, h->row_ptr_h.data(), sizeof(int) * (h->N + 1));
+    if (col) memcpy(col, h->col_h.data(), sizeof(int) * h->nnzb);
+    if (!val) return SORS_OK;
+    if (!q) return fail(SORS_ERR_ARG, "q is NULL");
+    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    st = mixed(h) ? eval_system<float>(h, dt, true) : eval_system<double>(h, dt, true);
+    if (st) return st;
+    size_t n = (size_t)h->nnzb * 9;
+    if (mixed(h)) {
+        std::vector<float> tmp(n);
+        CK(cudaMemcpyAsync(tmp.data(), h->H, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (size_t k = 0; k < n; k++) val[k] = tmp[k];
+    } else {
+        CK(cudaMemcpyAsync(val, h->H, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    int flag = 0;
+    CK(cudaMemcpy(&flag, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
+    return SORS_OK;
+}
+
+int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi, double* grad, double* hess) {
+    if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    const int n = 3 * h->nv;
+    double *dpsi = nullptr, *dgrad = nullptr, *dhess = nullptr;
+    auto cleanup = [&]() { cudaFree(dpsi); cudaFree(dgrad); cudaFree(dhess); };
+    if (psi && cudaMalloc(&dpsi, sizeof(double) * std::max(1, h->E)) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
+    if (grad && cudaMalloc(&dgrad, sizeof(double) * (size_t)std::max(1, h->E) * n) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
+    if (hess && cudaMalloc(&dhess, sizeof(double) * (size_t)std::max(1, h->E) * n * n) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
+    cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(h->status, 0, sizeof(int), h->stream);
+    if (mixed(h))
+        launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, project, dpsi, dgrad, dhess,
+                                h->status, h->stream);
+    else
+        launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, project, dpsi, dgrad, dhess,
+                                 h->status, h->stream);
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e == cudaSuccess && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * h->E, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && grad) e = cudaMemcpy(grad, dgrad, sizeof(double) * (size_t)h->E * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && hess) e = cudaMemcpy(hess, dhess, sizeof(double) * (size_t)h->E * n * n, cudaMemcpyDeviceToHost);
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, h->status, sizeof(int), cudaMemcpyDeviceToHost);
+    cleanup();
+    if (e != cudaSuccess) return fail(SORS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+    if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
+    return SORS_OK;
+}
+
+int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps, SorsStepStats* stats) {
+    if (!h || !q_in || !q_out) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpyAsync(h->q, q_in, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    st = step_resident(h, dt, substeps, stats);
+    if (st) return st;
+    CK(cudaMemcpyAsync(q_out, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
+
+int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substeps, SorsStepStats* stats) {
+    if (!h || !q_device) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpyAsync(h->q, q_device, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+    st = step_resident(h, dt, substeps, stats);
+    if (st) return st;
+    CK(cudaMemcpyAsync(q_device, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
+
+int sors_update_state(SorsHandle* h, const double* q, double dt) {
+    if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    launch_update_state(h->ndof, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, dt, h->s.time_stepping, h->stream);
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
+
+int64_t sors_device_bytes(const SorsHandle* h) { return h ? (int64_t)h->bytes : 0; }
+
+int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t* nnzb) {
+    if (!h) return fail(SORS_ERR_ARG, "NULL handle");
+    if (n_nodes) *n_nodes = h->N;
+    if (n_elems) *n_elems = h->E;
+    if (nnzb) *nnzb = h->nnzb;
+    return SORS_OK;
+}
+
+void* sors_stream(SorsHandle* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"

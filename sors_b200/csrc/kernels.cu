@@ -1,0 +1,877 @@
+// kernels.cu -- sm_100a kernels of the implicit-Euler FEM step.
+//
+// Assembly is row-owner: one warp owns one block-row (node) of the 3x3-block
+// CSR Hessian.  Its lanes evaluate the incident (element, local vertex) pairs
+// into shared memory, then sum them into the row's slots through the fixed
+// slot-item lists built at mesh load.  Every Hessian value and gradient entry
+// is written exactly once, by one warp, in a fixed order: no atomics, no
+// colouring, bit-reproducible.
+//
+// Reductions are deterministic two-stage sums (per-block partials in fixed
+// grid order, summed by the last block to finish).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fem_math.cuh"
+#include "sors_internal.h"
+
+namespace sors {
+
+// ---------------------------------------------------------------------------
+// deterministic reductions
+// ---------------------------------------------------------------------------
+template <int NS>
+__device__ __forceinline__ void warp_sum(double (&v)[NS]) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int s = 0; s < NS; s++) v[s] += __shfl_xor_sync(0xffffffffu, v[s], o);
+}
+
+// Block sum of v into partials[blockIdx.x*NS + s]; then the last block to
+// arrive sums all partials in grid order and returns true with totals in tot.
+template <int NS>
+__device__ bool reduce_grid(double (&v)[NS], double* partials, unsigned* counter, double (&tot)[NS]) {
+    __shared__ double sh[32][NS];
+    __shared__ bool am_last;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    warp_sum<NS>(v);
+    if (l == 0)
+#pragma unroll
+        for (int s = 0; s < NS; s++) sh[w][s] = v[s];
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) v[s] = (l < nw) ? sh[l][s] : 0.0;
+        warp_sum<NS>(v);
+        if (l == 0) {
+#pragma unroll
+            for (int s = 0; s < NS; s++) partials[blockIdx.x * NS + s] = v[s];
+            __threadfence();
+            unsigned t = atomicAdd(counter, 1u);
+            am_last = (t == gridDim.x - 1);
+        }
+    }
+    __syncthreads();
+    if (!am_last) return false;
+    __threadfence();
+    double a[NS];
+#pragma unroll
+    for (int s = 0; s < NS; s++) a[s] = 0.0;
+    const volatile double* vp = partials;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int s = 0; s < NS; s++) a[s] += vp[b * NS + s];
+    warp_sum<NS>(a);
+    __syncthreads();
+    if (l == 0)
+#pragma unroll
+        for (int s = 0; s < NS; s++) sh[w][s] = a[s];
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) a[s] = (l < nw) ? sh[l][s] : 0.0;
+        warp_sum<NS>(a);
+        if (l == 0)
+#pragma unroll
+            for (int s = 0; s < NS; s++) sh[0][s] = a[s];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NS; s++) tot[s] = sh[0][s];
+    if (threadIdx.x == 0) *counter = 0u;
+    return true;
+}
+
+static inline int red_grid(long long n, int per_thread = 1) {
+    long long b = (n + (long long)kRedThreads * per_thread - 1) / ((long long)kRedThreads * per_thread);
+    if (b < 1) b = 1;
+    if (b > kRedBlocks) b = kRedBlocks;
+    return (int)b;
+}
+
+// ---------------------------------------------------------------------------
+// element row evaluation shared by the assembly and the parity hook
+// ---------------------------------------------------------------------------
+template <typename HT, int NV, bool HESS>
+__device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const double* __restrict__ qg,
+                                         const int* __restrict__ conn, const double2* __restrict__ mat, int e,
+                                         int v, int material, bool project, double* g, HT* blk) {
+    double X[NV][3], x[NV][3];
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        int n = __ldg(conn + (size_t)e * NV + w);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            X[w][r] = __ldg(Xg + 3 * (size_t)n + r);
+            x[w][r] = qg[3 * (size_t)n + r];
+        }
+    }
+    if (HESS)
+        for (int k = 0; k < NV * 9; k++) blk[k] = HT(0);
+    if (material == 1) {
+        // quartic test element of the reference (cpp/src/_test.cpp:31-66)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double xv = x[v][r];
+            g[r] += (2 * xv - 1) * (2 * xv + 1) * xv;
+            if (HESS) blk[v * 9 + r * 3 + r] = (HT)(12 * xv * xv - 1);
+        }
+        return true;
+    }
+    double2 m = __ldg(mat + e);
+    bool ok = true;
+    double d[NV][3];
+    if (NV == 4) {
+        double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
+        ok = nh_qp_row<HT, NV, HESS>((const double(*)[3])d, (const double(*)[3])x, v, V, m.x, m.y, project, g, blk);
+    } else {
+        double V = hex_volume((const double(*)[3])X) * 0.125;
+        for (int s = 0; s < 8; s++) {
+            hex_shape((const double(*)[3])X, s, (double(*)[3])d);
+            ok &= nh_qp_row<HT, NV, HESS>((const double(*)[3])d, (const double(*)[3])x, v, V, m.x, m.y, project, g,
+                                          blk);
+        }
+    }
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// Row-owner assembly of gradient rows and Hessian block-rows.
+// ---------------------------------------------------------------------------
+template <typename HT, int NV>
+__global__ void __launch_bounds__(256) k_assemble(AsmArgs<HT> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int wpb = blockDim.x >> 5;
+    HT* stage = reinterpret_cast<HT*>(smem_raw) + (size_t)warp * a.stage_per_warp;
+    for (int row = blockIdx.x * wpb + warp; row < a.N; row += gridDim.x * wpb) {
+        const int p0 = a.pair_ptr[row];
+        const int np = a.pair_ptr[row + 1] - p0;
+        double g[3] = {0.0, 0.0, 0.0};
+        bool ok = true;
+        for (int k = lane; k < np; k += 32) {
+            int ev = __ldg(a.pair_ev + p0 + k);
+            int e = ev >> 3, v = ev & 7;
+            if (a.want_hess)
+                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, e, v, a.material, a.project != 0, g,
+                                             stage + (size_t)k * NV * 9);
+            else
+                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, e, v, a.material, false, g, nullptr);
+        }
+        if (!ok) atomicOr(a.status, kFlagInverted);
+        warp_sum<3>(g);
+        const unsigned mrow = a.node_mask[row];
+        if (lane < 3) {
+            double gv = (lane == 0) ? g[0] : (lane == 1 ? g[1] : g[2]);
+            if (a.apply_mask && ((mrow >> lane) & 1u)) gv = 0.0;
+            a.g_int[3 * (size_t)row + lane] = gv;
+        }
+        if (a.want_hess) {
+            __syncwarp();
+            const int b0 = a.row_ptr[row];
+            const int nb = a.row_ptr[row + 1] - b0;
+            const double md = a.inertia_coef * a.mass[row];
+            for (int t = lane; t < nb * 9; t += 32) {
+                const int s = t / 9, rc = t - s * 9, r = rc / 3, c = rc - r * 3;
+                const int bg = b0 + s;
+                const int i0 = __ldg(a.slot_item_ptr + bg), i1 = __ldg(a.slot_item_ptr + bg + 1);
+                HT acc = HT(0);
+                for (int it = i0; it < i1; ++it) acc += stage[(int)__ldg(a.slot_items + it) * 9 + rc];
+                const int j = __ldg(a.col + bg);
+                const unsigned mcol = a.node_mask[j];
+                const bool rmask = (mrow >> r) & 1u;
+                double val = (double)acc * a.hscale;
+                if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
+                if (j == row && r == c) {
+                    val += md;
+                    if (a.neumann_override && rmask) val = 1.0;
+                }
+                a.H[(size_t)bg * 9 + rc] = (HT)val;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+template <typename HT>
+void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
+    if (a.N == 0) return;
+    const int nv = a.nv;
+    size_t per_warp = (size_t)a.stage_per_warp * sizeof(HT);
+    int wpb = 8;
+    while (wpb > 1 && per_warp * wpb > 200 * 1024) wpb >>= 1;
+    size_t smem = per_warp * wpb;
+    int threads = wpb * 32;
+    long long rows_per_block = wpb;
+    long long blocks = (a.N + rows_per_block - 1) / rows_per_block;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (nv == 4) {
+        cudaFuncSetAttribute(k_assemble<HT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_assemble<HT, 4><<<(int)blocks, threads, smem, st>>>(a);
+    } else {
+        cudaFuncSetAttribute(k_assemble<HT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_assemble<HT, 8><<<(int)blocks, threads, smem, st>>>(a);
+    }
+    (void)max_pairs;
+}
+
+// Element-level parity hook: thread per (element, local vertex).
+template <typename HT, int NV>
+__global__ void k_elem_rows(int E, const double* X, const double* q, const int* conn, const double2* mat,
+                            int material, int project, double* psi, double* grad, double* hess, int* status) {
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)E * NV) return;
+    int e = (int)(t / NV), v = (int)(t - (long long)e * NV);
+    double g[3] = {0.0, 0.0, 0.0};
+    HT blk[NV * 9];
+    bool ok = elem_row<HT, NV, true>(X, q, conn, mat, e, v, material, project != 0, g, blk);
+    if (!ok) atomicOr(status, kFlagInverted);
+    const int n = 3 * NV;
+    if (grad)
+        for (int r = 0; r < 3; r++) grad[(size_t)e * n + 3 * v + r] = g[r];
+    if (hess)
+        for (int w = 0; w < NV; w++)
+            for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++)
+                    hess[(size_t)e * n * n + (size_t)(3 * v + k) * n + 3 * w + l] = (double)blk[w * 9 + k * 3 + l];
+    if (psi && v == 0) {
+        double Xl[NV][3], x[NV][3];
+        for (int w = 0; w < NV; w++) {
+            int nn = conn[(size_t)e * NV + w];
+            for (int r = 0; r < 3; r++) { Xl[w][r] = X[3 * (size_t)nn + r]; x[w][r] = q[3 * (size_t)nn + r]; }
+        }
+        double out = 0.0;
+        if (material == 1) {
+            for (int w = 0; w < NV; w++)
+                for (int r = 0; r < 3; r++) out += x[w][r] * x[w][r] * (x[w][r] * x[w][r] - 0.5);
+        } else {
+            double2 m = mat[e];
+            double d[NV][3], F[9];
+            if (NV == 4) {
+                double V = tet_shape((const double(*)[3])Xl, (double(*)[3])d);
+                for (int r = 0; r < 3; r++)
+                    for (int c = 0; c < 3; c++) {
+                        double acc = 0;
+                        for (int w = 0; w < NV; w++) acc += x[w][r] * d[w][c];
+                        F[r * 3 + c] = acc;
+                    }
+                out = V * nh_qp_energy(F, m.x, m.y);
+            } else {
+                double V = hex_volume((const double(*)[3])Xl);
+                double acc8 = 0.0;
+                for (int s = 0; s < 8; s++) {
+                    hex_shape((const double(*)[3])Xl, s, (double(*)[3])d);
+                    for (int r = 0; r < 3; r++)
+                        for (int c = 0; c < 3; c++) {
+                            double acc = 0;
+                            for (int w = 0; w < NV; w++) acc += x[w][r] * d[w][c];
+                            F[r * 3 + c] = acc;
+                        }
+                    acc8 += nh_qp_energy(F, m.x, m.y) * 0.125;
+                }
+                out = V * acc8;
+            }
+        }
+        psi[e] = out;
+    }
+}
+
+template <typename HT>
+void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                      int material, int project, double* psi, double* grad, double* hess, int* status,
+                      cudaStream_t st) {
+    long long n = (long long)E * nv;
+    if (n == 0) return;
+    int threads = 128;
+    int blocks = (int)((n + threads - 1) / threads);
+    if (nv == 4)
+        k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
+    else
+        k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
+}
+
+// ---------------------------------------------------------------------------
+// element energies (all elements, unmasked: energy.cpp:212-227)
+// ---------------------------------------------------------------------------
+template <int NV>
+__global__ void __launch_bounds__(kRedThreads) k_elem_energy(int E, const double* __restrict__ Xg,
+                                                             const double* __restrict__ qg,
+                                                             const int* __restrict__ conn,
+                                                             const double2* __restrict__ mat, int material,
+                                                             double* partials, DevScalars* sc) {
+    double acc[1] = {0.0};
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
+        double X[NV][3], x[NV][3];
+#pragma unroll
+        for (int w = 0; w < NV; w++) {
+            int n = __ldg(conn + (size_t)e * NV + w);
+#pragma unroll
+            for (int r = 0; r < 3; r++) { X[w][r] = __ldg(Xg + 3 * (size_t)n + r); x[w][r] = qg[3 * (size_t)n + r]; }
+        }
+        if (material == 1) {
+#pragma unroll
+            for (int w = 0; w < NV; w++)
+#pragma unroll
+                for (int r = 0; r < 3; r++) acc[0] += x[w][r] * x[w][r] * (x[w][r] * x[w][r] - 0.5);
+            continue;
+        }
+        double2 m = __ldg(mat + e);
+        double d[NV][3], F[9];
+        if (NV == 4) {
+            double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    double s = 0;
+#pragma unroll
+                    for (int w = 0; w < NV; w++) s += x[w][r] * d[w][c];
+                    F[r * 3 + c] = s;
+                }
+            acc[0] += V * nh_qp_energy(F, m.x, m.y);
+        } else {
+            double V = hex_volume((const double(*)[3])X);
+            double a8 = 0.0;
+            for (int s = 0; s < 8; s++) {
+                hex_shape((const double(*)[3])X, s, (double(*)[3])d);
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) {
+                        double t = 0;
+#pragma unroll
+                        for (int w = 0; w < NV; w++) t += x[w][r] * d[w][c];
+                        F[r * 3 + c] = t;
+                    }
+                a8 += nh_qp_energy(F, m.x, m.y) * 0.125;
+            }
+            acc[0] += V * a8;
+        }
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[0], tot) && threadIdx.x == 0) sc->e_elem = tot[0];
+}
+
+void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                        int material, double* partials, DevScalars* sc, cudaStream_t st) {
+    int blocks = red_grid(E);
+    if (nv == 4)
+        k_elem_energy<4><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
+    else
+        k_elem_energy<8><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
+}
+
+// ---------------------------------------------------------------------------
+// pressure force (pressureForce.cpp:14-56) and its Jacobian (:59-186),
+// row-owner over surface nodes
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void face_area(const int* f, int fnv, const double* q, double* area) {
+    const double* x0 = q + 3 * (size_t)f[0];
+    const double* x1 = q + 3 * (size_t)f[1];
+    const double* x2 = q + 3 * (size_t)f[2];
+    if (fnv == 3) {
+        double v1[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+        double v2[3] = {x2[0] - x0[0], x2[1] - x0[1], x2[2] - x0[2]};
+        area[0] = 0.5 * (v1[1] * v2[2] - v1[2] * v2[1]);
+        area[1] = 0.5 * (v1[2] * v2[0] - v1[0] * v2[2]);
+        area[2] = 0.5 * (v1[0] * v2[1] - v1[1] * v2[0]);
+    } else {
+        const double* x3 = q + 3 * (size_t)f[3];
+        double v1[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+        double v2[3] = {x3[0] - x0[0], x3[1] - x0[1], x3[2] - x0[2]};
+        double v3[3] = {x3[0] - x2[0], x3[1] - x2[1], x3[2] - x2[2]};
+        double v4[3] = {x1[0] - x2[0], x1[1] - x2[1], x1[2] - x2[2]};
+        area[0] = 0.5 * (v1[1] * v2[2] - v1[2] * v2[1]) + 0.5 * (v3[1] * v4[2] - v3[2] * v4[1]);
+        area[1] = 0.5 * (v1[2] * v2[0] - v1[0] * v2[2]) + 0.5 * (v3[2] * v4[0] - v3[0] * v4[2]);
+        area[2] = 0.5 * (v1[0] * v2[1] - v1[1] * v2[0]) + 0.5 * (v3[0] * v4[1] - v3[1] * v4[0]);
+    }
+}
+
+__global__ void k_pressure_force(PressureArgs p) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.nsurf) return;
+    int node = p.surf_nodes[s];
+    double f[3] = {0.0, 0.0, 0.0};
+    for (int t = p.sface_ptr[s]; t < p.sface_ptr[s + 1]; t++) {
+        int fl = p.sface_fl[t];
+        int face = fl >> 2;
+        const int* fv = p.faces + (size_t)face * p.fnv;
+        double area[3];
+        face_area(fv, p.fnv, p.q, area);
+        double pr = p.pressure[p.face_group[face]];
+        for (int k = 0; k < 3; k++) f[k] += -pr * area[k] / p.fnv;
+    }
+    for (int k = 0; k < 3; k++) p.f_ext[3 * (size_t)node + k] += f[k];
+}
+
+void launch_pressure_force(const PressureArgs& p, cudaStream_t st) {
+    if (p.nsurf == 0) return;
+    k_pressure_force<<<(p.nsurf + 127) / 128, 128, 0, st>>>(p);
+}
+
+// skew(b - a) as in pressureForce.cpp:76-90
+__device__ __forceinline__ void skew_ba(const double* a, const double* b, double* M) {
+    double d0 = b[0] - a[0], d1 = b[1] - a[1], d2 = b[2] - a[2];
+    M[0] = 0;   M[1] = -d2; M[2] = d1;
+    M[3] = d2;  M[4] = 0;   M[5] = -d0;
+    M[6] = -d1; M[7] = d0;  M[8] = 0;
+}
+
+__device__ void face_hess(const int* f, int fnv, const double* q, double (*h)[9]) {
+    const double* x0 = q + 3 * (size_t)f[0];
+    const double* x1 = q + 3 * (size_t)f[1];
+    const double* x2 = q + 3 * (size_t)f[2];
+    if (fnv == 3) {
+        skew_ba(x1, x2, h[0]);
+        skew_ba(x2, x0, h[1]);
+        skew_ba(x0, x1, h[2]);
+    } else {
+        const double* x3 = q + 3 * (size_t)f[3];
+        double t1[9], t3[9];
+        skew_ba(x1, x3, h[0]);
+        skew_ba(x3, x0, h[1]);
+        skew_ba(x0, x1, h[3]);
+        skew_ba(x3, x1, h[2]);
+        skew_ba(x2, x3, t1);
+        skew_ba(x1, x2, t3);
+        for (int k = 0; k < 9; k++) { h[1][k] += t1[k]; h[3][k] += t3[k]; }
+    }
+}
+
+// The reference's LDL^T reads the lower triangle of its input, so the
+// non-symmetric follower-load Jacobian enters as P(max(a,b), min(a,b)).
+template <typename HT>
+__global__ void k_pressure_jac(PressureArgs p, const int* row_ptr, const int* col, const uint8_t* node_mask,
+                               double cscale, HT* H) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.nsurf) return;
+    int i = p.surf_nodes[s];
+    int b0 = row_ptr[i], b1 = row_ptr[i + 1];
+    unsigned mi = node_mask[i];
+    for (int t = p.sface_ptr[s]; t < p.sface_ptr[s + 1]; t++) {
+        int fl = p.sface_fl[t];
+        int face = fl >> 2, ki = fl & 3;
+        const int* fv = p.faces + (size_t)face * p.fnv;
+        double h[4][9];
+        face_hess(fv, p.fnv, p.q, h);
+        double coef = cscale * p.pressure[p.face_group[face]] / 6.0;
+        for (int kj = 0; kj < p.fnv; kj++) {
+            int j = fv[kj];
+            int slot = -1;
+            for (int b = b0; b < b1; b++)
+                if (col[b] == j) { slot = b; break; }
+            if (slot < 0) continue;
+            unsigned mj = node_mask[j];
+            for (int l = 0; l < 3; l++) {
+                if ((mi >> l) & 1u) continue;
+                for (int m = 0; m < 3; m++) {
+                    if ((mj >> m) & 1u) continue;
+                    long long a = 3LL * i + l, b = 3LL * j + m;
+                    double val = 0.0;
+                    if (a > b) val = h[kj][l * 3 + m];
+                    else if (a < b) val = h[ki][m * 3 + l];
+                    if (val != 0.0) H[(size_t)slot * 9 + l * 3 + m] += (HT)(coef * val);
+                }
+            }
+        }
+    }
+}
+
+template <typename HT>
+void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
+                         double cscale, HT* H, cudaStream_t st) {
+    if (p.nsurf == 0) return;
+    k_pressure_jac<HT><<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, row_ptr, col, node_mask, cscale, H);
+}
+
+// ---------------------------------------------------------------------------
+// gradient finalisation: external forces, integrator, Neumann rows
+// (energy.cpp:282-306, integrator.cpp:45-84)
+// ---------------------------------------------------------------------------
+struct GradArgs {
+    int n;
+    const double *g_int, *f_ext, *q, *qPrev, *vPrev, *gPrev, *mass, *mval;
+    double* gPrevTmp;
+    const uint8_t* mask;
+    double dt, alpha, grav0, grav1, grav2;
+    int scheme, neumann_override, has_ext;
+    double* g;
+};
+
+__global__ void __launch_bounds__(kRedThreads) k_finalize_grad(GradArgs a, double* partials, DevScalars* sc) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        int node = i / 3, comp = i - 3 * node;
+        double m = a.mass[node];
+        double gr = comp == 0 ? a.grav0 : (comp == 1 ? a.grav1 : a.grav2);
+        double gi = a.g_int[i] - (a.has_ext ? a.f_ext[i] : 0.0);
+        double out;
+        if (a.dt == 0.0) {
+            out = -m * gr + gi;
+        } else {
+            a.gPrevTmp[i] = gi;
+            double v = a.scheme == 0 ? (a.q[i] - a.qPrev[i]) / a.dt : 2.0 * (a.q[i] - a.qPrev[i]) / a.dt - a.vPrev[i];
+            double inert = m * ((v - a.vPrev[i]) / a.dt) + (-m * gr) + a.alpha * m * v;
+            out = a.scheme == 0 ? inert + gi : inert + 0.5 * (gi + a.gPrev[i]);
+        }
+        if (a.neumann_override && ((a.mask[node] >> comp) & 1u)) out = -(a.qPrev[i] + a.dt * a.mval[i] - a.q[i]);
+        a.g[i] = out;
+        acc[0] += out * out;
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[1], tot) && threadIdx.x == 0) sc->gnorm2 = tot[0];
+}
+
+void launch_finalize_grad(int N, const double* g_int, const double* f_ext, const double* q, const double* qPrev,
+                          const double* vPrev, const double* gPrev, double* gPrevTmp, const double* mass,
+                          const uint8_t* mask, const double* mval, double dt, int scheme, double alpha,
+                          const double* grav, int neumann_override, int has_ext, double* g, double* partials,
+                          DevScalars* sc, cudaStream_t st) {
+    GradArgs a;
+    a.n = 3 * N; a.g_int = g_int; a.f_ext = f_ext; a.q = q; a.qPrev = qPrev; a.vPrev = vPrev; a.gPrev = gPrev;
+    a.gPrevTmp = gPrevTmp; a.mass = mass; a.mask = mask; a.mval = mval; a.dt = dt; a.scheme = scheme;
+    a.alpha = alpha; a.grav0 = grav[0]; a.grav1 = grav[1]; a.grav2 = grav[2];
+    a.neumann_override = neumann_override; a.has_ext = has_ext; a.g = g;
+    k_finalize_grad<<<red_grid(a.n, 4), kRedThreads, 0, st>>>(a, partials, sc);
+}
+
+// per-DOF energy terms (integrator.cpp:3-42, energy.cpp:229-244)
+struct DofEnergyArgs {
+    int n;
+    const double *q, *qPrev, *vPrev, *mass, *f_ext;
+    int has_ext, scheme;
+    double dt, alpha, grav0, grav1, grav2;
+};
+
+__global__ void __launch_bounds__(kRedThreads) k_dof_energy(DofEnergyArgs a, double* partials, DevScalars* sc) {
+    double acc[1] = {0.0};
+    double kc, dc;
+    if (a.scheme == 0) { kc = 0.5 * a.dt * a.dt; dc = 0.5 * a.alpha * a.dt; }
+    else { kc = 0.25 * a.dt * a.dt; dc = 0.25 * a.alpha * a.dt; }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        int node = i / 3, comp = i - 3 * node;
+        double m = a.mass[node];
+        double gr = comp == 0 ? a.grav0 : (comp == 1 ? a.grav1 : a.grav2);
+        double e = -m * a.q[i] * gr;
+        if (a.has_ext) e += a.f_ext[i] * (a.q[i] - a.qPrev[i]);
+        if (a.dt != 0.0) {
+            double v = a.scheme == 0 ? (a.q[i] - a.qPrev[i]) / a.dt : 2.0 * (a.q[i] - a.qPrev[i]) / a.dt - a.vPrev[i];
+            double ac = (v - a.vPrev[i]) / a.dt;
+            e += kc * m * ac * ac + dc * m * v * v;
+        }
+        acc[0] += e;
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[2], tot) && threadIdx.x == 0) sc->e_dof = tot[0];
+}
+
+void launch_dof_energy(int N, const double* q, const double* qPrev, const double* vPrev, const double* mass,
+                       const double* f_ext, int has_ext, double dt, int scheme, double alpha, const double* grav,
+                       double* partials, DevScalars* sc, cudaStream_t st) {
+    DofEnergyArgs a;
+    a.n = 3 * N; a.q = q; a.qPrev = qPrev; a.vPrev = vPrev; a.mass = mass; a.f_ext = f_ext; a.has_ext = has_ext;
+    a.scheme = scheme; a.dt = dt; a.alpha = alpha; a.grav0 = grav[0]; a.grav1 = grav[1]; a.grav2 = grav[2];
+    k_dof_energy<<<red_grid(a.n, 4), kRedThreads, 0, st>>>(a, partials, sc);
+}
+
+// ---------------------------------------------------------------------------
+// block-Jacobi preconditioner: inverse of each 3x3 diagonal block
+// ---------------------------------------------------------------------------
+template <typename HT, typename VT>
+__global__ void k_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const HT* b = H + (size_t)diag_slot[i] * 9;
+    double a[9], c[9];
+    for (int k = 0; k < 9; k++) a[k] = (double)b[k];
+    // symmetric part: the lower triangle defines the operator
+    a[1] = a[3]; a[2] = a[6]; a[5] = a[7];
+    cof3(a, c);
+    double det = a[0] * c[0] + a[1] * c[1] + a[2] * c[2];
+    VT* o = Minv + (size_t)i * 9;
+    if (det != 0.0 && det == det) {
+        double id = 1.0 / det;
+        for (int r = 0; r < 3; r++)
+            for (int cc = 0; cc < 3; cc++) o[r * 3 + cc] = (VT)(c[cc * 3 + r] * id);
+    } else {
+        for (int k = 0; k < 9; k++) o[k] = (VT)((k % 4 == 0) ? 1.0 : 0.0);
+    }
+}
+
+template <typename HT, typename VT>
+void launch_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st) {
+    if (N == 0) return;
+    k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, diag_slot, H, Minv);
+}
+
+// ---------------------------------------------------------------------------
+// PCG (block-Jacobi preconditioned CG), FP64 dots
+// ---------------------------------------------------------------------------
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r,
+                                                           VT* z, VT* p0, double eta2, double abs_tol2, int maxit,
+                                                           double* partials, DevScalars* sc) {
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT rr[3];
+        for (int k = 0; k < 3; k++) {
+            rr[k] = (VT)(-g[3 * (size_t)i + k]);
+            r[3 * (size_t)i + k] = rr[k];
+            x[3 * (size_t)i + k] = VT(0);
+            p0[3 * (size_t)i + k] = VT(0);
+        }
+        const VT* M = Minv + (size_t)i * 9;
+        for (int k = 0; k < 3; k++) {
+            VT zk = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
+            z[3 * (size_t)i + k] = zk;
+            acc[0] += (double)rr[k] * (double)zk;
+            acc[1] += (double)rr[k] * (double)rr[k];
+        }
+    }
+    double tot[2];
+    if (reduce_grid<2>(acc, partials, &sc->counters[3], tot) && threadIdx.x == 0) {
+        sc->rz = tot[0];
+        sc->rr = tot[1];
+        sc->bnorm2 = tot[1];
+        double t2 = eta2 * tot[1];
+        sc->tol2 = t2 > abs_tol2 ? t2 : abs_tol2;
+        sc->beta = 0.0;
+        sc->it = 0;
+        sc->maxit = maxit;
+        sc->breakdown = 0;
+        sc->done = (tot[1] <= sc->tol2 || maxit <= 0) ? 1 : 0;
+    }
+}
+
+template <typename HT, typename VT>
+void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
+                     double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st) {
+    k_pcg_init<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, Minv, x, r, z, p0, eta2, abs_tol2, maxit,
+                                                           partials, sc);
+}
+
+// q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q
+template <typename HT, typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __restrict__ row_ptr,
+                                                           const int* __restrict__ col, const HT* __restrict__ H,
+                                                           const VT* __restrict__ z, const VT* __restrict__ p_old,
+                                                           VT* __restrict__ p_new, VT* __restrict__ qv,
+                                                           double* partials, DevScalars* sc) {
+    if (*(volatile int*)&sc->done) return;
+    const double betad = sc->beta;
+    const VT beta = (VT)betad;
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    double acc[1] = {0.0};
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < N; row += gridDim.x * wpb) {
+        const int b0 = __ldg(row_ptr + row), nval = (__ldg(row_ptr + row + 1) - b0) * 9;
+        const HT* hv = H + (size_t)b0 * 9;
+        VT a0 = VT(0), a1 = VT(0), a2 = VT(0);
+        for (int t = lane; t < nval; t += 32) {
+            const int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
+            const int j = __ldg(col + b0 + blk);
+            const size_t jj = 3 * (size_t)j + c;
+            const VT pj = __ldg(z + jj) + beta * __ldg(p_old + jj);
+            const VT prod = (VT)__ldg(hv + t) * pj;
+            a0 += (r == 0) ? prod : VT(0);
+            a1 += (r == 1) ? prod : VT(0);
+            a2 += (r == 2) ? prod : VT(0);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane < 3) {
+            const size_t ii = 3 * (size_t)row + lane;
+            const VT qi = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
+            const VT pi = z[ii] + beta * p_old[ii];
+            p_new[ii] = pi;
+            qv[ii] = qi;
+            acc[0] += (double)pi * (double)qi;
+        }
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[4], tot) && threadIdx.x == 0) {
+        sc->pq = tot[0];
+        if (!(tot[0] > 0.0)) {
+            sc->breakdown = 1;
+            sc->done = 1;
+            sc->alpha = 0.0;
+        } else {
+            sc->alpha = sc->rz / tot[0];
+        }
+    }
+}
+
+template <typename HT, typename VT>
+void launch_pcg_spmv(int N, const int* row_ptr, const int* col, const HT* H, const VT* z, const VT* p_old,
+                     VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
+    int wpb = kRedThreads / 32;
+    long long blocks = (N + wpb - 1) / wpb;
+    if (blocks > kRedBlocks) blocks = kRedBlocks;
+    if (blocks < 1) blocks = 1;
+    k_pcg_spmv<HT, VT><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc);
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_pcg_update(int N, const VT* __restrict__ p, const VT* __restrict__ qv,
+                                                             const VT* __restrict__ Minv, VT* __restrict__ x,
+                                                             VT* __restrict__ r, VT* __restrict__ z,
+                                                             double* partials, DevScalars* sc) {
+    if (*(volatile int*)&sc->done) return;
+    const VT alpha = (VT)sc->alpha;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT rr[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t ii = 3 * (size_t)i + k;
+            x[ii] += alpha * p[ii];
+            rr[k] = r[ii] - alpha * qv[ii];
+            r[ii] = rr[k];
+        }
+        const VT* M = Minv + (size_t)i * 9;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            VT zk = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
+            z[3 * (size_t)i + k] = zk;
+            acc[0] += (double)rr[k] * (double)zk;
+            acc[1] += (double)rr[k] * (double)rr[k];
+        }
+    }
+    double tot[2];
+    if (reduce_grid<2>(acc, partials, &sc->counters[5], tot) && threadIdx.x == 0) {
+        sc->beta = tot[0] / sc->rz;
+        sc->rz = tot[0];
+        sc->rr = tot[1];
+        sc->it += 1;
+        if (tot[1] <= sc->tol2 || sc->it >= sc->maxit || !(tot[1] == tot[1])) sc->done = 1;
+    }
+}
+
+template <typename VT>
+void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
+                       DevScalars* sc, cudaStream_t st) {
+    k_pcg_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, Minv, x, r, z, partials, sc);
+}
+
+// ---------------------------------------------------------------------------
+// Newton update q = q0 + alpha dx, ||alpha dx||^2; g.dx; update_state
+// ---------------------------------------------------------------------------
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_newton_update(int n, const VT* dx, double alpha, double* q,
+                                                                const double* q0, double* partials, DevScalars* sc,
+                                                                int counter) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double d = alpha * (double)dx[i];
+        q[i] = q0[i] + d;
+        acc[0] += d * d;
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[counter], tot) && threadIdx.x == 0) sc->dxnorm2 = tot[0];
+}
+
+template <typename VT>
+void launch_newton_update(int n, const VT* dx, double alpha, double* q, const double* q0, double* partials,
+                          DevScalars* sc, int counter, cudaStream_t st) {
+    k_newton_update<VT><<<red_grid(n, 4), kRedThreads, 0, st>>>(n, dx, alpha, q, q0, partials, sc, counter);
+}
+
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_dot_gdx(int n, const double* g, const VT* dx, double* partials,
+                                                          DevScalars* sc) {
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) acc[0] += g[i] * (double)dx[i];
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[7], tot) && threadIdx.x == 0) sc->gdx = tot[0];
+}
+
+template <typename VT>
+void launch_dot_gdx(int n, const double* g, const VT* dx, double* partials, DevScalars* sc, cudaStream_t st) {
+    k_dot_gdx<VT><<<red_grid(n, 4), kRedThreads, 0, st>>>(n, g, dx, partials, sc);
+}
+
+__global__ void k_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
+                               const double* gPrevTmp, double dt, int scheme) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double v = scheme == 0 ? (q[i] - qPrev[i]) / dt : 2.0 * (q[i] - qPrev[i]) / dt - vPrev[i];
+    vPrev[i] = v;
+    qPrev[i] = q[i];
+    gPrev[i] = gPrevTmp[i];
+}
+
+void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
+                         const double* gPrevTmp, double dt, int scheme, cudaStream_t st) {
+    if (n == 0) return;
+    k_update_state<<<(n + 255) / 256, 256, 0, st>>>(n, q, qPrev, vPrev, gPrev, gPrevTmp, dt, scheme);
+}
+
+// y = H x (tests / diagnostics)
+template <typename HT>
+__global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y) {
+    int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (row >= N) return;
+    int b0 = row_ptr[row], nval = (row_ptr[row + 1] - b0) * 9;
+    double a[3] = {0, 0, 0};
+    for (int t = lane; t < nval; t += 32) {
+        int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
+        double pr = (double)H[(size_t)b0 * 9 + t] * x[3 * (size_t)col[b0 + blk] + c];
+        a[0] += r == 0 ? pr : 0.0; a[1] += r == 1 ? pr : 0.0; a[2] += r == 2 ? pr : 0.0;
+    }
+    warp_sum<3>(a);
+    if (lane < 3) y[3 * (size_t)row + lane] = a[lane];
+}
+
+template <typename HT>
+void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y,
+                       cudaStream_t st) {
+    if (N == 0) return;
+    k_spmv_plain<HT><<<(N + 7) / 8, 256, 0, st>>>(N, row_ptr, col, H, x, y);
+}
+
+// ---------------------------------------------------------------------------
+// explicit instantiations
+// ---------------------------------------------------------------------------
+template void launch_assemble<double>(const AsmArgs<double>&, int, cudaStream_t);
+template void launch_assemble<float>(const AsmArgs<float>&, int, cudaStream_t);
+template void launch_elem_rows<double>(int, int, const double*, const double*, const int*, const double2*, int, int,
+                                       double*, double*, double*, int*, cudaStream_t);
+template void launch_elem_rows<float>(int, int, const double*, const double*, const int*, const double2*, int, int,
+                                      double*, double*, double*, int*, cudaStream_t);
+template void launch_pressure_jac<double>(const PressureArgs&, const int*, const int*, const uint8_t*, double, double*,
+                                          cudaStream_t);
+template void launch_pressure_jac<float>(const PressureArgs&, const int*, const int*, const uint8_t*, double, float*,
+                                         cudaStream_t);
+template void launch_block_jacobi<double, double>(int, const int*, const double*, double*, cudaStream_t);
+template void launch_block_jacobi<float, float>(int, const int*, const float*, float*, cudaStream_t);
+template void launch_pcg_init<double, double>(int, const double*, const double*, double*, double*, double*, double*,
+                                              double, double, int, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_init<float, float>(int, const double*, const float*, float*, float*, float*, float*, double,
+                                            double, int, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_spmv<double, double>(int, const int*, const int*, const double*, const double*, const double*,
+                                              double*, double*, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_spmv<float, float>(int, const int*, const int*, const float*, const float*, const float*,
+                                            float*, float*, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_update<double>(int, const double*, const double*, const double*, double*, double*, double*,
+                                        double*, DevScalars*, cudaStream_t);
+template void launch_pcg_update<float>(int, const float*, const float*, const float*, float*, float*, float*, double*,
+                                       DevScalars*, cudaStream_t);
+template void launch_newton_update<double>(int, const double*, double, double*, const double*, double*, DevScalars*,
+                                           int, cudaStream_t);
+template void launch_newton_update<float>(int, const float*, double, double*, const double*, double*, DevScalars*, int,
+                                          cudaStream_t);
+template void launch_dot_gdx<double>(int, const double*, const double*, double*, DevScalars*, cudaStream_t);
+template void launch_dot_gdx<float>(int, const double*, const float*, double*, DevScalars*, cudaStream_t);
+template void launch_spmv_plain<double>(int, const int*, const int*, const double*, const double*, double*,
+                                        cudaStream_t);
+template void launch_spmv_plain<float>(int, const int*, const int*, const float*, const double*, double*,
+                                       cudaStream_t);
+
+}  // namespace sors

@@ -1,0 +1,124 @@
+// sors_internal.h -- device data layout and kernel launchers of libsors_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/sors_b200.h"
+
+namespace sors {
+
+// status bits raised by kernels
+enum : int { kFlagInverted = 1, kFlagPcgBreakdown = 2, kFlagNaN = 4 };
+
+// Reduction scratch: per-block partial sums + a completion counter per site.
+constexpr int kRedBlocks = 1184;      // 148 SMs x 8
+constexpr int kRedThreads = 256;
+constexpr int kMaxScalars = 4;
+
+struct DevScalars {
+    // Newton / energy reductions
+    double gnorm2;       // ||gradient||^2
+    double dxnorm2;      // ||dx||^2
+    double e_elem;       // sum of element energies
+    double e_dof;        // per-DOF energy terms
+    double gdx;          // gradient . dx
+    double minedge;      // CFL
+    double vmax;         // CFL
+    // PCG
+    double rz, pq, alpha, beta, rr, tol2, bnorm2;
+    int it, done, maxit, breakdown;
+    int status;          // kFlag* bits
+    unsigned counters[16];
+};
+
+// Row-owner assembly arguments (tet or hex).
+template <typename HT>
+struct AsmArgs {
+    int N, nv;
+    const double* X;        // 3N undeformed
+    const double* q;        // 3N current
+    const int* conn;        // E*nv
+    const double2* mat;     // (mu, lambda) per element
+    const int* pair_ptr;    // N+1
+    const int* pair_ev;     // e*8 + v
+    const int* row_ptr;     // N+1 (blocks)
+    const int* col;         // nnzb
+    const int* slot_item_ptr;   // nnzb+1
+    const uint16_t* slot_items; // k*nv + w
+    const uint8_t* node_mask;   // 3 bits per node
+    const double* mass;     // per node
+    HT* H;                  // nnzb*9
+    double* g_int;          // 3N (masked element gradient)
+    int* status;
+    int stage_per_warp;     // HT elements per warp of staging
+    int material;           // 0 NH, 1 quartic test
+    int project;
+    int apply_mask;         // drop masked DOFs from element terms (not SQP)
+    int neumann_override;   // diag = 1 on masked DOFs ("minimize_newton")
+    int want_hess;
+    double hscale;          // 0.5 for Crank-Nicolson with dt != 0
+    double inertia_coef;    // diag m * coef
+};
+
+struct PressureArgs {
+    int nsurf;                  // surface nodes with faces
+    const int* surf_nodes;      // node id per surface row
+    const int* sface_ptr;       // nsurf+1
+    const int* sface_fl;        // face*4 + local vertex index
+    const int* faces;           // F * fnv
+    const int* face_group;
+    int fnv;
+    const double* pressure;     // per group
+    const double* q;
+    double* f_ext;              // 3N (written for surface nodes)
+};
+
+// Launchers (kernels.cu)
+template <typename HT>
+void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st);
+template <typename HT>
+void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                      int material, int project, double* psi, double* grad, double* hess, int* status,
+                      cudaStream_t st);
+void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                        int material, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
+template <typename HT>
+void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
+                         double cscale, HT* H, cudaStream_t st);
+void launch_finalize_grad(int N, const double* g_int, const double* f_ext, const double* q, const double* qPrev,
+                          const double* vPrev, const double* gPrev, double* gPrevTmp, const double* mass,
+                          const uint8_t* mask, const double* mval, double dt, int scheme, double alpha,
+                          const double* grav, int neumann_override, int has_ext, double* g, double* partials,
+                          DevScalars* sc, cudaStream_t st);
+void launch_dof_energy(int N, const double* q, const double* qPrev, const double* vPrev, const double* mass,
+                       const double* f_ext, int has_ext, double dt, int scheme, double alpha, const double* grav,
+                       double* partials, DevScalars* sc, cudaStream_t st);
+template <typename HT, typename VT>
+void launch_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st);
+template <typename HT, typename VT>
+void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
+                     double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st);
+template <typename HT, typename VT>
+void launch_pcg_spmv(int N, const int* row_ptr, const int* col, const HT* H, const VT* z, const VT* p_old,
+                     VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
+                       DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_newton_update(int n, const VT* dx, double alpha, double* q, const double* q0, double* partials,
+                          DevScalars* sc, int counter, cudaStream_t st);
+template <typename VT>
+void launch_dot_gdx(int n, const double* g, const VT* dx, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
+                         const double* gPrevTmp, double dt, int scheme, cudaStream_t st);
+void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const double* vPrev, double* partials,
+                DevScalars* sc, cudaStream_t st);
+template <typename HT>
+void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y,
+                       cudaStream_t st);
+
+}  // namespace sors
