@@ -1,0 +1,370 @@
+#!/usr/bin/env python
+"""Implicit-Euler FEM step throughput on the jittered Neo-Hookean tet block.
+
+Workload (one "step" = one backward-Euler time step, i.e. one full Newton
+solve with block-Jacobi PCG linear solves, of the whole mesh):
+  beam 1.0 x 0.25 x 0.25 m as a 200 x 50 x 50 cell grid, 6 tets per cell
+  (3,000,000 tets, 522,801 nodes, 1,568,403 DOF); interior nodes jittered by
+  seeded U(+-10% h); per-element Young's modulus log-uniform in [5e4, 5e5] Pa,
+  nu = 0.45, rho = 1070; the x = 0 face clamped; gravity; dt = 5e-3 s.
+  Mixed precision (FP32 Hessian, SpMV and PCG vectors; FP64 residual, energy,
+  dots and log J) is the headline; the plain FP64 path is timed beside it.
+
+value   = elements x steps / s with the state resident in HBM (Solver.step_device)
+e2e     = the same through Solver.step with pinned host buffers (H2D of q and
+          D2H of the result inside every timed step)
+Inputs are larger than L2 (the assembled system is ~1.1 GB), so no flush.
+
+--impl reference times the CPU restatement of the reference path (oracle/,
+FP64, OpenMP element loops + sparse LDL^T Newton, all host threads) on a
+bounded sample of the same workload (a 24 x 12 x 12 cell block with the same
+spacing, jitter and material distribution), in the same unit.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fem_step_throughput"
+UNIT = "elem*steps/s"
+SIZE = (1.0, 0.25, 0.25)
+CELLS = (200, 50, 50)
+SAMPLE_CELLS = (24, 12, 12)
+DT = 5e-3
+
+
+def workload_name(cells, precision):
+    nx, ny, nz = cells
+    return (f"jittered 6-tet Neo-Hookean block {nx}x{ny}x{nz} cells ({6 * nx * ny * nz:,} tets, "
+            f"{(nx + 1) * (ny + 1) * (nz + 1):,} nodes), E log-uniform [5e4,5e5], nu 0.45, rho 1070, "
+            f"x=0 clamped, gravity, backward Euler dt 5e-3, {precision}")
+
+
+def block_mesh(cells, seed=0):
+    from sors_b200 import meshes
+    nx, ny, nz = cells
+    h = SIZE[0] / CELLS[0]
+    X, T, E = meshes.jittered_block_tets(nx, ny, nz, (nx * h, ny * h, nz * h), jitter=0.1, seed=seed)
+    mask, val = meshes.clamp_mask(X)
+    return X, T, E, mask, val
+
+
+def make_settings(precision):
+    from sors_b200 import py_sors as ps
+    s = ps.SimulationSettings()
+    s.meshType = "Tetrahedron"
+    s.dt = DT
+    s.substeps = 1
+    s.timeSteppingScheme = "backward_euler"
+    s.solverMethod = "minimize_newton"
+    s.precision = precision
+    s.hessianProjection = True
+    s.newtonResidualTol = 1e-8
+    return s
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"sors_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=open(self.path, "w"),
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for nm, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        try:
+            return float(json.load(open(p))["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(kernel_key, units):
+    """DRAM bytes per launch of a kernel from the committed ncu summary, scaled to `units`."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return None
+    try:
+        d = json.load(open(p)).get(kernel_key)
+        return float(d["dram_bytes_per_launch"]) * units / float(d["units"])
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# CPU restatement (oracle) on a bounded sample
+# ---------------------------------------------------------------------------
+def cpu_sample_run(steps, warmup, threads=None):
+    from oracle import oracle as orc
+    X, T, E, mask, val = block_mesh(SAMPLE_CELLS, seed=0)
+    nthreads = threads or os.cpu_count() or 1
+    o = orc.System(X, T, rho=1070.0, youngs=E, nu=0.45, grav=(0, 0, -9.81), scheme="backward_euler",
+                   method="minimize_newton", dt=DT, substeps=1, nthreads=nthreads)
+    o.set_neumann(mask, val)
+    q = X.ravel().copy()
+    for _ in range(warmup):
+        q, st = o.step(q)
+        if st != 0:
+            raise RuntimeError(f"oracle step failed ({st})")
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        q, st = o.step(q)
+        if st != 0:
+            raise RuntimeError(f"oracle step failed ({st})")
+    dt_wall = time.perf_counter() - t0
+    ne = T.shape[0]
+    return {"value": ne * steps / dt_wall, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": f"{SAMPLE_CELLS[0]}x{SAMPLE_CELLS[1]}x{SAMPLE_CELLS[2]} cells of the same block "
+                      f"({ne:,} tets, same spacing/jitter/material distribution), {steps} full implicit steps "
+                      f"after {warmup} warm-up, FP64 OpenMP assembly + sparse LDL^T Newton (||dx||<1e-9)",
+            "ms_per_step": 1e3 * dt_wall / steps, "elements": ne}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 6))
+    warmup = 1
+    cb = cpu_sample_run(steps, warmup)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
+            "warmup": warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": workload_name(SAMPLE_CELLS, "FP64 (CPU restatement of the reference path)")},
+            "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def build_energy(precision, X, T, E, mask, val, device):
+    from sors_b200 import py_sors as ps
+    s = make_settings(precision)
+    s.device = device
+    en = ps.EnergyTet.from_arrays(X, T, s, np.array([0.0, 0.0, -9.81]), 0.0, density=1070.0, youngsModulus=E,
+                                  poissonsRatio=0.45, neumannBCmask=mask, neumannBCvalue=val)
+    return en, ps.Solver(s)
+
+
+def timed_device_steps(torch, L, en, sol, q_dev, steps, stream):
+    """Device-resident steps timed with CUDA events on the library's stream."""
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    newton = pcg = 0
+    for _ in range(steps):
+        st = sol.step_device(q_dev.data_ptr(), en)
+        newton += st.newton_iters
+        pcg += st.pcg_iters
+    ev1.record(stream)
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1), newton, pcg
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+    from sors_b200 import _lib
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    torch.cuda.set_device(local_rank)
+    L = _lib.load()
+    cells = tuple(args.cells)
+    X, T, E, mask, val = block_mesh(cells, seed=0)
+    ne = T.shape[0]
+    nn = X.shape[0]
+    en, sol = build_energy(args.precision, X, T, E, mask, val, local_rank)
+    stream = torch.cuda.ExternalStream(L.sors_stream(en.handle()), device=local_rank)
+    q_dev = torch.tensor(X.ravel(), dtype=torch.float64, device=f"cuda:{local_rank}")
+    for _ in range(args.warmup):
+        sol.step_device(q_dev.data_ptr(), en)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.sors_kernel_launch_count()
+    with Clocks(local_rank) as clk:
+        ms, newton, pcg = timed_device_steps(torch, L, en, sol, q_dev, args.steps, stream)
+    launches = L.sors_kernel_launch_count() - launches0
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    value = world * ne * args.steps / (ms / 1e3)
+    # kernel roofline on the final assembled system
+    prof = _lib.SorsKernelProfile()
+    _lib.check(L.sors_profile_kernels(en.handle(), 20, __import__("ctypes").byref(prof)))
+    per_step = {
+        "pcg_spmv": (pcg / args.steps) * prof.spmv_ms,
+        "pcg_update": (pcg / args.steps) * prof.pcg_update_ms,
+        "assemble": (newton / args.steps) * prof.assemble_ms,
+    }
+    dom = max(per_step, key=per_step.get)
+    bytes_ = {"pcg_spmv": prof.spmv_bytes, "pcg_update": prof.pcg_update_bytes, "assemble": prof.assemble_bytes}[dom]
+    dur = {"pcg_spmv": prof.spmv_ms, "pcg_update": prof.pcg_update_ms, "assemble": prof.assemble_ms}[dom]
+    peak, peak_src = measured_peak_hbm()
+    achieved = bytes_ / (dur / 1e3) / 1e9
+    traffic = ncu_traffic(f"{dom}_{args.precision}", nn)
+    # end-to-end through Solver.step with pinned host buffers
+    q_host = torch.empty(3 * nn, dtype=torch.float64, pin_memory=True).numpy()
+    q_out = torch.empty(3 * nn, dtype=torch.float64, pin_memory=True).numpy()
+    q_host[:] = q_dev.cpu().numpy()
+    e2e_steps = args.steps
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(e2e_steps):
+        sol.step(q_host, en, out=q_out)
+        q_host[:] = q_out
+    ev1.record(stream)
+    ev1.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = world * ne * e2e_steps / (e2e_ms / 1e3)
+    # plain FP64 drop-in beside it (same trajectory length)
+    fp64 = None
+    if not args.no_fp64 and args.precision == "mixed":
+        del en  # free the mixed handle's memory first
+        en64, sol64 = build_energy("fp64", X, T, E, mask, val, local_rank)
+        q64 = torch.tensor(X.ravel(), dtype=torch.float64, device=f"cuda:{local_rank}")
+        for _ in range(args.warmup):
+            sol64.step_device(q64.data_ptr(), en64)
+        stream64 = torch.cuda.ExternalStream(L.sors_stream(en64.handle()), device=local_rank)
+        ms64, n64, p64 = timed_device_steps(torch, L, en64, sol64, q64, args.steps, stream64)
+        # the mixed run advanced W + K + K(e2e) steps; compare at equal step counts
+        qm = torch.tensor(X.ravel(), dtype=torch.float64, device=f"cuda:{local_rank}")
+        prof64 = _lib.SorsKernelProfile()
+        _lib.check(L.sors_profile_kernels(en64.handle(), 20, __import__("ctypes").byref(prof64)))
+        fp64 = {"value": ne * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
+                "newton_iters_per_step": n64 / args.steps, "pcg_iters_per_step": p64 / args.steps,
+                "spmv_gbs": prof64.spmv_bytes / (prof64.spmv_ms / 1e3) / 1e9,
+                "assemble_gbs": prof64.assemble_bytes / (prof64.assemble_ms / 1e3) / 1e9,
+                "final_disp_max": float((q64 - torch.tensor(X.ravel(), device=q64.device)).abs().max())}
+        del qm
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+        "config": {"workload": workload_name(cells, "mixed precision" if args.precision == "mixed" else "FP64"),
+                   "elements": ne, "nodes": nn, "dofs": 3 * nn, "precision": args.precision,
+                   "newton": "||dx||<1e-9 or ||g||<1e-8, Eisenstat-Walker PCG forcing",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (assembled system ~1 GB resident), no flush"},
+        "newton_steps_per_s": world * args.steps / (ms / 1e3),
+        "newton_iters_per_step": newton / args.steps, "pcg_iters_per_step": pcg / args.steps,
+        "assembly_gbs": prof.assemble_bytes / (prof.assemble_ms / 1e3) / 1e9,
+        "kernels": {"assemble_ms": prof.assemble_ms, "spmv_ms": prof.spmv_ms, "pcg_update_ms": prof.pcg_update_ms,
+                    "spmv_gbs": prof.spmv_bytes / (prof.spmv_ms / 1e3) / 1e9,
+                    "pcg_update_gbs": prof.pcg_update_bytes / (prof.pcg_update_ms / 1e3) / 1e9,
+                    "share_ms_per_step": per_step},
+        "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,
+                     "algorithmic_bytes_per_launch": bytes_},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 8 * 3 * nn, "d2h_bytes_per_step": 8 * 3 * nn},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+    }
+    if fp64:
+        line["fp64"] = fp64
+    if world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_sample_run(steps=3, warmup=1)
+            line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        except Exception as ex:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"failed: {ex}"}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+    else:
+        run_gpu(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

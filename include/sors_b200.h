@@ -147,6 +147,20 @@ int64_t sors_device_bytes(const SorsHandle* h);
 /* Sizes of the fixed pattern: N, E, nnz blocks. */
 int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t* nnzb);
 
+/* Per-launch device time (CUDA events on the handle's stream, averaged over
+ * `iters` back-to-back launches on the current assembled system) and the
+ * algorithmic bytes each launch must move: every input and output counted
+ * once.  Diagnostic only; no reference counterpart. */
+typedef struct SorsKernelProfile {
+    double assemble_ms, spmv_ms, pcg_update_ms, energy_ms;
+    double assemble_bytes, spmv_bytes, pcg_update_bytes, energy_bytes;
+} SorsKernelProfile;
+int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
+
+/* Number of kernels this library has launched in this process (graph
+ * launches count every kernel node).  Diagnostic only. */
+int64_t sors_kernel_launch_count(void);
+
 /* CUDA stream of the handle (cudaStream_t as void*), for callers that order
  * their own work after a step. */
 void* sors_stream(SorsHandle* h);

@@ -1412,6 +1412,9 @@ int orc_solve_with_hessian(OrcSystem* s, const double* q, double dt, const doubl
     return st;
 }
 
+/* Number of nonzeros of the last L factor (diagnostics). */
+int64_t orc_last_lnz(OrcSystem* s) { return s->ldl.Lp ? s->ldl.Lp[s->ldl.n] : 0; }
+
 int orc_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

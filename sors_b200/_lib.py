@@ -46,6 +46,11 @@ class SorsStepStats(C.Structure):
     ]
 
 
+class SorsKernelProfile(C.Structure):
+    _fields_ = [(n, C.c_double) for n in ("assemble_ms", "spmv_ms", "pcg_update_ms", "energy_ms", "assemble_bytes",
+                                          "spmv_bytes", "pcg_update_bytes", "energy_bytes")]
+
+
 # (name, restype, argtypes) of every exported symbol declared in include/sors_b200.h
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -73,6 +78,8 @@ SIGNATURES = [
     ("sors_update_state", C.c_int, [_h, _dp, C.c_double]),
     ("sors_device_bytes", C.c_int64, [_h]),
     ("sors_sizes", C.c_int, [_h, _lp, _lp, _lp]),
+    ("sors_profile_kernels", C.c_int, [_h, C.c_int32, C.POINTER(SorsKernelProfile)]),
+    ("sors_kernel_launch_count", C.c_int64, []),
     ("sors_stream", C.c_void_p, [_h]),
 ]
 

@@ -338,11 +338,13 @@ template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
     if (!h->pcg_exec && !h->graph_failed) {
         cudaGraph_t graph = nullptr;
+        const long long launches_before = g_kernel_launches.load();
         cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
             for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
             e = cudaStreamEndCapture(h->stream, &graph);
         }
+        g_kernel_launches.store(launches_before);  // captured launches run when the graph runs
         if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pcg_exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
         if (e != cudaSuccess) {
@@ -353,6 +355,7 @@ int pcg_chunk(SorsHandle* h) {
     }
     if (h->pcg_exec) {
         CK(cudaGraphLaunch(h->pcg_exec, h->stream));
+        g_kernel_launches.fetch_add(2 * kPcgChunk);
     } else {
         for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
         CK(cudaGetLastError());
@@ -846,5 +849,90 @@ int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t*
 }
 
 void* sors_stream(SorsHandle* h) { return h ? (void*)h->stream : nullptr; }
+
+int64_t sors_kernel_launch_count(void) { return (int64_t)g_kernel_launches.load(); }
+
+}  // extern "C"
+
+namespace {
+template <typename HT, typename VT>
+int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
+    const size_t hs = sizeof(HT), vs = sizeof(VT);
+    const double N = h->N, E = h->E, nnzb = (double)h->nnzb, nv = h->nv;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    float ms = 0.f;
+    const double dt = h->s.dt;
+    // assembly of gradient rows + Hessian block-rows at the current iterate
+    int st = eval_system<HT>(h, dt, true);
+    if (st) return st;
+    AsmArgs<HT> aa;
+    aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat;
+    aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
+    aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
+    aa.H = (HT*)h->H; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
+    aa.material = h->s.material; aa.project = h->s.project_spd; aa.apply_mask = 1;
+    aa.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0; aa.want_hess = 1;
+    aa.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0; aa.inertia_coef = inertia_coef(h, dt);
+    CK(cudaEventRecord(a, h->stream));
+    for (int i = 0; i < iters; i++) launch_assemble<HT>(aa, h->max_pairs, h->stream);
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&ms, a, b));
+    out->assemble_ms = ms / iters;
+    // compulsory bytes: conn, (mu,lambda), X, q, mask, mass, pair lists, slot maps, pattern; H and gradient out
+    out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
+                          (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
+    // PCG kernels on the assembled system
+    launch_block_jacobi<HT, VT>(h->N, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,
+                            1 << 30, h->partials, h->sc, h->stream);
+    CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
+    CK(cudaEventRecord(a, h->stream));
+    for (int i = 0; i < iters; i++)
+        launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
+                                (VT*)(i & 1 ? h->p0 : h->p1), (VT*)h->qv, h->partials, h->sc, h->stream);
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&ms, a, b));
+    out->spmv_ms = ms / iters;
+    // values + block columns + row pointers + z and p_old (read) + p_new and q (written)
+    out->spmv_bytes = nnzb * 9 * hs + nnzb * 4 + (N + 1) * 4 + 2 * 3 * N * vs + 2 * 3 * N * vs;
+    CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
+    CK(cudaEventRecord(a, h->stream));
+    for (int i = 0; i < iters; i++)
+        launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z,
+                              h->partials, h->sc, h->stream);
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&ms, a, b));
+    out->pcg_update_ms = ms / iters;
+    // p, q, Minv read; x, r read+written; z written
+    out->pcg_update_bytes = 3 * N * vs * 2 + 9 * N * vs + 3 * N * vs * 4 + 3 * N * vs;
+    CK(cudaEventRecord(a, h->stream));
+    for (int i = 0; i < iters; i++)
+        launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, h->partials, h->sc, h->stream);
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&ms, a, b));
+    out->energy_ms = ms / iters;
+    out->energy_bytes = E * nv * 4 + E * 16 + N * 48;
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    CK(cudaGetLastError());
+    return SORS_OK;
+}
+}  // namespace
+
+extern "C" {
+
+int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out) {
+    if (!h || !out || iters <= 0) return fail(SORS_ERR_ARG, "bad argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    memset(out, 0, sizeof(*out));
+    return mixed(h) ? profile_impl<float, float>(h, iters, out) : profile_impl<double, double>(h, iters, out);
+}
 
 }  // extern "C"

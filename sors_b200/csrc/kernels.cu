@@ -17,6 +17,9 @@
 
 namespace sors {
 
+std::atomic<long long> g_kernel_launches{0};
+static inline void counted(int n = 1) { g_kernel_launches.fetch_add(n, std::memory_order_relaxed); }
+
 // ---------------------------------------------------------------------------
 // deterministic reductions
 // ---------------------------------------------------------------------------
@@ -210,9 +213,11 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     if (nv == 4) {
         cudaFuncSetAttribute(k_assemble<HT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_assemble<HT, 4><<<(int)blocks, threads, smem, st>>>(a);
+        counted();
     } else {
         cudaFuncSetAttribute(k_assemble<HT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_assemble<HT, 8><<<(int)blocks, threads, smem, st>>>(a);
+        counted();
     }
     (void)max_pairs;
 }
@@ -290,6 +295,7 @@ void launch_elem_rows(int E, int nv, const double* X, const double* q, const int
         k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
     else
         k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -361,6 +367,7 @@ void launch_elem_energy(int E, int nv, const double* X, const double* q, const i
         k_elem_energy<4><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
     else
         k_elem_energy<8><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -409,6 +416,7 @@ __global__ void k_pressure_force(PressureArgs p) {
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st) {
     if (p.nsurf == 0) return;
     k_pressure_force<<<(p.nsurf + 127) / 128, 128, 0, st>>>(p);
+    counted();
 }
 
 // skew(b - a) as in pressureForce.cpp:76-90
@@ -484,6 +492,7 @@ void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* c
                          double cscale, HT* H, cudaStream_t st) {
     if (p.nsurf == 0) return;
     k_pressure_jac<HT><<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, row_ptr, col, node_mask, cscale, H);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -535,6 +544,7 @@ void launch_finalize_grad(int N, const double* g_int, const double* f_ext, const
     a.alpha = alpha; a.grav0 = grav[0]; a.grav1 = grav[1]; a.grav2 = grav[2];
     a.neumann_override = neumann_override; a.has_ext = has_ext; a.g = g;
     k_finalize_grad<<<red_grid(a.n, 4), kRedThreads, 0, st>>>(a, partials, sc);
+    counted();
 }
 
 // per-DOF energy terms (integrator.cpp:3-42, energy.cpp:229-244)
@@ -574,6 +584,7 @@ void launch_dof_energy(int N, const double* q, const double* qPrev, const double
     a.n = 3 * N; a.q = q; a.qPrev = qPrev; a.vPrev = vPrev; a.mass = mass; a.f_ext = f_ext; a.has_ext = has_ext;
     a.scheme = scheme; a.dt = dt; a.alpha = alpha; a.grav0 = grav[0]; a.grav1 = grav[1]; a.grav2 = grav[2];
     k_dof_energy<<<red_grid(a.n, 4), kRedThreads, 0, st>>>(a, partials, sc);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -604,6 +615,7 @@ template <typename HT, typename VT>
 void launch_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st) {
     if (N == 0) return;
     k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, diag_slot, H, Minv);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -650,6 +662,7 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
                      double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st) {
     k_pcg_init<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, Minv, x, r, z, p0, eta2, abs_tol2, maxit,
                                                            partials, sc);
+    counted();
 }
 
 // q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q
@@ -715,6 +728,7 @@ void launch_pcg_spmv(int N, const int* row_ptr, const int* col, const HT* H, con
     if (blocks > kRedBlocks) blocks = kRedBlocks;
     if (blocks < 1) blocks = 1;
     k_pcg_spmv<HT, VT><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc);
+    counted();
 }
 
 template <typename VT>
@@ -757,6 +771,7 @@ template <typename VT>
 void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
                        DevScalars* sc, cudaStream_t st) {
     k_pcg_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, Minv, x, r, z, partials, sc);
+    counted();
 }
 
 // ---------------------------------------------------------------------------
@@ -780,6 +795,7 @@ template <typename VT>
 void launch_newton_update(int n, const VT* dx, double alpha, double* q, const double* q0, double* partials,
                           DevScalars* sc, int counter, cudaStream_t st) {
     k_newton_update<VT><<<red_grid(n, 4), kRedThreads, 0, st>>>(n, dx, alpha, q, q0, partials, sc, counter);
+    counted();
 }
 
 template <typename VT>
@@ -794,6 +810,7 @@ __global__ void __launch_bounds__(kRedThreads) k_dot_gdx(int n, const double* g,
 template <typename VT>
 void launch_dot_gdx(int n, const double* g, const VT* dx, double* partials, DevScalars* sc, cudaStream_t st) {
     k_dot_gdx<VT><<<red_grid(n, 4), kRedThreads, 0, st>>>(n, g, dx, partials, sc);
+    counted();
 }
 
 __global__ void k_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
@@ -810,6 +827,7 @@ void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, d
                          const double* gPrevTmp, double dt, int scheme, cudaStream_t st) {
     if (n == 0) return;
     k_update_state<<<(n + 255) / 256, 256, 0, st>>>(n, q, qPrev, vPrev, gPrev, gPrevTmp, dt, scheme);
+    counted();
 }
 
 // y = H x (tests / diagnostics)
@@ -834,6 +852,7 @@ void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, c
                        cudaStream_t st) {
     if (N == 0) return;
     k_spmv_plain<HT><<<(N + 7) / 8, 256, 0, st>>>(N, row_ptr, col, H, x, y);
+    counted();
 }
 
 // ---------------------------------------------------------------------------

@@ -3,12 +3,16 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 #include <vector>
 
 #include "../../include/sors_b200.h"
 
 namespace sors {
+
+// kernels launched by this library (diagnostic counter)
+extern std::atomic<long long> g_kernel_launches;
 
 // status bits raised by kernels
 enum : int { kFlagInverted = 1, kFlagPcgBreakdown = 2, kFlagNaN = 4 };

@@ -160,7 +160,47 @@ class _EnergyBase:
         if material == 1:
             # elements without energies only carry mass (Energy with empty sets)
             material = 0
-        self._material = material or 0
+        self._init_arrays(X, T, settings, gravAcceleration, dampingAlpha, rho, E, nu, material or 0)
+        L = _lib.load()
+        cp = constraintParameterList if constraintParameterList is not None else Params()
+        fp = forceParameterList if forceParameterList is not None else Params()
+        self._forces = list(forceTypesList)
+        for c in constraintTypesList:
+            if c not in _REF_CONSTRAINTS:
+                raise RuntimeError(f"Unknown constraint type: {c}")
+            if c != "neumannBC":
+                raise NotImplementedError(f"constraint {c} is not built on the GPU path")
+            mask = np.ascontiguousarray(cp.get_value("neumannBCmask").ravel().astype(np.int32))
+            val = np.ascontiguousarray(cp.get_value("neumannBCvalue").ravel().astype(np.float64))
+            if mask.size != self.ndof or val.size != self.ndof:
+                raise ValueError("neumannBCmask/neumannBCvalue must have 3N entries")
+            _lib.check(L.sors_set_neumann(self._h, _p(mask, C.c_int32), _p(val, C.c_double)))
+        for f in forceTypesList:
+            if f not in _REF_FORCES:
+                raise RuntimeError(f"Unknown force type: {f}")
+            if f == "pressure":
+                faces = np.ascontiguousarray(fp.get_value("surfaceVertexIdx").astype(np.int32))
+                groups = np.ascontiguousarray(fp.get_value("surfaceGroups").ravel().astype(np.int32))
+                self._n_groups = int(groups.max()) + 1 if groups.size else 0
+                _lib.check(L.sors_set_pressure_faces(self._h, _p(faces, C.c_int32), faces.shape[0], faces.shape[1],
+                                                     _p(groups, C.c_int32), self._n_groups))
+            elif f == "vertexForce":
+                _lib.check(L.sors_enable_vertex_force(self._h, 1))
+
+    def _init_arrays(self, X, T, settings, gravAcceleration, dampingAlpha, rho, E, nu, material=0):
+        L = _lib.load()
+        X = np.ascontiguousarray(np.asarray(X, dtype=np.float64).reshape(-1, 3))
+        T = np.ascontiguousarray(np.asarray(T, dtype=np.int32).reshape(-1, self.NV))
+        ne = T.shape[0]
+        rho = np.ascontiguousarray(np.broadcast_to(np.asarray(rho, np.float64), (ne,)))
+        E = np.ascontiguousarray(np.broadcast_to(np.asarray(E, np.float64), (ne,)))
+        nu = np.ascontiguousarray(np.broadcast_to(np.asarray(nu, np.float64), (ne,)))
+        self.settings = settings
+        self.undeformedVertices = X
+        self.eleIdx = T
+        self._material = material
+        self._forces = []
+        self._n_groups = 0
         s = _lib.default_settings()
         if settings.timeSteppingScheme not in _SCHEMES:
             raise RuntimeError(f"Unknown time stepping scheme: {settings.timeSteppingScheme}")
@@ -192,31 +232,22 @@ class _EnergyBase:
         self.numVertices = X.shape[0]
         self.numElements = ne
         self.ndof = 3 * X.shape[0]
-        self._forces = list(forceTypesList)
-        self._n_groups = 0
-        cp = constraintParameterList if constraintParameterList is not None else Params()
-        fp = forceParameterList if forceParameterList is not None else Params()
-        for c in constraintTypesList:
-            if c not in _REF_CONSTRAINTS:
-                raise RuntimeError(f"Unknown constraint type: {c}")
-            if c != "neumannBC":
-                raise NotImplementedError(f"constraint {c} is not built on the GPU path")
-            mask = np.ascontiguousarray(cp.get_value("neumannBCmask").ravel().astype(np.int32))
-            val = np.ascontiguousarray(cp.get_value("neumannBCvalue").ravel().astype(np.float64))
-            if mask.size != self.ndof or val.size != self.ndof:
-                raise ValueError("neumannBCmask/neumannBCvalue must have 3N entries")
-            _lib.check(L.sors_set_neumann(self._h, _p(mask, C.c_int32), _p(val, C.c_double)))
-        for f in forceTypesList:
-            if f not in _REF_FORCES:
-                raise RuntimeError(f"Unknown force type: {f}")
-            if f == "pressure":
-                faces = np.ascontiguousarray(fp.get_value("surfaceVertexIdx").astype(np.int32))
-                groups = np.ascontiguousarray(fp.get_value("surfaceGroups").ravel().astype(np.int32))
-                self._n_groups = int(groups.max()) + 1 if groups.size else 0
-                _lib.check(L.sors_set_pressure_faces(self._h, _p(faces, C.c_int32), faces.shape[0], faces.shape[1],
-                                                     _p(groups, C.c_int32), self._n_groups))
-            elif f == "vertexForce":
-                _lib.check(L.sors_enable_vertex_force(self._h, 1))
+
+    @classmethod
+    def from_arrays(cls, undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha=0.0, *, density,
+                    youngsModulus, poissonsRatio, neumannBCmask=None, neumannBCvalue=None):
+        """Neo-Hookean mesh from per-element arrays instead of one Params per element.
+
+        Same system as the reference-style constructor; meant for meshes with
+        millions of elements where building Python Params objects dominates set-up."""
+        obj = cls.__new__(cls)
+        obj._init_arrays(undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha, density,
+                         youngsModulus, poissonsRatio)
+        if neumannBCmask is not None:
+            mask = np.ascontiguousarray(np.asarray(neumannBCmask).ravel().astype(np.int32))
+            val = np.ascontiguousarray(np.asarray(neumannBCvalue, dtype=np.float64).ravel())
+            _lib.check(_lib.load().sors_set_neumann(obj._h, _p(mask, C.c_int32), _p(val, C.c_double)))
+        return obj
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -346,8 +377,10 @@ class _SolverBase:
         self.settings = settings
         self.last_stats = None
 
-    def step(self, solution, systemEnergy, act=None, dt=0.0, substeps=0):
-        """Solver<3,E>::step (cpp/src/solver.cpp:5-52): returns the new solution."""
+    def step(self, solution, systemEnergy, act=None, dt=0.0, substeps=0, out=None):
+        """Solver<3,E>::step (cpp/src/solver.cpp:5-52): returns the new solution.
+
+        `out` (optional, 3N float64, e.g. pinned host memory) receives the result."""
         if isinstance(act, (int, float)) and not isinstance(act, bool):
             # step(solution, systemEnergy, dt, substeps) overload (cpp/py_sors.cpp:124-130)
             act, dt, substeps = None, float(act), int(dt) if dt else 0
@@ -355,7 +388,10 @@ class _SolverBase:
             raise TypeError("systemEnergy does not match the solver's mesh type")
         systemEnergy._apply_actuation(act)
         q = systemEnergy._q(solution)
-        out = np.empty_like(q)
+        if out is None:
+            out = np.empty_like(q)
+        elif out.dtype != np.float64 or out.size != q.size or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float64 array of 3N entries")
         st = _lib.SorsStepStats()
         _lib.check(_lib.load().sors_step(systemEnergy._h, _p(q, C.c_double), _p(out, C.c_double), float(dt),
                                          int(substeps), C.byref(st)))
