@@ -56,6 +56,9 @@ typedef struct SorsSettings {
     double pcg_rel_tol;      /* smallest PCG forcing term                         */
     int32_t pcg_max_iter;
     int32_t device;          /* CUDA device ordinal                              */
+    int32_t newton_predictor;/* 1: start each Newton solve from q + dt v_prev
+                                (falls back to q if that inverts an element);
+                                changes only the iterates, not the solution      */
 } SorsSettings;
 
 typedef struct SorsStepStats {

@@ -33,6 +33,7 @@ class SorsSettings(C.Structure):
         ("pcg_rel_tol", C.c_double),
         ("pcg_max_iter", C.c_int32),
         ("device", C.c_int32),
+        ("newton_predictor", C.c_int32),
     ]
 
 

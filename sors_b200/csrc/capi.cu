@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
@@ -44,6 +45,16 @@ int fail(int code, const std::string& msg) {
 
 constexpr int kPcgChunk = 16;  // PCG iterations per captured graph (even)
 
+// SORS_VERBOSE=1 prints one line per Newton iteration to stderr.
+bool verbose() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = getenv("SORS_VERBOSE");
+        v = (e && *e && *e != '0') ? 1 : 0;
+    }
+    return v == 1;
+}
+
 }  // namespace
 
 struct SorsHandle {
@@ -53,13 +64,14 @@ struct SorsHandle {
     cudaStream_t stream = nullptr;
     int64_t nnzb = 0;
     int max_pairs = 0;
+    int max_row_blocks = 0;
     size_t bytes = 0;
     std::vector<void*> allocs;
 
     // mesh + state
     double *X = nullptr, *q = nullptr, *q0 = nullptr, *qPrev = nullptr, *vPrev = nullptr, *gPrev = nullptr,
            *gPrevTmp = nullptr, *g = nullptr, *g_int = nullptr, *f_ext = nullptr, *mass = nullptr, *mval = nullptr,
-           *vforce = nullptr;
+           *vforce = nullptr, *q_save = nullptr;
     int* conn = nullptr;
     double2* mat = nullptr;
     int *row_ptr = nullptr, *col = nullptr, *diag_slot = nullptr, *pair_ptr = nullptr, *pair_ev = nullptr,
@@ -206,6 +218,7 @@ int build_pattern(SorsHandle* h, const int32_t* conn) {
     for (int i = 0; i < N; i++) {
         int nb = row_ptr[i + 1] - row_ptr[i];
         if (nb > 255 * 9) return fail(SORS_ERR_UNSUPPORTED, "Hessian row too long");
+        h->max_row_blocks = std::max(h->max_row_blocks, nb);
     }
     std::vector<int> diag(N);
     for (int i = 0; i < N; i++) {
@@ -324,11 +337,11 @@ int eval_energy(SorsHandle* h, double dt, double* out) {
 template <typename HT, typename VT>
 void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
-    launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
                           h->stream);
-    launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
                           h->stream);
@@ -366,7 +379,7 @@ int pcg_chunk(SorsHandle* h) {
 // Solves H dx = -g (dx in h->x).  Returns PCG iterations in *iters.
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters) {
-    launch_block_jacobi<HT, VT>(h->N, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, eta * eta,
                             abs_tol * abs_tol, h->s.pcg_max_iter, h->partials, h->sc, h->stream);
     CK(cudaGetLastError());
@@ -392,7 +405,7 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     const double res_tol = h->s.newton_res_tol;
     bool converged = false;
     int st = SORS_OK;
-    double prev_g = -1.0;
+    double prev_g = -1.0, prev_eta = 0.5;
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
     bool have_hess = false;
     for (int it = 0; it < h->s.newton_max_iter; it++) {
@@ -407,14 +420,21 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         if (stats) { stats->newton_iters++; stats->residual_norm = gn; }
         if (!(gn == gn)) break;  // NaN gradient: diverged
         if (res_tol > 0.0 && gn < res_tol) { converged = true; break; }
-        // forcing term (Eisenstat-Walker choice 2), floor pcg_rel_tol
+        // forcing term: Eisenstat-Walker choice 2 with its safeguard, never
+        // solving below what the residual target needs, floored at pcg_rel_tol
+        // (and at 1e-6 for FP32 PCG vectors)
         double eta = 0.5;
         if (prev_g > 0.0) {
-            double ratio = gn / prev_g;
-            eta = std::min(0.5, 0.9 * ratio * ratio);
+            const double ratio = gn / prev_g;
+            eta = 0.9 * ratio * ratio;
+            const double safe = 0.9 * prev_eta * prev_eta;
+            if (safe > 0.1) eta = std::max(eta, safe);
+            eta = std::min(eta, 0.5);
         }
-        eta = std::max(eta, h->s.pcg_rel_tol);
+        if (res_tol > 0.0) eta = std::max(eta, std::min(0.5, 0.5 * res_tol / gn));
+        eta = std::max(eta, mixed(h) ? std::max(h->s.pcg_rel_tol, 1e-6) : h->s.pcg_rel_tol);
         prev_g = gn;
+        prev_eta = eta;
         int pit = 0;
         if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
         if (stats) stats->pcg_iters += pit;
@@ -443,6 +463,9 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         CK(cudaStreamSynchronize(h->stream));
         double dxn = sqrt(h->sc_host->dxnorm2);
         if (stats) stats->dx_norm = dxn;
+        if (verbose())
+            fprintf(stderr, "[sors] newton %d |g|=%.3e eta=%.2e pcg=%d |r|/|b|=%.2e |dx|=%.3e\n", it, gn, eta, pit,
+                    sqrt(h->sc_host->rr / (h->sc_host->bnorm2 > 0 ? h->sc_host->bnorm2 : 1.0)), dxn);
         if (!(dxn == dxn)) break;  // "Newton's method diverged"
         if (dxn < dx_tol) { converged = true; break; }
     }
@@ -492,7 +515,19 @@ int step_resident(SorsHandle* h, double dt, int substeps, SorsStepStats* stats) 
     double dts = dt / substeps;
     if (stats) memset(stats, 0, sizeof(*stats));
     for (int j = 0; j < substeps; j++) {
-        int st = run_minimize(h, dts, stats);
+        int st;
+        if (h->s.newton_predictor && dts != 0.0) {
+            CK(cudaMemcpyAsync(h->q_save, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+            launch_predict(h->ndof, h->q, h->vPrev, dts, h->stream);
+            st = run_minimize(h, dts, stats);
+            if (st == SORS_ERR_INVERTED) {
+                // the predicted start inverted an element: restart from the given solution
+                CK(cudaMemcpyAsync(h->q, h->q_save, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+                st = run_minimize(h, dts, stats);
+            }
+        } else {
+            st = run_minimize(h, dts, stats);
+        }
         if (st) return st;
         launch_update_state(h->ndof, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, dts, h->s.time_stepping,
                             h->stream);
@@ -532,6 +567,7 @@ void sors_default_settings(SorsSettings* s) {
     s->pcg_rel_tol = 1e-10;
     s->pcg_max_iter = 20000;
     s->device = 0;
+    s->newton_predictor = 1;
 }
 
 int sors_last_error(char* buf, size_t n) {
@@ -580,7 +616,7 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if ((st = build_pattern(h, conn))) return bail(st);
     const size_t nd = (size_t)3 * N;
     double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,
-                       &h->mval, &h->vforce};
+                       &h->mval, &h->vforce, &h->q_save};
     for (double** p : vecs) {
         if ((st = dalloc_t(h, p, nd))) return bail(st);
         CK(cudaMemset(*p, 0, nd * sizeof(double)));
@@ -591,7 +627,7 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     h->mask_h.assign(N, 0);
     if ((st = upload(h, &h->node_mask, h->mask_h.data(), (size_t)N))) return bail(st);
     size_t hs = hsize(h);
-    if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs))) return bail(st);
+    if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs + 64))) return bail(st);
     if ((st = dalloc(h, &h->Minv, (size_t)N * 9 * hs))) return bail(st);
     void** vv[] = {&h->x, &h->r, &h->z, &h->p0, &h->p1, &h->qv};
     for (void** p : vv) {
@@ -759,15 +795,17 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
     st = mixed(h) ? eval_system<float>(h, dt, true) : eval_system<double>(h, dt, true);
     if (st) return st;
     size_t n = (size_t)h->nnzb * 9;
+    std::vector<double> raw(n);
     if (mixed(h)) {
         std::vector<float> tmp(n);
         CK(cudaMemcpyAsync(tmp.data(), h->H, n * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        for (size_t k = 0; k < n; k++) val[k] = tmp[k];
+        for (size_t k = 0; k < n; k++) raw[k] = tmp[k];
     } else {
-        CK(cudaMemcpyAsync(val, h->H, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(raw.data(), h->H, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
+    memcpy(val, raw.data(), n * sizeof(double));
     int flag = 0;
     CK(cudaMemcpy(&flag, h->status, sizeof(int), cudaMemcpyDeviceToHost));
     if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
@@ -885,13 +923,13 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
                           (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
     // PCG kernels on the assembled system
-    launch_block_jacobi<HT, VT>(h->N, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,
                             1 << 30, h->partials, h->sc, h->stream);
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
-        launch_pcg_spmv<HT, VT>(h->N, h->row_ptr, h->col, (const HT*)h->H, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
+        launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
                                 (VT*)(i & 1 ? h->p0 : h->p1), (VT*)h->qv, h->partials, h->sc, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));

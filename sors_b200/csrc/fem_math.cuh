@@ -109,9 +109,20 @@ __device__ void sym3_eig(T* a, T* w, T* v) {
     w[0] = a[0]; w[1] = a[4]; w[2] = a[8];
 }
 
-// Rotation-variant SVD of F with det(F) > 0: F = U diag(s) V^T, U, V rotations.
+// Swap eigenpairs a and b (a, b compile-time) when w[a] < w[b].
+template <typename T, int A, int B>
+__device__ __forceinline__ void eig_cswap(T* w, T* V) {
+    if (w[A] < w[B]) {
+        T t = w[A]; w[A] = w[B]; w[B] = t;
+#pragma unroll
+        for (int r = 0; r < 3; r++) { T u = V[r * 3 + A]; V[r * 3 + A] = V[r * 3 + B]; V[r * 3 + B] = u; }
+    }
+}
+
+// Rotation-variant SVD of F with det(F) > 0: F = U diag(s) V^T, U, V rotations,
+// s sorted descending.
 template <typename T>
-__device__ void svd3_rv(const T* F, T* U, T* s, T* V) {
+__device__ __forceinline__ void svd3_rv(const T* F, T* U, T* s, T* V) {
     T S[9];
 #pragma unroll
     for (int r = 0; r < 3; r++)
@@ -120,17 +131,10 @@ __device__ void svd3_rv(const T* F, T* U, T* s, T* V) {
                                                    F[2 * 3 + r] * F[2 * 3 + c];
     T w[3];
     sym3_eig(S, w, V);
-    // sort descending, permuting columns of V
-    int o0 = 0, o1 = 1, o2 = 2, tmp;
-    if (w[o0] < w[o1]) { tmp = o0; o0 = o1; o1 = tmp; }
-    if (w[o0] < w[o2]) { tmp = o0; o0 = o2; o2 = tmp; }
-    if (w[o1] < w[o2]) { tmp = o1; o1 = o2; o2 = tmp; }
-    T Vs[9];
-#pragma unroll
-    for (int r = 0; r < 3; r++) { Vs[r * 3 + 0] = V[r * 3 + o0]; Vs[r * 3 + 1] = V[r * 3 + o1]; Vs[r * 3 + 2] = V[r * 3 + o2]; }
-    if (det3(Vs) < T(0)) { Vs[2] = -Vs[2]; Vs[5] = -Vs[5]; Vs[8] = -Vs[8]; }
-#pragma unroll
-    for (int k = 0; k < 9; k++) V[k] = Vs[k];
+    eig_cswap<T, 0, 1>(w, V);
+    eig_cswap<T, 0, 2>(w, V);
+    eig_cswap<T, 1, 2>(w, V);
+    if (det3(V) < T(0)) { V[2] = -V[2]; V[5] = -V[5]; V[8] = -V[8]; }
     T B[9];  // B = F V
 #pragma unroll
     for (int r = 0; r < 3; r++)
@@ -151,76 +155,85 @@ __device__ void svd3_rv(const T* F, T* U, T* s, T* V) {
 }
 
 // ---------------------------------------------------------------------------
-// Projection data of one quadrature point: the negative modes of d2Psi/dF2
-// expressed in the (U, V) frames.
+// Eigen-modes of d2Psi/dF2 at one quadrature point, held in registers.
+// Mode slots are fixed: twist/flip of pair m in {(0,1), (0,2), (1,2)} and
+// three scaling modes; a slot whose eigenvalue is >= 0 is skipped.
 // ---------------------------------------------------------------------------
 template <typename T>
-struct ProjModes {
+struct NhModes {
     T U[9], V[9];
-    int n;          // number of negative modes
-    int kind[9];    // 0 twist, 1 flip, 2 scaling
-    int pi[9], pj[9];
-    T lam[9];
-    T y[9][3];      // scaling eigenvector (kind 2)
+    T lt[3], lf[3];   // twist / flip eigenvalues of pair m
+    T ls[3];          // scaling eigenvalues
+    T Y[9];           // scaling eigenvectors (columns)
+    bool any;
 };
 
-// Returns the negative eigen-modes; J > 0 required.
+// J > 0 required.  The scaling block S = mu I + D^-1 M D^-1 with
+// M = (mu - lam log J) I + lam 1 1^T is >= mu I when mu - lam log J >= 0,
+// so its eigen-solve is skipped then.
 template <typename T>
-__device__ void nh_negative_modes(const T* F, T J, T logJ, T mu, T lam, ProjModes<T>& pm) {
+__device__ __forceinline__ void nh_modes(const T* F, T J, T logJ, T mu, T lam, NhModes<T>& pm) {
     T s[3];
     svd3_rv(F, pm.U, s, pm.V);
-    T c = lam * logJ - mu;
-    pm.n = 0;
-    const int PI[3] = {0, 0, 1}, PJ[3] = {1, 2, 2}, PK[3] = {2, 1, 0};
+    const T cj = (lam * logJ - mu) / J;
+    // pair m = (0,1),(0,2),(1,2) uses the third singular value s[2], s[1], s[0]
+    pm.lt[0] = mu + cj * s[2]; pm.lt[1] = mu + cj * s[1]; pm.lt[2] = mu + cj * s[0];
+    pm.lf[0] = mu - cj * s[2]; pm.lf[1] = mu - cj * s[1]; pm.lf[2] = mu - cj * s[0];
+    pm.ls[0] = pm.ls[1] = pm.ls[2] = T(1);
 #pragma unroll
-    for (int m = 0; m < 3; m++) {
-        T lt = mu + (c / J) * s[PK[m]];
-        T lf = mu - (c / J) * s[PK[m]];
-        if (lt < T(0)) { int q = pm.n++; pm.kind[q] = 0; pm.pi[q] = PI[m]; pm.pj[q] = PJ[m]; pm.lam[q] = lt; }
-        if (lf < T(0)) { int q = pm.n++; pm.kind[q] = 1; pm.pi[q] = PI[m]; pm.pj[q] = PJ[m]; pm.lam[q] = lf; }
+    for (int k = 0; k < 9; k++) pm.Y[k] = T(0);
+    if (mu - lam * logJ < T(0)) {
+        T S[9];
+        const T base = mu + lam * (T(1) - logJ);
+#pragma unroll
+        for (int i = 0; i < 3; i++)
+#pragma unroll
+            for (int j = 0; j < 3; j++) S[i * 3 + j] = (i == j) ? mu + base / (s[i] * s[i]) : lam / (s[i] * s[j]);
+        sym3_eig(S, pm.ls, pm.Y);
     }
-    T S[9];
-    T base = mu + lam * (T(1) - logJ);
+    pm.any = false;
 #pragma unroll
-    for (int i = 0; i < 3; i++)
-#pragma unroll
-        for (int j = 0; j < 3; j++) S[i * 3 + j] = (i == j) ? mu + base / (s[i] * s[i]) : lam / (s[i] * s[j]);
-    T w[3], Y[9];
-    sym3_eig(S, w, Y);
-#pragma unroll
-    for (int m = 0; m < 3; m++)
-        if (w[m] < T(0)) {
-            int q = pm.n++;
-            pm.kind[q] = 2; pm.lam[q] = w[m];
-            pm.y[q][0] = Y[0 * 3 + m]; pm.y[q][1] = Y[1 * 3 + m]; pm.y[q][2] = Y[2 * 3 + m];
-        }
+    for (int m = 0; m < 3; m++) pm.any |= (pm.lt[m] < T(0)) | (pm.lf[m] < T(0)) | (pm.ls[m] < T(0));
 }
 
-// E_m (V^T d) for mode q, in the U frame.
-template <typename T>
-__device__ __forceinline__ void mode_apply(const ProjModes<T>& pm, int q, const T* dh, T* y) {
+// u = U y for the twist (sign -1) or flip (sign +1) mode of pair (I, JJ):
+// y_I = dh_JJ / sqrt2, y_JJ = sign * dh_I / sqrt2.
+template <typename T, int I, int JJ>
+__device__ __forceinline__ void tf_vec(const T* U, const T* dh, T sign, T* u) {
     const T r2 = T(0.70710678118654752440);
-    int k = pm.kind[q];
-    if (k == 2) {
-        y[0] = pm.y[q][0] * dh[0]; y[1] = pm.y[q][1] * dh[1]; y[2] = pm.y[q][2] * dh[2];
-    } else {
-        int i = pm.pi[q], j = pm.pj[q];
-        y[0] = y[1] = y[2] = T(0);
-        y[i] = dh[j] * r2;
-        y[j] = (k == 0 ? -dh[i] : dh[i]) * r2;
-    }
+    const T yi = dh[JJ] * r2, yj = sign * dh[I] * r2;
+#pragma unroll
+    for (int r = 0; r < 3; r++) u[r] = U[r * 3 + I] * yi + U[r * 3 + JJ] * yj;
+}
+
+template <typename T, int M>
+__device__ __forceinline__ void sc_vec(const T* U, const T* Y, const T* dh, T* u) {
+    const T y0 = Y[0 * 3 + M] * dh[0], y1 = Y[1 * 3 + M] * dh[1], y2 = Y[2 * 3 + M] * dh[2];
+#pragma unroll
+    for (int r = 0; r < 3; r++) u[r] = U[r * 3 + 0] * y0 + U[r * 3 + 1] * y1 + U[r * 3 + 2] * y2;
+}
+
+// blk (3x3) += coef * a b^T
+template <typename T>
+__device__ __forceinline__ void add_outer(T* blk, T coef, const T* a, const T* b) {
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int l = 0; l < 3; l++) blk[k * 3 + l] += coef * a[k] * b[l];
 }
 
 // ---------------------------------------------------------------------------
 // One quadrature point's contribution to row v of the element Hessian and
 // gradient.  d: shape gradients (NV x 3, FP64); x: current positions of the
-// element's vertices (NV x 3).  wV = undeformed volume x quadrature weight.
-// blk: NV blocks of 9, accumulated (+=).  g: 3 values accumulated (+=).
-// Returns false when J <= 0.
+// element's vertices (NV x 3); dvd = d[v].  wV = undeformed volume x
+// quadrature weight.  blk: NV blocks of 9 accumulated in registers (+=);
+// g: 3 values (+=).  All array indices are compile-time: v enters only
+// through dvd.  Returns false when J <= 0.
 // ---------------------------------------------------------------------------
 template <typename HT, int NV, bool HESS>
-__device__ __forceinline__ bool nh_qp_row(const double (*d)[3], const double (*x)[3], int v, double wV,
-                                          double mu, double lam, bool project, double* g, HT* blk) {
+__device__ __forceinline__ bool nh_qp_row(const double (&d)[NV][3], const double (&x)[NV][3], const double (&dvd)[3],
+                                          double wV, double mu, double lam, bool project, double* g,
+                                          HT (&blk)[NV * 9]) {
     double F[9];
 #pragma unroll
     for (int r = 0; r < 3; r++)
@@ -233,39 +246,38 @@ __device__ __forceinline__ bool nh_qp_row(const double (*d)[3], const double (*x
         }
     double C[9];
     cof3(F, C);
-    double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
-    double logJ = log(J);
-    double iJ = 1.0 / J;
+    const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+    const double logJ = log(J);
+    const double iJ = 1.0 / J;
     double G[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) G[k] = C[k] * iJ;
-    double cc = lam * logJ - mu;
+    const double cc = lam * logJ - mu;
     // gradient row v: wV * (mu F + c G) d_v
 #pragma unroll
     for (int r = 0; r < 3; r++) {
         double pr = 0.0;
 #pragma unroll
-        for (int c = 0; c < 3; c++) pr += (mu * F[r * 3 + c] + cc * G[r * 3 + c]) * d[v][c];
+        for (int c = 0; c < 3; c++) pr += (mu * F[r * 3 + c] + cc * G[r * 3 + c]) * dvd[c];
         g[r] += wV * pr;
     }
     if (!(J > 0.0)) return false;
     if (!HESS) return true;
-    // Hessian row blocks in HT precision
     HT Gh[9];
 #pragma unroll
     for (int k = 0; k < 9; k++) Gh[k] = (HT)G[k];
-    HT dv[3] = {(HT)d[v][0], (HT)d[v][1], (HT)d[v][2]};
+    const HT dv[3] = {(HT)dvd[0], (HT)dvd[1], (HT)dvd[2]};
     HT av[3];
 #pragma unroll
     for (int r = 0; r < 3; r++) av[r] = Gh[r * 3 + 0] * dv[0] + Gh[r * 3 + 1] * dv[1] + Gh[r * 3 + 2] * dv[2];
-    HT hmu = (HT)(wV * mu), hlam = (HT)(wV * lam), hc = (HT)(wV * cc);
+    const HT hmu = (HT)(wV * mu), hlam = (HT)(wV * lam), hc = (HT)(wV * cc);
 #pragma unroll
     for (int w = 0; w < NV; w++) {
-        HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
+        const HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
         HT aw[3];
 #pragma unroll
         for (int r = 0; r < 3; r++) aw[r] = Gh[r * 3 + 0] * dw[0] + Gh[r * 3 + 1] * dw[1] + Gh[r * 3 + 2] * dw[2];
-        HT dd = dv[0] * dw[0] + dv[1] * dw[1] + dv[2] * dw[2];
+        const HT dd = dv[0] * dw[0] + dv[1] * dw[1] + dv[2] * dw[2];
 #pragma unroll
         for (int k = 0; k < 3; k++)
 #pragma unroll
@@ -279,44 +291,46 @@ __device__ __forceinline__ bool nh_qp_row(const double (*d)[3], const double (*x
         HT Fh[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
-        ProjModes<HT> pm;
-        nh_negative_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)mu, (HT)lam, pm);
-        if (pm.n > 0) {
-            // dh_w = V^T d_w
+        NhModes<HT> pm;
+        nh_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)mu, (HT)lam, pm);
+        if (pm.any) {
+            const HT wv = (HT)wV;
             HT dhv[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) dhv[c] = pm.V[0 * 3 + c] * dv[0] + pm.V[1 * 3 + c] * dv[1] + pm.V[2 * 3 + c] * dv[2];
-            HT wv = (HT)wV;
+#pragma unroll
             for (int w = 0; w < NV; w++) {
-                HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
+                const HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
                 HT dhw[3];
 #pragma unroll
                 for (int c = 0; c < 3; c++) dhw[c] = pm.V[0 * 3 + c] * dw[0] + pm.V[1 * 3 + c] * dw[1] + pm.V[2 * 3 + c] * dw[2];
-                HT Cm[9];
-#pragma unroll
-                for (int k = 0; k < 9; k++) Cm[k] = HT(0);
-                for (int q = 0; q < pm.n; q++) {
-                    HT yv[3], yw[3];
-                    mode_apply(pm, q, dhv, yv);
-                    mode_apply(pm, q, dhw, yw);
-                    HT lm = -pm.lam[q] * wv;
-#pragma unroll
-                    for (int k = 0; k < 3; k++)
-#pragma unroll
-                        for (int l = 0; l < 3; l++) Cm[k * 3 + l] += lm * yv[k] * yw[l];
-                }
-                // blk += U Cm U^T
-                HT T1[9];
-#pragma unroll
-                for (int k = 0; k < 3; k++)
-#pragma unroll
-                    for (int l = 0; l < 3; l++)
-                        T1[k * 3 + l] = Cm[k * 3 + 0] * pm.U[l * 3 + 0] + Cm[k * 3 + 1] * pm.U[l * 3 + 1] + Cm[k * 3 + 2] * pm.U[l * 3 + 2];
-#pragma unroll
-                for (int k = 0; k < 3; k++)
-#pragma unroll
-                    for (int l = 0; l < 3; l++)
-                        blk[w * 9 + k * 3 + l] += pm.U[k * 3 + 0] * T1[0 * 3 + l] + pm.U[k * 3 + 1] * T1[1 * 3 + l] + pm.U[k * 3 + 2] * T1[2 * 3 + l];
+                HT* b = blk + w * 9;
+                HT uv[3], uw[3];
+#define SORS_TF(M, I, JJ)                                      \
+    if (pm.lt[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(-1), uv);              \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(-1), uw);              \
+        add_outer(b, -pm.lt[M] * wv, uv, uw);                  \
+    }                                                          \
+    if (pm.lf[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(1), uv);               \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(1), uw);               \
+        add_outer(b, -pm.lf[M] * wv, uv, uw);                  \
+    }
+                SORS_TF(0, 0, 1)
+                SORS_TF(1, 0, 2)
+                SORS_TF(2, 1, 2)
+#undef SORS_TF
+#define SORS_SC(M)                                             \
+    if (pm.ls[M] < HT(0)) {                                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhv, uv);                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhw, uw);                    \
+        add_outer(b, -pm.ls[M] * wv, uv, uw);                  \
+    }
+                SORS_SC(0)
+                SORS_SC(1)
+                SORS_SC(2)
+#undef SORS_SC
             }
         }
     }

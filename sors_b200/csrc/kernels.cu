@@ -99,41 +99,51 @@ static inline int red_grid(long long n, int per_thread = 1) {
 template <typename HT, int NV, bool HESS>
 __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const double* __restrict__ qg,
                                          const int* __restrict__ conn, const double2* __restrict__ mat, int e,
-                                         int v, int material, bool project, double* g, HT* blk) {
+                                         int v, int material, bool project, double* g, HT (&blk)[NV * 9]) {
     double X[NV][3], x[NV][3];
 #pragma unroll
     for (int w = 0; w < NV; w++) {
-        int n = __ldg(conn + (size_t)e * NV + w);
+        const int n = __ldg(conn + (size_t)e * NV + w);
 #pragma unroll
         for (int r = 0; r < 3; r++) {
             X[w][r] = __ldg(Xg + 3 * (size_t)n + r);
             x[w][r] = qg[3 * (size_t)n + r];
         }
     }
-    if (HESS)
-        for (int k = 0; k < NV * 9; k++) blk[k] = HT(0);
+#pragma unroll
+    for (int k = 0; k < NV * 9; k++) blk[k] = HT(0);
     if (material == 1) {
         // quartic test element of the reference (cpp/src/_test.cpp:31-66)
 #pragma unroll
-        for (int r = 0; r < 3; r++) {
-            double xv = x[v][r];
-            g[r] += (2 * xv - 1) * (2 * xv + 1) * xv;
-            if (HESS) blk[v * 9 + r * 3 + r] = (HT)(12 * xv * xv - 1);
-        }
+        for (int w = 0; w < NV; w++)
+            if (w == v) {
+#pragma unroll
+                for (int r = 0; r < 3; r++) {
+                    const double xv = x[w][r];
+                    g[r] += (2 * xv - 1) * (2 * xv + 1) * xv;
+                    if (HESS) blk[w * 9 + r * 3 + r] = (HT)(12 * xv * xv - 1);
+                }
+            }
         return true;
     }
-    double2 m = __ldg(mat + e);
+    const double2 m = __ldg(mat + e);
     bool ok = true;
     double d[NV][3];
+    double dv[3];
     if (NV == 4) {
-        double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
-        ok = nh_qp_row<HT, NV, HESS>((const double(*)[3])d, (const double(*)[3])x, v, V, m.x, m.y, project, g, blk);
+        const double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
+#pragma unroll
+        for (int w = 0; w < NV; w++)
+            if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
+        ok = nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
     } else {
-        double V = hex_volume((const double(*)[3])X) * 0.125;
+        const double V = hex_volume((const double(*)[3])X) * 0.125;
         for (int s = 0; s < 8; s++) {
             hex_shape((const double(*)[3])X, s, (double(*)[3])d);
-            ok &= nh_qp_row<HT, NV, HESS>((const double(*)[3])d, (const double(*)[3])x, v, V, m.x, m.y, project, g,
-                                          blk);
+#pragma unroll
+            for (int w = 0; w < NV; w++)
+                if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
+            ok &= nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
         }
     }
     return ok;
@@ -143,7 +153,7 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
 // Row-owner assembly of gradient rows and Hessian block-rows.
 // ---------------------------------------------------------------------------
 template <typename HT, int NV>
-__global__ void __launch_bounds__(256) k_assemble(AsmArgs<HT> a) {
+__global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_assemble(AsmArgs<HT> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -155,13 +165,17 @@ __global__ void __launch_bounds__(256) k_assemble(AsmArgs<HT> a) {
         double g[3] = {0.0, 0.0, 0.0};
         bool ok = true;
         for (int k = lane; k < np; k += 32) {
-            int ev = __ldg(a.pair_ev + p0 + k);
-            int e = ev >> 3, v = ev & 7;
-            if (a.want_hess)
-                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, e, v, a.material, a.project != 0, g,
-                                             stage + (size_t)k * NV * 9);
-            else
-                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, e, v, a.material, false, g, nullptr);
+            const int ev = __ldg(a.pair_ev + p0 + k);
+            const int e = ev >> 3, v = ev & 7;
+            HT blk[NV * 9];
+            if (a.want_hess) {
+                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, e, v, a.material, a.project != 0, g, blk);
+                HT* dst = stage + (size_t)k * NV * 9;
+#pragma unroll
+                for (int t = 0; t < NV * 9; t++) dst[t] = blk[t];
+            } else {
+                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, e, v, a.material, false, g, blk);
+            }
         }
         if (!ok) atomicOr(a.status, kFlagInverted);
         warp_sum<3>(g);
@@ -591,10 +605,12 @@ void launch_dof_energy(int N, const double* q, const double* qPrev, const double
 // block-Jacobi preconditioner: inverse of each 3x3 diagonal block
 // ---------------------------------------------------------------------------
 template <typename HT, typename VT>
-__global__ void k_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv) {
+__global__ void k_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
+    const int b0 = row_ptr[i], nb = row_ptr[i + 1] - b0;
     const HT* b = H + (size_t)diag_slot[i] * 9;
+    (void)nb;
     double a[9], c[9];
     for (int k = 0; k < 9; k++) a[k] = (double)b[k];
     // symmetric part: the lower triangle defines the operator
@@ -612,9 +628,9 @@ __global__ void k_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Min
 }
 
 template <typename HT, typename VT>
-void launch_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st) {
+void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st) {
     if (N == 0) return;
-    k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, diag_slot, H, Minv);
+    k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, row_ptr, diag_slot, H, Minv);
     counted();
 }
 
@@ -653,6 +669,8 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_init(int N, const double* g
         sc->it = 0;
         sc->maxit = maxit;
         sc->breakdown = 0;
+        sc->counters[4] = 0u;  // SpMV / update reduction sites start clean
+        sc->counters[5] = 0u;
         sc->done = (tot[1] <= sc->tol2 || maxit <= 0) ? 1 : 0;
     }
 }
@@ -665,42 +683,54 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
     counted();
 }
 
-// q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q
-template <typename HT, typename VT>
+// q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q.
+// A group of LPR lanes owns one block-row: lane b of the group takes block b
+// of the row, loads its column and 9 values and gathers p_new(col) at once,
+// so a row costs one dependent load chain; groups are reduced with shuffles.
+template <typename HT, typename VT, int LPR>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __restrict__ row_ptr,
                                                            const int* __restrict__ col, const HT* __restrict__ H,
                                                            const VT* __restrict__ z, const VT* __restrict__ p_old,
                                                            VT* __restrict__ p_new, VT* __restrict__ qv,
                                                            double* partials, DevScalars* sc) {
     if (*(volatile int*)&sc->done) return;
-    const double betad = sc->beta;
-    const VT beta = (VT)betad;
+    const VT beta = (VT)sc->beta;
     const int lane = threadIdx.x & 31;
-    const int wpb = blockDim.x >> 5;
+    const int sub = lane / LPR, sl = lane % LPR;
+    constexpr int RPW = 32 / LPR;
+    const int gwarp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
     double acc[1] = {0.0};
-    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < N; row += gridDim.x * wpb) {
-        const int b0 = __ldg(row_ptr + row), nval = (__ldg(row_ptr + row + 1) - b0) * 9;
-        const HT* hv = H + (size_t)b0 * 9;
+    for (int base = gwarp * RPW; base < N; base += nwarps * RPW) {
+        const int row = base + sub;
         VT a0 = VT(0), a1 = VT(0), a2 = VT(0);
-        for (int t = lane; t < nval; t += 32) {
-            const int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
-            const int j = __ldg(col + b0 + blk);
-            const size_t jj = 3 * (size_t)j + c;
-            const VT pj = __ldg(z + jj) + beta * __ldg(p_old + jj);
-            const VT prod = (VT)__ldg(hv + t) * pj;
-            a0 += (r == 0) ? prod : VT(0);
-            a1 += (r == 1) ? prod : VT(0);
-            a2 += (r == 2) ? prod : VT(0);
+        if (row < N) {
+            const int b0 = __ldg(row_ptr + row), b1 = __ldg(row_ptr + row + 1), nb = b1 - b0;
+            const HT* hrow = H + (size_t)b0 * 9;
+            for (int s = sl; s < nb; s += LPR) {
+                const int j = __ldg(col + b0 + s);
+                const HT* v = hrow + (size_t)s * 9;
+                const VT h0 = (VT)__ldg(v), h1 = (VT)__ldg(v + 1), h2 = (VT)__ldg(v + 2);
+                const VT h3 = (VT)__ldg(v + 3), h4 = (VT)__ldg(v + 4), h5 = (VT)__ldg(v + 5);
+                const VT h6 = (VT)__ldg(v + 6), h7 = (VT)__ldg(v + 7), h8 = (VT)__ldg(v + 8);
+                const size_t jj = 3 * (size_t)j;
+                const VT p0 = __ldg(z + jj) + beta * __ldg(p_old + jj);
+                const VT p1 = __ldg(z + jj + 1) + beta * __ldg(p_old + jj + 1);
+                const VT p2 = __ldg(z + jj + 2) + beta * __ldg(p_old + jj + 2);
+                a0 += h0 * p0 + h1 * p1 + h2 * p2;
+                a1 += h3 * p0 + h4 * p1 + h5 * p2;
+                a2 += h6 * p0 + h7 * p1 + h8 * p2;
+            }
         }
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = LPR / 2; o > 0; o >>= 1) {
             a0 += __shfl_xor_sync(0xffffffffu, a0, o);
             a1 += __shfl_xor_sync(0xffffffffu, a1, o);
             a2 += __shfl_xor_sync(0xffffffffu, a2, o);
         }
-        if (lane < 3) {
-            const size_t ii = 3 * (size_t)row + lane;
-            const VT qi = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
+        if (row < N && sl < 3) {
+            const size_t ii = 3 * (size_t)row + sl;
+            const VT qi = sl == 0 ? a0 : (sl == 1 ? a1 : a2);
             const VT pi = z[ii] + beta * p_old[ii];
             p_new[ii] = pi;
             qv[ii] = qi;
@@ -721,13 +751,19 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
 }
 
 template <typename HT, typename VT>
-void launch_pcg_spmv(int N, const int* row_ptr, const int* col, const HT* H, const VT* z, const VT* p_old,
-                     VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
-    int wpb = kRedThreads / 32;
-    long long blocks = (N + wpb - 1) / wpb;
+void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, const VT* z,
+                     const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
+    const int lpr = max_row_blocks <= 4 ? 4 : (max_row_blocks <= 8 ? 8 : (max_row_blocks <= 16 ? 16 : 32));
+    const int rows_per_block = (kRedThreads / 32) * (32 / lpr);
+    long long blocks = (N + rows_per_block - 1) / rows_per_block;
     if (blocks > kRedBlocks) blocks = kRedBlocks;
     if (blocks < 1) blocks = 1;
-    k_pcg_spmv<HT, VT><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc);
+    switch (lpr) {
+        case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
+        case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
+        case 16: k_pcg_spmv<HT, VT, 16><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
+        default: k_pcg_spmv<HT, VT, 32><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
+    }
     counted();
 }
 
@@ -830,6 +866,18 @@ void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, d
     counted();
 }
 
+// Newton predictor q += dt v_prev
+__global__ void k_predict(int n, double* q, const double* vPrev, double dt) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) q[i] += dt * vPrev[i];
+}
+
+void launch_predict(int n, double* q, const double* vPrev, double dt, cudaStream_t st) {
+    if (n == 0) return;
+    k_predict<<<(n + 255) / 256, 256, 0, st>>>(n, q, vPrev, dt);
+    counted();
+}
+
 // y = H x (tests / diagnostics)
 template <typename HT>
 __global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y) {
@@ -838,8 +886,9 @@ __global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT
     if (row >= N) return;
     int b0 = row_ptr[row], nval = (row_ptr[row + 1] - b0) * 9;
     double a[3] = {0, 0, 0};
+    const int nb = row_ptr[row + 1] - b0;
     for (int t = lane; t < nval; t += 32) {
-        int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
+        int rc = t / nb, blk = t - rc * nb, r = rc / 3, c = rc - r * 3;
         double pr = (double)H[(size_t)b0 * 9 + t] * x[3 * (size_t)col[b0 + blk] + c];
         a[0] += r == 0 ? pr : 0.0; a[1] += r == 1 ? pr : 0.0; a[2] += r == 2 ? pr : 0.0;
     }
@@ -868,15 +917,15 @@ template void launch_pressure_jac<double>(const PressureArgs&, const int*, const
                                           cudaStream_t);
 template void launch_pressure_jac<float>(const PressureArgs&, const int*, const int*, const uint8_t*, double, float*,
                                          cudaStream_t);
-template void launch_block_jacobi<double, double>(int, const int*, const double*, double*, cudaStream_t);
-template void launch_block_jacobi<float, float>(int, const int*, const float*, float*, cudaStream_t);
+template void launch_block_jacobi<double, double>(int, const int*, const int*, const double*, double*, cudaStream_t);
+template void launch_block_jacobi<float, float>(int, const int*, const int*, const float*, float*, cudaStream_t);
 template void launch_pcg_init<double, double>(int, const double*, const double*, double*, double*, double*, double*,
                                               double, double, int, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_init<float, float>(int, const double*, const float*, float*, float*, float*, float*, double,
                                             double, int, double*, DevScalars*, cudaStream_t);
-template void launch_pcg_spmv<double, double>(int, const int*, const int*, const double*, const double*, const double*,
-                                              double*, double*, double*, DevScalars*, cudaStream_t);
-template void launch_pcg_spmv<float, float>(int, const int*, const int*, const float*, const float*, const float*,
+template void launch_pcg_spmv<double, double>(int, int, const int*, const int*, const double*, const double*,
+                                              const double*, double*, double*, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_spmv<float, float>(int, int, const int*, const int*, const float*, const float*, const float*,
                                             float*, float*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_update<double>(int, const double*, const double*, const double*, double*, double*, double*,
                                         double*, DevScalars*, cudaStream_t);

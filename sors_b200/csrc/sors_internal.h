@@ -15,7 +15,7 @@ namespace sors {
 extern std::atomic<long long> g_kernel_launches;
 
 // status bits raised by kernels
-enum : int { kFlagInverted = 1, kFlagPcgBreakdown = 2, kFlagNaN = 4 };
+enum : int { kFlagInverted = 1, kFlagPcgBreakdown = 2, kFlagNaN = 4, kFlagTimeout = 8 };
 
 // Reduction scratch: per-block partial sums + a completion counter per site.
 constexpr int kRedBlocks = 1184;      // 148 SMs x 8
@@ -54,7 +54,7 @@ struct AsmArgs {
     const uint16_t* slot_items; // k*nv + w
     const uint8_t* node_mask;   // 3 bits per node
     const double* mass;     // per node
-    HT* H;                  // nnzb*9
+    HT* H;                  // nnzb*9, row-major 3x3 blocks in CSR order
     double* g_int;          // 3N (masked element gradient)
     int* status;
     int stage_per_warp;     // HT elements per warp of staging
@@ -102,13 +102,13 @@ void launch_dof_energy(int N, const double* q, const double* qPrev, const double
                        const double* f_ext, int has_ext, double dt, int scheme, double alpha, const double* grav,
                        double* partials, DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
-void launch_block_jacobi(int N, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st);
+void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st);
 template <typename HT, typename VT>
 void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
                      double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
-void launch_pcg_spmv(int N, const int* row_ptr, const int* col, const HT* H, const VT* z, const VT* p_old,
-                     VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, const VT* z,
+                     const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
 template <typename VT>
 void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
                        DevScalars* sc, cudaStream_t st);
@@ -119,6 +119,7 @@ template <typename VT>
 void launch_dot_gdx(int n, const double* g, const VT* dx, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
                          const double* gPrevTmp, double dt, int scheme, cudaStream_t st);
+void launch_predict(int n, double* q, const double* vPrev, double dt, cudaStream_t st);
 void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const double* vPrev, double* partials,
                 DevScalars* sc, cudaStream_t st);
 template <typename HT>

@@ -61,6 +61,7 @@ class SimulationSettings:
         self.pcgRelTol = 1e-10
         self.pcgMaxIter = 20000
         self.device = 0
+        self.newtonPredictor = True        # start Newton from q + dt v_prev (same solution, fewer iterations)
 
     def verbose_print(self):
         print("Simulation Description:", self.description or "not indicated")
@@ -224,6 +225,7 @@ class _EnergyBase:
         s.pcg_rel_tol = float(getattr(settings, "pcgRelTol", 1e-10))
         s.pcg_max_iter = int(getattr(settings, "pcgMaxIter", 20000))
         s.device = int(getattr(settings, "device", 0))
+        s.newton_predictor = int(bool(getattr(settings, "newtonPredictor", True)))
         self._settings_c = s
         h = C.c_void_p()
         _lib.check(L.sors_create(_p(X, C.c_double), X.shape[0], _p(T, C.c_int32), ne, self.NV, _p(rho, C.c_double),
