@@ -164,6 +164,23 @@ int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
  * launches count every kernel node).  Diagnostic only. */
 int64_t sors_kernel_launch_count(void);
 
+/* Sum of the Neo-Hookean element energies (volume x Psi, the element part of
+ * sors_energy) of a tet (nodes_per_elem = 4) or hex (8) mesh, computed from
+ * caller-owned DEVICE arrays, without any device allocation.  No counterpart
+ * in the reference: it exists for callers that cannot let a library call
+ * cudaMalloc (memory owned by their own pool or arena, or real-time loops that
+ * must not allocate after start-up).  X_device, q_device: 3N doubles;
+ * conn_device: n_elems x nodes_per_elem; youngs_device, poisson_device:
+ * n_elems; out_device: one double.  Launched on `stream` (NULL = default
+ * stream) and asynchronous to the host.  The kernel's scratch is a fixed
+ * 64 KiB array inside the library, shared by all calls: n_elems above
+ * 8,388,608 is rejected (SORS_ERR_ARG), and calls that overlap on the GPU
+ * race and must be serialised by the caller.  The first call on each device
+ * looks up the array's device address; make it before any stream capture. */
+int sors_elem_energy_noalloc(const double* X_device, const double* q_device, const int32_t* conn_device,
+                             int32_t n_elems, int32_t nodes_per_elem, const double* youngs_device,
+                             const double* poisson_device, double* out_device, void* stream);
+
 /* CUDA stream of the handle (cudaStream_t as void*), for callers that order
  * their own work after a step. */
 void* sors_stream(SorsHandle* h);

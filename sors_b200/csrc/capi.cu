@@ -57,6 +57,8 @@ bool verbose() {
 
 }  // namespace
 
+void sors::set_last_error(const std::string& msg) { g_last_error = msg; }
+
 struct SorsHandle {
     SorsSettings s{};
     int N = 0, E = 0, nv = 0, ndof = 0;

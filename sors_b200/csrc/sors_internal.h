@@ -80,6 +80,9 @@ struct PressureArgs {
     double* f_ext;              // 3N (written for surface nodes)
 };
 
+// Sets the message returned by sors_last_error on this thread (capi.cu).
+void set_last_error(const std::string& msg);
+
 // Launchers (kernels.cu)
 template <typename HT>
 void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st);
