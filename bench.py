@@ -345,6 +345,105 @@ def run_gpu(args, rank, world, local_rank):
         dist.destroy_process_group()
 
 
+def run_c3(args):
+    """Pressure-actuated arm: voxelised cylinder (R 20 mm, L 200 mm, h 1.25 mm) with
+    three closed chambers, base clamped, E 3e5, nu 0.48; static Newton solve per
+    load level, 10 levels 0 -> 50 kPa on one chamber.  One line per precision."""
+    import torch
+    from sors_b200 import meshes
+    from sors_b200 import py_sors as ps
+    torch.cuda.set_device(0)
+    X, H = meshes.voxel_cylinder(radius=0.02, length=0.2, h=1.25e-3, cap_layers=2)
+    groups, _ = meshes.extract_surfaces(X, H)
+    faces = np.concatenate(groups)
+    gid = np.concatenate([np.full(len(g), k) for k, g in enumerate(groups)])
+    mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
+    for precision in ("mixed", "fp64"):
+        s = ps.SimulationSettings()
+        s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
+        s.precision = precision; s.newtonResidualTol = 1e-8
+        fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
+        en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
+                                      poissonsRatio=0.48, neumannBCmask=mask, neumannBCvalue=np.zeros(mask.size),
+                                      forceTypesList=["pressure"], forceParameterList=fp)
+        sol = ps.Solver(s)
+        q = X.ravel().copy()
+        levels, newton, pcg = 10, 0, 0
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for lvl in range(1, levels + 1):
+            pr = np.zeros((len(groups), 1)); pr[1, 0] = 5e3 * lvl
+            q = sol.step(q, en, ps.Params(["pressure"], [pr]), 0.0)
+            newton += sol.last_stats.newton_iters; pcg += sol.last_stats.pcg_iters
+        wall = time.perf_counter() - t0
+        print(json.dumps({"workload": "c3 pressure-actuated hex arm, static 10-level ramp to 50 kPa (one chamber)",
+                          "precision": precision, "hexes": int(H.shape[0]), "nodes": int(X.shape[0]),
+                          "surface_groups": len(groups), "s_per_load_level": wall / levels,
+                          "newton_iters_per_level": newton / levels, "pcg_iters_per_level": pcg / levels,
+                          "tip_displacement_max_m": float(np.abs(q - X.ravel()).max())}), flush=True)
+        del en
+
+
+def run_serve(args):
+    """Mixed-size poke sweep: Poisson arrivals of cube rollouts (6-tet cubes with
+    log-uniform 5k-250k tets, E U[2e4, 2e5], nu U[0.30, 0.48], rho 1000, dt 1e-2).
+    Served form: mixed precision, continuous admission, 8 slots.  Baseline: the
+    plain FP64 drop-in, one rollout at a time, on the same requests."""
+    import torch
+    from sors_b200 import serving
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(7)
+
+    def make(precision):
+        r = np.random.default_rng(11)
+        out = []
+        for i in range(args.rollouts):
+            tets = float(np.exp(r.uniform(np.log(5e3), np.log(2.5e5))))
+            n = max(2, int(round((tets / 6.0) ** (1.0 / 3.0))))
+            out.append(serving.poke_cube_request(r, n, tag=i, steps=args.rollout_steps, dt=1e-2, precision=precision))
+        return out
+
+    def run(precision, slots, arrivals):
+        reqs = make(precision)
+        srv = serving.RolloutServer(max_slots=slots)
+        t0 = time.perf_counter()
+        for req, at in zip(reqs, arrivals):
+            now = time.perf_counter() - t0
+            if at > now:
+                time.sleep(at - now)
+            srv.submit(req)
+        res = srv.close()
+        wall = time.perf_counter() - t0
+        errs = [r.error for r in res if r.error]
+        steps = [x for r in res for x in r.step_latencies]
+        lat = [r.latency for r in res]
+        tets = sum(q.elements.shape[0] for q in reqs)
+        return {"rollouts_per_s": len(res) / wall, "makespan_s": wall, "errors": len(errs),
+                "step_latency_p50_ms": 1e3 * serving.percentile(steps, 50),
+                "step_latency_p99_ms": 1e3 * serving.percentile(steps, 99),
+                "rollout_latency_p50_s": serving.percentile(lat, 50),
+                "rollout_latency_p99_s": serving.percentile(lat, 99), "tets_total": tets}, res, reqs
+
+    gaps = rng.exponential(1.0 / args.rate, size=args.rollouts)
+    arrivals = np.cumsum(gaps) - gaps[0]
+    served, res_m, reqs = run("mixed", args.slots, arrivals)
+    saturated, _, _ = run("mixed", args.slots, np.zeros(args.rollouts))
+    plain, res_p, _ = run("fp64", 1, np.zeros(args.rollouts))
+    # accuracy of the served form against the plain FP64 path, per rollout,
+    # relative to that rollout's largest displacement
+    by_tag = {r.tag: r.final for r in res_p}
+    X0 = {q.tag: q.vertices.ravel() for q in reqs}
+    rel = [float(np.abs(r.final - by_tag[r.tag]).max() / max(np.abs(by_tag[r.tag] - X0[r.tag]).max(), 1e-30))
+           for r in res_m if r.final is not None and by_tag.get(r.tag) is not None]
+    print(json.dumps({"workload": f"poke sweep: {args.rollouts} rollouts x {args.rollout_steps} steps, "
+                                  f"Poisson arrivals at {args.rate}/s, 6-tet cubes 5k-250k tets",
+                      "slots": args.slots, "served_mixed": served, "served_mixed_all_at_once": saturated,
+                      "plain_fp64_sequential": plain,
+                      "capacity_speedup_rollouts_per_s": saturated["rollouts_per_s"] / plain["rollouts_per_s"],
+                      "speedup_rollouts_per_s": served["rollouts_per_s"] / plain["rollouts_per_s"],
+                      "max_rel_diff_vs_fp64": max(rel) if rel else None}), flush=True)
+
+
 def run_profile_only(args):
     """Builds the workload and runs only the kernel profiler (3 launches each)."""
     import ctypes
@@ -373,6 +472,13 @@ def main():
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "serve"],
+                    help="c2: the 3.0M-tet block (default); c3: pressure-actuated hex arm, static load ramp; "
+                         "serve: Poisson stream of poke rollouts")
+    ap.add_argument("--rollouts", type=int, default=24)
+    ap.add_argument("--rollout-steps", type=int, default=20)
+    ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (rollouts/s)")
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent rollouts")
     ap.add_argument("--profile-only", action="store_true",
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
@@ -382,6 +488,10 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+    elif args.workload == "c3":
+        run_c3(args)
+    elif args.workload == "serve":
+        run_serve(args)
     elif args.profile_only:
         run_profile_only(args)
     else:

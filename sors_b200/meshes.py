@@ -105,12 +105,13 @@ def hex_bar(nx=40, ny=8, nz=8, size=(0.2, 0.04, 0.04)):
 
 
 def voxel_cylinder(radius=0.02, length=0.2, h=1.25e-3, chamber_radius=0.004, chamber_offset=0.008,
-                   chamber_angles_deg=(0.0, 120.0, 240.0)):
+                   chamber_angles_deg=(0.0, 120.0, 240.0), cap_layers=0):
     """Voxelised cylinder along z with cylindrical chambers (hexes, h-sized voxels).
 
     A voxel is solid when its centre lies inside the outer radius and outside
-    every chamber.  Returns (X, hexes, chamber_id_of_node) where the node array
-    only holds nodes used by solid voxels.
+    every chamber; the first and last `cap_layers` voxel layers are solid
+    everywhere, which closes the chambers so each becomes its own surface.
+    Returns (X, hexes) with only the nodes used by solid voxels.
     """
     n_xy = int(np.ceil(2 * radius / h))
     nz = int(round(length / h))
@@ -127,9 +128,11 @@ def voxel_cylinder(radius=0.02, length=0.2, h=1.25e-3, chamber_radius=0.004, cha
         solid2d &= ~ch
     NX = NY = n_xy + 1
     ii, jj = np.nonzero(solid2d)
+    ii_in, jj_in = np.nonzero(inside)
     hexes = []
     for k in range(nz):
-        i, j = ii, jj
+        capped = k < cap_layers or k >= nz - cap_layers
+        i, j = (ii_in, jj_in) if capped else (ii, jj)
         hexes.append(np.stack([
             _vid(i, j, k, NX, NY), _vid(i + 1, j, k, NX, NY), _vid(i + 1, j + 1, k, NX, NY),
             _vid(i, j + 1, k, NX, NY), _vid(i, j, k + 1, NX, NY), _vid(i + 1, j, k + 1, NX, NY),

@@ -162,6 +162,12 @@ class _EnergyBase:
             # elements without energies only carry mass (Energy with empty sets)
             material = 0
         self._init_arrays(X, T, settings, gravAcceleration, dampingAlpha, rho, E, nu, material or 0)
+        self._setup_constraints_forces(constraintTypesList, constraintParameterList, forceTypesList,
+                                       forceParameterList)
+
+    def _setup_constraints_forces(self, constraintTypesList, constraintParameterList, forceTypesList,
+                                  forceParameterList):
+        """Constraint and force set-up of Energy<3,E>::Energy (cpp/src/energy.cpp:58-174)."""
         L = _lib.load()
         cp = constraintParameterList if constraintParameterList is not None else Params()
         fp = forceParameterList if forceParameterList is not None else Params()
@@ -237,7 +243,8 @@ class _EnergyBase:
 
     @classmethod
     def from_arrays(cls, undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha=0.0, *, density,
-                    youngsModulus, poissonsRatio, neumannBCmask=None, neumannBCvalue=None):
+                    youngsModulus, poissonsRatio, neumannBCmask=None, neumannBCvalue=None, forceTypesList=(),
+                    forceParameterList=None):
         """Neo-Hookean mesh from per-element arrays instead of one Params per element.
 
         Same system as the reference-style constructor; meant for meshes with
@@ -245,10 +252,12 @@ class _EnergyBase:
         obj = cls.__new__(cls)
         obj._init_arrays(undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha, density,
                          youngsModulus, poissonsRatio)
+        ctypes_, cp = [], Params()
         if neumannBCmask is not None:
-            mask = np.ascontiguousarray(np.asarray(neumannBCmask).ravel().astype(np.int32))
-            val = np.ascontiguousarray(np.asarray(neumannBCvalue, dtype=np.float64).ravel())
-            _lib.check(_lib.load().sors_set_neumann(obj._h, _p(mask, C.c_int32), _p(val, C.c_double)))
+            ctypes_ = ["neumannBC"]
+            cp.set_param("neumannBCmask", np.asarray(neumannBCmask, dtype=np.float64).ravel())
+            cp.set_param("neumannBCvalue", np.asarray(neumannBCvalue, dtype=np.float64).ravel())
+        obj._setup_constraints_forces(ctypes_, cp, forceTypesList, forceParameterList)
         return obj
 
     def __del__(self):

@@ -235,3 +235,56 @@ def test_deterministic(c1):
             q = sol.step(q, en)
         outs.append(q)
     assert np.array_equal(outs[0], outs[1])
+
+
+def _c3_case(length=0.015, h=2.5e-3):
+    """Voxel cylinder (R 20 mm) with three closed chambers; base clamped."""
+    X, H = meshes.voxel_cylinder(length=length, h=h, cap_layers=2)
+    groups, _ = meshes.extract_surfaces(X, H)
+    faces = np.concatenate(groups)
+    gid = np.concatenate([np.full(len(g), k) for k, g in enumerate(groups)])
+    return X, H, faces, gid, len(groups)
+
+
+C3_LEVELS = (1, 2, 3)
+
+
+@pytest.fixture(scope="module")
+def c3_reference(oracle):
+    X, H, faces, gid, ng = _c3_case()
+    mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
+    o = oracle.System(X, H, rho=1070.0, youngs=3e5, nu=0.48, grav=(0, 0, 0), dt=0.0)
+    o.set_neumann(mask, np.zeros(mask.size)); o.set_pressure(faces, gid)
+    qo = X.ravel().copy()
+    for level in C3_LEVELS:
+        pr = np.zeros(ng); pr[1] = 5e3 * level   # one chamber
+        qo, st = o.step(qo, dt=0.0, pressure=pr)
+        assert st == 0
+    return qo
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_c3_chamber_pressure_static(c3_reference, precision):
+    """Pressure-actuated arm, hexes, quasistatic (dt = 0): GPU vs oracle over a load ramp."""
+    from sors_b200 import py_sors as ps
+    X, H, faces, gid, ng = _c3_case()
+    assert ng == 4  # outer surface + three chambers
+    mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
+    s = ps.SimulationSettings()
+    s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
+    s.precision = precision; s.newtonResidualTol = 1e-10
+    ne = H.shape[0]
+    params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [1070.0, 3e5, 0.48])] * ne
+    cp = ps.Params(["neumannBCmask", "neumannBCvalue"], [mask.astype(float), np.zeros(mask.size)])
+    fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
+    en = ps.Energy(X, H, s, np.zeros(3), 0.0, [{"neohookean"}] * ne, params, ["neumannBC"], cp, ["pressure"], fp)
+    sol = ps.Solver(s)
+    q = X.ravel().copy()
+    for level in C3_LEVELS:
+        pr = np.zeros(ng); pr[1] = 5e3 * level   # one chamber
+        q = sol.step(q, en, ps.Params(["pressure"], [pr.reshape(-1, 1)]), 0.0)
+    qo = c3_reference
+    u = qo - X.ravel()
+    assert np.abs(u).max() > 1e-5
+    tol = 1e-8 if precision == "fp64" else 1e-6 * np.abs(u).max()
+    assert np.abs(q - qo).max() < tol, np.abs(q - qo).max()
