@@ -419,6 +419,7 @@ def run_serve(args):
         lat = [r.latency for r in res]
         tets = sum(q.elements.shape[0] for q in reqs)
         return {"rollouts_per_s": len(res) / wall, "makespan_s": wall, "errors": len(errs),
+                "error_messages": sorted(set(errs))[:3],
                 "step_latency_p50_ms": 1e3 * serving.percentile(steps, 50),
                 "step_latency_p99_ms": 1e3 * serving.percentile(steps, 99),
                 "rollout_latency_p50_s": serving.percentile(lat, 50),

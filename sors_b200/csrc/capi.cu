@@ -643,7 +643,10 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if (cudaMallocHost((void**)&h->sc_host, sizeof(DevScalars)) != cudaSuccess)
         return bail(fail(SORS_ERR_OOM, "pinned allocation failed"));
     if ((st = dalloc_t(h, &h->pressure_d, 1))) return bail(st);
-    CK(cudaDeviceSynchronize());
+    // synchronous copies above ran on the legacy stream; no device-wide sync here,
+    // so that a handle created while others are capturing PCG graphs does not
+    // invalidate their capture
+    CK(cudaStreamSynchronize(h->stream));
     *out = h;
     return SORS_OK;
 }
