@@ -101,8 +101,19 @@ int sors_set_pressure_faces(SorsHandle* h, const int32_t* faces, int32_t n_faces
 /* VertexForce (cpp/src/forces/vertexForce.cpp): enables the "vertexForce" actuation. */
 int sors_enable_vertex_force(SorsHandle* h, int32_t enable);
 
-/* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values)
- * or "vertexForce" (3N values, row-major N x 3). */
+/* SoftCon fibre terms, replacing the per-element "softconMuscle" energy and its
+ * Params muscleGroup / softconStiffness / softconDirection
+ * (cpp/src/geometries/tetrahedron.cpp:82-88, hexahedron.cpp:51-57,
+ * cpp/src/energies/softconMuscle.cpp).  group: E entries, -1 = no fibre term;
+ * stiffness: E; direction: E x 3 row-major.  Activations start at 0 and are set
+ * with the "softconMuscle" actuation.  Energy k/2 (|F m| - (1 - e))^2, whose
+ * gradient is the reference's; its exact Hessian (projected when project_spd). */
+int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffness, const double* direction,
+                     int32_t n_groups);
+
+/* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values),
+ * "vertexForce" (3N values, row-major N x 3) or "softconMuscle" (one activation
+ * per muscle group). */
 int sors_set_actuation(SorsHandle* h, const char* name, const double* values, int64_t n);
 
 /* Energy::set_initial_deformation / set_initial_velocity (cpp/headers/energy.h:203-204). */

@@ -47,6 +47,10 @@ def lib():
         L.orc_elem_eval.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]
         L.orc_elem_eval_batch.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp]
         L.orc_project_psd9.argtypes = [_dp]
+        L.orc_elem_eval_muscle.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_double, _dp, C.c_double,
+                                           C.c_int, C.c_int, _dp, _dp, _dp]
+        L.orc_set_muscles.argtypes = [C.c_void_p, _ip, _dp, _dp, C.c_int, C.c_int]
+        L.orc_set_muscle_act.argtypes = [C.c_void_p, _dp]
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.c_int, C.c_int, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp, C.c_double, C.c_int,
                                  C.c_int, C.c_int, C.c_int, C.c_int]
@@ -115,6 +119,21 @@ def elem_eval(X, x, youngs, nu, project=False):
     return float(psi[0]), g, H, st
 
 
+MUSCLE_REFERENCE = 0   # the reference's energy and Hessian forms (softconMuscle.cpp:30-31, :115-127)
+MUSCLE_CONSISTENT = 1  # energy k/2 (|Fm| - (1-e))^2 and its exact Hessian
+
+
+def elem_eval_muscle(X, x, youngs, nu, k, m, act, form=MUSCLE_CONSISTENT, project=False):
+    """Neo-Hookean + SoftCon fibre element: Psi*V, grad*V, hess*V, status."""
+    X = _d(X); x = _d(x)
+    nv = X.shape[0]
+    n = 3 * nv
+    psi = np.zeros(1); g = np.zeros(n); H = np.zeros((n, n))
+    st = lib().orc_elem_eval_muscle(nv, _pd(X), _pd(x), float(youngs), float(nu), float(k), _pd(_d(m)), float(act),
+                                    int(form), int(project), _pd(psi), _pd(g), _pd(H))
+    return float(psi[0]), g, H, st
+
+
 def elem_eval_batch(Xn, conn, xn, youngs, nu, project=False, want_hess=True):
     Xn = _d(Xn); xn = _d(xn); conn = _i(conn)
     ne, nv = conn.shape
@@ -170,6 +189,15 @@ class System:
         self._faces = _i(faces); self._groups = _i(groups)
         lib().orc_set_pressure(self.h, self._faces.shape[0], self._faces.shape[1], _pi(self._faces),
                                _pi(self._groups))
+
+    def set_muscles(self, group, stiffness, direction, n_groups, form=MUSCLE_CONSISTENT):
+        """SoftCon fibre terms: group per element (-1 none), stiffness, direction (E x 3)."""
+        self._mgroup = _i(group); self._mk = _d(stiffness); self._mdir = _d(direction).reshape(-1, 3)
+        lib().orc_set_muscles(self.h, _pi(self._mgroup), _pd(self._mk), _pd(self._mdir), int(n_groups), int(form))
+
+    def set_muscle_act(self, act):
+        self._mact = _d(act).ravel()
+        lib().orc_set_muscle_act(self.h, _pd(self._mact))
 
     def set_vertex_force(self, enabled=True):
         lib().orc_set_vertex_force(self.h, int(enabled))

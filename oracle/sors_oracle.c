@@ -366,8 +366,75 @@ static void elem_F(const ElemGeom* g, const double* x, double* F) {
 #define ORC_MAT_NEOHOOKEAN 0
 #define ORC_MAT_TEST_QUARTIC 1
 
+/* SoftCon fibre term of one element (cpp/src/energies/softconMuscle.cpp:12-132):
+ * stiffness k, fibre direction m, activation e of the element's muscle group. */
+typedef struct { double k, m[3], e; } OrcMuscle;
+/* form 0: the reference's energy k/2 |(1-r) F m| = k/2 |l-(1-e)| (:30-31) and its
+ * Hessian, whose second term sums d(Fm)_a/dx over a before the outer product
+ * (:115-127).  form 1: the energy k/2 (l-(1-e))^2, of which the reference's
+ * gradient (:56-73) is the gradient, and its exact Hessian (eigenvalue k along
+ * F m, k (1-r) across it; the latter clamped at 0 when projecting). */
+#define ORC_MUSCLE_REFERENCE 0
+#define ORC_MUSCLE_CONSISTENT 1
+
+/* Adds the fibre term (not yet scaled by the volume) to psi / grad / hess. */
+static void muscle_eval(const ElemGeom* g, const double* F, const OrcMuscle* mm, int form, int project,
+                        double* psi, double* grad, double* hess) {
+    int n = g->ncol;
+    double w = 1.0 / g->nqp;
+    double Bm[3][24];
+    for (int s = 0; s < g->nqp; s++) {
+        const double* f = F + 9 * s;
+        const double* Bs = g->B + (size_t)s * 9 * n;
+        double u[3];
+        for (int a = 0; a < 3; a++) u[a] = f[a * 3] * mm->m[0] + f[a * 3 + 1] * mm->m[1] + f[a * 3 + 2] * mm->m[2];
+        double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        double r = (1 - mm->e) / l;
+        /* Bm_a(i) = sum_c m_c dF_ac/dx_i */
+        for (int a = 0; a < 3; a++)
+            for (int i = 0; i < n; i++) {
+                double acc = 0;
+                for (int c = 0; c < 3; c++) acc += mm->m[c] * Bs[(a * 3 + c) * n + i];
+                Bm[a][i] = acc;
+            }
+        if (psi) {
+            double t = l - (1 - mm->e);
+            *psi += (form == ORC_MUSCLE_REFERENCE ? 0.5 * mm->k * fabs(t) : 0.5 * mm->k * t * t) * w;
+        }
+        if (grad)
+            for (int i = 0; i < n; i++)
+                grad[i] += mm->k * (1 - r) * (u[0] * Bm[0][i] + u[1] * Bm[1][i] + u[2] * Bm[2][i]) * w;
+        if (hess) {
+            if (form == ORC_MUSCLE_REFERENCE) {
+                for (int i = 0; i < n; i++) {
+                    double p1i = u[0] * Bm[0][i] + u[1] * Bm[1][i] + u[2] * Bm[2][i];
+                    double p2i = Bm[0][i] + Bm[1][i] + Bm[2][i];
+                    for (int j = 0; j < n; j++) {
+                        double p1j = u[0] * Bm[0][j] + u[1] * Bm[1][j] + u[2] * Bm[2][j];
+                        double p2j = Bm[0][j] + Bm[1][j] + Bm[2][j];
+                        hess[i * n + j] += mm->k * (r / (l * l) * p1i * p1j + (1 - r) * p2i * p2j) * w;
+                    }
+                }
+            } else {
+                double c = 1 - r;
+                if (project && c < 0) c = 0;
+                double M[9];
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) M[a * 3 + b] = (1 - c) * u[a] * u[b] / (l * l) + (a == b ? c : 0.0);
+                for (int i = 0; i < n; i++)
+                    for (int j = 0; j < n; j++) {
+                        double acc = 0;
+                        for (int a = 0; a < 3; a++)
+                            for (int b = 0; b < 3; b++) acc += M[a * 3 + b] * Bm[a][i] * Bm[b][j];
+                        hess[i * n + j] += mm->k * acc * w;
+                    }
+            }
+        }
+    }
+}
+
 static int elem_eval_geom(const ElemGeom* g, int material, const double* x, double mu, double lam, int project,
-                          double* psi, double* grad, double* hess) {
+                          const OrcMuscle* mm, int mform, double* psi, double* grad, double* hess) {
     int n = g->ncol;
     if (material == ORC_MAT_TEST_QUARTIC) {
         if (psi) {
@@ -386,15 +453,15 @@ static int elem_eval_geom(const ElemGeom* g, int material, const double* x, doub
     double F[72];
     elem_F(g, x, F);
     int st = ORC_OK;
-    if (psi) *psi = nh_energy(F, g->nqp, mu, lam) * g->vol;
-    if (grad) {
-        nh_gradient(F, g->B, g->nqp, n, mu, lam, grad);
+    if (psi) *psi = nh_energy(F, g->nqp, mu, lam);
+    if (grad) nh_gradient(F, g->B, g->nqp, n, mu, lam, grad);
+    if (hess) st = nh_hessian(F, g->B, g->nqp, n, mu, lam, project, hess);
+    if (mm) muscle_eval(g, F, mm, mform, project, psi, grad, hess);
+    if (psi) *psi *= g->vol;
+    if (grad)
         for (int k = 0; k < n; k++) grad[k] *= g->vol;
-    }
-    if (hess) {
-        st = nh_hessian(F, g->B, g->nqp, n, mu, lam, project, hess);
+    if (hess)
         for (int k = 0; k < n * n; k++) hess[k] *= g->vol;
-    }
     return st;
 }
 
@@ -405,7 +472,19 @@ int orc_elem_eval(int nv, const double* X, const double* x, double youngs, doubl
     elem_geom(nv, X, &g);
     double mu, lam;
     lame(youngs, nu, &mu, &lam);
-    return elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, psi, grad, hess);
+    return elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, NULL, 0, psi, grad, hess);
+}
+
+/* Neo-Hookean + SoftCon fibre element (form: ORC_MUSCLE_*). */
+int orc_elem_eval_muscle(int nv, const double* X, const double* x, double youngs, double nu, double k,
+                         const double* m, double act, int form, int project, double* psi, double* grad,
+                         double* hess) {
+    ElemGeom g;
+    elem_geom(nv, X, &g);
+    double mu, lam;
+    lame(youngs, nu, &mu, &lam);
+    OrcMuscle mm = {k, {m[0], m[1], m[2]}, act};
+    return elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, &mm, form, psi, grad, hess);
 }
 
 /* Batched element evaluation over a mesh (OpenMP).  Outputs per element:
@@ -427,7 +506,7 @@ int orc_elem_eval_batch(int nv, int ne, const double* Xn, const int32_t* conn, c
         elem_geom(nv, X, &g);
         double mu, lam;
         lame(youngs[e], nu[e], &mu, &lam);
-        int st = elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, psi ? psi + e : NULL,
+        int st = elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, NULL, 0, psi ? psi + e : NULL,
                                 grad ? grad + (size_t)e * n : NULL, hess ? hess + (size_t)e * n * n : NULL);
         if (st != ORC_OK) {
 #pragma omp atomic write
@@ -746,6 +825,12 @@ typedef struct {
     int32_t* face_group;
     int has_pressure;
     int has_vertex_force;
+    /* SoftCon fibre terms: group per element (-1 none), k, direction; activation per group */
+    int32_t* mgroup;
+    double* mk;
+    double* mdir;
+    double* mact;
+    int n_mgroups, muscle_form;
     /* integrator state (integrator.h:109-117) */
     double* qPrev;
     double* vPrev;
@@ -835,6 +920,7 @@ OrcSystem* orc_create(int nv, int N, const double* X, int E, const int32_t* conn
 }
 
 void orc_destroy(OrcSystem* s) {
+    free(s->mgroup); free(s->mk); free(s->mdir); free(s->mact);
     if (!s) return;
     free(s->X); free(s->conn); free(s->mu); free(s->lam); free(s->geom); free(s->mass);
     free(s->mask); free(s->mval); free(s->faces); free(s->face_group);
@@ -882,6 +968,34 @@ int orc_last_newton_iters(OrcSystem* s) { return s->last_newton_iters; }
 static void gather_elem(const OrcSystem* s, const double* q, int e, double* x) {
     for (int j = 0; j < s->nv; j++)
         for (int k = 0; k < 3; k++) x[j * 3 + k] = q[3 * s->conn[e * s->nv + j] + k];
+}
+
+/* The element's fibre term, or NULL (element.h:50-53 looks the activation up
+ * under the energy's name, "softconMuscle", by the element's muscle group). */
+static const OrcMuscle* elem_muscle(const OrcSystem* s, int e, OrcMuscle* mm) {
+    if (!s->mgroup || s->mgroup[e] < 0) return NULL;
+    mm->k = s->mk[e];
+    for (int c = 0; c < 3; c++) mm->m[c] = s->mdir[3 * (size_t)e + c];
+    mm->e = s->mact[s->mgroup[e]];
+    return mm;
+}
+
+void orc_set_muscles(OrcSystem* s, const int32_t* group, const double* k, const double* dir, int n_groups,
+                     int form) {
+    free(s->mgroup); free(s->mk); free(s->mdir); free(s->mact);
+    s->mgroup = (int32_t*)malloc(sizeof(int32_t) * (size_t)(s->E ? s->E : 1));
+    s->mk = (double*)malloc(sizeof(double) * (size_t)(s->E ? s->E : 1));
+    s->mdir = (double*)malloc(sizeof(double) * 3 * (size_t)(s->E ? s->E : 1));
+    s->mact = (double*)calloc((size_t)(n_groups > 0 ? n_groups : 1), sizeof(double));
+    memcpy(s->mgroup, group, sizeof(int32_t) * (size_t)s->E);
+    memcpy(s->mk, k, sizeof(double) * (size_t)s->E);
+    memcpy(s->mdir, dir, sizeof(double) * 3 * (size_t)s->E);
+    s->n_mgroups = n_groups;
+    s->muscle_form = form;
+}
+
+void orc_set_muscle_act(OrcSystem* s, const double* act) {
+    if (s->mact) memcpy(s->mact, act, sizeof(double) * (size_t)s->n_mgroups);
 }
 
 /* pressureForce.cpp:14-56.  act: pressure per group. */
@@ -1018,7 +1132,9 @@ double orc_energy(OrcSystem* s, const double* q, double dt, const double* pressu
     for (int el = 0; el < s->E; el++) {
         double x[24], psi;
         gather_elem(s, q, el, x);
-        elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], 0, &psi, NULL, NULL);
+        OrcMuscle mm;
+        elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], 0, elem_muscle(s, el, &mm),
+                       s->muscle_form, &psi, NULL, NULL);
         e += psi;
     }
     if (s->has_pressure || s->has_vertex_force) {
@@ -1044,7 +1160,9 @@ void orc_gradient(OrcSystem* s, const double* q, double dt, const double* pressu
     for (int el = 0; el < s->E; el++) {
         double x[24];
         gather_elem(s, q, el, x);
-        elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], 0, NULL, ge + (size_t)el * ncol, NULL);
+        OrcMuscle mm;
+        elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], 0, elem_muscle(s, el, &mm),
+                       s->muscle_form, NULL, ge + (size_t)el * ncol, NULL);
     }
     for (int el = 0; el < s->E; el++)
         for (int j = 0; j < nv; j++)
@@ -1101,7 +1219,9 @@ static int hessian_csr(OrcSystem* s, const double* q, double dt, const double* p
         for (int el = 0; el < s->E; el++) {
             double x[24];
             gather_elem(s, q, el, x);
-            int st = elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], s->project, NULL, NULL, He);
+            OrcMuscle mm;
+            int st = elem_eval_geom(&s->geom[el], s->material, x, s->mu[el], s->lam[el], s->project,
+                                    elem_muscle(s, el, &mm), s->muscle_form, NULL, NULL, He);
             if (st != ORC_OK) {
 #pragma omp atomic write
                 status = st;

@@ -98,6 +98,12 @@ struct SorsHandle {
     int *faces = nullptr, *face_group = nullptr, *surf_nodes = nullptr, *sface_ptr = nullptr, *sface_fl = nullptr;
     double* pressure_d = nullptr;
 
+    // SoftCon fibre terms
+    int* mgroup = nullptr;
+    double4* mparam = nullptr;
+    double* mact = nullptr;
+    int n_mgroups = 0;
+
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
     bool graph_failed = false;
@@ -108,6 +114,11 @@ struct SorsHandle {
 namespace {
 
 bool mixed(const SorsHandle* h) { return h->s.precision == 1; }
+MuscleArgs muscles(const SorsHandle* h) {
+    MuscleArgs m;
+    if (h->mgroup) { m.group = h->mgroup; m.param = h->mparam; m.act = h->mact; }
+    return m;
+}
 size_t hsize(const SorsHandle* h) { return mixed(h) ? sizeof(float) : sizeof(double); }
 
 int dalloc(SorsHandle* h, void** p, size_t bytes) {
@@ -298,7 +309,7 @@ int eval_system(SorsHandle* h, double dt, bool want_hess) {
     int st = compute_external(h);
     if (st) return st;
     AsmArgs<HT> a;
-    a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat;
+    a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
     a.H = (HT*)h->H; a.g_int = h->g_int; a.status = h->status;
@@ -327,7 +338,7 @@ int eval_system(SorsHandle* h, double dt, bool want_hess) {
 int eval_energy(SorsHandle* h, double dt, double* out) {
     int st = compute_external(h);
     if (st) return st;
-    launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, h->partials, h->sc, h->stream);
+    launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->partials, h->sc, h->stream);
     launch_dof_energy(h->N, h->q, h->qPrev, h->vPrev, h->mass, h->f_ext, (h->has_vforce || h->has_pressure) ? 1 : 0,
                       dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav, h->partials, h->sc, h->stream);
     CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
@@ -735,7 +746,41 @@ int sors_set_actuation(SorsHandle* h, const char* name, const double* values, in
         CK(cudaMemcpy(h->vforce, values, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
         return SORS_OK;
     }
-    return SORS_OK;  // other Params keys (e.g. softconMuscle) are not used by Neo-Hookean elements
+    if (nm == "softconMuscle") {
+        if (!h->mgroup) return SORS_OK;  // no element carries a fibre term
+        if (n < h->n_mgroups) return fail(SORS_ERR_ARG, "softconMuscle actuation has fewer entries than muscle groups");
+        CK(cudaMemcpy(h->mact, values, sizeof(double) * h->n_mgroups, cudaMemcpyHostToDevice));
+        return SORS_OK;
+    }
+    return SORS_OK;  // other Params keys are not used by this mesh's energies
+}
+
+int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffness, const double* direction,
+                     int32_t n_groups) {
+    if (!h || !group || !stiffness || !direction) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_groups < 1) return fail(SORS_ERR_ARG, "n_groups must be positive");
+    int st;
+    if ((st = set_device(h))) return st;
+    std::vector<double4> prm((size_t)std::max(1, h->E));
+    for (int e = 0; e < h->E; e++) {
+        if (group[e] >= n_groups || group[e] < -1) return fail(SORS_ERR_ARG, "muscle group out of range");
+        prm[e] = make_double4(direction[3 * (size_t)e], direction[3 * (size_t)e + 1], direction[3 * (size_t)e + 2],
+                              stiffness[e]);
+    }
+    if (!h->mgroup) {
+        if ((st = dalloc_t(h, &h->mgroup, (size_t)std::max(1, h->E)))) return st;
+        if ((st = dalloc_t(h, &h->mparam, (size_t)std::max(1, h->E)))) return st;
+    }
+    if (n_groups > h->n_mgroups) {
+        if ((st = dalloc_t(h, &h->mact, (size_t)n_groups))) return st;
+        CK(cudaMemset(h->mact, 0, sizeof(double) * n_groups));
+    }
+    h->n_mgroups = std::max(h->n_mgroups, (int)n_groups);
+    if (h->E) {
+        CK(cudaMemcpy(h->mgroup, group, sizeof(int) * h->E, cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->mparam, prm.data(), sizeof(double4) * h->E, cudaMemcpyHostToDevice));
+    }
+    return SORS_OK;
 }
 
 int sors_set_initial_deformation(SorsHandle* h, const double* q) {
@@ -830,10 +875,10 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
     cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(h->status, 0, sizeof(int), h->stream);
     if (mixed(h))
-        launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, project, dpsi, dgrad, dhess,
+        launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                 h->status, h->stream);
     else
-        launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, project, dpsi, dgrad, dhess,
+        launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                  h->status, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e == cudaSuccess && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * h->E, cudaMemcpyDeviceToHost);
@@ -911,7 +956,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     int st = eval_system<HT>(h, dt, true);
     if (st) return st;
     AsmArgs<HT> aa;
-    aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat;
+    aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat; aa.mus = muscles(h);
     aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
     aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
     aa.H = (HT*)h->H; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
@@ -955,7 +1000,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     out->pcg_update_bytes = 3 * N * vs * 2 + 9 * N * vs + 3 * N * vs * 4 + 3 * N * vs;
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
-        launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->s.material, h->partials, h->sc, h->stream);
+        launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->partials, h->sc, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&ms, a, b));

@@ -348,6 +348,61 @@ __device__ __forceinline__ double nh_qp_energy(const double* F, double mu, doubl
 }
 
 // ---------------------------------------------------------------------------
+// SoftCon fibre term at one quadrature point (cpp/src/energies/softconMuscle.cpp).
+// With u = F m = sum_w x_w s_w, s_w = d_w . m, l = |u| and r = (1 - e) / l the
+// reference's gradient k (1 - r) u . du/dx (softconMuscle.cpp:56-73) is the
+// gradient of k/2 (l - (1 - e))^2; this is the energy used here, with its exact
+// Hessian: block (v,w) = k s_v s_w [u u^T / l^2 + c (I - u u^T / l^2)], c = 1 - r,
+// clamped at 0 when the Hessian is projected (the u direction always has
+// eigenvalue k).  mp = (m_x, m_y, m_z, k).
+// ---------------------------------------------------------------------------
+template <typename HT, int NV, bool HESS>
+__device__ __forceinline__ void muscle_qp_row(const double (&d)[NV][3], const double (&x)[NV][3],
+                                              const double (&dvd)[3], double wV, double4 mp, double eact,
+                                              bool project, double* g, HT (&blk)[NV * 9]) {
+    double s[NV];
+    double u[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        s[w] = d[w][0] * mp.x + d[w][1] * mp.y + d[w][2] * mp.z;
+#pragma unroll
+        for (int r = 0; r < 3; r++) u[r] += x[w][r] * s[w];
+    }
+    const double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double rr = (1.0 - eact) / l;
+    const double sv = dvd[0] * mp.x + dvd[1] * mp.y + dvd[2] * mp.z;
+    const double gc = wV * mp.w * (1.0 - rr) * sv;
+#pragma unroll
+    for (int r = 0; r < 3; r++) g[r] += gc * u[r];
+    if (!HESS) return;
+    double c = 1.0 - rr;
+    if (project && c < 0.0) c = 0.0;
+    const double il2 = 1.0 / (l * l);
+    HT M[9];
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) M[k * 3 + q] = (HT)((1.0 - c) * u[k] * u[q] * il2 + (k == q ? c : 0.0));
+    const double hv = wV * mp.w * sv;
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        const HT f = (HT)(hv * s[w]);
+#pragma unroll
+        for (int k = 0; k < 9; k++) blk[w * 9 + k] += f * M[k];
+    }
+}
+
+// Energy density of the fibre term at one quadrature point: k/2 (|F m| - (1 - e))^2.
+__device__ __forceinline__ double muscle_qp_energy(const double* F, double4 mp, double eact) {
+    double u[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) u[r] = F[r * 3 + 0] * mp.x + F[r * 3 + 1] * mp.y + F[r * 3 + 2] * mp.z;
+    const double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const double t = l - (1.0 - eact);
+    return 0.5 * mp.w * t * t;
+}
+
+// ---------------------------------------------------------------------------
 // Element geometry: shape gradients d (NV x 3) at a quadrature point and the
 // undeformed volume, from the undeformed vertex positions X (NV x 3).
 // ---------------------------------------------------------------------------

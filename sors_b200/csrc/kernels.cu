@@ -98,8 +98,9 @@ static inline int red_grid(long long n, int per_thread = 1) {
 // ---------------------------------------------------------------------------
 template <typename HT, int NV, bool HESS>
 __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const double* __restrict__ qg,
-                                         const int* __restrict__ conn, const double2* __restrict__ mat, int e,
-                                         int v, int material, bool project, double* g, HT (&blk)[NV * 9]) {
+                                         const int* __restrict__ conn, const double2* __restrict__ mat,
+                                         const MuscleArgs& mus, int e, int v, int material, bool project, double* g,
+                                         HT (&blk)[NV * 9]) {
     double X[NV][3], x[NV][3];
 #pragma unroll
     for (int w = 0; w < NV; w++) {
@@ -127,6 +128,10 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
         return true;
     }
     const double2 m = __ldg(mat + e);
+    const int grp = mus.group ? __ldg(mus.group + e) : -1;
+    double4 mp = make_double4(0.0, 0.0, 0.0, 0.0);
+    double eact = 0.0;
+    if (grp >= 0) { mp = mus.param[e]; eact = __ldg(mus.act + grp); }
     bool ok = true;
     double d[NV][3];
     double dv[3];
@@ -136,6 +141,7 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
         for (int w = 0; w < NV; w++)
             if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
         ok = nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
+        if (grp >= 0) muscle_qp_row<HT, NV, HESS>(d, x, dv, V, mp, eact, project, g, blk);
     } else {
         const double V = hex_volume((const double(*)[3])X) * 0.125;
         for (int s = 0; s < 8; s++) {
@@ -144,9 +150,59 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
             for (int w = 0; w < NV; w++)
                 if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
             ok &= nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
+            if (grp >= 0) muscle_qp_row<HT, NV, HESS>(d, x, dv, V, mp, eact, project, g, blk);
         }
     }
     return ok;
+}
+
+// Energy of element e (element.h:40-58): volume x quadrature mean of the
+// Neo-Hookean density plus the fibre term where the element has one.
+template <int NV>
+__device__ __forceinline__ double elem_energy(const double* __restrict__ Xg, const double* __restrict__ qg,
+                                              const int* __restrict__ conn, const double2* __restrict__ mat,
+                                              const MuscleArgs& mus, int e, int material) {
+    double X[NV][3], x[NV][3];
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        const int n = __ldg(conn + (size_t)e * NV + w);
+#pragma unroll
+        for (int r = 0; r < 3; r++) { X[w][r] = __ldg(Xg + 3 * (size_t)n + r); x[w][r] = qg[3 * (size_t)n + r]; }
+    }
+    if (material == 1) {
+        double out = 0.0;
+#pragma unroll
+        for (int w = 0; w < NV; w++)
+#pragma unroll
+            for (int r = 0; r < 3; r++) out += x[w][r] * x[w][r] * (x[w][r] * x[w][r] - 0.5);
+        return out;
+    }
+    const double2 m = __ldg(mat + e);
+    const int grp = mus.group ? __ldg(mus.group + e) : -1;
+    double4 mp = make_double4(0.0, 0.0, 0.0, 0.0);
+    double eact = 0.0;
+    if (grp >= 0) { mp = mus.param[e]; eact = __ldg(mus.act + grp); }
+    double d[NV][3], F[9];
+    const int nqp = (NV == 4) ? 1 : 8;
+    const double V = (NV == 4) ? 0.0 : hex_volume((const double(*)[3])X);
+    double Vt = 0.0, acc = 0.0;
+    for (int s = 0; s < nqp; s++) {
+        if (NV == 4) Vt = tet_shape((const double(*)[3])X, (double(*)[3])d);
+        else hex_shape((const double(*)[3])X, s, (double(*)[3])d);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double t = 0.0;
+#pragma unroll
+                for (int w = 0; w < NV; w++) t += x[w][r] * d[w][c];
+                F[r * 3 + c] = t;
+            }
+        double qe = nh_qp_energy(F, m.x, m.y);
+        if (grp >= 0) qe += muscle_qp_energy(F, mp, eact);
+        acc += (NV == 4) ? qe : qe * 0.125;
+    }
+    return (NV == 4 ? Vt : V) * acc;
 }
 
 // ---------------------------------------------------------------------------
@@ -169,12 +225,12 @@ __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_a
             const int e = ev >> 3, v = ev & 7;
             HT blk[NV * 9];
             if (a.want_hess) {
-                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, e, v, a.material, a.project != 0, g, blk);
+                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, a.project != 0, g, blk);
                 HT* dst = stage + (size_t)k * NV * 9;
 #pragma unroll
                 for (int t = 0; t < NV * 9; t++) dst[t] = blk[t];
             } else {
-                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, e, v, a.material, false, g, blk);
+                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, false, g, blk);
             }
         }
         if (!ok) atomicOr(a.status, kFlagInverted);
@@ -239,13 +295,14 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
 // Element-level parity hook: thread per (element, local vertex).
 template <typename HT, int NV>
 __global__ void k_elem_rows(int E, const double* X, const double* q, const int* conn, const double2* mat,
-                            int material, int project, double* psi, double* grad, double* hess, int* status) {
+                            MuscleArgs mus, int material, int project, double* psi, double* grad, double* hess,
+                            int* status) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)E * NV) return;
     int e = (int)(t / NV), v = (int)(t - (long long)e * NV);
     double g[3] = {0.0, 0.0, 0.0};
     HT blk[NV * 9];
-    bool ok = elem_row<HT, NV, true>(X, q, conn, mat, e, v, material, project != 0, g, blk);
+    bool ok = elem_row<HT, NV, true>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk);
     if (!ok) atomicOr(status, kFlagInverted);
     const int n = 3 * NV;
     if (grad)
@@ -255,60 +312,23 @@ __global__ void k_elem_rows(int E, const double* X, const double* q, const int* 
             for (int k = 0; k < 3; k++)
                 for (int l = 0; l < 3; l++)
                     hess[(size_t)e * n * n + (size_t)(3 * v + k) * n + 3 * w + l] = (double)blk[w * 9 + k * 3 + l];
-    if (psi && v == 0) {
-        double Xl[NV][3], x[NV][3];
-        for (int w = 0; w < NV; w++) {
-            int nn = conn[(size_t)e * NV + w];
-            for (int r = 0; r < 3; r++) { Xl[w][r] = X[3 * (size_t)nn + r]; x[w][r] = q[3 * (size_t)nn + r]; }
-        }
-        double out = 0.0;
-        if (material == 1) {
-            for (int w = 0; w < NV; w++)
-                for (int r = 0; r < 3; r++) out += x[w][r] * x[w][r] * (x[w][r] * x[w][r] - 0.5);
-        } else {
-            double2 m = mat[e];
-            double d[NV][3], F[9];
-            if (NV == 4) {
-                double V = tet_shape((const double(*)[3])Xl, (double(*)[3])d);
-                for (int r = 0; r < 3; r++)
-                    for (int c = 0; c < 3; c++) {
-                        double acc = 0;
-                        for (int w = 0; w < NV; w++) acc += x[w][r] * d[w][c];
-                        F[r * 3 + c] = acc;
-                    }
-                out = V * nh_qp_energy(F, m.x, m.y);
-            } else {
-                double V = hex_volume((const double(*)[3])Xl);
-                double acc8 = 0.0;
-                for (int s = 0; s < 8; s++) {
-                    hex_shape((const double(*)[3])Xl, s, (double(*)[3])d);
-                    for (int r = 0; r < 3; r++)
-                        for (int c = 0; c < 3; c++) {
-                            double acc = 0;
-                            for (int w = 0; w < NV; w++) acc += x[w][r] * d[w][c];
-                            F[r * 3 + c] = acc;
-                        }
-                    acc8 += nh_qp_energy(F, m.x, m.y) * 0.125;
-                }
-                out = V * acc8;
-            }
-        }
-        psi[e] = out;
-    }
+    if (psi && v == 0) psi[e] = elem_energy<NV>(X, q, conn, mat, mus, e, material);
 }
 
 template <typename HT>
 void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                      int material, int project, double* psi, double* grad, double* hess, int* status,
+                      const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
                       cudaStream_t st) {
     long long n = (long long)E * nv;
     if (n == 0) return;
     int threads = 128;
     int blocks = (int)((n + threads - 1) / threads);
     if (nv == 4)
-        k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
+        k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, project, psi, grad, hess,
+                                                       status);
     else
-        k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, material, project, psi, grad, hess, status);
+        k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, project, psi, grad, hess,
+                                                       status);
     counted();
 }
 
@@ -319,68 +339,22 @@ template <int NV>
 __global__ void __launch_bounds__(kRedThreads) k_elem_energy(int E, const double* __restrict__ Xg,
                                                              const double* __restrict__ qg,
                                                              const int* __restrict__ conn,
-                                                             const double2* __restrict__ mat, int material,
-                                                             double* partials, DevScalars* sc) {
+                                                             const double2* __restrict__ mat, MuscleArgs mus,
+                                                             int material, double* partials, DevScalars* sc) {
     double acc[1] = {0.0};
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x) {
-        double X[NV][3], x[NV][3];
-#pragma unroll
-        for (int w = 0; w < NV; w++) {
-            int n = __ldg(conn + (size_t)e * NV + w);
-#pragma unroll
-            for (int r = 0; r < 3; r++) { X[w][r] = __ldg(Xg + 3 * (size_t)n + r); x[w][r] = qg[3 * (size_t)n + r]; }
-        }
-        if (material == 1) {
-#pragma unroll
-            for (int w = 0; w < NV; w++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) acc[0] += x[w][r] * x[w][r] * (x[w][r] * x[w][r] - 0.5);
-            continue;
-        }
-        double2 m = __ldg(mat + e);
-        double d[NV][3], F[9];
-        if (NV == 4) {
-            double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-#pragma unroll
-                for (int c = 0; c < 3; c++) {
-                    double s = 0;
-#pragma unroll
-                    for (int w = 0; w < NV; w++) s += x[w][r] * d[w][c];
-                    F[r * 3 + c] = s;
-                }
-            acc[0] += V * nh_qp_energy(F, m.x, m.y);
-        } else {
-            double V = hex_volume((const double(*)[3])X);
-            double a8 = 0.0;
-            for (int s = 0; s < 8; s++) {
-                hex_shape((const double(*)[3])X, s, (double(*)[3])d);
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-#pragma unroll
-                    for (int c = 0; c < 3; c++) {
-                        double t = 0;
-#pragma unroll
-                        for (int w = 0; w < NV; w++) t += x[w][r] * d[w][c];
-                        F[r * 3 + c] = t;
-                    }
-                a8 += nh_qp_energy(F, m.x, m.y) * 0.125;
-            }
-            acc[0] += V * a8;
-        }
-    }
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += gridDim.x * blockDim.x)
+        acc[0] += elem_energy<NV>(Xg, qg, conn, mat, mus, e, material);
     double tot[1];
     if (reduce_grid<1>(acc, partials, &sc->counters[0], tot) && threadIdx.x == 0) sc->e_elem = tot[0];
 }
 
 void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                        int material, double* partials, DevScalars* sc, cudaStream_t st) {
+                        const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st) {
     int blocks = red_grid(E);
     if (nv == 4)
-        k_elem_energy<4><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
+        k_elem_energy<4><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, mus, material, partials, sc);
     else
-        k_elem_energy<8><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, material, partials, sc);
+        k_elem_energy<8><<<blocks, kRedThreads, 0, st>>>(E, X, q, conn, mat, mus, material, partials, sc);
     counted();
 }
 
@@ -909,9 +883,11 @@ void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, c
 // ---------------------------------------------------------------------------
 template void launch_assemble<double>(const AsmArgs<double>&, int, cudaStream_t);
 template void launch_assemble<float>(const AsmArgs<float>&, int, cudaStream_t);
-template void launch_elem_rows<double>(int, int, const double*, const double*, const int*, const double2*, int, int,
+template void launch_elem_rows<double>(int, int, const double*, const double*, const int*, const double2*,
+                                       const MuscleArgs&, int, int,
                                        double*, double*, double*, int*, cudaStream_t);
-template void launch_elem_rows<float>(int, int, const double*, const double*, const int*, const double2*, int, int,
+template void launch_elem_rows<float>(int, int, const double*, const double*, const int*, const double2*,
+                                      const MuscleArgs&, int, int,
                                       double*, double*, double*, int*, cudaStream_t);
 template void launch_pressure_jac<double>(const PressureArgs&, const int*, const int*, const uint8_t*, double, double*,
                                           cudaStream_t);

@@ -38,6 +38,15 @@ struct DevScalars {
     unsigned counters[16];
 };
 
+// SoftCon fibre terms (cpp/src/energies/softconMuscle.cpp): per element a
+// muscle group (-1 = none) and (m_x, m_y, m_z, stiffness); activation per group.
+// group == nullptr means no element has a fibre term.
+struct MuscleArgs {
+    const int* group = nullptr;
+    const double4* param = nullptr;
+    const double* act = nullptr;
+};
+
 // Row-owner assembly arguments (tet or hex).
 template <typename HT>
 struct AsmArgs {
@@ -46,6 +55,7 @@ struct AsmArgs {
     const double* q;        // 3N current
     const int* conn;        // E*nv
     const double2* mat;     // (mu, lambda) per element
+    MuscleArgs mus;
     const int* pair_ptr;    // N+1
     const int* pair_ev;     // e*8 + v
     const int* row_ptr;     // N+1 (blocks)
@@ -88,10 +98,10 @@ template <typename HT>
 void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st);
 template <typename HT>
 void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                      int material, int project, double* psi, double* grad, double* hess, int* status,
+                      const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
                       cudaStream_t st);
 void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                        int material, double* partials, DevScalars* sc, cudaStream_t st);
+                        const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
 template <typename HT>
 void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,

@@ -139,15 +139,23 @@ class _EnergyBase:
         if len(elementEnergiesList) != ne or len(elementParameterList) != ne:
             raise ValueError("one energy set and one Params per element are required")
         rho = np.empty(ne); E = np.empty(ne); nu = np.empty(ne)
+        mgroup = mk = mdir = None
         material = None
         for i, (es, pr) in enumerate(zip(elementEnergiesList, elementParameterList)):
             es = set(es)
             for name in es:
                 if name not in _REF_ENERGIES:
                     raise RuntimeError(f"Unknown energy type: {name}")
-            if es - {"neohookean"}:
+            if es - {"neohookean", "softconMuscle"}:
                 raise NotImplementedError(
-                    f"element energies {sorted(es - {'neohookean'})} are not built on the GPU path")
+                    f"element energies {sorted(es - {'neohookean', 'softconMuscle'})} are not built on the GPU path")
+            if "softconMuscle" in es:
+                # tetrahedron.cpp:82-88 / hexahedron.cpp:51-57
+                if mgroup is None:
+                    mgroup = np.full(ne, -1, np.int32); mk = np.zeros(ne); mdir = np.zeros((ne, 3))
+                mgroup[i] = int(pr.get_value("muscleGroup")[0, 0])
+                mk[i] = float(pr.get_value("softconStiffness")[0, 0])
+                mdir[i] = np.asarray(pr.get_value("softconDirection"), dtype=np.float64).ravel()[:3]
             rho[i] = float(pr.get_value("density")[0, 0])
             if "neohookean" in es:
                 E[i] = float(pr.get_value("youngsModulus")[0, 0])
@@ -162,6 +170,8 @@ class _EnergyBase:
             # elements without energies only carry mass (Energy with empty sets)
             material = 0
         self._init_arrays(X, T, settings, gravAcceleration, dampingAlpha, rho, E, nu, material or 0)
+        if mgroup is not None:
+            self.set_muscles(mgroup, mk, mdir)
         self._setup_constraints_forces(constraintTypesList, constraintParameterList, forceTypesList,
                                        forceParameterList)
 
@@ -244,7 +254,7 @@ class _EnergyBase:
     @classmethod
     def from_arrays(cls, undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha=0.0, *, density,
                     youngsModulus, poissonsRatio, neumannBCmask=None, neumannBCvalue=None, forceTypesList=(),
-                    forceParameterList=None):
+                    forceParameterList=None, muscleGroup=None, softconStiffness=None, softconDirection=None):
         """Neo-Hookean mesh from per-element arrays instead of one Params per element.
 
         Same system as the reference-style constructor; meant for meshes with
@@ -252,6 +262,8 @@ class _EnergyBase:
         obj = cls.__new__(cls)
         obj._init_arrays(undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha, density,
                          youngsModulus, poissonsRatio)
+        if muscleGroup is not None:
+            obj.set_muscles(muscleGroup, softconStiffness, softconDirection)
         ctypes_, cp = [], Params()
         if neumannBCmask is not None:
             ctypes_ = ["neumannBC"]
@@ -259,6 +271,18 @@ class _EnergyBase:
             cp.set_param("neumannBCvalue", np.asarray(neumannBCvalue, dtype=np.float64).ravel())
         obj._setup_constraints_forces(ctypes_, cp, forceTypesList, forceParameterList)
         return obj
+
+    def set_muscles(self, muscleGroup, softconStiffness, softconDirection, n_groups=None):
+        """SoftCon fibre terms per element (group -1 = none); activations via act["softconMuscle"]."""
+        L = _lib.load()
+        g = np.ascontiguousarray(np.asarray(muscleGroup).ravel().astype(np.int32))
+        k = np.ascontiguousarray(np.broadcast_to(np.asarray(softconStiffness, np.float64), g.shape))
+        d = np.ascontiguousarray(np.broadcast_to(np.asarray(softconDirection, np.float64).reshape(-1, 3), (g.size, 3)))
+        if g.size != self.numElements:
+            raise ValueError("one muscle group per element is required")
+        self._n_mgroups = int(n_groups if n_groups is not None else max(int(g.max()) + 1, 1))
+        _lib.check(L.sors_set_muscles(self._h, _p(g, C.c_int32), _p(k, C.c_double), _p(d, C.c_double),
+                                      self._n_mgroups))
 
     def __del__(self):
         h = getattr(self, "_h", None)
@@ -277,6 +301,9 @@ class _EnergyBase:
         if "pressure" in self._forces and act.has("pressure"):
             p = np.ascontiguousarray(act.get_value("pressure").T.ravel())
             _lib.check(L.sors_set_actuation(self._h, b"pressure", _p(p, C.c_double), p.size))
+        if getattr(self, "_n_mgroups", 0) and act.has("softconMuscle"):
+            a = np.ascontiguousarray(np.asarray(act.get_value("softconMuscle"), np.float64).ravel())
+            _lib.check(L.sors_set_actuation(self._h, b"softconMuscle", _p(a, C.c_double), a.size))
         if "vertexForce" in self._forces and act.has("vertexForce"):
             v = np.ascontiguousarray(act.get_value("vertexForce").ravel())  # (N,3) row-major = transpose().reshaped()
             _lib.check(L.sors_set_actuation(self._h, b"vertexForce", _p(v, C.c_double), v.size))

@@ -8,7 +8,8 @@ from sors_b200 import meshes
 
 def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha=0.0, dt=1e-3,
               scheme="backward_euler", method="minimize_newton", precision="fp64", project=True,
-              clamp=True, res_tol=0.0, faces=None, groups=None, vertex_force=False, oracle_project=False):
+              clamp=True, res_tol=0.0, faces=None, groups=None, vertex_force=False, oracle_project=False,
+              muscles=None):
     """(gpu_energy, gpu_solver, oracle_system, X) on one mesh."""
     from oracle import oracle as orc
     from sors_b200 import py_sors as ps
@@ -29,6 +30,15 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     s.newtonResidualTol = res_tol
     energies = [{"neohookean"}] * ne
     params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [rhov[i], Ev[i], nuv[i]]) for i in range(ne)]
+    if muscles is not None:
+        # per-element "softconMuscle" energies with their Params (tetrahedron.cpp:82-88)
+        energies = list(energies)
+        for i in range(ne):
+            if muscles["group"][i] >= 0:
+                energies[i] = {"neohookean", "softconMuscle"}
+                params[i].set_param("muscleGroup", float(muscles["group"][i]))
+                params[i].set_param("softconStiffness", float(muscles["k"][i]))
+                params[i].set_param("softconDirection", np.asarray(muscles["dir"][i], float).reshape(1, 3))
     ctypes_, cparams = [], ps.Params()
     mask = val = None
     if clamp:
@@ -53,6 +63,8 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
         o.set_pressure(np.asarray(faces), np.asarray(groups))
     if vertex_force:
         o.set_vertex_force(True)
+    if muscles is not None:
+        o.set_muscles(muscles["group"], muscles["k"], muscles["dir"], int(max(muscles["group"])) + 1)
     return en, sol, o, s
 
 

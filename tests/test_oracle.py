@@ -203,3 +203,82 @@ def test_ldl_matches_dense_solve(oracle):
     x = b.copy()
     lib().orc_solve_with_hessian(s.h, _pd(q), 1e-3, None, _pd(x))
     np.testing.assert_allclose(x, np.linalg.solve(Hs, b), rtol=1e-9, atol=1e-12 * np.abs(x).max())
+
+
+# --- SoftCon fibre term (cpp/src/energies/softconMuscle.cpp) ----------------
+
+def _torch_muscle(X, x, k, m, act):
+    """Consistent fibre energy k/2 (|F m| - (1 - e))^2 x V, tet or hex."""
+    from oracle import oracle as orc
+    nv = X.shape[0]
+    xt = torch.tensor(x, dtype=torch.float64, requires_grad=True)
+    if nv == 4:
+        Dm = torch.tensor((X[:3] - X[3]).T)
+        Fs = [(xt[:3] - xt[3]).T @ torch.linalg.inv(Dm)]
+        V = abs(np.linalg.det(X[:3] - X[3])) / 6
+    else:
+        G, _, V = orc.hex_init(X)
+        Fs = [xt.T @ torch.tensor(G[s]) for s in range(8)]
+    mt = torch.tensor(m, dtype=torch.float64)
+    psi = 0
+    for F in Fs:
+        ll = torch.linalg.norm(F @ mt)
+        psi = psi + 0.5 * k * (ll - (1 - act)) ** 2 / len(Fs)
+    return psi * V, xt
+
+
+@pytest.mark.parametrize("nv", [4, 8])
+def test_muscle_consistent_vs_autograd(oracle, nv):
+    rng = np.random.default_rng(21 + nv)
+    if nv == 4:
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.01
+    else:
+        from sors_b200.meshes import hex_grid_elements, grid_nodes
+        X = grid_nodes(1, 1, 1, (0.01, 0.012, 0.009))[hex_grid_elements(1, 1, 1)[0]]
+    for trial in range(4):
+        x = X @ (np.eye(3) + rng.uniform(-0.2, 0.2, (3, 3))).T
+        m = rng.standard_normal(3); m /= np.linalg.norm(m)
+        k, act = 1e4 * (1 + trial), 0.3 * trial
+        psi_nh, g_nh, H_nh, _ = oracle.elem_eval(X, x, 1e5, 0.4)
+        psi, g, H, st = oracle.elem_eval_muscle(X, x, 1e5, 0.4, k, m, act, form=oracle.MUSCLE_CONSISTENT)
+        assert st == 0
+        tpsi, xt = _torch_muscle(X, x, k, m, act)
+        tg = torch.autograd.grad(tpsi, xt, create_graph=True)[0]
+        tH = torch.stack([torch.autograd.grad(tg.reshape(-1)[i], xt, retain_graph=True)[0].reshape(-1)
+                          for i in range(3 * nv)])
+        assert abs((psi - psi_nh) - tpsi.item()) <= 1e-10 * abs(tpsi.item()) + 1e-18
+        np.testing.assert_allclose(g - g_nh, tg.detach().numpy().ravel(), rtol=1e-9,
+                                   atol=1e-10 * np.abs(g - g_nh).max())
+        np.testing.assert_allclose(H - H_nh, tH.numpy(), rtol=1e-8, atol=1e-9 * np.abs(H - H_nh).max())
+
+
+def test_muscle_reference_forms(oracle):
+    # The reference's gradient is shared by both forms; its energy |l-(1-e)| and
+    # its Hessian differ from the consistent ones (the deviation this build records).
+    rng = np.random.default_rng(5)
+    X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.01
+    x = X @ (np.eye(3) + rng.uniform(-0.1, 0.1, (3, 3))).T
+    m = np.array([0.0, 0.0, 1.0])
+    a = oracle.elem_eval_muscle(X, x, 1e5, 0.4, 1e5, m, 0.4, form=oracle.MUSCLE_REFERENCE)
+    b = oracle.elem_eval_muscle(X, x, 1e5, 0.4, 1e5, m, 0.4, form=oracle.MUSCLE_CONSISTENT)
+    np.testing.assert_array_equal(a[1], b[1])
+    assert abs(a[0] - b[0]) > 1e-6 * abs(b[0])
+    assert np.abs(a[2] - b[2]).max() > 1e-6 * np.abs(b[2]).max()
+
+
+def test_softcon_contraction_oracle(oracle, golden):
+    # TestCube::test_softcon_muscle (cpp/src/_test.cpp:563-625), reference forms.
+    d = golden["test_cube"]
+    X = np.array(d["vertices"]); T = np.array(d["elements"])
+    ne = T.shape[0]
+    s = oracle.System(X, T, rho=1000.0, youngs=1e6, nu=0.4, grav=(0, 0, 0), scheme="backward_euler",
+                      method="minimize_newton", dt=d["dt"], substeps=1, nthreads=1)
+    s.set_muscles(np.array([0, 1] + [-1] * (ne - 2)), np.full(ne, 1e5), np.tile([0, 0, 1.0], (ne, 1)), 2,
+                  form=oracle.MUSCLE_REFERENCE)
+    q = X.ravel().copy()
+    for i in range(1, 10):
+        s.set_muscle_act(np.full(2, 2.0 * i / 10))
+        q, st = s.step(q)
+        assert st == 0
+    z = q.reshape(-1, 3)[:, 2]
+    assert z.max() - z.min() < X[:, 2].max() - X[:, 2].min()
