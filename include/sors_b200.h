@@ -111,6 +111,10 @@ int sors_enable_vertex_force(SorsHandle* h, int32_t enable);
 int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffness, const double* direction,
                      int32_t n_groups);
 
+/* Replaces every element's Young's modulus and Poisson ratio (E entries each),
+ * as constructing Energy<3,E> again with new Params would (mass unchanged). */
+int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson);
+
 /* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values),
  * "vertexForce" (3N values, row-major N x 3) or "softconMuscle" (one activation
  * per muscle group). */
@@ -147,6 +151,23 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
  * the settings.  q_in and q_out may alias. */
 int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps,
               SorsStepStats* stats);
+
+/* Adjoint of one backward-Euler step (no reference counterpart: SORS has no
+ * differentiation).  A step took the state (q_n, v_n) to q_next with this
+ * handle's materials and the activations set at the time; call this with the
+ * same activations set.  Given dL/dq_next (3N) it solves J^T lam = dL/dq_next,
+ * J the Jacobian of the step's residual at q_next (exact, unprojected; Neumann
+ * rows as identity), and writes (any output may be NULL):
+ *   dL/dq_n (3N), dL/dv_n (3N)  through the residual's old-state terms,
+ *   dL/dyoungs (E)               per element,
+ *   dL/dact (one per muscle group, "softconMuscle" activations),
+ *   dL/dneumann (3N)             the Neumann velocities, nonzero on fixed DOFs.
+ * Any dependence of the loss on v_next = (q_next - q_n)/dt is the caller's to
+ * add to dL/dq_next (and subtract from dL/dq_n).  Pressure loads and
+ * Crank-Nicolson steps return SORS_ERR_UNSUPPORTED.  dt = 0 takes settings.dt. */
+int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next, double* dL_dq_prev,
+                      double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
+                      SorsStepStats* stats);
 
 /* Same step on a device-resident FP64 solution vector (in place). */
 int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substeps,

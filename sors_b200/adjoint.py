@@ -1,0 +1,151 @@
+"""Differentiable rollouts: the adjoint of the implicit backward-Euler step.
+
+No reference counterpart: SORS has no differentiation.  A rollout runs T steps
+of `Solver.step` from (q0, v0) with per-element Young's moduli E and per-step
+SoftCon activations act[t] (one per muscle group), and returns the final
+positions.  Its gradient runs backwards through the steps: each step's
+implicit residual g(q_{t+1}; q_t, v_t, E, act_t) = 0 is differentiated by
+`sors_adjoint_step` (one transpose solve with the step's exact Hessian plus
+element-level derivatives on the GPU), chained through the state
+(q_{t+1}, v_{t+1} = (q_{t+1} - q_t) / dt).
+
+States are checkpointed every `checkpoint_every` steps during the forward pass;
+the backward pass recomputes each segment from its checkpoint (the GPU path is
+deterministic, so the recomputed states equal the forward ones bit for bit).
+
+`rollout(...)` is the torch entry point: a torch.autograd.Function whose inputs
+are float64 tensors E (E,) and act (T, G).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+def _p(a, ct=C.c_double):
+    return a.ctypes.data_as(C.POINTER(ct)) if a is not None else None
+
+
+class RolloutAdjoint:
+    """Forward rollout with checkpoints, and its adjoint, on one Energy/Solver pair."""
+
+    def __init__(self, energy, solver, steps: int, dt: float, q0=None, v0=None, poisson=None,
+                 checkpoint_every: int = 1):
+        self.en = energy
+        self.sol = solver
+        self.steps = int(steps)
+        self.dt = float(dt)
+        n = energy.ndof
+        self.q0 = np.ascontiguousarray(energy.undeformedVertices.ravel() if q0 is None else q0, dtype=np.float64)
+        self.v0 = np.zeros(n) if v0 is None else np.ascontiguousarray(v0, dtype=np.float64).ravel()
+        ne = energy.numElements
+        self.poisson = np.ascontiguousarray(np.broadcast_to(
+            np.asarray(0.45 if poisson is None else poisson, np.float64), (ne,)))
+        self.k = max(1, int(checkpoint_every))
+        self._ckpt = {}
+        self._E = None
+        self._act = None
+        self.last_pcg_iters = 0
+
+    # -- helpers --------------------------------------------------------------
+    def _set_material(self, E):
+        L = _lib.load()
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        _lib.check(L.sors_set_material(self.en._h, _p(E), _p(self.poisson)))
+
+    def _set_act(self, a):
+        if a is None or a.size == 0:
+            return
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        _lib.check(_lib.load().sors_set_actuation(self.en._h, b"softconMuscle", _p(a), a.size))
+
+    def _restore(self, q, v):
+        self.en.set_initial_deformation(q)
+        self.en.set_initial_velocity(v)
+
+    def _step(self, q, t):
+        self._set_act(None if self._act is None else self._act[t])
+        return self.sol.step(q, self.en, None, self.dt)
+
+    # -- forward ----------------------------------------------------------------
+    def forward(self, E, act=None):
+        """Runs the rollout; returns q_T.  E: (E,), act: (T, G) or None."""
+        self._E = np.array(E, dtype=np.float64)
+        self._act = None if act is None else np.array(act, dtype=np.float64).reshape(self.steps, -1)
+        self._set_material(self._E)
+        self._restore(self.q0, self.v0)
+        q = self.q0.copy()
+        v = self.v0.copy()
+        self._ckpt = {}
+        for t in range(self.steps):
+            if t % self.k == 0:
+                self._ckpt[t] = (q.copy(), v.copy())
+            qn = self._step(q, t)
+            v = (qn - q) / self.dt
+            q = qn
+        return q
+
+    # -- backward ---------------------------------------------------------------
+    def backward(self, dL_dqT, dL_dvT=None):
+        """Gradient of L(q_T, v_T): returns (dL/dE, dL/dact or None, dL/dq0, dL/dv0)."""
+        L = _lib.load()
+        n = self.en.ndof
+        ne = self.en.numElements
+        G = 0 if self._act is None else self._act.shape[1]
+        Qb = np.array(dL_dqT, dtype=np.float64).ravel().copy()
+        Vb = np.zeros(n) if dL_dvT is None else np.array(dL_dvT, dtype=np.float64).ravel().copy()
+        gE = np.zeros(ne)
+        gA = None if self._act is None else np.zeros_like(self._act)
+        dq = np.zeros(n); dv = np.zeros(n); dE = np.zeros(ne); dA = np.zeros(max(G, 1))
+        stats = _lib.SorsStepStats()
+        self.last_pcg_iters = 0
+        self._set_material(self._E)
+        starts = sorted(self._ckpt)
+        for s in reversed(starts):
+            e = min(s + self.k, self.steps)
+            q, v = self._ckpt[s]
+            self._restore(q, v)
+            qs = [q.copy()]
+            for t in range(s, e):
+                qs.append(self._step(qs[-1], t))
+            for t in range(e - 1, s - 1, -1):
+                self._set_act(None if self._act is None else self._act[t])
+                b = Qb + Vb / self.dt
+                _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b), _p(dq), _p(dv),
+                                               _p(dE), _p(dA) if G else None, None, C.byref(stats)))
+                self.last_pcg_iters += stats.pcg_iters
+                gE += dE
+                if G:
+                    gA[t] = dA[:G]
+                Qb = dq - Vb / self.dt
+                Vb = dv.copy()
+        return gE, gA, Qb, Vb
+
+
+def rollout(energy, solver, E, act, steps, dt, q0=None, v0=None, poisson=None, checkpoint_every=1):
+    """Differentiable final positions q_T (torch float64, shape (3N,)).
+
+    E: torch tensor (E,) of Young's moduli; act: torch tensor (T, G) of SoftCon
+    activations or None.  Gradients flow to E and act."""
+    import torch
+
+    runner = RolloutAdjoint(energy, solver, steps, dt, q0=q0, v0=v0, poisson=poisson,
+                            checkpoint_every=checkpoint_every)
+
+    class _Rollout(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, Et, At):
+            qT = runner.forward(Et.detach().cpu().numpy(), None if At is None else At.detach().cpu().numpy())
+            return torch.from_numpy(qT)
+
+        @staticmethod
+        def backward(ctx, gq):
+            gE, gA, _, _ = runner.backward(gq.detach().cpu().numpy())
+            return torch.from_numpy(gE), (None if gA is None else torch.from_numpy(gA))
+
+    out = _Rollout.apply(E, act)
+    out.runner = runner
+    return out

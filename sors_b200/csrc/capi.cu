@@ -98,6 +98,11 @@ struct SorsHandle {
     int *faces = nullptr, *face_group = nullptr, *surf_nodes = nullptr, *sface_ptr = nullptr, *sface_fl = nullptr;
     double* pressure_d = nullptr;
 
+    // host copies used by the adjoint
+    std::vector<double> youngs_h, poisson_h, mass_h;
+    std::vector<int> mgroup_h;
+    double *adj_l = nullptr, *adj_y = nullptr, *adj_e = nullptr;
+
     // SoftCon fibre terms
     int* mgroup = nullptr;
     double4* mparam = nullptr;
@@ -121,6 +126,22 @@ MuscleArgs muscles(const SorsHandle* h) {
 }
 size_t hsize(const SorsHandle* h) { return mixed(h) ? sizeof(float) : sizeof(double); }
 
+// Host<->device copies and fills go through the handle's stream: it is a
+// non-blocking stream, so legacy-stream operations would not be ordered with
+// its kernels.  They are complete when these return.
+cudaError_t h2d(SorsHandle* h, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, h->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+cudaError_t d2h(SorsHandle* h, void* dst, const void* src, size_t bytes) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, h->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+cudaError_t dzero(SorsHandle* h, void* dst, size_t bytes) {
+    cudaError_t e = cudaMemsetAsync(dst, 0, bytes, h->stream);
+    return e == cudaSuccess ? cudaStreamSynchronize(h->stream) : e;
+}
+
 int dalloc(SorsHandle* h, void** p, size_t bytes) {
     if (bytes == 0) bytes = 16;
     cudaError_t e = cudaMalloc(p, bytes);
@@ -143,7 +164,7 @@ template <typename T>
 int upload(SorsHandle* h, T** p, const T* src, size_t count) {
     int st = dalloc_t(h, p, count);
     if (st) return st;
-    if (count) CK(cudaMemcpy(*p, src, count * sizeof(T), cudaMemcpyHostToDevice));
+    if (count) CK(h2d(h, *p, src, count * sizeof(T)));
     return SORS_OK;
 }
 
@@ -304,8 +325,13 @@ int compute_external(SorsHandle* h) {
 }
 
 // Gradient (and Hessian when want_hess) at h->q.  Leaves gnorm2 in sc.
+// Assembly modes: the step's own (Neumann rows identity for "minimize_newton",
+// unmasked otherwise), Neumann rows identity regardless of the method, or the
+// unmasked system.
+enum AsmMode { kAsmStep = 0, kAsmMaskedIdentity = 1, kAsmFull = 2 };
+
 template <typename HT>
-int eval_system(SorsHandle* h, double dt, bool want_hess) {
+int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmStep) {
     int st = compute_external(h);
     if (st) return st;
     AsmArgs<HT> a;
@@ -314,8 +340,10 @@ int eval_system(SorsHandle* h, double dt, bool want_hess) {
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
     a.H = (HT*)h->H; a.g_int = h->g_int; a.status = h->status;
     a.stage_per_warp = h->max_pairs * h->nv * 9;
-    a.material = h->s.material; a.project = h->s.project_spd; a.apply_mask = 1;
-    a.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0;
+    a.material = h->s.material; a.project = h->s.project_spd;
+    a.apply_mask = mode == kAsmFull ? 0 : 1;
+    a.neumann_override = mode == kAsmFull ? 0
+                         : ((mode == kAsmMaskedIdentity || method(h) == 0) && h->has_neumann) ? 1 : 0;
     a.want_hess = want_hess ? 1 : 0;
     a.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0;
     a.inertia_coef = inertia_coef(h, dt);
@@ -407,6 +435,81 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters) {
     *iters = h->sc_host->it;
     if (h->sc_host->breakdown && h->sc_host->it == 0)
         return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
+    return SORS_OK;
+}
+
+// Adjoint of one backward-Euler step (see sors_adjoint_step).  The residual of
+// the step is g_f = grad Psi(q) - f + m (v - v_n)/dt - m grav + alpha m v on
+// free DOFs, v = (q - q_n)/dt, and g_m = q_m - q_n,m - dt val_m on Neumann DOFs
+// (energy.cpp:296-306).  Its Jacobian J = [[H_ff, H_fm], [0, I]], so J^T lam = b
+// splits into H_ff lam_f = b_f and lam_m = b_m - H_mf lam_f; then
+// dL/dtheta = -lam^T dg/dtheta for every input theta of the step.
+template <typename HT, typename VT>
+int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b, double* dq, double* dv,
+                 double* dE, double* dact, double* dneu, SorsStepStats* stats) {
+    const int n = h->ndof, N = h->N, E = h->E;
+    int st;
+    if (!h->adj_l) {
+        if ((st = dalloc_t(h, &h->adj_l, (size_t)n))) return st;
+        if ((st = dalloc_t(h, &h->adj_y, (size_t)n))) return st;
+        if ((st = dalloc_t(h, &h->adj_e, (size_t)2 * std::max(1, E)))) return st;
+    }
+    CK(h2d(h, h->q, q_next, sizeof(double) * n));
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    // the exact Jacobian: no SPD projection, Neumann rows as identity
+    struct ProjectionOff {
+        SorsHandle* h;
+        int saved;
+        explicit ProjectionOff(SorsHandle* hh) : h(hh), saved(hh->s.project_spd) { h->s.project_spd = 0; }
+        ~ProjectionOff() { h->s.project_spd = saved; }
+    } projection_off(h);
+    if ((st = eval_system<HT>(h, dt, true, kAsmMaskedIdentity))) return st;
+    auto fixed = [&](int i) { return h->has_neumann && ((h->mask_h[i / 3] >> (i % 3)) & 1u); };
+    std::vector<double> lam(n);
+    for (int i = 0; i < n; i++) lam[i] = fixed(i) ? 0.0 : -b[i];  // pcg_solve solves H x = -g
+    CK(h2d(h, h->g, lam.data(), sizeof(double) * n));
+    const double eta = mixed(h) ? 1e-6 : std::max(1e-12, 0.01 * h->s.pcg_rel_tol);
+    int pit = 0;
+    if ((st = pcg_solve<HT, VT>(h, eta, 0.0, &pit))) return st;
+    if (h->sc_host->status & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
+    if (stats) { stats->pcg_iters += pit; stats->residual_norm = sqrt(h->sc_host->rr); }
+    if (sizeof(VT) == sizeof(double)) {
+        CK(d2h(h, lam.data(), h->x, sizeof(double) * n));
+    } else {
+        std::vector<float> lf(n);
+        CK(d2h(h, lf.data(), h->x, sizeof(float) * n));
+        for (int i = 0; i < n; i++) lam[i] = lf[i];
+    }
+    CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
+    // element contractions with lam_hat (fixed DOFs zero: their residual rows do
+    // not depend on the material or the activations)
+    launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->adj_l, h->adj_e, h->stream);
+    std::vector<double> ge((size_t)2 * std::max(1, E));
+    CK(d2h(h, ge.data(), h->adj_e, sizeof(double) * 2 * (size_t)E));
+    if (h->has_neumann) {
+        if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
+        launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->adj_l, h->adj_y, h->stream);
+        std::vector<double> y(n);
+        CK(d2h(h, y.data(), h->adj_y, sizeof(double) * n));
+        for (int i = 0; i < n; i++)
+            if (fixed(i)) lam[i] = b[i] - y[i];
+    }
+    const double a = h->s.damping_alpha;
+    for (int i = 0; i < n; i++) {
+        const double m = h->mass_h[i / 3];
+        const bool f = fixed(i);
+        if (dq) dq[i] = f ? lam[i] : (dt != 0.0 ? lam[i] * (m / (dt * dt) + a * m / dt) : 0.0);
+        if (dv) dv[i] = f ? 0.0 : (dt != 0.0 ? lam[i] * m / dt : 0.0);
+        if (dneu) dneu[i] = f ? lam[i] * dt : 0.0;
+    }
+    if (dE)
+        for (int e = 0; e < E; e++) dE[e] = h->youngs_h[e] != 0.0 ? -ge[e] / h->youngs_h[e] : 0.0;
+    if (dact) {
+        for (int g = 0; g < h->n_mgroups; g++) dact[g] = 0.0;
+        if (!h->mgroup_h.empty())
+            for (int e = 0; e < E; e++)
+                if (h->mgroup_h[e] >= 0) dact[h->mgroup_h[e]] -= ge[(size_t)E + e];
+    }
     return SORS_OK;
 }
 
@@ -622,6 +725,9 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
         double m = density[e] * elem_volume(X, conn + (size_t)e * nv, nv);
         for (int v = 0; v < nv; v++) mass[conn[(size_t)e * nv + v]] += m / nv;
     }
+    h->youngs_h.assign(youngs, youngs + E);
+    h->poisson_h.assign(poisson, poisson + E);
+    h->mass_h = mass;
     if ((st = upload(h, &h->X, X, (size_t)3 * N))) return bail(st);
     if ((st = upload(h, &h->conn, conn, (size_t)E * nv))) return bail(st);
     if ((st = upload(h, &h->mat, mat.data(), (size_t)E))) return bail(st);
@@ -632,11 +738,11 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
                        &h->mval, &h->vforce, &h->q_save};
     for (double** p : vecs) {
         if ((st = dalloc_t(h, p, nd))) return bail(st);
-        CK(cudaMemset(*p, 0, nd * sizeof(double)));
+        CK(dzero(h, *p, nd * sizeof(double)));
     }
     // TimeIntegrator(settings, undeformed vertices): qPrev = X (integrator.h:155-161)
-    CK(cudaMemcpy(h->qPrev, X, nd * sizeof(double), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->q, X, nd * sizeof(double), cudaMemcpyHostToDevice));
+    CK(h2d(h, h->qPrev, X, nd * sizeof(double)));
+    CK(h2d(h, h->q, X, nd * sizeof(double)));
     h->mask_h.assign(N, 0);
     if ((st = upload(h, &h->node_mask, h->mask_h.data(), (size_t)N))) return bail(st);
     size_t hs = hsize(h);
@@ -645,11 +751,11 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     void** vv[] = {&h->x, &h->r, &h->z, &h->p0, &h->p1, &h->qv};
     for (void** p : vv) {
         if ((st = dalloc(h, p, nd * hs))) return bail(st);
-        CK(cudaMemset(*p, 0, nd * hs));
+        CK(dzero(h, *p, nd * hs));
     }
     if ((st = dalloc_t(h, &h->partials, (size_t)kRedBlocks * kMaxScalars))) return bail(st);
     if ((st = dalloc_t(h, &h->sc, 1))) return bail(st);
-    CK(cudaMemset(h->sc, 0, sizeof(DevScalars)));
+    CK(dzero(h, h->sc, sizeof(DevScalars)));
     h->status = &h->sc->status;
     if (cudaMallocHost((void**)&h->sc_host, sizeof(DevScalars)) != cudaSuccess)
         return bail(fail(SORS_ERR_OOM, "pinned allocation failed"));
@@ -683,8 +789,8 @@ int sors_set_neumann(SorsHandle* h, const int32_t* mask, const double* value) {
             if (mask[3 * i + k] == 1) m |= (uint8_t)(1u << k);
         h->mask_h[i] = m;
     }
-    CK(cudaMemcpy(h->node_mask, h->mask_h.data(), h->N, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->mval, value, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    CK(h2d(h, h->node_mask, h->mask_h.data(), h->N));
+    CK(h2d(h, h->mval, value, sizeof(double) * h->ndof));
     h->has_neumann = true;
     return SORS_OK;
 }
@@ -719,7 +825,7 @@ int sors_set_pressure_faces(SorsHandle* h, const int32_t* faces, int32_t n_faces
     if ((st = upload(h, &h->sface_ptr, ptr.data(), ptr.size()))) return st;
     if ((st = upload(h, &h->sface_fl, fl.data(), fl.size()))) return st;
     if ((st = dalloc_t(h, &h->pressure_d, (size_t)std::max(1, n_groups)))) return st;
-    CK(cudaMemset(h->pressure_d, 0, sizeof(double) * std::max(1, n_groups)));
+    CK(dzero(h, h->pressure_d, sizeof(double) * std::max(1, n_groups)));
     h->has_pressure = true;
     return SORS_OK;
 }
@@ -738,18 +844,18 @@ int sors_set_actuation(SorsHandle* h, const char* name, const double* values, in
     if (nm == "pressure") {
         if (!h->has_pressure) return SORS_OK;  // unused actuation entries are ignored
         if (n < h->n_groups) return fail(SORS_ERR_ARG, "pressure actuation has fewer entries than surface groups");
-        CK(cudaMemcpy(h->pressure_d, values, sizeof(double) * h->n_groups, cudaMemcpyHostToDevice));
+        CK(h2d(h, h->pressure_d, values, sizeof(double) * h->n_groups));
         return SORS_OK;
     }
     if (nm == "vertexForce") {
         if (n != h->ndof) return fail(SORS_ERR_ARG, "vertexForce actuation must have 3N entries");
-        CK(cudaMemcpy(h->vforce, values, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+        CK(h2d(h, h->vforce, values, sizeof(double) * h->ndof));
         return SORS_OK;
     }
     if (nm == "softconMuscle") {
         if (!h->mgroup) return SORS_OK;  // no element carries a fibre term
         if (n < h->n_mgroups) return fail(SORS_ERR_ARG, "softconMuscle actuation has fewer entries than muscle groups");
-        CK(cudaMemcpy(h->mact, values, sizeof(double) * h->n_mgroups, cudaMemcpyHostToDevice));
+        CK(h2d(h, h->mact, values, sizeof(double) * h->n_mgroups));
         return SORS_OK;
     }
     return SORS_OK;  // other Params keys are not used by this mesh's energies
@@ -773,12 +879,13 @@ int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffnes
     }
     if (n_groups > h->n_mgroups) {
         if ((st = dalloc_t(h, &h->mact, (size_t)n_groups))) return st;
-        CK(cudaMemset(h->mact, 0, sizeof(double) * n_groups));
+        CK(dzero(h, h->mact, sizeof(double) * n_groups));
     }
     h->n_mgroups = std::max(h->n_mgroups, (int)n_groups);
+    h->mgroup_h.assign(group, group + h->E);
     if (h->E) {
-        CK(cudaMemcpy(h->mgroup, group, sizeof(int) * h->E, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h->mparam, prm.data(), sizeof(double4) * h->E, cudaMemcpyHostToDevice));
+        CK(h2d(h, h->mgroup, group, sizeof(int) * h->E));
+        CK(h2d(h, h->mparam, prm.data(), sizeof(double4) * h->E));
     }
     return SORS_OK;
 }
@@ -787,7 +894,7 @@ int sors_set_initial_deformation(SorsHandle* h, const double* q) {
     if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpy(h->qPrev, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    CK(h2d(h, h->qPrev, q, sizeof(double) * h->ndof));
     return SORS_OK;
 }
 
@@ -795,7 +902,7 @@ int sors_set_initial_velocity(SorsHandle* h, const double* v) {
     if (!h || !v) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpy(h->vPrev, v, sizeof(double) * h->ndof, cudaMemcpyHostToDevice));
+    CK(h2d(h, h->vPrev, v, sizeof(double) * h->ndof));
     return SORS_OK;
 }
 
@@ -804,8 +911,8 @@ int sors_get_state(SorsHandle* h, double* q_prev, double* v_prev) {
     int st;
     if ((st = set_device(h))) return st;
     CK(cudaStreamSynchronize(h->stream));
-    if (q_prev) CK(cudaMemcpy(q_prev, h->qPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost));
-    if (v_prev) CK(cudaMemcpy(v_prev, h->vPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost));
+    if (q_prev) CK(d2h(h, q_prev, h->qPrev, sizeof(double) * h->ndof));
+    if (v_prev) CK(d2h(h, v_prev, h->vPrev, sizeof(double) * h->ndof));
     return SORS_OK;
 }
 
@@ -857,7 +964,7 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
     }
     memcpy(val, raw.data(), n * sizeof(double));
     int flag = 0;
-    CK(cudaMemcpy(&flag, h->status, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(d2h(h, &flag, h->status, sizeof(int)));
     if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
     return SORS_OK;
 }
@@ -881,15 +988,49 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
         launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                  h->status, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e == cudaSuccess && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * h->E, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && grad) e = cudaMemcpy(grad, dgrad, sizeof(double) * (size_t)h->E * n, cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess && hess) e = cudaMemcpy(hess, dhess, sizeof(double) * (size_t)h->E * n * n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && psi) e = d2h(h, psi, dpsi, sizeof(double) * h->E);
+    if (e == cudaSuccess && grad) e = d2h(h, grad, dgrad, sizeof(double) * (size_t)h->E * n);
+    if (e == cudaSuccess && hess) e = d2h(h, hess, dhess, sizeof(double) * (size_t)h->E * n * n);
     int flag = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&flag, h->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = d2h(h, &flag, h->status, sizeof(int));
     cleanup();
     if (e != cudaSuccess) return fail(SORS_ERR_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
     if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
     return SORS_OK;
+}
+
+int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson) {
+    if (!h || !youngs || !poisson) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    std::vector<double2> mat((size_t)std::max(1, h->E));
+    for (int e = 0; e < h->E; e++) {
+        const double Ey = youngs[e], nu = poisson[e];
+        mat[e].y = (Ey * nu) / ((1 + nu) * (1 - 2 * nu));
+        mat[e].x = Ey / (2 * (1 + nu));
+    }
+    h->youngs_h.assign(youngs, youngs + h->E);
+    h->poisson_h.assign(poisson, poisson + h->E);
+    if (h->E) CK(h2d(h, h->mat, mat.data(), sizeof(double2) * h->E));
+    return SORS_OK;
+}
+
+int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next, double* dL_dq_prev,
+                      double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
+                      SorsStepStats* stats) {
+    if (!h || !q_next || !dL_dq_next) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    if (dt == 0.0) dt = h->s.dt;
+    if (h->s.time_stepping != 0 && dt != 0.0)
+        return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for backward Euler steps");
+    if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
+    if (h->s.material != 0) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
+    if (stats) *stats = SorsStepStats{};
+    return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, dL_dq_prev, dL_dv_prev, dL_dyoungs,
+                                                 dL_dact, dL_dneumann, stats)
+                    : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, dL_dq_prev, dL_dv_prev, dL_dyoungs,
+                                                   dL_dact, dL_dneumann, stats);
 }
 
 int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps, SorsStepStats* stats) {

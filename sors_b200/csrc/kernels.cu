@@ -205,6 +205,83 @@ __device__ __forceinline__ double elem_energy(const double* __restrict__ Xg, con
     return (NV == 4 ? Vt : V) * acc;
 }
 
+// Per-element adjoint contractions for the parameter gradients of one step.
+// out[e]     = lam_e . g_e^NH: the Neo-Hookean element gradient is proportional
+//              to Young's modulus (mu and lambda are, neoHookean.cpp:10-11);
+// out[E + e] = lam_e . d g_e^fibre / d e: with g_v = wV k (1 - (1-e)/l) u s_v,
+//              d/de gives wV k u s_v / l.
+template <int NV>
+__global__ void k_adjoint_elem(int E, const double* __restrict__ Xg, const double* __restrict__ qg,
+                               const int* __restrict__ conn, const double2* __restrict__ mat, MuscleArgs mus,
+                               const double* __restrict__ lam, double* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    double X[NV][3], x[NV][3], L[NV][3];
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        const int n = __ldg(conn + (size_t)e * NV + w);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            X[w][r] = __ldg(Xg + 3 * (size_t)n + r);
+            x[w][r] = qg[3 * (size_t)n + r];
+            L[w][r] = lam[3 * (size_t)n + r];
+        }
+    }
+    const double2 m = __ldg(mat + e);
+    const int grp = mus.group ? __ldg(mus.group + e) : -1;
+    double4 mp = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (grp >= 0) mp = mus.param[e];
+    double d[NV][3];
+    const int nqp = (NV == 4) ? 1 : 8;
+    const double Vh = (NV == 4) ? 0.0 : hex_volume((const double(*)[3])X) * 0.125;
+    double acc_nh = 0.0, acc_mu = 0.0;
+    for (int s = 0; s < nqp; s++) {
+        double wV;
+        if (NV == 4) wV = tet_shape((const double(*)[3])X, (double(*)[3])d);
+        else { hex_shape((const double(*)[3])X, s, (double(*)[3])d); wV = Vh; }
+        double F[9], LD[9];
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                double t = 0.0, u = 0.0;
+#pragma unroll
+                for (int w = 0; w < NV; w++) { t += x[w][r] * d[w][c]; u += L[w][r] * d[w][c]; }
+                F[r * 3 + c] = t;
+                LD[r * 3 + c] = u;
+            }
+        double C[9];
+        cof3(F, C);
+        const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+        const double cc = (m.y * log(J) - m.x) / J;
+        double pd = 0.0;
+#pragma unroll
+        for (int k = 0; k < 9; k++) pd += (m.x * F[k] + cc * C[k]) * LD[k];
+        acc_nh += wV * pd;
+        if (grp >= 0) {
+            double u[3], ls[3];
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                u[r] = F[r * 3 + 0] * mp.x + F[r * 3 + 1] * mp.y + F[r * 3 + 2] * mp.z;
+                ls[r] = LD[r * 3 + 0] * mp.x + LD[r * 3 + 1] * mp.y + LD[r * 3 + 2] * mp.z;
+            }
+            const double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+            acc_mu += wV * mp.w * (u[0] * ls[0] + u[1] * ls[1] + u[2] * ls[2]) / l;
+        }
+    }
+    out[e] = acc_nh;
+    out[(size_t)E + e] = acc_mu;
+}
+
+void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                         const MuscleArgs& mus, const double* lam, double* out, cudaStream_t st) {
+    if (E == 0) return;
+    const int threads = 128, blocks = (E + threads - 1) / threads;
+    if (nv == 4) k_adjoint_elem<4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, lam, out);
+    else k_adjoint_elem<8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, lam, out);
+    counted();
+}
+
 // ---------------------------------------------------------------------------
 // Row-owner assembly of gradient rows and Hessian block-rows.
 // ---------------------------------------------------------------------------
@@ -860,9 +937,9 @@ __global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT
     if (row >= N) return;
     int b0 = row_ptr[row], nval = (row_ptr[row + 1] - b0) * 9;
     double a[3] = {0, 0, 0};
-    const int nb = row_ptr[row + 1] - b0;
+    // blocks are stored one after another, 3x3 row-major each
     for (int t = lane; t < nval; t += 32) {
-        int rc = t / nb, blk = t - rc * nb, r = rc / 3, c = rc - r * 3;
+        int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
         double pr = (double)H[(size_t)b0 * 9 + t] * x[3 * (size_t)col[b0 + blk] + c];
         a[0] += r == 0 ? pr : 0.0; a[1] += r == 1 ? pr : 0.0; a[2] += r == 2 ? pr : 0.0;
     }

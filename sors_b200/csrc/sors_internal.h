@@ -103,6 +103,8 @@ void launch_elem_rows(int E, int nv, const double* X, const double* q, const int
 void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
                         const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
+void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
+                         const MuscleArgs& mus, const double* lam, double* out, cudaStream_t st);
 template <typename HT>
 void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
                          double cscale, HT* H, cudaStream_t st);
