@@ -38,7 +38,7 @@ extern "C" {
 typedef struct SorsSettings {
     int32_t time_stepping;   /* 0 "backward_euler", 1 "crank_nicolson"           */
     int32_t solver_method;   /* 0 "minimize_newton", 1 "minimize_newton_linesearch",
-                                2 "minimize_frozenhessian"                        */
+                                2 "minimize_frozenhessian", 3 "minimize_SQP"      */
     double dt;               /* settings.dt, used when a call passes dt == 0      */
     int32_t substeps;        /* settings.substeps                                */
     int32_t cfl;             /* settings.CFLtimeSteppingFlag                     */
@@ -114,6 +114,27 @@ int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffnes
 /* Replaces every element's Young's modulus and Poisson ratio (E entries each),
  * as constructing Energy<3,E> again with new Params would (mass unchanged). */
 int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson);
+
+/* PlaneContact (cpp/src/constraints/planeContact.cpp, energy.cpp:69-84): planes
+ * given by a point and a normal (n_planes x 3 each, row-major) and the surface
+ * vertices that may touch them ("surfaceVerticesIdx").  Used by solver_method 3
+ * ("minimize_SQP"): a surface vertex whose signed distance to its closest plane
+ * is below 0.01 at the start of a step gets the constraint n . (x - p) >= 0. */
+int sors_set_plane_contact(SorsHandle* h, const double* points, const double* normals, int32_t n_planes,
+                           const int32_t* surface_vertices, int32_t n_surface);
+
+/* DiskContact (cpp/src/constraints/diskContact.cpp, energy.cpp:85-108): disks
+ * (centers, normals n_disks x 3, radii n_disks) and candidate surface vertices.
+ * The captured footprint stays frozen until all of it is 3 x 0.01 above its
+ * disk (diskContact.cpp:94-205).  Normals are normalised. */
+int sors_set_disk_contact(SorsHandle* h, const double* centers, const double* normals, const double* radii,
+                          int32_t n_disks, const int32_t* surface_vertices, int32_t n_surface);
+
+/* DiskContact::set_disk (cpp/py_sors.cpp:231-245): moves disk disk_idx. */
+int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const double* normal, double radius);
+
+/* Number of contact constraints active in the last SQP step. */
+int32_t sors_active_contacts(SorsHandle* h);
 
 /* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values),
  * "vertexForce" (3N values, row-major N x 3) or "softconMuscle" (one activation

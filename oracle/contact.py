@@ -1,0 +1,198 @@
+"""Oracle for the contact step (Solver::minimize_SQP with PlaneContact / DiskContact).
+
+TEST INFRASTRUCTURE ONLY: used by tests/ as the checker, never by the product.
+
+Restates, on top of the oracle's FP64 system (oracle.System with method
+"minimize_SQP": element terms on every DOF, no Neumann override,
+cpp/src/energy.cpp:275,:337):
+  - PlaneContact::update_active_constraints (cpp/src/constraints/planeContact.cpp:89-124)
+  - DiskContact::update_active_constraints  (cpp/src/constraints/diskContact.cpp:94-205)
+  - Energy::compute_constraint_bounds / compute_constraint_matrix_qp (cpp/src/energy.cpp:394-474):
+      Neumann rows  dx_i = -(x_i - qPrev_i - dt val_i)            (neumannBC.cpp:4-21)
+      contact rows  n . dx_v >= -n . (x_v - p)                      (planeContact.cpp:4-42)
+  - Solver::minimize_SQP (cpp/src/solver.cpp:109-197): x += dx until ||dx|| < 1e-9, at most 100 iterations.
+The reference solves each QP with OSQP (max_iter 250, eps 1e-3); OSQP is not in
+the container, so this oracle solves each QP exactly (primal-dual active set on
+the KKT system, SuperLU): parity with OSQP's own iterates is unpinned, the
+converged step is the KKT point both approximate.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+PLANE_CONSTRAINT_THRESHOLD = 0.01      # cpp/headers/common.h:29
+DISK_PLANAR_CONSTRAINT_THRESHOLD = 0.01  # common.h:33
+DISK_RADIAL_CONSTRAINT_THRESHOLD = 0.001  # common.h:35
+MAX_ITER = 100
+DX_TOL = 1e-9
+
+
+class PlaneContact:
+    def __init__(self, points, normals, surface):
+        self.p = np.asarray(points, float).reshape(-1, 3)
+        self.n = np.asarray(normals, float).reshape(-1, 3)
+        self.surf = np.asarray(surface, int).ravel()
+        self.mask = -np.ones(self.surf.size, int)
+
+    def update(self, x):
+        xs = x.reshape(-1, 3)[self.surf]
+        for i in range(self.surf.size):
+            best, idx = np.inf, -1
+            for k in range(self.p.shape[0]):
+                d = float(self.n[k] @ (xs[i] - self.p[k]))
+                if d < PLANE_CONSTRAINT_THRESHOLD and d < best:
+                    best, idx = d, k
+            self.mask[i] = idx
+
+    def rows(self):
+        return [(int(self.surf[i]), self.p[k], self.n[k]) for i, k in enumerate(self.mask) if k >= 0]
+
+
+class DiskContact:
+    def __init__(self, centers, normals, radii, surface):
+        self.c = np.asarray(centers, float).reshape(-1, 3).copy()
+        n = np.asarray(normals, float).reshape(-1, 3)
+        self.n = n / np.linalg.norm(n, axis=1, keepdims=True)
+        self.r = np.asarray(radii, float).ravel().copy()
+        self.surf = np.asarray(surface, int).ravel()
+        self.mask = -np.ones(self.surf.size, int)
+        self.frozen = False
+
+    def set_disk(self, center, normal, radius, idx=0):
+        self.c[idx] = center
+        self.n[idx] = np.asarray(normal, float) / np.linalg.norm(normal)
+        self.r[idx] = radius
+
+    def _pd(self, d, x):
+        return float(self.n[d] @ (x - self.c[d]))
+
+    def _rd(self, d, x):
+        v = x - self.c[d]
+        return float(np.linalg.norm(v - (self.n[d] @ v) * self.n[d]))
+
+    def update(self, x):
+        xs = x.reshape(-1, 3)[self.surf]
+        clear = 3.0 * DISK_PLANAR_CONSTRAINT_THRESHOLD
+        depth = 5.0 * DISK_PLANAR_CONSTRAINT_THRESHOLD
+        if self.frozen:
+            if all(self._pd(d, xs[i]) >= clear for i, d in enumerate(self.mask) if d >= 0):
+                self.frozen = False
+                self.mask[:] = -1
+            return
+        hit = np.zeros(self.c.shape[0], bool)
+        for i in range(self.surf.size):
+            for d in range(self.c.shape[0]):
+                if self._pd(d, xs[i]) >= DISK_PLANAR_CONSTRAINT_THRESHOLD:
+                    continue
+                if self._rd(d, xs[i]) > self.r[d] + DISK_RADIAL_CONSTRAINT_THRESHOLD:
+                    continue
+                hit[d] = True
+        self.mask[:] = -1
+        if not hit.any():
+            return
+        active = 0
+        for d in range(self.c.shape[0]):
+            if not hit[d]:
+                continue
+            for i in range(self.surf.size):
+                pd = self._pd(d, xs[i])
+                if pd > DISK_PLANAR_CONSTRAINT_THRESHOLD or pd < -depth:
+                    continue
+                if self._rd(d, xs[i]) > self.r[d] + DISK_RADIAL_CONSTRAINT_THRESHOLD:
+                    continue
+                if self.mask[i] == -1:
+                    self.mask[i] = d
+                    active += 1
+                elif abs(pd) < abs(self._pd(self.mask[i], xs[i])):
+                    self.mask[i] = d
+        if active:
+            self.frozen = True
+
+    def rows(self):
+        return [(int(self.surf[i]), self.c[d], self.n[d]) for i, d in enumerate(self.mask) if d >= 0]
+
+
+def solve_qp(H, g, Aeq, beq, Ain, bin_, max_iter=50):
+    """min 1/2 dx'H dx + g'dx s.t. Aeq dx = beq, Ain dx >= bin_ (exact, active set)."""
+    n = H.shape[0]
+    m = Ain.shape[0]
+    work = bin_ > 0.0
+    for _ in range(max_iter):
+        A = sp.vstack([Aeq, Ain[work]]).tocsr()
+        b = np.concatenate([beq, bin_[work]])
+        K = sp.bmat([[H, A.T], [A, None]]).tocsc()
+        z = spla.spsolve(K, np.concatenate([-g, b]))
+        dx = z[:n]
+        y = -z[n:]
+        mu = np.zeros(m)
+        mu[work] = y[Aeq.shape[0]:]
+        slack = Ain @ dx - bin_
+        scale_s = 1e-12 + 1e-9 * (np.abs(bin_).max() if m else 0.0)
+        scale_mu = 1e-14 + 1e-8 * (np.abs(mu).max() if m else 0.0)
+        add = (~work) & (slack < -scale_s)
+        drop = work & (mu < -scale_mu)
+        if not add.any() and not drop.any():
+            return dx, work, mu
+        work = (work | add) & ~drop
+    return dx, work, mu
+
+
+class SQPOracle:
+    """One rollout of Solver::step with minimize_SQP (backward Euler)."""
+
+    def __init__(self, system, planes=None, disks=None, neumann=None):
+        self.s = system
+        self.planes = planes
+        self.disks = disks
+        self.mask = None if neumann is None else np.asarray(neumann[0]).ravel().astype(bool)
+        self.val = None if neumann is None else np.asarray(neumann[1], float).ravel()
+        self.last_iters = 0
+        self.last_active = 0
+
+    def minimize(self, q, dt):
+        x = np.array(q, float).ravel().copy()
+        n = x.size
+        for c in (self.planes, self.disks):
+            if c is not None:
+                c.update(x)
+        rows = []
+        taken = set()
+        fixed_nodes = set() if self.mask is None else set(np.nonzero(self.mask.reshape(-1, 3).any(1))[0].tolist())
+        for c in (self.planes, self.disks):
+            if c is None:
+                continue
+            for v, p, nn in c.rows():
+                if v in taken or v in fixed_nodes:
+                    continue
+                taken.add(v)
+                rows.append((v, p, nn))
+        self.last_active = len(rows)
+        qPrev, _, _ = self.s.state()
+        eq = np.nonzero(self.mask)[0] if self.mask is not None else np.zeros(0, int)
+        Aeq = sp.csr_matrix((np.ones(eq.size), (np.arange(eq.size), eq)), shape=(eq.size, n))
+        ri, ci, vi = [], [], []
+        for r, (v, p, nn) in enumerate(rows):
+            for k in range(3):
+                ri.append(r); ci.append(3 * v + k); vi.append(nn[k])
+        Ain = sp.csr_matrix((vi, (ri, ci)), shape=(len(rows), n))
+        for it in range(MAX_ITER):
+            g = self.s.gradient(x, dt)
+            H, st = self.s.hessian_csr(x, dt)
+            assert st == 0, "inverted element"
+            beq = -(x[eq] - qPrev[eq] - dt * self.val[eq]) if eq.size else np.zeros(0)
+            bin_ = np.array([-(nn @ (x[3 * v:3 * v + 3] - p)) for v, p, nn in rows])
+            dx, _, _ = solve_qp(H, g, Aeq, beq, Ain, bin_)
+            x += dx
+            if np.isnan(dx).any():
+                raise RuntimeError("SQP method diverged")
+            if np.linalg.norm(dx) < DX_TOL:
+                self.last_iters = it + 1
+                return x
+        raise RuntimeError("SQP method did not converge")
+
+    def step(self, q, dt):
+        x = self.minimize(q, dt)
+        self.s.update_state(x, dt)
+        return x

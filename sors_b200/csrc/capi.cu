@@ -19,6 +19,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <limits>
 #include <vector>
 
 #include "../../include/sors_b200.h"
@@ -108,6 +109,29 @@ struct SorsHandle {
     double4* mparam = nullptr;
     double* mact = nullptr;
     int n_mgroups = 0;
+
+    // contact (planeContact / diskContact) and the SQP subproblem
+    struct Plane { double p[3], n[3]; };
+    struct Disk { double c[3], n[3], r; };
+    std::vector<Plane> planes;
+    std::vector<int> plane_surf, plane_mask;
+    std::vector<Disk> disks;
+    std::vector<int> disk_surf, disk_mask;
+    bool disk_frozen = false;
+    uint8_t* pflag_d = nullptr;
+    double4* pn_d = nullptr;
+    std::vector<uint8_t> pflag_h;
+    std::vector<double4> pn_h;
+    int* cnode_d = nullptr;
+    double4* cnb_d = nullptr;
+    double *cout_d = nullptr, *cpos_d = nullptr;
+    int c_cap = 0;
+    double *qp_x0 = nullptr, *qp_y = nullptr, *qp_g2 = nullptr, *qp_dx = nullptr;
+    int last_active = 0;
+    // projection used by the PCG kernels (null: none)
+    const uint8_t* proj_flag = nullptr;
+    const double4* proj_n = nullptr;
+    bool pcg_exec_proj = false;
 
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
@@ -380,17 +404,23 @@ void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
     launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
-    launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
-                          h->stream);
+    launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
+                          h->proj_n, h->partials, h->sc, h->stream);
     launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
-    launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->partials, h->sc,
-                          h->stream);
+    launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
+                          h->proj_n, h->partials, h->sc, h->stream);
 }
 
 template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
+    if (h->pcg_exec && h->pcg_exec_proj != (h->proj_flag != nullptr)) {
+        // the captured launches carry the projection pointers: capture again
+        cudaGraphExecDestroy(h->pcg_exec);
+        h->pcg_exec = nullptr;
+    }
     if (!h->pcg_exec && !h->graph_failed) {
+        h->pcg_exec_proj = h->proj_flag != nullptr;
         cudaGraph_t graph = nullptr;
         const long long launches_before = g_kernel_launches.load();
         cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
@@ -417,12 +447,15 @@ int pcg_chunk(SorsHandle* h) {
     return SORS_OK;
 }
 
-// Solves H dx = -g (dx in h->x).  Returns PCG iterations in *iters.
+// Solves H dx = -g (dx in h->x), g = h->g unless given.  With h->proj_flag set
+// the solve runs on the subspace the constraint projection leaves free.
+// Returns PCG iterations in *iters.
 template <typename HT, typename VT>
-int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters) {
+int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
-    launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, eta * eta,
-                            abs_tol * abs_tol, h->s.pcg_max_iter, h->partials, h->sc, h->stream);
+    launch_pcg_init<HT, VT>(h->N, g ? g : h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0,
+                            eta * eta, abs_tol * abs_tol, h->s.pcg_max_iter, h->proj_flag, h->proj_n, h->partials,
+                            h->sc, h->stream);
     CK(cudaGetLastError());
     int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
     for (int c = 0; c < maxchunks; c++) {
@@ -589,7 +622,224 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     return SORS_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Contact active sets (host), restating PlaneContact/DiskContact::
+// update_active_constraints (cpp/src/constraints/planeContact.cpp:89-124,
+// diskContact.cpp:94-205) with the thresholds of cpp/headers/common.h:29-35.
+// ---------------------------------------------------------------------------
+constexpr double kPlaneThreshold = 0.01;
+constexpr double kDiskPlaneThreshold = 0.01;
+constexpr double kDiskRadialThreshold = 0.001;
+
+void update_plane_contacts(SorsHandle* h, const double* q) {
+    h->plane_mask.assign(h->plane_surf.size(), -1);
+    for (size_t i = 0; i < h->plane_surf.size(); i++) {
+        const double* x = q + 3 * (size_t)h->plane_surf[i];
+        double best = std::numeric_limits<double>::max();
+        int idx = -1;
+        for (size_t k = 0; k < h->planes.size(); k++) {
+            const auto& P = h->planes[k];
+            const double d = P.n[0] * (x[0] - P.p[0]) + P.n[1] * (x[1] - P.p[1]) + P.n[2] * (x[2] - P.p[2]);
+            if (d < kPlaneThreshold && d < best) { best = d; idx = (int)k; }
+        }
+        h->plane_mask[i] = idx;
+    }
+}
+
+double disk_plane_dist(const SorsHandle::Disk& D, const double* x) {
+    return D.n[0] * (x[0] - D.c[0]) + D.n[1] * (x[1] - D.c[1]) + D.n[2] * (x[2] - D.c[2]);
+}
+double disk_radial_dist(const SorsHandle::Disk& D, const double* x) {
+    double v[3] = {x[0] - D.c[0], x[1] - D.c[1], x[2] - D.c[2]};
+    const double d = D.n[0] * v[0] + D.n[1] * v[1] + D.n[2] * v[2];
+    for (int k = 0; k < 3; k++) v[k] -= d * D.n[k];
+    return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+}
+
+void update_disk_contacts(SorsHandle* h, const double* q) {
+    const size_t ns = h->disk_surf.size();
+    if (h->disk_mask.size() != ns) h->disk_mask.assign(ns, -1);
+    const double clear = 3.0 * kDiskPlaneThreshold, depth = 5.0 * kDiskPlaneThreshold;
+    if (h->disk_frozen) {
+        // keep the captured footprint until every vertex of it is clearly above its disk
+        bool all_clear = true;
+        for (size_t i = 0; i < ns && all_clear; i++) {
+            const int d = h->disk_mask[i];
+            if (d < 0) continue;
+            if (disk_plane_dist(h->disks[d], q + 3 * (size_t)h->disk_surf[i]) < clear) all_clear = false;
+        }
+        if (all_clear) {
+            h->disk_frozen = false;
+            std::fill(h->disk_mask.begin(), h->disk_mask.end(), -1);
+        }
+        return;
+    }
+    std::vector<char> hit(h->disks.size(), 0);
+    bool any = false;
+    for (size_t i = 0; i < ns; i++) {
+        const double* x = q + 3 * (size_t)h->disk_surf[i];
+        for (size_t d = 0; d < h->disks.size(); d++) {
+            const auto& D = h->disks[d];
+            if (disk_plane_dist(D, x) >= kDiskPlaneThreshold) continue;
+            if (disk_radial_dist(D, x) > D.r + kDiskRadialThreshold) continue;
+            hit[d] = 1;
+            any = true;
+        }
+    }
+    std::fill(h->disk_mask.begin(), h->disk_mask.end(), -1);
+    if (!any) return;
+    int active = 0;
+    for (size_t d = 0; d < h->disks.size(); d++) {
+        if (!hit[d]) continue;
+        const auto& D = h->disks[d];
+        for (size_t i = 0; i < ns; i++) {
+            const double* x = q + 3 * (size_t)h->disk_surf[i];
+            const double pd = disk_plane_dist(D, x);
+            if (pd > kDiskPlaneThreshold || pd < -depth) continue;
+            if (disk_radial_dist(D, x) > D.r + kDiskRadialThreshold) continue;
+            int& slot = h->disk_mask[i];
+            if (slot == -1) { slot = (int)d; active++; }
+            else if (fabs(pd) < fabs(disk_plane_dist(h->disks[slot], x))) slot = (int)d;
+        }
+    }
+    if (active > 0) h->disk_frozen = true;
+}
+
+int ensure_sqp_buffers(SorsHandle* h, int m) {
+    int st;
+    const size_t n = (size_t)h->ndof;
+    if (!h->qp_x0) {
+        double** v[] = {&h->qp_x0, &h->qp_y, &h->qp_g2, &h->qp_dx};
+        for (double** p : v)
+            if ((st = dalloc_t(h, p, n))) return st;
+        if ((st = dalloc_t(h, &h->pflag_d, (size_t)h->N))) return st;
+        if ((st = dalloc_t(h, &h->pn_d, (size_t)h->N))) return st;
+        h->pn_h.assign(h->N, make_double4(0, 0, 0, 0));
+    }
+    if (m > h->c_cap) {
+        const int cap = std::max(m, 2 * h->c_cap);
+        if ((st = dalloc_t(h, &h->cnode_d, (size_t)cap))) return st;
+        if ((st = dalloc_t(h, &h->cnb_d, (size_t)cap))) return st;
+        if ((st = dalloc_t(h, &h->cout_d, (size_t)2 * cap))) return st;
+        if ((st = dalloc_t(h, &h->cpos_d, (size_t)3 * cap))) return st;
+        h->c_cap = cap;
+    }
+    return SORS_OK;
+}
+
+// Solver::minimize_SQP (solver.cpp:109-197): at each iteration the QP
+//   min 1/2 dx^T H dx + g^T dx  s.t.  dx_i = -(x_i - qPrev_i - dt val_i) (Neumann),
+//                                     n_c . dx_v >= -n_c . (x_v - p_c)   (contact)
+// is solved exactly by an active-set iteration: the working contacts are held
+// as equalities (PCG on the subspace the constraints leave free, from a
+// particular solution x0), violated contacts join, contacts with negative
+// multipliers leave; x += dx until ||dx|| < DX_TOL.  (The reference solves the
+// same QP with OSQP to its default 1e-3 tolerances.)
+template <typename HT, typename VT>
+int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
+    const int n = h->ndof, N = h->N;
+    int st;
+    CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
+    // active constraints from the initial guess (solver.cpp:122-123)
+    std::vector<double> qh(n);
+    CK(d2h(h, qh.data(), h->q, sizeof(double) * n));
+    if (!h->planes.empty()) update_plane_contacts(h, qh.data());
+    if (!h->disks.empty()) update_disk_contacts(h, qh.data());
+    std::vector<int> cnode;
+    std::vector<double> cpt, cn;  // point and normal per constraint
+    std::vector<char> taken(N, 0);
+    auto add = [&](int v, const double* p, const double* nrm) {
+        if (taken[v] || (h->has_neumann && h->mask_h[v])) return;  // one contact per node; Neumann nodes stay fixed
+        taken[v] = 1;
+        cnode.push_back(v);
+        cpt.insert(cpt.end(), p, p + 3);
+        cn.insert(cn.end(), nrm, nrm + 3);
+    };
+    for (size_t i = 0; i < h->plane_mask.size(); i++)
+        if (h->plane_mask[i] >= 0) add(h->plane_surf[i], h->planes[h->plane_mask[i]].p, h->planes[h->plane_mask[i]].n);
+    for (size_t i = 0; i < h->disk_mask.size(); i++)
+        if (h->disk_mask[i] >= 0) add(h->disk_surf[i], h->disks[h->disk_mask[i]].c, h->disks[h->disk_mask[i]].n);
+    const int m = (int)cnode.size();
+    h->last_active = m;
+    if ((st = ensure_sqp_buffers(h, m))) return st;
+    if (m) CK(h2d(h, h->cnode_d, cnode.data(), sizeof(int) * m));
+    std::vector<char> inW(m, 0);
+    std::vector<double> b(m), xc(3 * (size_t)m), chk(2 * (size_t)m);
+    std::vector<double4> cnb(m);
+    // projection: Neumann bits always; contact bits for the working set
+    h->pflag_h.assign(N, 0);
+    if (h->has_neumann)
+        for (int v = 0; v < N; v++) h->pflag_h[v] = h->mask_h[v] & 7u;
+    bool converged = false;
+    const double eta = mixed(h) ? std::max(h->s.pcg_rel_tol, 1e-6) : h->s.pcg_rel_tol;
+    for (int it = 0; it < h->s.newton_max_iter; it++) {
+        if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
+        launch_gather_nodes(m, h->cnode_d, h->q, h->cpos_d, h->stream);
+        if (m) CK(d2h(h, xc.data(), h->cpos_d, sizeof(double) * 3 * m));
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        if (h->sc_host->status & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
+        for (int c = 0; c < m; c++) {
+            const double* nn = &cn[3 * (size_t)c];
+            const double* pp = &cpt[3 * (size_t)c];
+            b[c] = -(nn[0] * (xc[3 * c] - pp[0]) + nn[1] * (xc[3 * c + 1] - pp[1]) + nn[2] * (xc[3 * c + 2] - pp[2]));
+            cnb[c] = make_double4(nn[0], nn[1], nn[2], b[c]);
+            if (it == 0) inW[c] = b[c] > 0.0;  // start with the constraints violated now
+        }
+        if (m) CK(h2d(h, h->cnb_d, cnb.data(), sizeof(double4) * m));
+        if (stats) { stats->newton_iters++; stats->residual_norm = sqrt(h->sc_host->gnorm2); }
+        for (int inner = 0; inner < 25; inner++) {
+            for (int c = 0; c < m; c++) {
+                const int v = cnode[c];
+                h->pflag_h[v] = (uint8_t)((h->pflag_h[v] & 7u) | (inW[c] ? 8u : 0u));
+                h->pn_h[v] = cnb[c];
+            }
+            CK(h2d(h, h->pflag_d, h->pflag_h.data(), (size_t)N));
+            if (m) CK(h2d(h, h->pn_d, h->pn_h.data(), sizeof(double4) * N));
+            launch_qp_x0(N, h->pflag_d, h->pn_d, h->q, h->qPrev, h->mval, dt, h->qp_x0, h->stream);
+            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->qp_x0, h->qp_y, h->stream);
+            launch_add_vec<double>(n, h->g, h->qp_y, h->qp_g2, h->stream);
+            h->proj_flag = h->pflag_d;
+            h->proj_n = h->pn_d;
+            int pit = 0;
+            st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
+            h->proj_flag = nullptr;
+            h->proj_n = nullptr;
+            if (st) return st;
+            if (stats) stats->pcg_iters += pit;
+            launch_add_vec<VT>(n, h->qp_x0, (const VT*)h->x, h->qp_dx, h->stream);
+            if (m == 0) break;
+            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->qp_dx, h->qp_y, h->stream);
+            launch_qp_check(m, h->cnode_d, h->cnb_d, h->qp_dx, h->qp_y, h->g, h->cout_d, h->stream);
+            CK(d2h(h, chk.data(), h->cout_d, sizeof(double) * 2 * m));
+            double mu_scale = 0.0, b_scale = 0.0;
+            for (int c = 0; c < m; c++) {
+                mu_scale = std::max(mu_scale, fabs(chk[m + c]));
+                b_scale = std::max(b_scale, fabs(b[c]));
+            }
+            const double tol_s = 1e-12 + 1e-9 * b_scale, tol_mu = 1e-14 + 1e-8 * mu_scale;
+            bool changed = false;
+            for (int c = 0; c < m; c++) {
+                if (!inW[c] && chk[c] < -tol_s) { inW[c] = 1; changed = true; }
+                else if (inW[c] && chk[m + c] < -tol_mu) { inW[c] = 0; changed = true; }
+            }
+            if (!changed) break;
+        }
+        CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+        launch_newton_update<double>(n, h->qp_dx, 1.0, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        const double dxn = sqrt(h->sc_host->dxnorm2);
+        if (stats) stats->dx_norm = dxn;
+        if (!(dxn == dxn)) break;  // "SQP method diverged"
+        if (dxn < h->s.newton_dx_tol) { converged = true; break; }
+    }
+    if (!converged) return fail(SORS_ERR_NOT_CONVERGED, "SQP method did not converge");
+    return SORS_OK;
+}
+
 int run_minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
+    if (method(h) == 3) return mixed(h) ? minimize_sqp<float, float>(h, dt, stats) : minimize_sqp<double, double>(h, dt, stats);
     if (mixed(h)) return minimize<float, float>(h, dt, stats);
     return minimize<double, double>(h, dt, stats);
 }
@@ -632,7 +882,7 @@ int step_resident(SorsHandle* h, double dt, int substeps, SorsStepStats* stats) 
     if (stats) memset(stats, 0, sizeof(*stats));
     for (int j = 0; j < substeps; j++) {
         int st;
-        if (h->s.newton_predictor && dts != 0.0) {
+        if (h->s.newton_predictor && dts != 0.0 && method(h) != 3) {
             CK(cudaMemcpyAsync(h->q_save, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
             launch_predict(h->ndof, h->q, h->vPrev, dts, h->stream);
             st = run_minimize(h, dts, stats);
@@ -999,6 +1249,60 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
     return SORS_OK;
 }
 
+int sors_set_plane_contact(SorsHandle* h, const double* points, const double* normals, int32_t n_planes,
+                           const int32_t* surface_vertices, int32_t n_surface) {
+    if (!h || (n_planes > 0 && (!points || !normals)) || (n_surface > 0 && !surface_vertices))
+        return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_planes < 0 || n_surface < 0) return fail(SORS_ERR_ARG, "negative count");
+    h->planes.clear();
+    for (int k = 0; k < n_planes; k++) {
+        SorsHandle::Plane P;
+        for (int c = 0; c < 3; c++) { P.p[c] = points[3 * k + c]; P.n[c] = normals[3 * k + c]; }
+        h->planes.push_back(P);
+    }
+    for (int i = 0; i < n_surface; i++)
+        if (surface_vertices[i] < 0 || surface_vertices[i] >= h->N) return fail(SORS_ERR_ARG, "surface vertex out of range");
+    h->plane_surf.assign(surface_vertices, surface_vertices + n_surface);
+    h->plane_mask.assign(n_surface, -1);
+    return SORS_OK;
+}
+
+int sors_set_disk_contact(SorsHandle* h, const double* centers, const double* normals, const double* radii,
+                          int32_t n_disks, const int32_t* surface_vertices, int32_t n_surface) {
+    if (!h || (n_disks > 0 && (!centers || !normals || !radii)) || (n_surface > 0 && !surface_vertices))
+        return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_disks < 0 || n_surface < 0) return fail(SORS_ERR_ARG, "negative count");
+    h->disks.clear();
+    for (int k = 0; k < n_disks; k++) {
+        SorsHandle::Disk D;
+        double nn = sqrt(normals[3 * k] * normals[3 * k] + normals[3 * k + 1] * normals[3 * k + 1] +
+                         normals[3 * k + 2] * normals[3 * k + 2]);
+        if (!(nn > 0)) return fail(SORS_ERR_ARG, "zero disk normal");
+        for (int c = 0; c < 3; c++) { D.c[c] = centers[3 * k + c]; D.n[c] = normals[3 * k + c] / nn; }
+        D.r = radii[k];
+        h->disks.push_back(D);
+    }
+    for (int i = 0; i < n_surface; i++)
+        if (surface_vertices[i] < 0 || surface_vertices[i] >= h->N) return fail(SORS_ERR_ARG, "surface vertex out of range");
+    h->disk_surf.assign(surface_vertices, surface_vertices + n_surface);
+    h->disk_mask.assign(n_surface, -1);
+    h->disk_frozen = false;
+    return SORS_OK;
+}
+
+int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const double* normal, double radius) {
+    if (!h || !center || !normal) return fail(SORS_ERR_ARG, "NULL argument");
+    if (disk_idx < 0 || disk_idx >= (int)h->disks.size()) return fail(SORS_ERR_ARG, "diskIdx out of range in set_disk()");
+    auto& D = h->disks[disk_idx];
+    double nn = sqrt(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+    if (!(nn > 0)) return fail(SORS_ERR_ARG, "zero disk normal");
+    for (int c = 0; c < 3; c++) { D.c[c] = center[c]; D.n[c] = normal[c] / nn; }
+    D.r = radius;
+    return SORS_OK;
+}
+
+int32_t sors_active_contacts(SorsHandle* h) { return h ? h->last_active : 0; }
+
 int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson) {
     if (!h || !youngs || !poisson) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
@@ -1116,7 +1420,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     // PCG kernels on the assembled system
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,
-                            1 << 30, h->partials, h->sc, h->stream);
+                            1 << 30, nullptr, nullptr, h->partials, h->sc, h->stream);
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
@@ -1132,7 +1436,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
         launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z,
-                              h->partials, h->sc, h->stream);
+                              nullptr, nullptr, h->partials, h->sc, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&ms, a, b));

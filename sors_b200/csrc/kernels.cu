@@ -688,24 +688,51 @@ void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const 
 // ---------------------------------------------------------------------------
 // PCG (block-Jacobi preconditioned CG), FP64 dots
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Constraint projection for the SQP subproblems: per node a flag byte (bits
+// 0-2: DOF held by a Neumann equality, bit 3: contact normal held) and the
+// contact normal in pn[i].xyz.  Projects a 3-vector onto the free subspace.
+// ---------------------------------------------------------------------------
+template <typename VT>
+__device__ __forceinline__ void project3(const uint8_t* __restrict__ pflag, const double4* __restrict__ pn, int i,
+                                         VT (&y)[3]) {
+    if (!pflag) return;
+    const unsigned f = __ldg(pflag + i);
+    if (!f) return;
+    if (f & 1u) y[0] = VT(0);
+    if (f & 2u) y[1] = VT(0);
+    if (f & 4u) y[2] = VT(0);
+    if (f & 8u) {
+        const double4 n = pn[i];
+        const VT d = (VT)n.x * y[0] + (VT)n.y * y[1] + (VT)n.z * y[2];
+        y[0] -= d * (VT)n.x;
+        y[1] -= d * (VT)n.y;
+        y[2] -= d * (VT)n.z;
+    }
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r,
                                                            VT* z, VT* p0, double eta2, double abs_tol2, int maxit,
+                                                           const uint8_t* pflag, const double4* pn,
                                                            double* partials, DevScalars* sc) {
     double acc[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
         VT rr[3];
         for (int k = 0; k < 3; k++) {
             rr[k] = (VT)(-g[3 * (size_t)i + k]);
-            r[3 * (size_t)i + k] = rr[k];
             x[3 * (size_t)i + k] = VT(0);
             p0[3 * (size_t)i + k] = VT(0);
         }
+        project3<VT>(pflag, pn, i, rr);
+        for (int k = 0; k < 3; k++) r[3 * (size_t)i + k] = rr[k];
         const VT* M = Minv + (size_t)i * 9;
+        VT zz[3];
+        for (int k = 0; k < 3; k++) zz[k] = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
+        project3<VT>(pflag, pn, i, zz);
         for (int k = 0; k < 3; k++) {
-            VT zk = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
-            z[3 * (size_t)i + k] = zk;
-            acc[0] += (double)rr[k] * (double)zk;
+            z[3 * (size_t)i + k] = zz[k];
+            acc[0] += (double)rr[k] * (double)zz[k];
             acc[1] += (double)rr[k] * (double)rr[k];
         }
     }
@@ -728,9 +755,10 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_init(int N, const double* g
 
 template <typename HT, typename VT>
 void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
-                     double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st) {
-    k_pcg_init<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, Minv, x, r, z, p0, eta2, abs_tol2, maxit,
-                                                           partials, sc);
+                     double abs_tol2, int maxit, const uint8_t* pflag, const double4* pn, double* partials,
+                     DevScalars* sc, cudaStream_t st) {
+    k_pcg_init<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, Minv, x, r, z, p0, eta2, abs_tol2, maxit, pflag,
+                                                           pn, partials, sc);
     counted();
 }
 
@@ -822,25 +850,36 @@ template <typename VT>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int N, const VT* __restrict__ p, const VT* __restrict__ qv,
                                                              const VT* __restrict__ Minv, VT* __restrict__ x,
                                                              VT* __restrict__ r, VT* __restrict__ z,
-                                                             double* partials, DevScalars* sc) {
+                                                             const uint8_t* __restrict__ pflag,
+                                                             const double4* __restrict__ pn, double* partials,
+                                                             DevScalars* sc) {
     if (*(volatile int*)&sc->done) return;
     const VT alpha = (VT)sc->alpha;
     double acc[2] = {0.0, 0.0};
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        VT rr[3];
+        VT rr[3], qq[3];
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const size_t ii = 3 * (size_t)i + k;
             x[ii] += alpha * p[ii];
-            rr[k] = r[ii] - alpha * qv[ii];
+            qq[k] = qv[ii];
+        }
+        project3<VT>(pflag, pn, i, qq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t ii = 3 * (size_t)i + k;
+            rr[k] = r[ii] - alpha * qq[k];
             r[ii] = rr[k];
         }
         const VT* M = Minv + (size_t)i * 9;
+        VT zz[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) zz[k] = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
+        project3<VT>(pflag, pn, i, zz);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
-            VT zk = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
-            z[3 * (size_t)i + k] = zk;
-            acc[0] += (double)rr[k] * (double)zk;
+            z[3 * (size_t)i + k] = zz[k];
+            acc[0] += (double)rr[k] * (double)zz[k];
             acc[1] += (double)rr[k] * (double)rr[k];
         }
     }
@@ -855,9 +894,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int N, const VT* __r
 }
 
 template <typename VT>
-void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
-                       DevScalars* sc, cudaStream_t st) {
-    k_pcg_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, Minv, x, r, z, partials, sc);
+void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, const uint8_t* pflag,
+                       const double4* pn, double* partials, DevScalars* sc, cudaStream_t st) {
+    k_pcg_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, Minv, x, r, z, pflag, pn, partials, sc);
     counted();
 }
 
@@ -956,6 +995,88 @@ void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, c
 }
 
 // ---------------------------------------------------------------------------
+// SQP subproblem helpers (minimize_SQP)
+// ---------------------------------------------------------------------------
+// Particular solution of the working constraints: Neumann DOFs move to their
+// prescribed position, dx_i = -(q_i - qPrev_i - dt val_i) (neumannBC.cpp:4-21),
+// contact nodes move by b along their normal (pn.w = b); zero elsewhere.
+__global__ void k_qp_x0(int N, const uint8_t* __restrict__ pflag, const double4* __restrict__ pn,
+                        const double* __restrict__ q, const double* __restrict__ qPrev,
+                        const double* __restrict__ mval, double dt, double* __restrict__ x0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const unsigned f = pflag[i];
+    double x[3] = {0.0, 0.0, 0.0};
+    if (f & 8u) {
+        const double4 n = pn[i];
+        x[0] = n.w * n.x; x[1] = n.w * n.y; x[2] = n.w * n.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        if ((f >> k) & 1u) {
+            const size_t ii = 3 * (size_t)i + k;
+            x[k] = -(q[ii] - qPrev[ii] - dt * mval[ii]);
+        }
+#pragma unroll
+    for (int k = 0; k < 3; k++) x0[3 * (size_t)i + k] = x[k];
+}
+
+// out = a + b (b of the PCG vector type)
+template <typename VT>
+__global__ void k_add_vec(int n, const double* __restrict__ a, const VT* __restrict__ b, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = a[i] + (double)b[i];
+}
+
+// Per contact constraint c at node v with normal n and bound b:
+// slack = n.dx_v - b (>= 0 when satisfied), mu = n.(H dx + g)_v (the multiplier
+// when the constraint is held).  cnb[c] = (n, b).
+__global__ void k_qp_check(int m, const int* __restrict__ cnode, const double4* __restrict__ cnb,
+                           const double* __restrict__ dx, const double* __restrict__ y, const double* __restrict__ g,
+                           double* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= m) return;
+    const int v = cnode[c];
+    const double4 n = cnb[c];
+    const size_t b = 3 * (size_t)v;
+    out[c] = n.x * dx[b] + n.y * dx[b + 1] + n.z * dx[b + 2] - n.w;
+    out[(size_t)m + c] = n.x * (y[b] + g[b]) + n.y * (y[b + 1] + g[b + 1]) + n.z * (y[b + 2] + g[b + 2]);
+}
+
+// out[3c + k] = q[3 node_c + k]
+__global__ void k_gather_nodes(int m, const int* __restrict__ node, const double* __restrict__ q,
+                               double* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 3 * m) return;
+    const int c = t / 3, k = t - 3 * c;
+    out[t] = q[3 * (size_t)node[c] + k];
+}
+
+void launch_qp_x0(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
+                  const double* mval, double dt, double* x0, cudaStream_t st) {
+    k_qp_x0<<<(N + 255) / 256, 256, 0, st>>>(N, pflag, pn, q, qPrev, mval, dt, x0);
+    counted();
+}
+template <typename VT>
+void launch_add_vec(int n, const double* a, const VT* b, double* out, cudaStream_t st) {
+    k_add_vec<VT><<<(n + 255) / 256, 256, 0, st>>>(n, a, b, out);
+    counted();
+}
+void launch_qp_check(int m, const int* cnode, const double4* cnb, const double* dx, const double* y,
+                     const double* g, double* out, cudaStream_t st) {
+    if (m == 0) return;
+    k_qp_check<<<(m + 127) / 128, 128, 0, st>>>(m, cnode, cnb, dx, y, g, out);
+    counted();
+}
+void launch_gather_nodes(int m, const int* node, const double* q, double* out, cudaStream_t st) {
+    if (m == 0) return;
+    k_gather_nodes<<<(3 * m + 255) / 256, 256, 0, st>>>(m, node, q, out);
+    counted();
+}
+template void launch_add_vec<double>(int, const double*, const double*, double*, cudaStream_t);
+template void launch_add_vec<float>(int, const double*, const float*, double*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
 // explicit instantiations
 // ---------------------------------------------------------------------------
 template void launch_assemble<double>(const AsmArgs<double>&, int, cudaStream_t);
@@ -973,17 +1094,19 @@ template void launch_pressure_jac<float>(const PressureArgs&, const int*, const 
 template void launch_block_jacobi<double, double>(int, const int*, const int*, const double*, double*, cudaStream_t);
 template void launch_block_jacobi<float, float>(int, const int*, const int*, const float*, float*, cudaStream_t);
 template void launch_pcg_init<double, double>(int, const double*, const double*, double*, double*, double*, double*,
-                                              double, double, int, double*, DevScalars*, cudaStream_t);
+                                              double, double, int, const uint8_t*, const double4*, double*,
+                                              DevScalars*, cudaStream_t);
 template void launch_pcg_init<float, float>(int, const double*, const float*, float*, float*, float*, float*, double,
-                                            double, int, double*, DevScalars*, cudaStream_t);
+                                            double, int, const uint8_t*, const double4*, double*, DevScalars*,
+                                            cudaStream_t);
 template void launch_pcg_spmv<double, double>(int, int, const int*, const int*, const double*, const double*,
                                               const double*, double*, double*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_spmv<float, float>(int, int, const int*, const int*, const float*, const float*, const float*,
                                             float*, float*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_update<double>(int, const double*, const double*, const double*, double*, double*, double*,
-                                        double*, DevScalars*, cudaStream_t);
-template void launch_pcg_update<float>(int, const float*, const float*, const float*, float*, float*, float*, double*,
-                                       DevScalars*, cudaStream_t);
+                                        const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_update<float>(int, const float*, const float*, const float*, float*, float*, float*,
+                                       const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_newton_update<double>(int, const double*, double, double*, const double*, double*, DevScalars*,
                                            int, cudaStream_t);
 template void launch_newton_update<float>(int, const float*, double, double*, const double*, double*, DevScalars*, int,

@@ -120,13 +120,21 @@ template <typename HT, typename VT>
 void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st);
 template <typename HT, typename VT>
 void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
-                     double abs_tol2, int maxit, double* partials, DevScalars* sc, cudaStream_t st);
+                     double abs_tol2, int maxit, const uint8_t* pflag, const double4* pn, double* partials,
+                     DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
 void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, const VT* z,
                      const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
 template <typename VT>
-void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, double* partials,
-                       DevScalars* sc, cudaStream_t st);
+void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, const uint8_t* pflag,
+                       const double4* pn, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_qp_x0(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
+                  const double* mval, double dt, double* x0, cudaStream_t st);
+template <typename VT>
+void launch_add_vec(int n, const double* a, const VT* b, double* out, cudaStream_t st);
+void launch_qp_check(int m, const int* cnode, const double4* cnb, const double* dx, const double* y,
+                     const double* g, double* out, cudaStream_t st);
+void launch_gather_nodes(int m, const int* node, const double* q, double* out, cudaStream_t st);
 template <typename VT>
 void launch_newton_update(int n, const VT* dx, double alpha, double* q, const double* q0, double* partials,
                           DevScalars* sc, int counter, cudaStream_t st);

@@ -28,8 +28,8 @@ from . import _lib
 from . import meshes as _meshes
 
 _SCHEMES = {"backward_euler": 0, "crank_nicolson": 1}
-_METHODS = {"minimize_newton": 0, "minimize_newton_linesearch": 1, "minimize_frozenhessian": 2}
-_REF_ONLY_METHODS = {"minimize_SQP"}
+_METHODS = {"minimize_newton": 0, "minimize_newton_linesearch": 1, "minimize_frozenhessian": 2, "minimize_SQP": 3}
+_REF_ONLY_METHODS = set()
 _REF_ENERGIES = {"neohookean", "stableneohookean", "pseudostrain", "softconMuscle"}
 _REF_CONSTRAINTS = {"neumannBC", "planeContact", "diskContact", "maxDistance"}
 _REF_FORCES = {"pressure", "vertexForce"}
@@ -182,16 +182,37 @@ class _EnergyBase:
         cp = constraintParameterList if constraintParameterList is not None else Params()
         fp = forceParameterList if forceParameterList is not None else Params()
         self._forces = list(forceTypesList)
+        self._constraints = list(constraintTypesList)
         for c in constraintTypesList:
             if c not in _REF_CONSTRAINTS:
                 raise RuntimeError(f"Unknown constraint type: {c}")
-            if c != "neumannBC":
+            if c == "neumannBC":
+                mask = np.ascontiguousarray(cp.get_value("neumannBCmask").ravel().astype(np.int32))
+                val = np.ascontiguousarray(cp.get_value("neumannBCvalue").ravel().astype(np.float64))
+                if mask.size != self.ndof or val.size != self.ndof:
+                    raise ValueError("neumannBCmask/neumannBCvalue must have 3N entries")
+                _lib.check(L.sors_set_neumann(self._h, _p(mask, C.c_int32), _p(val, C.c_double)))
+            elif c == "planeContact":
+                # energy.cpp:69-84
+                pts = np.ascontiguousarray(cp.get_value("positionVectorListPlanes").ravel().astype(np.float64))
+                nrm = np.ascontiguousarray(cp.get_value("normalVectorListPlanes").ravel().astype(np.float64))
+                surf = np.ascontiguousarray(cp.get_value("surfaceVerticesIdx").ravel().astype(np.int32))
+                if pts.size != nrm.size or pts.size % 3:
+                    raise ValueError("plane points and normals must be lists of 3-vectors of the same length")
+                _lib.check(L.sors_set_plane_contact(self._h, _p(pts, C.c_double), _p(nrm, C.c_double), pts.size // 3,
+                                                    _p(surf, C.c_int32), surf.size))
+            elif c == "diskContact":
+                # energy.cpp:85-108
+                cen = np.ascontiguousarray(cp.get_value("diskCenterVectorList").ravel().astype(np.float64))
+                nrm = np.ascontiguousarray(cp.get_value("diskNormalVectorList").ravel().astype(np.float64))
+                rad = np.ascontiguousarray(cp.get_value("diskRadiusList").ravel().astype(np.float64))
+                surf = np.ascontiguousarray(cp.get_value("surfaceVerticesIdx").ravel().astype(np.int32))
+                if cen.size != nrm.size or cen.size % 3 or rad.size != cen.size // 3:
+                    raise ValueError("DiskContact: centers/normals must be same length and multiples of 3")
+                _lib.check(L.sors_set_disk_contact(self._h, _p(cen, C.c_double), _p(nrm, C.c_double),
+                                                   _p(rad, C.c_double), rad.size, _p(surf, C.c_int32), surf.size))
+            else:
                 raise NotImplementedError(f"constraint {c} is not built on the GPU path")
-            mask = np.ascontiguousarray(cp.get_value("neumannBCmask").ravel().astype(np.int32))
-            val = np.ascontiguousarray(cp.get_value("neumannBCvalue").ravel().astype(np.float64))
-            if mask.size != self.ndof or val.size != self.ndof:
-                raise ValueError("neumannBCmask/neumannBCvalue must have 3N entries")
-            _lib.check(L.sors_set_neumann(self._h, _p(mask, C.c_int32), _p(val, C.c_double)))
         for f in forceTypesList:
             if f not in _REF_FORCES:
                 raise RuntimeError(f"Unknown force type: {f}")
@@ -381,6 +402,10 @@ class _EnergyBase:
     def device_bytes(self):
         return int(_lib.load().sors_device_bytes(self._h))
 
+    def active_contacts(self):
+        """Contact constraints active in the last SQP step."""
+        return int(_lib.load().sors_active_contacts(self._h))
+
     def handle(self):
         return self._h
 
@@ -393,6 +418,29 @@ class EnergyTet(_EnergyBase):
 class EnergyHex(_EnergyBase):
     NV = 8
     MESH = "Hexahedron"
+
+
+class DiskContact:
+    """Handle on an Energy's diskContact constraint (cpp/py_sors.cpp:230-245)."""
+
+    def __init__(self, energy):
+        self._energy = energy
+
+    def set_disk(self, center, normal, radius, diskIdx=0):
+        c = np.ascontiguousarray(np.asarray(center, np.float64).ravel())
+        n = np.ascontiguousarray(np.asarray(normal, np.float64).ravel())
+        _lib.check(_lib.load().sors_set_disk(self._energy._h, int(diskIdx), _p(c, C.c_double), _p(n, C.c_double),
+                                             float(radius)))
+
+
+def get_disk_contact_constraint(energy, idx):
+    """cpp/py_sors.cpp:248-261: the diskContact constraint at index idx of constraintTypesList."""
+    cons = getattr(energy, "_constraints", [])
+    if idx < 0 or idx >= len(cons):
+        raise IndexError("constraint index out of range")
+    if cons[idx] != "diskContact":
+        raise ValueError("constraint at index is not DiskContact")
+    return DiskContact(energy)
 
 
 def Energy(undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha=0.0, elementEnergiesList=None,

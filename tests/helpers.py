@@ -78,3 +78,61 @@ def deform(X, rng, amp=0.05, scale=None):
     L = np.ptp(X, axis=0).max() if scale is None else scale
     A = np.eye(3) + rng.uniform(-amp, amp, (3, 3))
     return (X @ A.T + rng.uniform(-amp, amp, X.shape) * L * 0.02).ravel()
+
+
+def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1e5, nu=0.45,
+                 grav=(0.0, 0.0, -9.81), dt=1e-3, precision="fp64", project=True, neumann=None, muscles=None):
+    """GPU Energy/Solver with minimize_SQP and the oracle's SQP on the same scene.
+
+    planes: (points (k,3), normals (k,3)); disks: (centers, normals, radii);
+    surface: candidate contact vertices (all surface vertices when None);
+    neumann: (mask 3N, value 3N) or None."""
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    from sors_b200 import py_sors as ps
+    X = np.asarray(X, float)
+    T = np.asarray(T, np.int32)
+    ne = T.shape[0]
+    if surface is None:
+        groups, _ = meshes.extract_surfaces(X, T)
+        surface = np.unique(np.concatenate([g.ravel() for g in groups]))
+    surface = np.asarray(surface, np.int32)
+    Ev = np.broadcast_to(np.asarray(E, float), (ne,)).copy()
+    s = ps.SimulationSettings()
+    s.meshType = "Tetrahedron" if T.shape[1] == 4 else "Hexahedron"
+    s.dt = dt
+    s.timeSteppingScheme = "backward_euler"
+    s.solverMethod = "minimize_SQP"
+    s.precision = precision
+    s.hessianProjection = project
+    ctypes_, cp = [], ps.Params()
+    if neumann is not None:
+        ctypes_.append("neumannBC")
+        cp.set_param("neumannBCmask", np.asarray(neumann[0], float))
+        cp.set_param("neumannBCvalue", np.asarray(neumann[1], float))
+    if planes is not None:
+        ctypes_.append("planeContact")
+        cp.set_param("positionVectorListPlanes", np.asarray(planes[0], float).ravel())
+        cp.set_param("normalVectorListPlanes", np.asarray(planes[1], float).ravel())
+    if disks is not None:
+        ctypes_.append("diskContact")
+        cp.set_param("diskCenterVectorList", np.asarray(disks[0], float).ravel())
+        cp.set_param("diskNormalVectorList", np.asarray(disks[1], float).ravel())
+        cp.set_param("diskRadiusList", np.asarray(disks[2], float).ravel())
+    if planes is not None or disks is not None:
+        cp.set_param("surfaceVerticesIdx", surface.astype(float))
+    en = ps.EnergyTet.from_arrays if T.shape[1] == 4 else ps.EnergyHex.from_arrays
+    en = en(X, T, s, np.asarray(grav, float), 0.0, density=rho, youngsModulus=Ev, poissonsRatio=nu,
+            muscleGroup=None if muscles is None else muscles["group"],
+            softconStiffness=None if muscles is None else muscles["k"],
+            softconDirection=None if muscles is None else muscles["dir"])
+    en._setup_constraints_forces(ctypes_, cp, (), None)
+    sol = ps.Solver(s)
+    o = orc.System(X, T, rho=rho, youngs=Ev, nu=nu, grav=grav, scheme="backward_euler", method="minimize_SQP",
+                   project=False, dt=dt, substeps=1)
+    if muscles is not None:
+        o.set_muscles(muscles["group"], muscles["k"], muscles["dir"], int(max(muscles["group"])) + 1)
+    pl = None if planes is None else oc.PlaneContact(planes[0], planes[1], surface)
+    dk = None if disks is None else oc.DiskContact(disks[0], disks[1], disks[2], surface)
+    sq = oc.SQPOracle(o, pl, dk, neumann)
+    return en, sol, sq, surface
