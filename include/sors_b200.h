@@ -136,6 +136,16 @@ int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const d
 /* Number of contact constraints active in the last SQP step. */
 int32_t sors_active_contacts(SorsHandle* h);
 
+/* Contacts held (at their bound) when the last SQP step converged: nodes and
+ * normals (3 per node).  Writes min(count, cap) entries; returns the count. */
+int32_t sors_held_contacts(SorsHandle* h, int32_t* nodes, double* normals, int32_t cap);
+
+/* The disk contacts' state between steps (frozen flag and captured footprint),
+ * for restarting a rollout from a saved step.  get returns the length and fills
+ * state when cap is large enough; set takes that many entries. */
+int32_t sors_get_contact_state(SorsHandle* h, int32_t* state, int32_t cap);
+int sors_set_contact_state(SorsHandle* h, const int32_t* state, int32_t n);
+
 /* Params actuation entries (cpp/headers/params.h): "pressure" (n_groups values),
  * "vertexForce" (3N values, row-major N x 3) or "softconMuscle" (one activation
  * per muscle group). */
@@ -176,17 +186,21 @@ int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32
 /* Adjoint of one backward-Euler step (no reference counterpart: SORS has no
  * differentiation).  A step took the state (q_n, v_n) to q_next with this
  * handle's materials and the activations set at the time; call this with the
- * same activations set.  Given dL/dq_next (3N) it solves J^T lam = dL/dq_next,
- * J the Jacobian of the step's residual at q_next (exact, unprojected; Neumann
- * rows as identity), and writes (any output may be NULL):
- *   dL/dq_n (3N), dL/dv_n (3N)  through the residual's old-state terms,
+ * same activations set.  held_nodes / held_normals (n_held, may be 0) are the
+ * contacts the step held (sors_held_contacts right after it).  Given
+ * dL/dq_next (3N) it solves the transpose system of the step's residual at
+ * q_next (exact, unprojected Hessian) on the subspace the Neumann DOFs and the
+ * held contacts leave free, and writes (any output may be NULL):
+ *   dL/dq_n (3N), dL/dv_n (3N)  through the residual's old-state terms and the
+ *                                Neumann targets q_n + dt val,
  *   dL/dyoungs (E)               per element,
  *   dL/dact (one per muscle group, "softconMuscle" activations),
  *   dL/dneumann (3N)             the Neumann velocities, nonzero on fixed DOFs.
  * Any dependence of the loss on v_next = (q_next - q_n)/dt is the caller's to
  * add to dL/dq_next (and subtract from dL/dq_n).  Pressure loads and
  * Crank-Nicolson steps return SORS_ERR_UNSUPPORTED.  dt = 0 takes settings.dt. */
-int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next, double* dL_dq_prev,
+int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
+                      const int32_t* held_nodes, const double* held_normals, int32_t n_held, double* dL_dq_prev,
                       double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
                       SorsStepStats* stats);
 

@@ -9,9 +9,11 @@ implicit residual g(q_{t+1}; q_t, v_t, E, act_t) = 0 is differentiated by
 element-level derivatives on the GPU), chained through the state
 (q_{t+1}, v_{t+1} = (q_{t+1} - q_t) / dt).
 
-States are checkpointed every `checkpoint_every` steps during the forward pass;
-the backward pass recomputes each segment from its checkpoint (the GPU path is
-deterministic, so the recomputed states equal the forward ones bit for bit).
+States are checkpointed every `checkpoint_every` steps during the forward pass
+(positions, velocities and the disk contacts' state); the backward pass
+recomputes each segment from its checkpoint (the GPU path is deterministic, so
+the recomputed states equal the forward ones bit for bit).  Contact steps
+(minimize_SQP) are differentiated with the contacts they held as equalities.
 
 `rollout(...)` is the torch entry point: a torch.autograd.Function whose inputs
 are float64 tensors E (E,) and act (T, G).
@@ -33,7 +35,7 @@ class RolloutAdjoint:
     """Forward rollout with checkpoints, and its adjoint, on one Energy/Solver pair."""
 
     def __init__(self, energy, solver, steps: int, dt: float, q0=None, v0=None, poisson=None,
-                 checkpoint_every: int = 1):
+                 checkpoint_every: int = 1, before_step=None):
         self.en = energy
         self.sol = solver
         self.steps = int(steps)
@@ -45,7 +47,10 @@ class RolloutAdjoint:
         self.poisson = np.ascontiguousarray(np.broadcast_to(
             np.asarray(0.45 if poisson is None else poisson, np.float64), (ne,)))
         self.k = max(1, int(checkpoint_every))
+        self.before_step = before_step  # callable(t): moves disks etc. before step t
         self._ckpt = {}
+        self._held = {}
+        self._cstate0 = None
         self._E = None
         self._act = None
         self.last_pcg_iters = 0
@@ -62,13 +67,33 @@ class RolloutAdjoint:
         a = np.ascontiguousarray(a, dtype=np.float64)
         _lib.check(_lib.load().sors_set_actuation(self.en._h, b"softconMuscle", _p(a), a.size))
 
-    def _restore(self, q, v):
+    def _contact_state(self):
+        L = _lib.load()
+        k = L.sors_get_contact_state(self.en._h, None, 0)
+        st = np.zeros(k, np.int32)
+        L.sors_get_contact_state(self.en._h, _p(st, C.c_int32), k)
+        return st
+
+    def _restore(self, q, v, cstate):
         self.en.set_initial_deformation(q)
         self.en.set_initial_velocity(v)
+        _lib.check(_lib.load().sors_set_contact_state(self.en._h, _p(cstate, C.c_int32), cstate.size))
+
+    def _held_now(self):
+        L = _lib.load()
+        k = L.sors_held_contacts(self.en._h, None, None, 0)
+        nodes = np.zeros(max(k, 1), np.int32); normals = np.zeros((max(k, 1), 3))
+        if k:
+            L.sors_held_contacts(self.en._h, _p(nodes, C.c_int32), _p(normals), k)
+        return nodes[:k].copy(), normals[:k].copy()
 
     def _step(self, q, t):
+        if self.before_step is not None:
+            self.before_step(t)
         self._set_act(None if self._act is None else self._act[t])
-        return self.sol.step(q, self.en, None, self.dt)
+        qn = self.sol.step(q, self.en, None, self.dt)
+        self._held[t] = self._held_now()
+        return qn
 
     # -- forward ----------------------------------------------------------------
     def forward(self, E, act=None):
@@ -76,13 +101,16 @@ class RolloutAdjoint:
         self._E = np.array(E, dtype=np.float64)
         self._act = None if act is None else np.array(act, dtype=np.float64).reshape(self.steps, -1)
         self._set_material(self._E)
-        self._restore(self.q0, self.v0)
+        self._restore(self.q0, self.v0, self._contact_state() if self._cstate0 is None else self._cstate0)
+        if self._cstate0 is None:
+            self._cstate0 = self._contact_state()
         q = self.q0.copy()
         v = self.v0.copy()
         self._ckpt = {}
+        self._held = {}
         for t in range(self.steps):
             if t % self.k == 0:
-                self._ckpt[t] = (q.copy(), v.copy())
+                self._ckpt[t] = (q.copy(), v.copy(), self._contact_state())
             qn = self._step(q, t)
             v = (qn - q) / self.dt
             q = qn
@@ -106,16 +134,20 @@ class RolloutAdjoint:
         starts = sorted(self._ckpt)
         for s in reversed(starts):
             e = min(s + self.k, self.steps)
-            q, v = self._ckpt[s]
-            self._restore(q, v)
+            q, v, cst = self._ckpt[s]
+            self._restore(q, v, cst)
             qs = [q.copy()]
             for t in range(s, e):
                 qs.append(self._step(qs[-1], t))
             for t in range(e - 1, s - 1, -1):
                 self._set_act(None if self._act is None else self._act[t])
                 b = Qb + Vb / self.dt
-                _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b), _p(dq), _p(dv),
-                                               _p(dE), _p(dA) if G else None, None, C.byref(stats)))
+                hn, hv = self._held[t]
+                hv = np.ascontiguousarray(hv)
+                _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b),
+                                               _p(hn, C.c_int32) if hn.size else None, _p(hv) if hn.size else None,
+                                               hn.size, _p(dq), _p(dv), _p(dE), _p(dA) if G else None, None,
+                                               C.byref(stats)))
                 self.last_pcg_iters += stats.pcg_iters
                 gE += dE
                 if G:
@@ -125,7 +157,8 @@ class RolloutAdjoint:
         return gE, gA, Qb, Vb
 
 
-def rollout(energy, solver, E, act, steps, dt, q0=None, v0=None, poisson=None, checkpoint_every=1):
+def rollout(energy, solver, E, act, steps, dt, q0=None, v0=None, poisson=None, checkpoint_every=1,
+            before_step=None):
     """Differentiable final positions q_T (torch float64, shape (3N,)).
 
     E: torch tensor (E,) of Young's moduli; act: torch tensor (T, G) of SoftCon
@@ -133,7 +166,7 @@ def rollout(energy, solver, E, act, steps, dt, q0=None, v0=None, poisson=None, c
     import torch
 
     runner = RolloutAdjoint(energy, solver, steps, dt, q0=q0, v0=v0, poisson=poisson,
-                            checkpoint_every=checkpoint_every)
+                            checkpoint_every=checkpoint_every, before_step=before_step)
 
     class _Rollout(torch.autograd.Function):
         @staticmethod

@@ -128,6 +128,8 @@ struct SorsHandle {
     int c_cap = 0;
     double *qp_x0 = nullptr, *qp_y = nullptr, *qp_g2 = nullptr, *qp_dx = nullptr;
     int last_active = 0;
+    std::vector<int> held_nodes;      // contacts held at the end of the last SQP step
+    std::vector<double> held_normals;
     // projection used by the PCG kernels (null: none)
     const uint8_t* proj_flag = nullptr;
     const double4* proj_n = nullptr;
@@ -471,15 +473,21 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
     return SORS_OK;
 }
 
-// Adjoint of one backward-Euler step (see sors_adjoint_step).  The residual of
-// the step is g_f = grad Psi(q) - f + m (v - v_n)/dt - m grav + alpha m v on
-// free DOFs, v = (q - q_n)/dt, and g_m = q_m - q_n,m - dt val_m on Neumann DOFs
-// (energy.cpp:296-306).  Its Jacobian J = [[H_ff, H_fm], [0, I]], so J^T lam = b
-// splits into H_ff lam_f = b_f and lam_m = b_m - H_mf lam_f; then
-// dL/dtheta = -lam^T dg/dtheta for every input theta of the step.
+int ensure_sqp_buffers(SorsHandle* h, int m);
+
+// Adjoint of one backward-Euler step (see sors_adjoint_step).  At the step's
+// solution q the residual g = grad Psi(q) - f + m (v - v_n)/dt - m grav +
+// alpha m v (v = (q - q_n)/dt) vanishes on the subspace the held constraints
+// leave free, and the held constraints fix the rest: Neumann DOFs at
+// q_n + dt val (energy.cpp:296-306, neumannBC.cpp:4-21) and contact nodes on
+// their plane or disk (n . (q_v - p) = 0).  With Z a basis of that subspace,
+// lam = Z (Z^T H Z)^-1 Z^T b is a projected solve with the exact Hessian, and
+//   dL/dtheta = -lam^T dg/dtheta  for the material, activations and old state,
+//   r = b - H lam                 carries dL through the fixed DOFs' targets.
 template <typename HT, typename VT>
-int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b, double* dq, double* dv,
-                 double* dE, double* dact, double* dneu, SorsStepStats* stats) {
+int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b, const int* held_nodes,
+                 const double* held_normals, int n_held, double* dq, double* dv, double* dE, double* dact,
+                 double* dneu, SorsStepStats* stats) {
     const int n = h->ndof, N = h->N, E = h->E;
     int st;
     if (!h->adj_l) {
@@ -487,23 +495,41 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         if ((st = dalloc_t(h, &h->adj_y, (size_t)n))) return st;
         if ((st = dalloc_t(h, &h->adj_e, (size_t)2 * std::max(1, E)))) return st;
     }
+    if ((st = ensure_sqp_buffers(h, 0))) return st;
     CK(h2d(h, h->q, q_next, sizeof(double) * n));
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
-    // the exact Jacobian: no SPD projection, Neumann rows as identity
+    // the exact Hessian: no SPD projection, every element term on every DOF
     struct ProjectionOff {
         SorsHandle* h;
         int saved;
         explicit ProjectionOff(SorsHandle* hh) : h(hh), saved(hh->s.project_spd) { h->s.project_spd = 0; }
         ~ProjectionOff() { h->s.project_spd = saved; }
     } projection_off(h);
-    if ((st = eval_system<HT>(h, dt, true, kAsmMaskedIdentity))) return st;
+    if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
     auto fixed = [&](int i) { return h->has_neumann && ((h->mask_h[i / 3] >> (i % 3)) & 1u); };
+    h->pflag_h.assign(N, 0);
+    if (h->has_neumann)
+        for (int v = 0; v < N; v++) h->pflag_h[v] = h->mask_h[v] & 7u;
+    for (int c = 0; c < n_held; c++) {
+        const int v = held_nodes[c];
+        if (v < 0 || v >= N) return fail(SORS_ERR_ARG, "held contact node out of range");
+        if (h->pflag_h[v]) continue;  // Neumann nodes carry no contact
+        h->pflag_h[v] = 8u;
+        h->pn_h[v] = make_double4(held_normals[3 * c], held_normals[3 * c + 1], held_normals[3 * c + 2], 0.0);
+    }
+    CK(h2d(h, h->pflag_d, h->pflag_h.data(), (size_t)N));
+    CK(h2d(h, h->pn_d, h->pn_h.data(), sizeof(double4) * N));
     std::vector<double> lam(n);
-    for (int i = 0; i < n; i++) lam[i] = fixed(i) ? 0.0 : -b[i];  // pcg_solve solves H x = -g
-    CK(h2d(h, h->g, lam.data(), sizeof(double) * n));
+    for (int i = 0; i < n; i++) lam[i] = -b[i];  // pcg_solve solves H x = -g
+    CK(h2d(h, h->qp_g2, lam.data(), sizeof(double) * n));
     const double eta = mixed(h) ? 1e-6 : std::max(1e-12, 0.01 * h->s.pcg_rel_tol);
     int pit = 0;
-    if ((st = pcg_solve<HT, VT>(h, eta, 0.0, &pit))) return st;
+    h->proj_flag = h->pflag_d;
+    h->proj_n = h->pn_d;
+    st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
+    h->proj_flag = nullptr;
+    h->proj_n = nullptr;
+    if (st) return st;
     if (h->sc_host->status & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
     if (stats) { stats->pcg_iters += pit; stats->residual_norm = sqrt(h->sc_host->rr); }
     if (sizeof(VT) == sizeof(double)) {
@@ -514,26 +540,24 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         for (int i = 0; i < n; i++) lam[i] = lf[i];
     }
     CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
-    // element contractions with lam_hat (fixed DOFs zero: their residual rows do
-    // not depend on the material or the activations)
+    // element contractions with lam (zero on fixed DOFs and along held normals)
     launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->adj_l, h->adj_e, h->stream);
     std::vector<double> ge((size_t)2 * std::max(1, E));
     CK(d2h(h, ge.data(), h->adj_e, sizeof(double) * 2 * (size_t)E));
+    std::vector<double> r(n, 0.0);
     if (h->has_neumann) {
-        if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
         launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->adj_l, h->adj_y, h->stream);
-        std::vector<double> y(n);
-        CK(d2h(h, y.data(), h->adj_y, sizeof(double) * n));
-        for (int i = 0; i < n; i++)
-            if (fixed(i)) lam[i] = b[i] - y[i];
+        CK(d2h(h, r.data(), h->adj_y, sizeof(double) * n));
+        for (int i = 0; i < n; i++) r[i] = b[i] - r[i];
     }
     const double a = h->s.damping_alpha;
     for (int i = 0; i < n; i++) {
         const double m = h->mass_h[i / 3];
         const bool f = fixed(i);
-        if (dq) dq[i] = f ? lam[i] : (dt != 0.0 ? lam[i] * (m / (dt * dt) + a * m / dt) : 0.0);
-        if (dv) dv[i] = f ? 0.0 : (dt != 0.0 ? lam[i] * m / dt : 0.0);
-        if (dneu) dneu[i] = f ? lam[i] * dt : 0.0;
+        const double inert = dt != 0.0 ? lam[i] * (m / (dt * dt) + a * m / dt) : 0.0;
+        if (dq) dq[i] = f ? r[i] : inert;
+        if (dv) dv[i] = dt != 0.0 ? lam[i] * m / dt : 0.0;
+        if (dneu) dneu[i] = f ? r[i] * dt : 0.0;
     }
     if (dE)
         for (int e = 0; e < E; e++) dE[e] = h->youngs_h[e] != 0.0 ? -ge[e] / h->youngs_h[e] : 0.0;
@@ -835,6 +859,13 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
         if (dxn < h->s.newton_dx_tol) { converged = true; break; }
     }
     if (!converged) return fail(SORS_ERR_NOT_CONVERGED, "SQP method did not converge");
+    h->held_nodes.clear();
+    h->held_normals.clear();
+    for (int c = 0; c < m; c++)
+        if (inW[c]) {
+            h->held_nodes.push_back(cnode[c]);
+            h->held_normals.insert(h->held_normals.end(), &cn[3 * (size_t)c], &cn[3 * (size_t)c] + 3);
+        }
     return SORS_OK;
 }
 
@@ -1303,6 +1334,35 @@ int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const d
 
 int32_t sors_active_contacts(SorsHandle* h) { return h ? h->last_active : 0; }
 
+int32_t sors_held_contacts(SorsHandle* h, int32_t* nodes, double* normals, int32_t cap) {
+    if (!h) return 0;
+    const int k = (int)h->held_nodes.size();
+    for (int c = 0; c < k && c < cap; c++) {
+        if (nodes) nodes[c] = h->held_nodes[c];
+        if (normals)
+            for (int j = 0; j < 3; j++) normals[3 * c + j] = h->held_normals[3 * (size_t)c + j];
+    }
+    return k;
+}
+
+int32_t sors_get_contact_state(SorsHandle* h, int32_t* state, int32_t cap) {
+    if (!h) return 0;
+    const int k = 1 + (int)h->disk_mask.size();
+    if (state && cap >= k) {
+        state[0] = h->disk_frozen ? 1 : 0;
+        for (size_t i = 0; i < h->disk_mask.size(); i++) state[1 + i] = h->disk_mask[i];
+    }
+    return k;
+}
+
+int sors_set_contact_state(SorsHandle* h, const int32_t* state, int32_t n) {
+    if (!h || !state) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n != 1 + (int)h->disk_mask.size()) return fail(SORS_ERR_ARG, "contact state size mismatch");
+    h->disk_frozen = state[0] != 0;
+    for (size_t i = 0; i < h->disk_mask.size(); i++) h->disk_mask[i] = state[1 + i];
+    return SORS_OK;
+}
+
 int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson) {
     if (!h || !youngs || !poisson) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
@@ -1319,10 +1379,12 @@ int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson
     return SORS_OK;
 }
 
-int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next, double* dL_dq_prev,
+int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
+                      const int32_t* held_nodes, const double* held_normals, int32_t n_held, double* dL_dq_prev,
                       double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
                       SorsStepStats* stats) {
     if (!h || !q_next || !dL_dq_next) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_held < 0 || (n_held > 0 && (!held_nodes || !held_normals))) return fail(SORS_ERR_ARG, "held contacts");
     int st;
     if ((st = set_device(h))) return st;
     if (dt == 0.0) dt = h->s.dt;
@@ -1331,10 +1393,10 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
     if (h->s.material != 0) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
     if (stats) *stats = SorsStepStats{};
-    return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, dL_dq_prev, dL_dv_prev, dL_dyoungs,
-                                                 dL_dact, dL_dneumann, stats)
-                    : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, dL_dq_prev, dL_dv_prev, dL_dyoungs,
-                                                   dL_dact, dL_dneumann, stats);
+    return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
+                                                 dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats)
+                    : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
+                                                   dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats);
 }
 
 int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps, SorsStepStats* stats) {

@@ -112,7 +112,8 @@ def test_adjoint_neumann_velocity(oracle):
     dneu = np.zeros(n); dq = np.zeros(n); dv = np.zeros(n)
     p = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
     st = _lib.SorsStepStats()
-    _lib.check(L.sors_adjoint_step(en._h, p(q1), DT, p(w), p(dq), p(dv), None, None, p(dneu), C.byref(st)))
+    _lib.check(L.sors_adjoint_step(en._h, p(q1), DT, p(w), None, None, 0, p(dq), p(dv), None, None, p(dneu),
+                                   C.byref(st)))
 
     def f(v):
         oo = oracle.System(X, T, rho=1070.0, youngs=1e5, nu=0.45, grav=(0, 0, -9.81), dt=DT, substeps=1)
