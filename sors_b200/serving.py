@@ -42,6 +42,12 @@ class RolloutRequest:
     newton_res_tol: float = 1e-8
     tag: object = None
     submitted: float = field(default=0.0)
+    # contact (minimize_SQP): planes (points, normals), disks (centers, normals,
+    # radii) moving at disk_velocity (m/s, per disk) and the candidate surface vertices
+    planes: tuple | None = None
+    disks: tuple | None = None
+    disk_velocity: np.ndarray | None = None
+    surface: np.ndarray | None = None
 
 
 @dataclass
@@ -145,22 +151,21 @@ class RolloutServer:
         final = None
         err = None
         try:
-            s = ps.SimulationSettings()
-            s.meshType = "Tetrahedron" if req.elements.shape[1] == 4 else "Hexahedron"
-            s.dt = req.dt
-            s.timeSteppingScheme = req.scheme
-            s.solverMethod = "minimize_newton"
-            s.precision = req.precision
-            s.newtonResidualTol = req.newton_res_tol
-            s.device = self.device
-            cls = ps.EnergyTet if req.elements.shape[1] == 4 else ps.EnergyHex
-            en = cls.from_arrays(req.vertices, req.elements, s, np.asarray(req.gravity, float), 0.0,
-                                 density=req.density, youngsModulus=req.youngs, poissonsRatio=req.poisson,
-                                 neumannBCmask=req.neumann_mask, neumannBCvalue=req.neumann_value)
-            sol = ps.Solver(s)
+            en, sol = build_rollout(req, self.device)
+            disk = None
+            if req.disks is not None:
+                disk = ps.get_disk_contact_constraint(en, en._constraints.index("diskContact"))
+                c0 = np.asarray(req.disks[0], float).reshape(-1, 3)
+                nrm = np.asarray(req.disks[1], float).reshape(-1, 3)
+                rad = np.asarray(req.disks[2], float).ravel()
+                vel = np.zeros_like(c0) if req.disk_velocity is None else np.asarray(req.disk_velocity,
+                                                                                       float).reshape(-1, 3)
             q = np.ascontiguousarray(req.vertices, dtype=np.float64).ravel().copy()
-            for _ in range(req.steps):
+            for t in range(req.steps):
                 t0 = time.perf_counter()
+                if disk is not None:
+                    for d in range(c0.shape[0]):
+                        disk.set_disk(c0[d] + vel[d] * req.dt * t, nrm[d], rad[d], d)
                 q = sol.step(q, en)
                 steps_lat.append(time.perf_counter() - t0)
                 newton += sol.last_stats.newton_iters
@@ -178,20 +183,62 @@ class RolloutServer:
             self._lock.notify_all()
 
 
+def build_rollout(req: RolloutRequest, device: int = 0):
+    """Energy and Solver for one request (the reference-style py_sors objects)."""
+    s = ps.SimulationSettings()
+    s.meshType = "Tetrahedron" if req.elements.shape[1] == 4 else "Hexahedron"
+    s.dt = req.dt
+    s.timeSteppingScheme = req.scheme
+    contact = req.planes is not None or req.disks is not None
+    s.solverMethod = "minimize_SQP" if contact else "minimize_newton"
+    s.precision = req.precision
+    s.newtonResidualTol = 0.0 if contact else req.newton_res_tol
+    s.device = device
+    cls = ps.EnergyTet if req.elements.shape[1] == 4 else ps.EnergyHex
+    en = cls.from_arrays(req.vertices, req.elements, s, np.asarray(req.gravity, float), 0.0,
+                         density=req.density, youngsModulus=req.youngs, poissonsRatio=req.poisson,
+                         neumannBCmask=req.neumann_mask, neumannBCvalue=req.neumann_value)
+    if contact:
+        types, cp = [], ps.Params()
+        if req.neumann_mask is not None:
+            types.append("neumannBC")
+            cp.set_param("neumannBCmask", np.asarray(req.neumann_mask, float).ravel())
+            cp.set_param("neumannBCvalue", np.asarray(req.neumann_value, float).ravel())
+        if req.planes is not None:
+            types.append("planeContact")
+            cp.set_param("positionVectorListPlanes", np.asarray(req.planes[0], float).ravel())
+            cp.set_param("normalVectorListPlanes", np.asarray(req.planes[1], float).ravel())
+        if req.disks is not None:
+            types.append("diskContact")
+            cp.set_param("diskCenterVectorList", np.asarray(req.disks[0], float).ravel())
+            cp.set_param("diskNormalVectorList", np.asarray(req.disks[1], float).ravel())
+            cp.set_param("diskRadiusList", np.asarray(req.disks[2], float).ravel())
+        cp.set_param("surfaceVerticesIdx", np.asarray(req.surface, float).ravel())
+        en._setup_constraints_forces(types, cp, (), None)
+    return en, ps.Solver(s)
+
+
 def percentile(values, p):
     if not values:
         return float("nan")
     return float(np.percentile(np.asarray(values, float), p))
 
 
+def cube_surface_nodes(n_cells: int) -> np.ndarray:
+    """Boundary node ids of an n^3-cell grid (vid = i + NX (j + NY k))."""
+    n1 = n_cells + 1
+    k, j, i = np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1), indexing="ij")
+    on = (i == 0) | (i == n_cells) | (j == 0) | (j == n_cells) | (k == 0) | (k == n_cells)
+    return np.nonzero(on.ravel())[0].astype(np.int32)
+
+
 def poke_cube_request(rng: np.random.Generator, n_cells: int, tag=None, steps: int = 100, dt: float = 1e-2,
                       precision: str = "mixed") -> RolloutRequest:
-    """A poke rollout on a 6-tet cube (side U[30, 60] mm, n_cells^3 cells).
-
-    The cube's bottom face is held; the top-face nodes within 10 mm of a
-    seeded (x, y) point are driven down at 10 mm per second (a prescribed
-    indenter motion standing in for the rigid disk contact).
-    """
+    """A poke rollout: a 6-tet cube (side U[30, 60] mm, n_cells^3 cells) resting on
+    the ground plane z = 0 under gravity, pressed by a rigid disk (radius 10 mm,
+    normal -z) that starts 1 mm above the top face at a seeded (x, y) offset and
+    moves 10 mm down over the rollout (the PokeFlex set-up, planeContact +
+    diskContact with minimize_SQP)."""
     from . import meshes
     side = float(rng.uniform(0.03, 0.06))
     X = meshes.grid_nodes(n_cells, n_cells, n_cells, (side, side, side))
@@ -199,14 +246,9 @@ def poke_cube_request(rng: np.random.Generator, n_cells: int, tag=None, steps: i
     E = float(rng.uniform(2e4, 2e5))
     nu = float(rng.uniform(0.30, 0.48))
     cx, cy = rng.uniform(0.3 * side, 0.7 * side, size=2)
-    bottom = X[:, 2] < 1e-12
-    top = X[:, 2] > side - 1e-12
-    under = top & ((X[:, 0] - cx) ** 2 + (X[:, 1] - cy) ** 2 <= 0.01 ** 2)
-    mask = np.zeros(3 * X.shape[0], np.int32)
-    val = np.zeros(3 * X.shape[0])
-    for node in np.nonzero(bottom | under)[0]:
-        mask[3 * node:3 * node + 3] = 1
-    for node in np.nonzero(under)[0]:
-        val[3 * node + 2] = -0.01
-    return RolloutRequest(X, T, 1000.0, E, nu, steps, dt, gravity=(0.0, 0.0, -9.81), neumann_mask=mask,
-                          neumann_value=val, precision=precision, tag=tag)
+    travel = 0.01
+    vz = -travel / (steps * dt)
+    return RolloutRequest(X, T, 1000.0, E, nu, steps, dt, gravity=(0.0, 0.0, -9.81), precision=precision, tag=tag,
+                          planes=(np.zeros((1, 3)), np.array([[0.0, 0.0, 1.0]])),
+                          disks=(np.array([[cx, cy, side + 0.001]]), np.array([[0.0, 0.0, -1.0]]), np.array([0.01])),
+                          disk_velocity=np.array([[0.0, 0.0, vz]]), surface=cube_surface_nodes(n_cells))

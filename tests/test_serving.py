@@ -40,3 +40,32 @@ def test_memory_admission_rejects_oversize():
     srv.submit(_requests(1)[0])
     res = srv.close()
     assert res[0].error is not None and "budget" in res[0].error
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_served_poke_matches_oracle(precision):
+    # one poke rollout (ground plane + moving disk) through the server against
+    # the oracle's SQP rollout: FP64 1e-8 m, mixed 1e-6 of the displacement
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    from sors_b200.serving import RolloutServer, poke_cube_request
+    rng = np.random.default_rng(5)
+    req = poke_cube_request(rng, 4, tag=0, steps=8, dt=1e-2, precision=precision)
+    srv = RolloutServer(max_slots=2)
+    srv.submit(req)
+    res = srv.close()[0]
+    assert res.error is None, res.error
+    o = orc.System(req.vertices, req.elements, rho=req.density, youngs=req.youngs, nu=req.poisson,
+                   grav=req.gravity, scheme="backward_euler", method="minimize_SQP", dt=req.dt, substeps=1)
+    dk = oc.DiskContact(req.disks[0], req.disks[1], req.disks[2], req.surface)
+    sq = oc.SQPOracle(o, oc.PlaneContact(req.planes[0], req.planes[1], req.surface), dk)
+    q = req.vertices.ravel().copy()
+    held = 0
+    for t in range(req.steps):
+        dk.set_disk(req.disks[0][0] + req.disk_velocity[0] * req.dt * t, req.disks[1][0], req.disks[2][0])
+        q = sq.step(q, req.dt)
+        held += sq.last_active
+    assert held > 0
+    disp = np.abs(q - req.vertices.ravel()).max()
+    err = np.abs(res.final - q).max()
+    assert err <= (1e-8 if precision == "fp64" else 1e-6 * disp), (err, disp)
