@@ -384,11 +384,129 @@ def run_c3(args):
         del en
 
 
+def c4_case(seed, steps):
+    """Differentiation workload: hex bar 0.2 x 0.04 x 0.04 m (40 x 8 x 8 hexes),
+    fibres +x in every element, a_e(t) ~ U[0, 1] seeded, E 2e5, nu 0.45, rho
+    1070, dropped from 0.05 m onto the plane z = 0 (planeContact, minimize_SQP),
+    backward Euler dt 2e-3.  Loss (z_com(T) - 0.08)^2."""
+    from sors_b200 import meshes
+    X, H = meshes.hex_bar(40, 8, 8, (0.2, 0.04, 0.04))
+    X = X + np.array([0.0, 0.0, 0.05])
+    ne = H.shape[0]
+    rng = np.random.default_rng(seed)
+    act = rng.uniform(0.0, 1.0, (steps, ne))
+    E = np.full(ne, 2e5)
+    groups, _ = meshes.extract_surfaces(X, H)
+    surf = np.unique(np.concatenate([g.ravel() for g in groups]))
+    return X, H, E, act, surf
+
+
+def c4_energy(X, H, E, surf, precision="fp64"):
+    from sors_b200 import py_sors as ps
+    s = ps.SimulationSettings()
+    s.meshType = "Hexahedron"; s.dt = 2e-3; s.timeSteppingScheme = "backward_euler"
+    s.solverMethod = "minimize_SQP"; s.precision = precision
+    ne = H.shape[0]
+    en = ps.EnergyHex.from_arrays(X, H, s, np.array([0.0, 0.0, -9.81]), 0.0, density=1070.0, youngsModulus=E,
+                                  poissonsRatio=0.45, muscleGroup=np.arange(ne), softconStiffness=np.full(ne, 5e4),
+                                  softconDirection=np.tile([1.0, 0.0, 0.0], (ne, 1)))
+    cp = ps.Params()
+    cp.set_param("positionVectorListPlanes", np.zeros(3))
+    cp.set_param("normalVectorListPlanes", np.array([0.0, 0.0, 1.0]))
+    cp.set_param("surfaceVerticesIdx", surf.astype(float))
+    en._setup_constraints_forces(["planeContact"], cp, (), None)
+    return en, ps.Solver(s)
+
+
+def c4_mass(X, H):
+    """Lumped node masses of the C4 bar (uniform hexes: rho V / 8 per corner)."""
+    m = np.zeros(X.shape[0])
+    np.add.at(m, H.ravel(), 1070.0 * (0.2 * 0.04 * 0.04 / H.shape[0]) / 8)
+    return m
+
+
+def run_c4(args):
+    """Gradient of the C4 loss w.r.t. per-element E and a_e(t) by the adjoint:
+    seeds run concurrently (one handle and stream each); the directional
+    derivative is checked against central differences (h = 1e-6) of the GPU
+    FP64 forward along seeded directions."""
+    import threading
+
+    import torch
+    from sors_b200.adjoint import RolloutAdjoint
+    torch.cuda.set_device(0)
+    steps = args.c4_steps
+    dt = 2e-3
+    cases = [c4_case(sd, steps) for sd in range(args.seeds)]
+    runners = []
+    for X, H, E, act, surf in cases:
+        en, sol = c4_energy(X, H, E, surf)
+        runners.append((RolloutAdjoint(en, sol, steps, dt, poisson=0.45, checkpoint_every=args.checkpoint_every),
+                        en))
+    m = c4_mass(cases[0][0], cases[0][1])
+
+    def loss_grad(k, out):
+        try:
+            r, en = runners[k]
+            _, H, E, act, _ = cases[k]
+            t0 = time.perf_counter()
+            qT = r.forward(E, act)
+            t1 = time.perf_counter()
+            z = (qT[2::3] * m).sum() / m.sum()
+            dq = np.zeros_like(qT)
+            dq[2::3] = 2 * (z - 0.08) * m / m.sum()
+            gE, gA, _, _ = r.backward(dq)
+            t2 = time.perf_counter()
+            out[k] = ((z - 0.08) ** 2, gE, gA, t1 - t0, t2 - t1, r.last_pcg_iters)
+        except Exception as ex:  # reported below
+            out[k] = ex
+
+    res = {}
+    threads = [threading.Thread(target=loss_grad, args=(k, res)) for k in range(len(cases))]
+    t0 = time.perf_counter()
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    wall = time.perf_counter() - t0
+    errors = [str(v) for v in res.values() if isinstance(v, Exception)]
+    if errors:
+        print(json.dumps({"workload": "c4", "errors": errors}), flush=True)
+        return
+    r, en = runners[0]
+    _, H, E, act, _ = cases[0]
+
+    def L(Ev, Av):
+        q = r.forward(Ev, Av)
+        return ((q[2::3] * m).sum() / m.sum() - 0.08) ** 2
+
+    loss0, gE, gA = res[0][0], res[0][1], res[0][2]
+    rng = np.random.default_rng(99)
+    errs = []
+    h = 1e-6
+    for _ in range(args.fd_dirs):
+        rE = rng.standard_normal(E.size); rA = rng.standard_normal(act.shape)
+        d_adj = gE @ (E * rE) + (gA * rA).sum()
+        d_fd = (L(E * (1 + h * rE), act + h * rA) - L(E * (1 - h * rE), act - h * rA)) / (2 * h)
+        errs.append(abs(d_adj - d_fd) / max(abs(d_fd), 1e-300))
+    X = cases[0][0]
+    print(json.dumps({"workload": "c4 SoftCon hex bar 40x8x8 dropped from 0.05 m on z=0, adjoint of E and a_e(t), "
+                                  "FP64", "hexes": int(H.shape[0]), "nodes": int(X.shape[0]), "steps": steps,
+                      "seeds": len(cases), "gradients_per_s": len(cases) / wall, "wall_s": wall,
+                      "forward_ms_per_step": 1e3 * float(np.mean([v[3] for v in res.values()])) / steps,
+                      "backward_ms_per_step": 1e3 * float(np.mean([v[4] for v in res.values()])) / steps,
+                      "adjoint_pcg_iters_per_step": float(np.mean([v[5] for v in res.values()])) / steps,
+                      "checkpoint_every": args.checkpoint_every, "loss_seed0": loss0,
+                      "fd_directions": args.fd_dirs, "fd_h": h, "fd_max_rel_err": max(errs) if errs else None,
+                      "active_contacts_last_step": en.active_contacts()}), flush=True)
+
+
 def run_serve(args):
     """Mixed-size poke sweep: Poisson arrivals of cube rollouts (6-tet cubes with
     log-uniform 5k-250k tets, E U[2e4, 2e5], nu U[0.30, 0.48], rho 1000, dt 1e-2).
-    Served form: mixed precision, continuous admission, 8 slots.  Baseline: the
-    plain FP64 drop-in, one rollout at a time, on the same requests."""
+    Served form: mixed precision, continuous admission, compatible waiting
+    rollouts packed into union handles, several handles in flight.  Baseline:
+    the plain FP64 drop-in, one rollout at a time, on the same requests."""
     import torch
     from sors_b200 import serving
     torch.cuda.set_device(0)
@@ -403,9 +521,9 @@ def run_serve(args):
             out.append(serving.poke_cube_request(r, n, tag=i, steps=args.rollout_steps, dt=1e-2, precision=precision))
         return out
 
-    def run(precision, slots, arrivals):
+    def run(precision, slots, arrivals, batch=1):
         reqs = make(precision)
-        srv = serving.RolloutServer(max_slots=slots)
+        srv = serving.RolloutServer(max_slots=slots, batch_max=batch)
         t0 = time.perf_counter()
         for req, at in zip(reqs, arrivals):
             now = time.perf_counter() - t0
@@ -419,6 +537,7 @@ def run_serve(args):
         lat = [r.latency for r in res]
         tets = sum(q.elements.shape[0] for q in reqs)
         return {"rollouts_per_s": len(res) / wall, "makespan_s": wall, "errors": len(errs),
+                "mean_batch": float(np.mean([r.batch for r in res])) if res else 0.0,
                 "error_messages": sorted(set(errs))[:3],
                 "step_latency_p50_ms": 1e3 * serving.percentile(steps, 50),
                 "step_latency_p99_ms": 1e3 * serving.percentile(steps, 99),
@@ -427,8 +546,9 @@ def run_serve(args):
 
     gaps = rng.exponential(1.0 / args.rate, size=args.rollouts)
     arrivals = np.cumsum(gaps) - gaps[0]
-    served, res_m, reqs = run("mixed", args.slots, arrivals)
-    saturated, _, _ = run("mixed", args.slots, np.zeros(args.rollouts))
+    served, res_m, reqs = run("mixed", args.slots, arrivals, args.batch)
+    saturated, _, _ = run("mixed", args.slots, np.zeros(args.rollouts), args.batch)
+    unbatched, _, _ = run("mixed", args.slots, np.zeros(args.rollouts), 1)
     plain, res_p, _ = run("fp64", 1, np.zeros(args.rollouts))
     # accuracy of the served form against the plain FP64 path, per rollout,
     # relative to that rollout's largest displacement
@@ -437,8 +557,10 @@ def run_serve(args):
     rel = [float(np.abs(r.final - by_tag[r.tag]).max() / max(np.abs(by_tag[r.tag] - X0[r.tag]).max(), 1e-30))
            for r in res_m if r.final is not None and by_tag.get(r.tag) is not None]
     print(json.dumps({"workload": f"poke sweep: {args.rollouts} rollouts x {args.rollout_steps} steps, "
-                                  f"Poisson arrivals at {args.rate}/s, 6-tet cubes 5k-250k tets",
-                      "slots": args.slots, "served_mixed": served, "served_mixed_all_at_once": saturated,
+                                  f"Poisson arrivals at {args.rate}/s, 6-tet cubes 5k-250k tets on z=0 "
+                                  f"pressed by a 10 mm disk moving 10 mm down (minimize_SQP contact)",
+                      "slots": args.slots, "batch_max": args.batch, "served_mixed": served,
+                      "served_mixed_all_at_once": saturated, "served_mixed_all_at_once_unbatched": unbatched,
                       "plain_fp64_sequential": plain,
                       "capacity_speedup_rollouts_per_s": saturated["rollouts_per_s"] / plain["rollouts_per_s"],
                       "speedup_rollouts_per_s": served["rollouts_per_s"] / plain["rollouts_per_s"],
@@ -473,13 +595,18 @@ def main():
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "serve"],
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "serve"],
                     help="c2: the 3.0M-tet block (default); c3: pressure-actuated hex arm, static load ramp; "
                          "serve: Poisson stream of poke rollouts")
     ap.add_argument("--rollouts", type=int, default=24)
     ap.add_argument("--rollout-steps", type=int, default=20)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (rollouts/s)")
-    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent rollouts")
+    ap.add_argument("--slots", type=int, default=8, help="serve: concurrent handles")
+    ap.add_argument("--batch", type=int, default=8, help="serve: rollouts packed into one union handle")
+    ap.add_argument("--seeds", type=int, default=4, help="c4: rollouts differentiated concurrently")
+    ap.add_argument("--c4-steps", type=int, default=100, help="c4: steps per rollout")
+    ap.add_argument("--fd-dirs", type=int, default=4, help="c4: finite-difference directions checked")
+    ap.add_argument("--checkpoint-every", type=int, default=10, help="c4: checkpoint interval (steps)")
     ap.add_argument("--profile-only", action="store_true",
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
@@ -491,6 +618,8 @@ def main():
         run_reference(args, rank, world)
     elif args.workload == "c3":
         run_c3(args)
+    elif args.workload == "c4":
+        run_c4(args)
     elif args.workload == "serve":
         run_serve(args)
     elif args.profile_only:

@@ -130,6 +130,14 @@ int sors_set_plane_contact(SorsHandle* h, const double* points, const double* no
 int sors_set_disk_contact(SorsHandle* h, const double* centers, const double* normals, const double* radii,
                           int32_t n_disks, const int32_t* surface_vertices, int32_t n_surface);
 
+/* Disks that act as independent DiskContact constraints (no reference
+ * counterpart as one call): disk k may touch only surface_vertices
+ * [surface_ptr[k], surface_ptr[k+1]) and keeps its own frozen footprint, as if
+ * each disk were a separate diskContact entry.  Used to step several meshes in
+ * one handle (serving), each with its own indenter. */
+int sors_set_disk_contact_groups(SorsHandle* h, const double* centers, const double* normals, const double* radii,
+                                 int32_t n_disks, const int32_t* surface_vertices, const int32_t* surface_ptr);
+
 /* DiskContact::set_disk (cpp/py_sors.cpp:231-245): moves disk disk_idx. */
 int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const double* normal, double radius);
 
@@ -140,9 +148,9 @@ int32_t sors_active_contacts(SorsHandle* h);
  * normals (3 per node).  Writes min(count, cap) entries; returns the count. */
 int32_t sors_held_contacts(SorsHandle* h, int32_t* nodes, double* normals, int32_t cap);
 
-/* The disk contacts' state between steps (frozen flag and captured footprint),
- * for restarting a rollout from a saved step.  get returns the length and fills
- * state when cap is large enough; set takes that many entries. */
+/* The disk contacts' state between steps (per DiskContact: frozen flag and
+ * captured footprint), for restarting a rollout from a saved step.  get returns
+ * the length and fills state when cap is large enough; set takes that many. */
 int32_t sors_get_contact_state(SorsHandle* h, int32_t* state, int32_t cap);
 int sors_set_contact_state(SorsHandle* h, const int32_t* state, int32_t n);
 

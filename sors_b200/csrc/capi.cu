@@ -116,8 +116,13 @@ struct SorsHandle {
     std::vector<Plane> planes;
     std::vector<int> plane_surf, plane_mask;
     std::vector<Disk> disks;
-    std::vector<int> disk_surf, disk_mask;
-    bool disk_frozen = false;
+    // one DiskContact per group: its disks, candidate vertices, captured
+    // footprint (global disk index per candidate, -1 none) and frozen flag
+    struct DiskGroup {
+        std::vector<int> disks, surf, mask;
+        bool frozen = false;
+    };
+    std::vector<DiskGroup> disk_groups;
     uint8_t* pflag_d = nullptr;
     double4* pn_d = nullptr;
     std::vector<uint8_t> pflag_h;
@@ -680,53 +685,58 @@ double disk_radial_dist(const SorsHandle::Disk& D, const double* x) {
     return sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
 }
 
-void update_disk_contacts(SorsHandle* h, const double* q) {
-    const size_t ns = h->disk_surf.size();
-    if (h->disk_mask.size() != ns) h->disk_mask.assign(ns, -1);
+void update_disk_group(SorsHandle* h, SorsHandle::DiskGroup& G, const double* q) {
+    const size_t ns = G.surf.size();
+    if (G.mask.size() != ns) G.mask.assign(ns, -1);
     const double clear = 3.0 * kDiskPlaneThreshold, depth = 5.0 * kDiskPlaneThreshold;
-    if (h->disk_frozen) {
+    if (G.frozen) {
         // keep the captured footprint until every vertex of it is clearly above its disk
         bool all_clear = true;
         for (size_t i = 0; i < ns && all_clear; i++) {
-            const int d = h->disk_mask[i];
+            const int d = G.mask[i];
             if (d < 0) continue;
-            if (disk_plane_dist(h->disks[d], q + 3 * (size_t)h->disk_surf[i]) < clear) all_clear = false;
+            if (disk_plane_dist(h->disks[d], q + 3 * (size_t)G.surf[i]) < clear) all_clear = false;
         }
         if (all_clear) {
-            h->disk_frozen = false;
-            std::fill(h->disk_mask.begin(), h->disk_mask.end(), -1);
+            G.frozen = false;
+            std::fill(G.mask.begin(), G.mask.end(), -1);
         }
         return;
     }
-    std::vector<char> hit(h->disks.size(), 0);
+    std::vector<char> hit(G.disks.size(), 0);
     bool any = false;
     for (size_t i = 0; i < ns; i++) {
-        const double* x = q + 3 * (size_t)h->disk_surf[i];
-        for (size_t d = 0; d < h->disks.size(); d++) {
-            const auto& D = h->disks[d];
+        const double* x = q + 3 * (size_t)G.surf[i];
+        for (size_t k = 0; k < G.disks.size(); k++) {
+            const auto& D = h->disks[G.disks[k]];
             if (disk_plane_dist(D, x) >= kDiskPlaneThreshold) continue;
             if (disk_radial_dist(D, x) > D.r + kDiskRadialThreshold) continue;
-            hit[d] = 1;
+            hit[k] = 1;
             any = true;
         }
     }
-    std::fill(h->disk_mask.begin(), h->disk_mask.end(), -1);
+    std::fill(G.mask.begin(), G.mask.end(), -1);
     if (!any) return;
     int active = 0;
-    for (size_t d = 0; d < h->disks.size(); d++) {
-        if (!hit[d]) continue;
+    for (size_t k = 0; k < G.disks.size(); k++) {
+        if (!hit[k]) continue;
+        const int d = G.disks[k];
         const auto& D = h->disks[d];
         for (size_t i = 0; i < ns; i++) {
-            const double* x = q + 3 * (size_t)h->disk_surf[i];
+            const double* x = q + 3 * (size_t)G.surf[i];
             const double pd = disk_plane_dist(D, x);
             if (pd > kDiskPlaneThreshold || pd < -depth) continue;
             if (disk_radial_dist(D, x) > D.r + kDiskRadialThreshold) continue;
-            int& slot = h->disk_mask[i];
-            if (slot == -1) { slot = (int)d; active++; }
-            else if (fabs(pd) < fabs(disk_plane_dist(h->disks[slot], x))) slot = (int)d;
+            int& slot = G.mask[i];
+            if (slot == -1) { slot = d; active++; }
+            else if (fabs(pd) < fabs(disk_plane_dist(h->disks[slot], x))) slot = d;
         }
     }
-    if (active > 0) h->disk_frozen = true;
+    if (active > 0) G.frozen = true;
+}
+
+void update_disk_contacts(SorsHandle* h, const double* q) {
+    for (auto& G : h->disk_groups) update_disk_group(h, G, q);
 }
 
 int ensure_sqp_buffers(SorsHandle* h, int m) {
@@ -781,8 +791,9 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
     };
     for (size_t i = 0; i < h->plane_mask.size(); i++)
         if (h->plane_mask[i] >= 0) add(h->plane_surf[i], h->planes[h->plane_mask[i]].p, h->planes[h->plane_mask[i]].n);
-    for (size_t i = 0; i < h->disk_mask.size(); i++)
-        if (h->disk_mask[i] >= 0) add(h->disk_surf[i], h->disks[h->disk_mask[i]].c, h->disks[h->disk_mask[i]].n);
+    for (const auto& G : h->disk_groups)
+        for (size_t i = 0; i < G.mask.size(); i++)
+            if (G.mask[i] >= 0) add(G.surf[i], h->disks[G.mask[i]].c, h->disks[G.mask[i]].n);
     const int m = (int)cnode.size();
     h->last_active = m;
     if ((st = ensure_sqp_buffers(h, m))) return st;
@@ -1315,9 +1326,30 @@ int sors_set_disk_contact(SorsHandle* h, const double* centers, const double* no
     }
     for (int i = 0; i < n_surface; i++)
         if (surface_vertices[i] < 0 || surface_vertices[i] >= h->N) return fail(SORS_ERR_ARG, "surface vertex out of range");
-    h->disk_surf.assign(surface_vertices, surface_vertices + n_surface);
-    h->disk_mask.assign(n_surface, -1);
-    h->disk_frozen = false;
+    h->disk_groups.assign(1, SorsHandle::DiskGroup{});
+    auto& G = h->disk_groups[0];
+    for (int k = 0; k < n_disks; k++) G.disks.push_back(k);
+    G.surf.assign(surface_vertices, surface_vertices + n_surface);
+    G.mask.assign(n_surface, -1);
+    return SORS_OK;
+}
+
+int sors_set_disk_contact_groups(SorsHandle* h, const double* centers, const double* normals, const double* radii,
+                                 int32_t n_disks, const int32_t* surface_vertices, const int32_t* surface_ptr) {
+    if (!h || !surface_ptr || (n_disks > 0 && (!centers || !normals || !radii))) return fail(SORS_ERR_ARG, "NULL argument");
+    const int total = n_disks > 0 ? surface_ptr[n_disks] : 0;
+    if (total > 0 && !surface_vertices) return fail(SORS_ERR_ARG, "NULL argument");
+    for (int k = 0; k < n_disks; k++)
+        if (surface_ptr[k] > surface_ptr[k + 1] || surface_ptr[k] < 0) return fail(SORS_ERR_ARG, "surface_ptr not monotone");
+    int st = sors_set_disk_contact(h, centers, normals, radii, n_disks, surface_vertices, total);
+    if (st) return st;
+    h->disk_groups.assign(n_disks, SorsHandle::DiskGroup{});
+    for (int k = 0; k < n_disks; k++) {
+        auto& G = h->disk_groups[k];
+        G.disks = {k};
+        G.surf.assign(surface_vertices + surface_ptr[k], surface_vertices + surface_ptr[k + 1]);
+        G.mask.assign(G.surf.size(), -1);
+    }
     return SORS_OK;
 }
 
@@ -1347,19 +1379,28 @@ int32_t sors_held_contacts(SorsHandle* h, int32_t* nodes, double* normals, int32
 
 int32_t sors_get_contact_state(SorsHandle* h, int32_t* state, int32_t cap) {
     if (!h) return 0;
-    const int k = 1 + (int)h->disk_mask.size();
+    int k = 0;
+    for (const auto& G : h->disk_groups) k += 1 + (int)G.mask.size();
     if (state && cap >= k) {
-        state[0] = h->disk_frozen ? 1 : 0;
-        for (size_t i = 0; i < h->disk_mask.size(); i++) state[1 + i] = h->disk_mask[i];
+        int o = 0;
+        for (const auto& G : h->disk_groups) {
+            state[o++] = G.frozen ? 1 : 0;
+            for (int m : G.mask) state[o++] = m;
+        }
     }
     return k;
 }
 
 int sors_set_contact_state(SorsHandle* h, const int32_t* state, int32_t n) {
-    if (!h || !state) return fail(SORS_ERR_ARG, "NULL argument");
-    if (n != 1 + (int)h->disk_mask.size()) return fail(SORS_ERR_ARG, "contact state size mismatch");
-    h->disk_frozen = state[0] != 0;
-    for (size_t i = 0; i < h->disk_mask.size(); i++) h->disk_mask[i] = state[1 + i];
+    if (!h || (n > 0 && !state)) return fail(SORS_ERR_ARG, "NULL argument");
+    int k = 0;
+    for (const auto& G : h->disk_groups) k += 1 + (int)G.mask.size();
+    if (n != k) return fail(SORS_ERR_ARG, "contact state size mismatch");
+    int o = 0;
+    for (auto& G : h->disk_groups) {
+        G.frozen = state[o++] != 0;
+        for (auto& m : G.mask) m = state[o++];
+    }
     return SORS_OK;
 }
 

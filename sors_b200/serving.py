@@ -1,16 +1,25 @@
 """Rollout serving: many independent rollouts resident on one GPU.
 
 Requests (a mesh, its material, boundary conditions and a number of steps)
-arrive at any time.  The server admits a request when a slot is free and its
-estimated device footprint fits the memory budget; every admitted rollout
-keeps its mesh, state and Hessian pattern resident in its own library handle
-(one CUDA stream each) and is stepped by a worker thread, so the steps of
-different rollouts overlap on the device.  When a rollout finishes its slot
-and memory are released and the next waiting request is admitted at once
-(continuous admission).  Per-step and per-rollout latencies are recorded.
+arrive at any time.  The server admits work when a slot is free and its
+estimated device footprint fits the memory budget (continuous admission).
 
-The library calls release the GIL (ctypes), so worker threads really run
-their steps concurrently.
+Batching: compatible requests waiting at admission time (same element type,
+step count, dt, scheme, precision, gravity and planes) are packed into one
+union mesh, up to `batch_max` requests and `batch_elems` elements: one library
+handle whose nodes and elements are the concatenation of theirs.  The meshes
+share no element, so the union's gradient, Hessian and contact constraints are
+the direct sum of theirs; one Newton / SQP iteration, one PCG kernel sequence
+and one captured CUDA graph per chunk then serve all of them at once (each
+kernel launch does the work of the whole batch).  Each rollout keeps its own
+disk indenter (an independent disk contact group).  Results are sliced back
+per request; they equal the rollout run alone up to the solver tolerances
+(the Krylov iterates of the union differ from those of each mesh alone).
+
+Every admitted batch keeps its union mesh, state and Hessian pattern resident
+in its own handle (one CUDA stream) and is stepped by a worker thread, so the
+batches overlap on the device.  Per-step and per-rollout latencies are
+recorded per request.  The library calls release the GIL (ctypes).
 """
 from __future__ import annotations
 
@@ -60,6 +69,7 @@ class RolloutResult:
     newton_iters: int
     pcg_iters: int
     error: str | None = None
+    batch: int = 1            # requests stepped together in one union handle
 
 
 def estimate_device_bytes(n_nodes: int, n_elems: int, nodes_per_elem: int, precision: str) -> int:
@@ -84,9 +94,13 @@ def estimate_device_bytes(n_nodes: int, n_elems: int, nodes_per_elem: int, preci
 class RolloutServer:
     """Continuous-admission server for independent rollouts on one GPU."""
 
-    def __init__(self, max_slots: int = 8, memory_budget_bytes: int | None = None, device: int = 0):
+    def __init__(self, max_slots: int = 8, memory_budget_bytes: int | None = None, device: int = 0,
+                 batch_max: int = 1, batch_elems: int = 2_000_000):
         import torch
         self.device = device
+        self.batch_max = max(1, int(batch_max))
+        self.batch_elems = int(batch_elems)
+        self._held: list[RolloutRequest] = []
         if memory_budget_bytes is None:
             free, _total = torch.cuda.mem_get_info(device)
             memory_budget_bytes = int(free * 0.8)
@@ -122,74 +136,176 @@ class RolloutServer:
         return list(self._results)
 
     # -- internals ----------------------------------------------------------
+    def _next(self, block: bool):
+        if self._held:
+            return self._held.pop(0)
+        try:
+            return self._pending.get(block=block)
+        except queue.Empty:
+            return False
+
     def _dispatch(self):
+        closing = False
         while True:
-            req = self._pending.get()
+            if closing:
+                if not self._held:
+                    return
+                req = self._held.pop(0)
+            else:
+                req = self._next(block=True)
             if req is None:
-                return
-            need = estimate_device_bytes(req.vertices.shape[0], req.elements.shape[0], req.elements.shape[1],
-                                         req.precision)
+                closing = True
+                continue
+            batch = [req]
+            if self.batch_max > 1:
+                # pack compatible requests that are waiting now (no waiting for new arrivals)
+                rest = []
+                while len(batch) < self.batch_max:
+                    nxt = self._held.pop(0) if (closing and self._held) else (False if closing else self._next(False))
+                    if nxt is False:
+                        break
+                    if nxt is None:
+                        closing = True
+                        break
+                    if (compatible(batch[0], nxt) and
+                            sum(r.elements.shape[0] for r in batch) + nxt.elements.shape[0] <= self.batch_elems):
+                        batch.append(nxt)
+                    else:
+                        rest.append(nxt)
+                self._held = rest + self._held
+            need = sum(estimate_device_bytes(r.vertices.shape[0], r.elements.shape[0], r.elements.shape[1],
+                                             r.precision) for r in batch)
             if need > self.budget:
-                self._results.append(RolloutResult(req.tag, None, [], 0.0, 0.0, 0, 0,
-                                                   error=f"rollout needs ~{need} bytes, budget is {self.budget}"))
+                for r in batch:
+                    self._results.append(RolloutResult(r.tag, None, [], 0.0, 0.0, 0, 0,
+                                                       error=f"rollout needs ~{need} bytes, budget is {self.budget}"))
                 continue
             with self._lock:
                 while self._active >= self.max_slots or self._in_use + need > self.budget:
                     self._lock.wait()
                 self._active += 1
                 self._in_use += need
-            t = threading.Thread(target=self._run, args=(req, need), daemon=True)
+            t = threading.Thread(target=self._run, args=(batch, need), daemon=True)
             self._threads.append(t)
             t.start()
 
-    def _run(self, req: RolloutRequest, need: int):
+    def _run(self, batch, need: int):
         import torch
         torch.cuda.set_device(self.device)
         started = time.perf_counter()
         steps_lat = []
         newton = pcg = 0
-        final = None
+        finals = [None] * len(batch)
         err = None
         try:
-            en, sol = build_rollout(req, self.device)
-            disk = None
-            if req.disks is not None:
-                disk = ps.get_disk_contact_constraint(en, en._constraints.index("diskContact"))
-                c0 = np.asarray(req.disks[0], float).reshape(-1, 3)
-                nrm = np.asarray(req.disks[1], float).reshape(-1, 3)
-                rad = np.asarray(req.disks[2], float).ravel()
-                vel = np.zeros_like(c0) if req.disk_velocity is None else np.asarray(req.disk_velocity,
-                                                                                       float).reshape(-1, 3)
-            q = np.ascontiguousarray(req.vertices, dtype=np.float64).ravel().copy()
-            for t in range(req.steps):
+            en, sol, slices, disks = build_union(batch, self.device)
+            ref = batch[0]
+            q = np.concatenate([np.ascontiguousarray(r.vertices, dtype=np.float64).ravel() for r in batch])
+            for t in range(ref.steps):
                 t0 = time.perf_counter()
-                if disk is not None:
-                    for d in range(c0.shape[0]):
-                        disk.set_disk(c0[d] + vel[d] * req.dt * t, nrm[d], rad[d], d)
+                for d, (c0, nrm, rad, vel) in enumerate(disks):
+                    _lib_set_disk(en, d, c0 + vel * ref.dt * t, nrm, rad)
                 q = sol.step(q, en)
                 steps_lat.append(time.perf_counter() - t0)
                 newton += sol.last_stats.newton_iters
                 pcg += sol.last_stats.pcg_iters
-            final = q
+            finals = [q[a:b].copy() for a, b in slices]
             del en
         except Exception as ex:  # reported per rollout, the server keeps running
             err = str(ex)
         done = time.perf_counter()
-        self._results.append(RolloutResult(req.tag, final, steps_lat, started - req.submitted, done - req.submitted,
-                                           newton, pcg, err))
+        for r, f in zip(batch, finals):
+            self._results.append(RolloutResult(r.tag, f, list(steps_lat), started - r.submitted, done - r.submitted,
+                                               newton, pcg, err, batch=len(batch)))
         with self._lock:
             self._active -= 1
             self._in_use -= need
             self._lock.notify_all()
 
 
-def build_rollout(req: RolloutRequest, device: int = 0):
+def compatible(a: RolloutRequest, b: RolloutRequest) -> bool:
+    """Requests that can share one union handle."""
+    def planes_key(r):
+        return None if r.planes is None else (np.asarray(r.planes[0], float).tobytes(),
+                                              np.asarray(r.planes[1], float).tobytes())
+    return (a.elements.shape[1] == b.elements.shape[1] and a.steps == b.steps and a.dt == b.dt and
+            a.scheme == b.scheme and a.precision == b.precision and tuple(a.gravity) == tuple(b.gravity) and
+            planes_key(a) == planes_key(b) and (a.disks is None) == (b.disks is None) and
+            (a.neumann_mask is None) == (b.neumann_mask is None) and a.newton_res_tol == b.newton_res_tol)
+
+
+def _lib_set_disk(en, d, c, n, r):
+    import ctypes as C
+    from . import _lib
+    c = np.ascontiguousarray(c, dtype=np.float64); n = np.ascontiguousarray(n, dtype=np.float64)
+    _lib.check(_lib.load().sors_set_disk(en._h, int(d), c.ctypes.data_as(C.POINTER(C.c_double)),
+                                         n.ctypes.data_as(C.POINTER(C.c_double)), float(r)))
+
+
+def build_union(batch, device: int = 0):
+    """One Energy/Solver over the union of the batch's meshes.
+
+    Returns (energy, solver, slices, disks): slices[k] = (a, b) DOF range of
+    request k; disks: (center0, normal, radius, velocity) per disk, in the
+    order of the handle's disk contact groups."""
+    import ctypes as C
+    from . import _lib
+    if len(batch) == 1 and batch[0].disks is None:
+        en, sol = build_rollout(batch[0], device)
+        return en, sol, [(0, batch[0].vertices.size)], []
+    ref = batch[0]
+    offs = np.cumsum([0] + [r.vertices.shape[0] for r in batch])
+    X = np.concatenate([np.asarray(r.vertices, float) for r in batch])
+    T = np.concatenate([np.asarray(r.elements, np.int32) + offs[k] for k, r in enumerate(batch)])
+    bc = lambda v, r: np.broadcast_to(np.asarray(v, float), (r.elements.shape[0],))
+    rho = np.concatenate([bc(r.density, r) for r in batch])
+    E = np.concatenate([bc(r.youngs, r) for r in batch])
+    nu = np.concatenate([bc(r.poisson, r) for r in batch])
+    mask = val = None
+    if ref.neumann_mask is not None:
+        mask = np.concatenate([np.asarray(r.neumann_mask).ravel() for r in batch])
+        val = np.concatenate([np.asarray(r.neumann_value, float).ravel() for r in batch])
+    surf = None
+    if ref.surface is not None:
+        surf = np.concatenate([np.asarray(r.surface) + offs[k] for k, r in enumerate(batch)])
+    union = RolloutRequest(X, T, rho, E, nu, ref.steps, ref.dt, gravity=ref.gravity, neumann_mask=mask,
+                           neumann_value=val, precision=ref.precision, scheme=ref.scheme,
+                           newton_res_tol=ref.newton_res_tol, planes=ref.planes, disks=None, surface=surf)
+    en, sol = build_rollout(union, device, sqp=ref.planes is not None or ref.disks is not None)
+    disks = []
+    if ref.disks is not None:
+        cen, nrm, rad, ptr, dsurf = [], [], [], [0], []
+        for k, r in enumerate(batch):
+            c0 = np.asarray(r.disks[0], float).reshape(-1, 3)
+            nn = np.asarray(r.disks[1], float).reshape(-1, 3)
+            rr = np.asarray(r.disks[2], float).ravel()
+            vel = (np.zeros_like(c0) if r.disk_velocity is None
+                   else np.asarray(r.disk_velocity, float).reshape(-1, 3))
+            s_k = np.asarray(r.surface, np.int32) + offs[k]
+            for d in range(c0.shape[0]):
+                cen.append(c0[d]); nrm.append(nn[d]); rad.append(rr[d])
+                dsurf.append(s_k); ptr.append(ptr[-1] + s_k.size)
+                disks.append((c0[d], nn[d], rr[d], vel[d]))
+        cen = np.ascontiguousarray(cen, dtype=np.float64); nrm = np.ascontiguousarray(nrm, dtype=np.float64)
+        rad = np.ascontiguousarray(rad, dtype=np.float64)
+        dsurf = np.ascontiguousarray(np.concatenate(dsurf), dtype=np.int32)
+        ptr = np.ascontiguousarray(ptr, np.int32)
+        dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int32))
+        _lib.check(_lib.load().sors_set_disk_contact_groups(en._h, dp(cen), dp(nrm), dp(rad), len(disks), ip(dsurf),
+                                                            ip(ptr)))
+        en._constraints = list(en._constraints) + ["diskContact"]
+    slices = [(3 * offs[k], 3 * offs[k + 1]) for k in range(len(batch))]
+    return en, sol, slices, disks
+
+
+def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None):
     """Energy and Solver for one request (the reference-style py_sors objects)."""
     s = ps.SimulationSettings()
     s.meshType = "Tetrahedron" if req.elements.shape[1] == 4 else "Hexahedron"
     s.dt = req.dt
     s.timeSteppingScheme = req.scheme
-    contact = req.planes is not None or req.disks is not None
+    contact = (req.planes is not None or req.disks is not None) if sqp is None else sqp
     s.solverMethod = "minimize_SQP" if contact else "minimize_newton"
     s.precision = req.precision
     s.newtonResidualTol = 0.0 if contact else req.newton_res_tol
@@ -213,7 +329,8 @@ def build_rollout(req: RolloutRequest, device: int = 0):
             cp.set_param("diskCenterVectorList", np.asarray(req.disks[0], float).ravel())
             cp.set_param("diskNormalVectorList", np.asarray(req.disks[1], float).ravel())
             cp.set_param("diskRadiusList", np.asarray(req.disks[2], float).ravel())
-        cp.set_param("surfaceVerticesIdx", np.asarray(req.surface, float).ravel())
+        if req.surface is not None:
+            cp.set_param("surfaceVerticesIdx", np.asarray(req.surface, float).ravel())
         en._setup_constraints_forces(types, cp, (), None)
     return en, ps.Solver(s)
 

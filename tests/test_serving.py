@@ -69,3 +69,34 @@ def test_served_poke_matches_oracle(precision):
     disp = np.abs(q - req.vertices.ravel()).max()
     err = np.abs(res.final - q).max()
     assert err <= (1e-8 if precision == "fp64" else 1e-6 * disp), (err, disp)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batched_equals_alone(precision):
+    # six pokes packed into one union handle against each run alone
+    from sors_b200.serving import RolloutServer, poke_cube_request
+
+    def reqs():
+        rng = np.random.default_rng(8)
+        return [poke_cube_request(rng, int(rng.integers(3, 7)), tag=i, steps=6, dt=1e-2, precision=precision)
+                for i in range(6)]
+    alone = {}
+    for r in reqs():
+        srv = RolloutServer(max_slots=1)
+        srv.submit(r)
+        res = srv.close()[0]
+        assert res.error is None, res.error
+        alone[r.tag] = res.final
+    rs = reqs()
+    srv = RolloutServer(max_slots=2, batch_max=6)
+    for r in rs:
+        srv.submit(r)
+    out = {r.tag: r for r in srv.close()}
+    assert sorted(out) == sorted(alone)
+    assert max(r.batch for r in out.values()) > 1
+    for tag, res in out.items():
+        assert res.error is None, res.error
+        disp = np.abs(alone[tag] - rs[tag].vertices.ravel()).max()
+        err = np.abs(res.final - alone[tag]).max()
+        # FP64: within the SQP stopping tolerance ||dx|| < 1e-9 m; mixed: 1e-6 of the displacement
+        assert err <= (1e-9 if precision == "fp64" else 1e-6 * disp), (tag, err, disp)
