@@ -47,7 +47,9 @@ typedef struct SorsSettings {
     int32_t precision;       /* 0: FP64 everywhere; 1: FP32 Hessian + PCG, FP64
                                 residual, energy, dots and log(J)                */
     int32_t project_spd;     /* 1: clamp negative eigenvalues of dP/dF per
-                                quadrature point before assembly                  */
+                                quadrature point before assembly; 0: exact
+                                Hessian; 2 (default): exact, and projected for
+                                an iteration whose PCG met negative curvature    */
     int32_t material;        /* 0 "neohookean"; 1 the reference's quartic test
                                 element (cpp/src/_test.cpp:8-66)                 */
     double newton_dx_tol;    /* ||dx|| stop, reference DX_TOL = 1e-9              */

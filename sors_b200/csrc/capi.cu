@@ -145,6 +145,9 @@ struct SorsHandle {
     bool graph_failed = false;
 
     double prev_gnorm = -1.0;
+    // project_spd == 2: the exact Hessian first, the projected one for this
+    // iteration after PCG met negative curvature
+    bool proj_fallback = false;
 };
 
 namespace {
@@ -369,9 +372,9 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
     a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
-    a.H = (HT*)h->H; a.g_int = h->g_int; a.status = h->status;
+    a.H = (HT*)h->H; a.nnzb = h->nnzb; a.g_int = h->g_int; a.status = h->status;
     a.stage_per_warp = h->max_pairs * h->nv * 9;
-    a.material = h->s.material; a.project = h->s.project_spd;
+    a.material = h->s.material; a.project = h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd;
     a.apply_mask = mode == kAsmFull ? 0 : 1;
     a.neumann_override = mode == kAsmFull ? 0
                          : ((mode == kAsmMaskedIdentity || method(h) == 0) && h->has_neumann) ? 1 : 0;
@@ -384,7 +387,7 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
         p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
         p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
         p.f_ext = h->f_ext;
-        launch_pressure_jac<HT>(p, h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->stream);
+        launch_pressure_jac<HT>(p, h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->nnzb, h->stream);
     }
     launch_finalize_grad(h->N, h->g_int, h->f_ext, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, h->mass,
                          h->node_mask, h->mval, dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav,
@@ -409,11 +412,11 @@ int eval_energy(SorsHandle* h, double dt, double* out) {
 template <typename HT, typename VT>
 void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
-    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
                           h->proj_n, h->partials, h->sc, h->stream);
-    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
                           h->proj_n, h->partials, h->sc, h->stream);
@@ -459,7 +462,7 @@ int pcg_chunk(SorsHandle* h) {
 // Returns PCG iterations in *iters.
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
-    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, g ? g : h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0,
                             eta * eta, abs_tol * abs_tol, h->s.pcg_max_iter, h->proj_flag, h->proj_n, h->partials,
                             h->sc, h->stream);
@@ -473,7 +476,7 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
         if (h->sc_host->done) break;
     }
     *iters = h->sc_host->it;
-    if (h->sc_host->breakdown && h->sc_host->it == 0)
+    if (h->sc_host->breakdown && h->sc_host->it == 0 && !(h->s.project_spd == 2 && !h->proj_fallback))
         return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
     return SORS_OK;
 }
@@ -551,7 +554,7 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     CK(d2h(h, ge.data(), h->adj_e, sizeof(double) * 2 * (size_t)E));
     std::vector<double> r(n, 0.0);
     if (h->has_neumann) {
-        launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->adj_l, h->adj_y, h->stream);
+        launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->adj_l, h->adj_y, h->stream);
         CK(d2h(h, r.data(), h->adj_y, sizeof(double) * n));
         for (int i = 0; i < n; i++) r[i] = b[i] - r[i];
     }
@@ -588,6 +591,7 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     bool have_hess = false;
     for (int it = 0; it < h->s.newton_max_iter; it++) {
         bool want_hess = (m != 2) || !have_hess;  // frozen Hessian: assemble once
+        if (want_hess) h->proj_fallback = (m == 2);  // adaptive: the frozen Hessian is the projected one
         if ((st = eval_system<HT>(h, dt, want_hess))) return st;
         if (want_hess) have_hess = true;
         CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
@@ -616,6 +620,13 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         int pit = 0;
         if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
         if (stats) stats->pcg_iters += pit;
+        if (h->s.project_spd == 2 && !h->proj_fallback && h->sc_host->breakdown) {
+            // negative curvature in the exact Hessian: solve this iteration with the projected one
+            h->proj_fallback = true;
+            if ((st = eval_system<HT>(h, dt, true))) return st;
+            if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
+            if (stats) stats->pcg_iters += pit;
+        }
         if (m == 1) {
             // Armijo backtracking (solver.cpp:201-264): c = 0.1, beta = 0.5
             CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
@@ -806,8 +817,19 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
     if (h->has_neumann)
         for (int v = 0; v < N; v++) h->pflag_h[v] = h->mask_h[v] & 7u;
     bool converged = false;
-    const double eta = mixed(h) ? std::max(h->s.pcg_rel_tol, 1e-6) : h->s.pcg_rel_tol;
+    // forcing: loose while the step is far from converged, tightened with the
+    // squared contraction of ||dx|| (Eisenstat-Walker choice 2 on ||dx||)
+    const double eta_min = mixed(h) ? std::max(h->s.pcg_rel_tol, 1e-6) : h->s.pcg_rel_tol;
+    double eta = 1e-4, dx_prev = -1.0, dx_prev2 = -1.0;
     for (int it = 0; it < h->s.newton_max_iter; it++) {
+        h->proj_fallback = false;
+        if (dx_prev > 0.0 && dx_prev2 > 0.0) {
+            const double ratio = dx_prev / dx_prev2;
+            eta = std::min(1e-4, 0.9 * ratio * ratio);
+        }
+        eta = std::max(eta, eta_min);
+        if (dx_prev > 0.0 && dx_prev < 1e3 * h->s.newton_dx_tol) eta = eta_min;  // the last iterations solve tight
+        double abs_tol = 0.0;   // set by the first (cold) solve of this iteration
         if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
         launch_gather_nodes(m, h->cnode_d, h->q, h->cpos_d, h->stream);
         if (m) CK(d2h(h, xc.data(), h->cpos_d, sizeof(double) * 3 * m));
@@ -823,7 +845,9 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
         }
         if (m) CK(h2d(h, h->cnb_d, cnb.data(), sizeof(double4) * m));
         if (stats) { stats->newton_iters++; stats->residual_norm = sqrt(h->sc_host->gnorm2); }
+        int inner_used = 0, pcg_used = 0, adds = 0, drops = 0;
         for (int inner = 0; inner < 25; inner++) {
+            inner_used++;
             for (int c = 0; c < m; c++) {
                 const int v = cnode[c];
                 h->pflag_h[v] = (uint8_t)((h->pflag_h[v] & 7u) | (inW[c] ? 8u : 0u));
@@ -831,20 +855,33 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
             }
             CK(h2d(h, h->pflag_d, h->pflag_h.data(), (size_t)N));
             if (m) CK(h2d(h, h->pn_d, h->pn_h.data(), sizeof(double4) * N));
-            launch_qp_x0(N, h->pflag_d, h->pn_d, h->q, h->qPrev, h->mval, dt, h->qp_x0, h->stream);
-            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->qp_x0, h->qp_y, h->stream);
+            // particular solution: the constraints alone on the first solve, the
+            // previous step with the new working set imposed on re-solves
+            if (inner == 0) launch_qp_x0(N, h->pflag_d, h->pn_d, h->q, h->qPrev, h->mval, dt, h->qp_x0, h->stream);
+            else launch_qp_warm(N, h->pflag_d, h->pn_d, h->q, h->qPrev, h->mval, dt, h->qp_dx, h->qp_x0, h->stream);
+            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->qp_x0, h->qp_y, h->stream);
             launch_add_vec<double>(n, h->g, h->qp_y, h->qp_g2, h->stream);
             h->proj_flag = h->pflag_d;
             h->proj_n = h->pn_d;
             int pit = 0;
-            st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
+            // re-solves stop at the accuracy the cold solve asked for, in absolute terms
+            st = pcg_solve<HT, VT>(h, inner == 0 ? eta : 0.0, abs_tol, &pit, h->qp_g2);
+            if (inner == 0) abs_tol = eta * sqrt(h->sc_host->bnorm2);
             h->proj_flag = nullptr;
             h->proj_n = nullptr;
             if (st) return st;
             if (stats) stats->pcg_iters += pit;
+            pcg_used += pit;
+            if (h->s.project_spd == 2 && !h->proj_fallback && h->sc_host->breakdown) {
+                // negative curvature in the exact Hessian: redo with the projected one
+                h->proj_fallback = true;
+                if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
+                inner--;
+                continue;
+            }
             launch_add_vec<VT>(n, h->qp_x0, (const VT*)h->x, h->qp_dx, h->stream);
             if (m == 0) break;
-            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->qp_dx, h->qp_y, h->stream);
+            launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->qp_dx, h->qp_y, h->stream);
             launch_qp_check(m, h->cnode_d, h->cnb_d, h->qp_dx, h->qp_y, h->g, h->cout_d, h->stream);
             CK(d2h(h, chk.data(), h->cout_d, sizeof(double) * 2 * m));
             double mu_scale = 0.0, b_scale = 0.0;
@@ -855,17 +892,47 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
             const double tol_s = 1e-12 + 1e-9 * b_scale, tol_mu = 1e-14 + 1e-8 * mu_scale;
             bool changed = false;
             for (int c = 0; c < m; c++) {
-                if (!inW[c] && chk[c] < -tol_s) { inW[c] = 1; changed = true; }
-                else if (inW[c] && chk[m + c] < -tol_mu) { inW[c] = 0; changed = true; }
+                if (!inW[c] && chk[c] < -tol_s) { inW[c] = 1; changed = true; adds++; }
+                else if (inW[c] && chk[m + c] < -tol_mu) { inW[c] = 0; changed = true; drops++; }
             }
             if (!changed) break;
         }
         CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
-        launch_newton_update<double>(n, h->qp_dx, 1.0, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+        double alpha = 1.0;
+        if (it >= 1 && h->proj_fallback) {
+            // A step from the projected Hessian (the exact one had negative
+            // curvature) is a descent direction but not a Newton step: backtrack
+            // on the energy (Armijo, c = 1e-4, halving), as full steps can cycle.
+            // The held constraints are satisfied after the first iteration and
+            // are linear, so every alpha in (0, 1] keeps them.
+            double e0, e1;
+            launch_dot_gdx<double>(n, h->g, h->qp_dx, h->partials, h->sc, h->stream);
+            if ((st = eval_energy(h, dt, &e0))) return st;
+            const double gdx = h->sc_host->gdx;
+            if (gdx < 0.0) {
+                for (int ls = 0; ls < 20; ls++) {
+                    launch_newton_update<double>(n, h->qp_dx, alpha, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+                    if ((st = eval_energy(h, dt, &e1))) return st;
+                    if (e1 <= e0 + 1e-4 * alpha * gdx) break;
+                    alpha *= 0.5;
+                }
+            }
+        }
+        launch_newton_update<double>(n, h->qp_dx, alpha, h->q, h->q0, h->partials, h->sc, 6, h->stream);
         CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        const double dxn = sqrt(h->sc_host->dxnorm2);
+        // convergence is judged on the full step, as the reference does
+        const double dxn = sqrt(h->sc_host->dxnorm2) / alpha;
+        dx_prev2 = dx_prev;
+        dx_prev = dxn;
         if (stats) stats->dx_norm = dxn;
+        if (verbose()) {
+            int held = 0;
+            for (int c = 0; c < m; c++) held += inW[c];
+            fprintf(stderr, "sqp it %d |g| %.3e dx %.3e alpha %.3f contacts %d held %d inner %d (+%d -%d) pcg %d eta %.1e%s\n",
+                    it, sqrt(h->sc_host->gnorm2), dxn, alpha, m, held, inner_used, adds, drops, pcg_used, eta,
+                    h->proj_fallback ? " projected" : "");
+        }
         if (!(dxn == dxn)) break;  // "SQP method diverged"
         if (dxn < h->s.newton_dx_tol) { converged = true; break; }
     }
@@ -967,7 +1034,7 @@ void sors_default_settings(SorsSettings* s) {
     s->cfl = 0;
     s->damping_alpha = 0.0;
     s->precision = 0;
-    s->project_spd = 1;
+    s->project_spd = 2;
     s->material = 0;
     s->newton_dx_tol = 1e-9;
     s->newton_res_tol = 0.0;
@@ -1254,7 +1321,11 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
         CK(cudaMemcpyAsync(raw.data(), h->H, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
-    memcpy(val, raw.data(), n * sizeof(double));
+    // device storage is split (entries 0-7 of every block, then every entry 8);
+    // the ABI returns each block's 9 values contiguously
+    const size_t nb = (size_t)h->nnzb;
+    for (size_t b = 0; b < nb; b++)
+        for (int rc = 0; rc < 9; rc++) val[b * 9 + rc] = raw[hval(b, rc, nb)];
     int flag = 0;
     CK(d2h(h, &flag, h->status, sizeof(int)));
     if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
@@ -1507,8 +1578,8 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat; aa.mus = muscles(h);
     aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
     aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
-    aa.H = (HT*)h->H; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
-    aa.material = h->s.material; aa.project = h->s.project_spd; aa.apply_mask = 1;
+    aa.H = (HT*)h->H; aa.nnzb = h->nnzb; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
+    aa.material = h->s.material; aa.project = h->s.project_spd != 0; aa.apply_mask = 1;
     aa.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0; aa.want_hess = 1;
     aa.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0; aa.inertia_coef = inertia_coef(h, dt);
     CK(cudaEventRecord(a, h->stream));
@@ -1521,13 +1592,13 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
                           (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
     // PCG kernels on the assembled system
-    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, (VT*)h->Minv, h->stream);
+    launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,
                             1 << 30, nullptr, nullptr, h->partials, h->sc, h->stream);
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
-        launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
+        launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
                                 (VT*)(i & 1 ? h->p0 : h->p1), (VT*)h->qv, h->partials, h->sc, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));

@@ -338,7 +338,7 @@ __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_a
                     val += md;
                     if (a.neumann_override && rmask) val = 1.0;
                 }
-                a.H[(size_t)bg * 9 + rc] = (HT)val;
+                a.H[hval(bg, rc, a.nnzb)] = (HT)val;
             }
             __syncwarp();
         }
@@ -517,7 +517,7 @@ __device__ void face_hess(const int* f, int fnv, const double* q, double (*h)[9]
 // non-symmetric follower-load Jacobian enters as P(max(a,b), min(a,b)).
 template <typename HT>
 __global__ void k_pressure_jac(PressureArgs p, const int* row_ptr, const int* col, const uint8_t* node_mask,
-                               double cscale, HT* H) {
+                               double cscale, HT* H, long long nnzb) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= p.nsurf) return;
     int i = p.surf_nodes[s];
@@ -545,7 +545,7 @@ __global__ void k_pressure_jac(PressureArgs p, const int* row_ptr, const int* co
                     double val = 0.0;
                     if (a > b) val = h[kj][l * 3 + m];
                     else if (a < b) val = h[ki][m * 3 + l];
-                    if (val != 0.0) H[(size_t)slot * 9 + l * 3 + m] += (HT)(coef * val);
+                    if (val != 0.0) H[hval(slot, l * 3 + m, nnzb)] += (HT)(coef * val);
                 }
             }
         }
@@ -554,9 +554,9 @@ __global__ void k_pressure_jac(PressureArgs p, const int* row_ptr, const int* co
 
 template <typename HT>
 void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
-                         double cscale, HT* H, cudaStream_t st) {
+                         double cscale, HT* H, long long nnzb, cudaStream_t st) {
     if (p.nsurf == 0) return;
-    k_pressure_jac<HT><<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, row_ptr, col, node_mask, cscale, H);
+    k_pressure_jac<HT><<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, row_ptr, col, node_mask, cscale, H, nnzb);
     counted();
 }
 
@@ -656,14 +656,13 @@ void launch_dof_energy(int N, const double* q, const double* qPrev, const double
 // block-Jacobi preconditioner: inverse of each 3x3 diagonal block
 // ---------------------------------------------------------------------------
 template <typename HT, typename VT>
-__global__ void k_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv) {
+__global__ void k_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, long long nnzb,
+                               VT* Minv) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= N) return;
-    const int b0 = row_ptr[i], nb = row_ptr[i + 1] - b0;
-    const HT* b = H + (size_t)diag_slot[i] * 9;
-    (void)nb;
+    const size_t d = (size_t)diag_slot[i];
     double a[9], c[9];
-    for (int k = 0; k < 9; k++) a[k] = (double)b[k];
+    for (int k = 0; k < 9; k++) a[k] = (double)H[hval(d, k, nnzb)];
     // symmetric part: the lower triangle defines the operator
     a[1] = a[3]; a[2] = a[6]; a[5] = a[7];
     cof3(a, c);
@@ -679,9 +678,10 @@ __global__ void k_block_jacobi(int N, const int* row_ptr, const int* diag_slot, 
 }
 
 template <typename HT, typename VT>
-void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st) {
+void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, long long nnzb, VT* Minv,
+                         cudaStream_t st) {
     if (N == 0) return;
-    k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, row_ptr, diag_slot, H, Minv);
+    k_block_jacobi<HT, VT><<<(N + 255) / 256, 256, 0, st>>>(N, row_ptr, diag_slot, H, nnzb, Minv);
     counted();
 }
 
@@ -762,6 +762,31 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
     counted();
 }
 
+// One 3x3 block in split storage (hval): two 16-byte loads (FP32) or four
+// (FP64) for entries 0-7 and one scalar load for entry 8.
+template <typename HT, typename VT>
+__device__ __forceinline__ void load_block(const HT* __restrict__ H, size_t b, size_t nnzb, VT (&h)[9]);
+template <>
+__device__ __forceinline__ void load_block<float, float>(const float* __restrict__ H, size_t b, size_t nnzb,
+                                                         float (&h)[9]) {
+    const float4* m = reinterpret_cast<const float4*>(H) + 2 * b;
+    const float4 u = __ldg(m), w = __ldg(m + 1);
+    h[0] = u.x; h[1] = u.y; h[2] = u.z; h[3] = u.w;
+    h[4] = w.x; h[5] = w.y; h[6] = w.z; h[7] = w.w;
+    h[8] = __ldg(H + 8 * nnzb + b);
+}
+template <>
+__device__ __forceinline__ void load_block<double, double>(const double* __restrict__ H, size_t b, size_t nnzb,
+                                                           double (&h)[9]) {
+    const double2* m = reinterpret_cast<const double2*>(H) + 4 * b;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const double2 u = __ldg(m + k);
+        h[2 * k] = u.x; h[2 * k + 1] = u.y;
+    }
+    h[8] = __ldg(H + 8 * nnzb + b);
+}
+
 // q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q.
 // A group of LPR lanes owns one block-row: lane b of the group takes block b
 // of the row, loads its column and 9 values and gathers p_new(col) at once,
@@ -769,6 +794,7 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
 template <typename HT, typename VT, int LPR>
 __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __restrict__ row_ptr,
                                                            const int* __restrict__ col, const HT* __restrict__ H,
+                                                           long long nnzb,
                                                            const VT* __restrict__ z, const VT* __restrict__ p_old,
                                                            VT* __restrict__ p_new, VT* __restrict__ qv,
                                                            double* partials, DevScalars* sc) {
@@ -785,13 +811,12 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
         VT a0 = VT(0), a1 = VT(0), a2 = VT(0);
         if (row < N) {
             const int b0 = __ldg(row_ptr + row), b1 = __ldg(row_ptr + row + 1), nb = b1 - b0;
-            const HT* hrow = H + (size_t)b0 * 9;
             for (int s = sl; s < nb; s += LPR) {
                 const int j = __ldg(col + b0 + s);
-                const HT* v = hrow + (size_t)s * 9;
-                const VT h0 = (VT)__ldg(v), h1 = (VT)__ldg(v + 1), h2 = (VT)__ldg(v + 2);
-                const VT h3 = (VT)__ldg(v + 3), h4 = (VT)__ldg(v + 4), h5 = (VT)__ldg(v + 5);
-                const VT h6 = (VT)__ldg(v + 6), h7 = (VT)__ldg(v + 7), h8 = (VT)__ldg(v + 8);
+                VT hb[9];
+                load_block<HT, VT>(H, (size_t)(b0 + s), (size_t)nnzb, hb);
+                const VT h0 = hb[0], h1 = hb[1], h2 = hb[2], h3 = hb[3], h4 = hb[4], h5 = hb[5];
+                const VT h6 = hb[6], h7 = hb[7], h8 = hb[8];
                 const size_t jj = 3 * (size_t)j;
                 const VT p0 = __ldg(z + jj) + beta * __ldg(p_old + jj);
                 const VT p1 = __ldg(z + jj + 1) + beta * __ldg(p_old + jj + 1);
@@ -830,18 +855,19 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
 }
 
 template <typename HT, typename VT>
-void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, const VT* z,
-                     const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
+void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
+                     const VT* z, const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc,
+                     cudaStream_t st) {
     const int lpr = max_row_blocks <= 4 ? 4 : (max_row_blocks <= 8 ? 8 : (max_row_blocks <= 16 ? 16 : 32));
     const int rows_per_block = (kRedThreads / 32) * (32 / lpr);
     long long blocks = (N + rows_per_block - 1) / rows_per_block;
     if (blocks > kRedBlocks) blocks = kRedBlocks;
     if (blocks < 1) blocks = 1;
     switch (lpr) {
-        case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
-        case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
-        case 16: k_pcg_spmv<HT, VT, 16><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
-        default: k_pcg_spmv<HT, VT, 32><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, z, p_old, p_new, qv, partials, sc); break;
+        case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
+        case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
+        case 16: k_pcg_spmv<HT, VT, 16><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
+        default: k_pcg_spmv<HT, VT, 32><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
     }
     counted();
 }
@@ -970,16 +996,17 @@ void launch_predict(int n, double* q, const double* vPrev, double dt, cudaStream
 
 // y = H x (tests / diagnostics)
 template <typename HT>
-__global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y) {
+__global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, long long nnzb, const double* x,
+                             double* y) {
     int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (row >= N) return;
     int b0 = row_ptr[row], nval = (row_ptr[row + 1] - b0) * 9;
     double a[3] = {0, 0, 0};
-    // blocks are stored one after another, 3x3 row-major each
+    // t runs over (block of the row, entry of the block)
     for (int t = lane; t < nval; t += 32) {
         int blk = t / 9, rc = t - blk * 9, r = rc / 3, c = rc - r * 3;
-        double pr = (double)H[(size_t)b0 * 9 + t] * x[3 * (size_t)col[b0 + blk] + c];
+        double pr = (double)H[hval((size_t)b0 + blk, rc, nnzb)] * x[3 * (size_t)col[b0 + blk] + c];
         a[0] += r == 0 ? pr : 0.0; a[1] += r == 1 ? pr : 0.0; a[2] += r == 2 ? pr : 0.0;
     }
     warp_sum<3>(a);
@@ -987,10 +1014,10 @@ __global__ void k_spmv_plain(int N, const int* row_ptr, const int* col, const HT
 }
 
 template <typename HT>
-void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y,
-                       cudaStream_t st) {
+void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, long long nnzb, const double* x,
+                       double* y, cudaStream_t st) {
     if (N == 0) return;
-    k_spmv_plain<HT><<<(N + 7) / 8, 256, 0, st>>>(N, row_ptr, col, H, x, y);
+    k_spmv_plain<HT><<<(N + 7) / 8, 256, 0, st>>>(N, row_ptr, col, H, nnzb, x, y);
     counted();
 }
 
@@ -1019,6 +1046,41 @@ __global__ void k_qp_x0(int N, const uint8_t* __restrict__ pflag, const double4*
         }
 #pragma unroll
     for (int k = 0; k < 3; k++) x0[3 * (size_t)i + k] = x[k];
+}
+
+// Warm start for a re-solve after the working set changed: the previous step
+// dx with the constraints of the new working set imposed again (Neumann DOFs
+// at their target, held contact nodes moved to their bound along the normal,
+// tangential motion kept).
+__global__ void k_qp_warm(int N, const uint8_t* __restrict__ pflag, const double4* __restrict__ pn,
+                          const double* __restrict__ q, const double* __restrict__ qPrev,
+                          const double* __restrict__ mval, double dt, const double* __restrict__ dx_prev,
+                          double* __restrict__ x0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const unsigned f = pflag[i];
+    double x[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) x[k] = dx_prev[3 * (size_t)i + k];
+    if (f & 8u) {
+        const double4 n = pn[i];
+        const double d = n.w - (n.x * x[0] + n.y * x[1] + n.z * x[2]);
+        x[0] += d * n.x; x[1] += d * n.y; x[2] += d * n.z;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+        if ((f >> k) & 1u) {
+            const size_t ii = 3 * (size_t)i + k;
+            x[k] = -(q[ii] - qPrev[ii] - dt * mval[ii]);
+        }
+#pragma unroll
+    for (int k = 0; k < 3; k++) x0[3 * (size_t)i + k] = x[k];
+}
+
+void launch_qp_warm(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
+                    const double* mval, double dt, const double* dx_prev, double* x0, cudaStream_t st) {
+    k_qp_warm<<<(N + 255) / 256, 256, 0, st>>>(N, pflag, pn, q, qPrev, mval, dt, dx_prev, x0);
+    counted();
 }
 
 // out = a + b (b of the PCG vector type)
@@ -1088,21 +1150,24 @@ template void launch_elem_rows<float>(int, int, const double*, const double*, co
                                       const MuscleArgs&, int, int,
                                       double*, double*, double*, int*, cudaStream_t);
 template void launch_pressure_jac<double>(const PressureArgs&, const int*, const int*, const uint8_t*, double, double*,
-                                          cudaStream_t);
+                                          long long, cudaStream_t);
 template void launch_pressure_jac<float>(const PressureArgs&, const int*, const int*, const uint8_t*, double, float*,
-                                         cudaStream_t);
-template void launch_block_jacobi<double, double>(int, const int*, const int*, const double*, double*, cudaStream_t);
-template void launch_block_jacobi<float, float>(int, const int*, const int*, const float*, float*, cudaStream_t);
+                                         long long, cudaStream_t);
+template void launch_block_jacobi<double, double>(int, const int*, const int*, const double*, long long, double*,
+                                                  cudaStream_t);
+template void launch_block_jacobi<float, float>(int, const int*, const int*, const float*, long long, float*,
+                                                cudaStream_t);
 template void launch_pcg_init<double, double>(int, const double*, const double*, double*, double*, double*, double*,
                                               double, double, int, const uint8_t*, const double4*, double*,
                                               DevScalars*, cudaStream_t);
 template void launch_pcg_init<float, float>(int, const double*, const float*, float*, float*, float*, float*, double,
                                             double, int, const uint8_t*, const double4*, double*, DevScalars*,
                                             cudaStream_t);
-template void launch_pcg_spmv<double, double>(int, int, const int*, const int*, const double*, const double*,
-                                              const double*, double*, double*, double*, DevScalars*, cudaStream_t);
-template void launch_pcg_spmv<float, float>(int, int, const int*, const int*, const float*, const float*, const float*,
-                                            float*, float*, double*, DevScalars*, cudaStream_t);
+template void launch_pcg_spmv<double, double>(int, int, const int*, const int*, const double*, long long,
+                                              const double*, const double*, double*, double*, double*, DevScalars*,
+                                              cudaStream_t);
+template void launch_pcg_spmv<float, float>(int, int, const int*, const int*, const float*, long long, const float*,
+                                            const float*, float*, float*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_update<double>(int, const double*, const double*, const double*, double*, double*, double*,
                                         const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_update<float>(int, const float*, const float*, const float*, float*, float*, float*,
@@ -1113,9 +1178,9 @@ template void launch_newton_update<float>(int, const float*, double, double*, co
                                           cudaStream_t);
 template void launch_dot_gdx<double>(int, const double*, const double*, double*, DevScalars*, cudaStream_t);
 template void launch_dot_gdx<float>(int, const double*, const float*, double*, DevScalars*, cudaStream_t);
-template void launch_spmv_plain<double>(int, const int*, const int*, const double*, const double*, double*,
-                                        cudaStream_t);
-template void launch_spmv_plain<float>(int, const int*, const int*, const float*, const double*, double*,
+template void launch_spmv_plain<double>(int, const int*, const int*, const double*, long long, const double*,
+                                        double*, cudaStream_t);
+template void launch_spmv_plain<float>(int, const int*, const int*, const float*, long long, const double*, double*,
                                        cudaStream_t);
 
 }  // namespace sors

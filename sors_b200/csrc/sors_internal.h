@@ -47,6 +47,14 @@ struct MuscleArgs {
     const double* act = nullptr;
 };
 
+// Hessian value storage for nnzb 3x3 blocks: entries 0-7 of block b (row-major)
+// at H[8 b .. 8 b + 7], so a block is two 16-byte vector loads in FP32 (four
+// in FP64), and entry 8 at H[8 nnzb + b].  Same bytes as 9 contiguous values,
+// a third of the load instructions.
+__host__ __device__ __forceinline__ size_t hval(size_t b, int rc, size_t nnzb) {
+    return rc < 8 ? 8 * b + (size_t)rc : 8 * nnzb + b;
+}
+
 // Row-owner assembly arguments (tet or hex).
 template <typename HT>
 struct AsmArgs {
@@ -64,7 +72,8 @@ struct AsmArgs {
     const uint16_t* slot_items; // k*nv + w
     const uint8_t* node_mask;   // 3 bits per node
     const double* mass;     // per node
-    HT* H;                  // nnzb*9, row-major 3x3 blocks in CSR order
+    HT* H;                  // nnzb*9, blocks in CSR order, split storage (hval)
+    long long nnzb;
     double* g_int;          // 3N (masked element gradient)
     int* status;
     int stage_per_warp;     // HT elements per warp of staging
@@ -107,7 +116,7 @@ void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const 
                          const MuscleArgs& mus, const double* lam, double* out, cudaStream_t st);
 template <typename HT>
 void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
-                         double cscale, HT* H, cudaStream_t st);
+                         double cscale, HT* H, long long nnzb, cudaStream_t st);
 void launch_finalize_grad(int N, const double* g_int, const double* f_ext, const double* q, const double* qPrev,
                           const double* vPrev, const double* gPrev, double* gPrevTmp, const double* mass,
                           const uint8_t* mask, const double* mval, double dt, int scheme, double alpha,
@@ -117,19 +126,23 @@ void launch_dof_energy(int N, const double* q, const double* qPrev, const double
                        const double* f_ext, int has_ext, double dt, int scheme, double alpha, const double* grav,
                        double* partials, DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
-void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, VT* Minv, cudaStream_t st);
+void launch_block_jacobi(int N, const int* row_ptr, const int* diag_slot, const HT* H, long long nnzb, VT* Minv,
+                         cudaStream_t st);
 template <typename HT, typename VT>
 void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
                      double abs_tol2, int maxit, const uint8_t* pflag, const double4* pn, double* partials,
                      DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
-void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, const VT* z,
-                     const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
+                     const VT* z, const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc,
+                     cudaStream_t st);
 template <typename VT>
 void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, const uint8_t* pflag,
                        const double4* pn, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_qp_x0(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
                   const double* mval, double dt, double* x0, cudaStream_t st);
+void launch_qp_warm(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
+                    const double* mval, double dt, const double* dx_prev, double* x0, cudaStream_t st);
 template <typename VT>
 void launch_add_vec(int n, const double* a, const VT* b, double* out, cudaStream_t st);
 void launch_qp_check(int m, const int* cnode, const double4* cnb, const double* dx, const double* y,
@@ -146,7 +159,7 @@ void launch_predict(int n, double* q, const double* vPrev, double dt, cudaStream
 void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const double* vPrev, double* partials,
                 DevScalars* sc, cudaStream_t st);
 template <typename HT>
-void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, const double* x, double* y,
-                       cudaStream_t st);
+void launch_spmv_plain(int N, const int* row_ptr, const int* col, const HT* H, long long nnzb, const double* x,
+                       double* y, cudaStream_t st);
 
 }  // namespace sors

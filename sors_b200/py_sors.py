@@ -54,7 +54,9 @@ class SimulationSettings:
         self.numThreads = 1
         # device-solver options (no reference counterpart)
         self.precision = "fp64"            # "fp64" | "mixed"
-        self.hessianProjection = True      # SPD projection of dP/dF per quadrature point
+        # SPD projection of dP/dF per quadrature point: True always, False never,
+        # "adaptive" (default) the exact Hessian unless PCG meets negative curvature
+        self.hessianProjection = "adaptive"
         self.newtonResidualTol = 0.0       # absolute ||gradient|| stop; 0 = reference dx test only
         self.newtonDxTol = 1e-9            # reference DX_TOL (cpp/headers/common.h:25)
         self.newtonMaxIter = 100           # reference MAX_ITER (cpp/headers/common.h:21)
@@ -254,7 +256,8 @@ class _EnergyBase:
             s.grav[k] = float(g[k])
         s.damping_alpha = float(dampingAlpha)
         s.precision = 1 if getattr(settings, "precision", "fp64") == "mixed" else 0
-        s.project_spd = int(bool(getattr(settings, "hessianProjection", True)))
+        hp = getattr(settings, "hessianProjection", "adaptive")
+        s.project_spd = 2 if (isinstance(hp, str) and hp == "adaptive") else int(bool(hp))
         s.material = int(getattr(settings, "_material_override", self._material))
         s.newton_dx_tol = float(getattr(settings, "newtonDxTol", 1e-9))
         s.newton_res_tol = float(getattr(settings, "newtonResidualTol", 0.0))
@@ -372,7 +375,7 @@ class _EnergyBase:
         q = self._q(q)
         n = 3 * self.NV
         psi = np.empty(self.numElements); g = np.empty((self.numElements, n)); H = np.empty((self.numElements, n, n))
-        proj = int(self._settings_c.project_spd if project is None else bool(project))
+        proj = int(self._settings_c.project_spd == 1) if project is None else int(bool(project))
         _lib.check(_lib.load().sors_elem_eval(self._h, _p(q, C.c_double), proj, _p(psi, C.c_double),
                                               _p(g, C.c_double), _p(H, C.c_double)))
         return psi, g, H

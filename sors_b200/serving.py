@@ -4,9 +4,10 @@ Requests (a mesh, its material, boundary conditions and a number of steps)
 arrive at any time.  The server admits work when a slot is free and its
 estimated device footprint fits the memory budget (continuous admission).
 
-Batching: compatible requests waiting at admission time (same element type,
-step count, dt, scheme, precision, gravity and planes) are packed into one
-union mesh, up to `batch_max` requests and `batch_elems` elements: one library
+Batching: compatible small requests waiting at admission time (same element
+type, step count, dt, scheme, precision, gravity and planes; at most
+`batch_small` elements each) are packed into one union mesh, up to
+`batch_max` requests and `batch_elems` elements: one library
 handle whose nodes and elements are the concatenation of theirs.  The meshes
 share no element, so the union's gradient, Hessian and contact constraints are
 the direct sum of theirs; one Newton / SQP iteration, one PCG kernel sequence
@@ -95,11 +96,14 @@ class RolloutServer:
     """Continuous-admission server for independent rollouts on one GPU."""
 
     def __init__(self, max_slots: int = 8, memory_budget_bytes: int | None = None, device: int = 0,
-                 batch_max: int = 1, batch_elems: int = 2_000_000):
+                 batch_max: int = 1, batch_elems: int = 400_000, batch_small: int = 50_000):
         import torch
         self.device = device
         self.batch_max = max(1, int(batch_max))
         self.batch_elems = int(batch_elems)
+        # only meshes up to batch_small elements are packed: larger ones already
+        # fill the GPU alone, and a union's iterations are those of its hardest member
+        self.batch_small = int(batch_small)
         self._held: list[RolloutRequest] = []
         if memory_budget_bytes is None:
             free, _total = torch.cuda.mem_get_info(device)
@@ -157,7 +161,7 @@ class RolloutServer:
                 closing = True
                 continue
             batch = [req]
-            if self.batch_max > 1:
+            if self.batch_max > 1 and req.elements.shape[0] <= self.batch_small:
                 # pack compatible requests that are waiting now (no waiting for new arrivals)
                 rest = []
                 while len(batch) < self.batch_max:
@@ -167,7 +171,7 @@ class RolloutServer:
                     if nxt is None:
                         closing = True
                         break
-                    if (compatible(batch[0], nxt) and
+                    if (compatible(batch[0], nxt) and nxt.elements.shape[0] <= self.batch_small and
                             sum(r.elements.shape[0] for r in batch) + nxt.elements.shape[0] <= self.batch_elems):
                         batch.append(nxt)
                     else:
