@@ -1321,8 +1321,7 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
         CK(cudaMemcpyAsync(raw.data(), h->H, n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
     }
-    // device storage is split (entries 0-7 of every block, then every entry 8);
-    // the ABI returns each block's 9 values contiguously
+    // the ABI returns each block's 9 values contiguously, row-major
     const size_t nb = (size_t)h->nnzb;
     for (size_t b = 0; b < nb; b++)
         for (int rc = 0; rc < 9; rc++) val[b * 9 + rc] = raw[hval(b, rc, nb)];

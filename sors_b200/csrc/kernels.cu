@@ -762,29 +762,12 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
     counted();
 }
 
-// One 3x3 block in split storage (hval): two 16-byte loads (FP32) or four
-// (FP64) for entries 0-7 and one scalar load for entry 8.
+// One 3x3 block (hval layout): nine scalar loads.
 template <typename HT, typename VT>
-__device__ __forceinline__ void load_block(const HT* __restrict__ H, size_t b, size_t nnzb, VT (&h)[9]);
-template <>
-__device__ __forceinline__ void load_block<float, float>(const float* __restrict__ H, size_t b, size_t nnzb,
-                                                         float (&h)[9]) {
-    const float4* m = reinterpret_cast<const float4*>(H) + 2 * b;
-    const float4 u = __ldg(m), w = __ldg(m + 1);
-    h[0] = u.x; h[1] = u.y; h[2] = u.z; h[3] = u.w;
-    h[4] = w.x; h[5] = w.y; h[6] = w.z; h[7] = w.w;
-    h[8] = __ldg(H + 8 * nnzb + b);
-}
-template <>
-__device__ __forceinline__ void load_block<double, double>(const double* __restrict__ H, size_t b, size_t nnzb,
-                                                           double (&h)[9]) {
-    const double2* m = reinterpret_cast<const double2*>(H) + 4 * b;
+__device__ __forceinline__ void load_block(const HT* __restrict__ H, size_t b, size_t nnzb, VT (&h)[9]) {
+    const HT* v = H + hval(b, 0, nnzb);
 #pragma unroll
-    for (int k = 0; k < 4; k++) {
-        const double2 u = __ldg(m + k);
-        h[2 * k] = u.x; h[2 * k + 1] = u.y;
-    }
-    h[8] = __ldg(H + 8 * nnzb + b);
+    for (int k = 0; k < 9; k++) h[k] = (VT)__ldg(v + k);
 }
 
 // q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q.

@@ -47,12 +47,13 @@ struct MuscleArgs {
     const double* act = nullptr;
 };
 
-// Hessian value storage for nnzb 3x3 blocks: entries 0-7 of block b (row-major)
-// at H[8 b .. 8 b + 7], so a block is two 16-byte vector loads in FP32 (four
-// in FP64), and entry 8 at H[8 nnzb + b].  Same bytes as 9 contiguous values,
-// a third of the load instructions.
+// Hessian value storage: nnzb 3x3 blocks in CSR order, each block's 9 values
+// contiguous and row-major.  (Splitting entries 0-7 from entry 8 for 16-byte
+// vector loads was measured slower in the SpMV.)  nnzb is carried so the
+// layout can change in one place.
 __host__ __device__ __forceinline__ size_t hval(size_t b, int rc, size_t nnzb) {
-    return rc < 8 ? 8 * b + (size_t)rc : 8 * nnzb + b;
+    (void)nnzb;
+    return 9 * b + (size_t)rc;
 }
 
 // Row-owner assembly arguments (tet or hex).
@@ -72,7 +73,7 @@ struct AsmArgs {
     const uint16_t* slot_items; // k*nv + w
     const uint8_t* node_mask;   // 3 bits per node
     const double* mass;     // per node
-    HT* H;                  // nnzb*9, blocks in CSR order, split storage (hval)
+    HT* H;                  // nnzb*9, blocks in CSR order (hval)
     long long nnzb;
     double* g_int;          // 3N (masked element gradient)
     int* status;
