@@ -59,6 +59,10 @@ def block_mesh(cells, seed=0):
     return X, T, E, mask, val
 
 
+PROJECTION = {"true": True, "false": False, "adaptive": "adaptive"}
+_projection = "adaptive"
+
+
 def make_settings(precision):
     from sors_b200 import py_sors as ps
     s = ps.SimulationSettings()
@@ -68,7 +72,7 @@ def make_settings(precision):
     s.timeSteppingScheme = "backward_euler"
     s.solverMethod = "minimize_newton"
     s.precision = precision
-    s.hessianProjection = True
+    s.hessianProjection = PROJECTION[_projection]
     s.newtonResidualTol = 1e-8
     return s
 
@@ -315,6 +319,7 @@ def run_gpu(args, rank, world, local_rank):
         "config": {"workload": workload_name(cells, "mixed precision" if args.precision == "mixed" else "FP64"),
                    "elements": ne, "nodes": nn, "dofs": 3 * nn, "precision": args.precision,
                    "newton": "||dx||<1e-9 or ||g||<1e-8, Eisenstat-Walker PCG forcing",
+                   "hessian_projection": _projection,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (assembled system ~1 GB resident), no flush"},
         "newton_steps_per_s": world * args.steps / (ms / 1e3),
@@ -594,6 +599,9 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--projection", default="adaptive", choices=sorted(PROJECTION),
+                    help="SPD projection of the element Hessians: always, never, or only where PCG meets "
+                         "negative curvature")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "serve"],
                     help="c2: the 3.0M-tet block (default); c3: pressure-actuated hex arm, static load ramp; "
@@ -611,6 +619,8 @@ def main():
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global _projection
+    _projection = args.projection
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

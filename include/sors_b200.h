@@ -61,6 +61,9 @@ typedef struct SorsSettings {
     int32_t newton_predictor;/* 1: start each Newton solve from q + dt v_prev
                                 (falls back to q if that inverts an element);
                                 changes only the iterates, not the solution      */
+    int32_t max_blocks;      /* largest grid of any kernel of this handle; 0 = the
+                                whole GPU (148 x 8 blocks).  Smaller grids let the
+                                kernels of several handles run side by side     */
 } SorsSettings;
 
 typedef struct SorsStepStats {

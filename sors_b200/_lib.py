@@ -34,6 +34,7 @@ class SorsSettings(C.Structure):
         ("pcg_max_iter", C.c_int32),
         ("device", C.c_int32),
         ("newton_predictor", C.c_int32),
+        ("max_blocks", C.c_int32),
     ]
 
 

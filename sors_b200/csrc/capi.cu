@@ -1015,6 +1015,7 @@ int step_resident(SorsHandle* h, double dt, int substeps, SorsStepStats* stats) 
 
 int set_device(SorsHandle* h) {
     CK(cudaSetDevice(h->device));
+    set_grid_cap(h->s.max_blocks);
     return SORS_OK;
 }
 
@@ -1043,6 +1044,7 @@ void sors_default_settings(SorsSettings* s) {
     s->pcg_max_iter = 20000;
     s->device = 0;
     s->newton_predictor = 1;
+    s->max_blocks = 0;
 }
 
 int sors_last_error(char* buf, size_t n) {

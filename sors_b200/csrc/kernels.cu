@@ -86,11 +86,22 @@ __device__ bool reduce_grid(double (&v)[NS], double* partials, unsigned* counter
     return true;
 }
 
+// Largest grid the launchers of this thread use (0: none below the defaults).
+// The library sets it from the calling handle's settings on every entry, so
+// captured graphs carry the grid of the handle that captured them.
+thread_local int t_grid_cap = 0;
+void set_grid_cap(int blocks) { t_grid_cap = blocks > 0 ? blocks : 0; }
+
+static inline long long cap_grid(long long b) {
+    if (t_grid_cap > 0 && b > t_grid_cap) b = t_grid_cap;
+    return b < 1 ? 1 : b;
+}
+
 static inline int red_grid(long long n, int per_thread = 1) {
     long long b = (n + (long long)kRedThreads * per_thread - 1) / ((long long)kRedThreads * per_thread);
     if (b < 1) b = 1;
     if (b > kRedBlocks) b = kRedBlocks;
-    return (int)b;
+    return (int)cap_grid(b);
 }
 
 // ---------------------------------------------------------------------------
@@ -357,6 +368,7 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     long long rows_per_block = wpb;
     long long blocks = (a.N + rows_per_block - 1) / rows_per_block;
     if (blocks > 148 * 64) blocks = 148 * 64;
+    blocks = cap_grid(blocks);
     if (nv == 4) {
         cudaFuncSetAttribute(k_assemble<HT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_assemble<HT, 4><<<(int)blocks, threads, smem, st>>>(a);
@@ -846,6 +858,7 @@ void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* c
     long long blocks = (N + rows_per_block - 1) / rows_per_block;
     if (blocks > kRedBlocks) blocks = kRedBlocks;
     if (blocks < 1) blocks = 1;
+    blocks = cap_grid(blocks);
     switch (lpr) {
         case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
         case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;

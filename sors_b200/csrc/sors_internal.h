@@ -100,6 +100,9 @@ struct PressureArgs {
     double* f_ext;              // 3N (written for surface nodes)
 };
 
+// Caps the grid of every kernel launched from this thread (kernels.cu).
+void set_grid_cap(int blocks);
+
 // Sets the message returned by sors_last_error on this thread (capi.cu).
 void set_last_error(const std::string& msg);
 

@@ -57,6 +57,7 @@ class SimulationSettings:
         # SPD projection of dP/dF per quadrature point: True always, False never,
         # "adaptive" (default) the exact Hessian unless PCG meets negative curvature
         self.hessianProjection = "adaptive"
+        self.maxBlocksPerKernel = 0        # grid cap per kernel (0: whole GPU)
         self.newtonResidualTol = 0.0       # absolute ||gradient|| stop; 0 = reference dx test only
         self.newtonDxTol = 1e-9            # reference DX_TOL (cpp/headers/common.h:25)
         self.newtonMaxIter = 100           # reference MAX_ITER (cpp/headers/common.h:21)
@@ -266,6 +267,7 @@ class _EnergyBase:
         s.pcg_max_iter = int(getattr(settings, "pcgMaxIter", 20000))
         s.device = int(getattr(settings, "device", 0))
         s.newton_predictor = int(bool(getattr(settings, "newtonPredictor", True)))
+        s.max_blocks = int(getattr(settings, "maxBlocksPerKernel", 0))
         self._settings_c = s
         h = C.c_void_p()
         _lib.check(L.sors_create(_p(X, C.c_double), X.shape[0], _p(T, C.c_int32), ne, self.NV, _p(rho, C.c_double),

@@ -96,9 +96,14 @@ class RolloutServer:
     """Continuous-admission server for independent rollouts on one GPU."""
 
     def __init__(self, max_slots: int = 8, memory_budget_bytes: int | None = None, device: int = 0,
-                 batch_max: int = 1, batch_elems: int = 400_000, batch_small: int = 50_000):
+                 batch_max: int = 1, batch_elems: int = 400_000, batch_small: int = 50_000,
+                 max_blocks: int | None = None):
         import torch
         self.device = device
+        # kernels of concurrent handles share the GPU: cap each grid so that
+        # several run side by side (0 = the whole GPU, used for one slot)
+        self.max_blocks = (max(148, 2 * 1184 // max_slots) if max_slots > 1 else 0) if max_blocks is None \
+            else int(max_blocks)
         self.batch_max = max(1, int(batch_max))
         self.batch_elems = int(batch_elems)
         # only meshes up to batch_small elements are packed: larger ones already
@@ -202,7 +207,7 @@ class RolloutServer:
         finals = [None] * len(batch)
         err = None
         try:
-            en, sol, slices, disks = build_union(batch, self.device)
+            en, sol, slices, disks = build_union(batch, self.device, self.max_blocks)
             ref = batch[0]
             q = np.concatenate([np.ascontiguousarray(r.vertices, dtype=np.float64).ravel() for r in batch])
             for t in range(ref.steps):
@@ -246,7 +251,7 @@ def _lib_set_disk(en, d, c, n, r):
                                          n.ctypes.data_as(C.POINTER(C.c_double)), float(r)))
 
 
-def build_union(batch, device: int = 0):
+def build_union(batch, device: int = 0, max_blocks: int = 0):
     """One Energy/Solver over the union of the batch's meshes.
 
     Returns (energy, solver, slices, disks): slices[k] = (a, b) DOF range of
@@ -255,7 +260,7 @@ def build_union(batch, device: int = 0):
     import ctypes as C
     from . import _lib
     if len(batch) == 1 and batch[0].disks is None:
-        en, sol = build_rollout(batch[0], device)
+        en, sol = build_rollout(batch[0], device, max_blocks=max_blocks)
         return en, sol, [(0, batch[0].vertices.size)], []
     ref = batch[0]
     offs = np.cumsum([0] + [r.vertices.shape[0] for r in batch])
@@ -275,7 +280,8 @@ def build_union(batch, device: int = 0):
     union = RolloutRequest(X, T, rho, E, nu, ref.steps, ref.dt, gravity=ref.gravity, neumann_mask=mask,
                            neumann_value=val, precision=ref.precision, scheme=ref.scheme,
                            newton_res_tol=ref.newton_res_tol, planes=ref.planes, disks=None, surface=surf)
-    en, sol = build_rollout(union, device, sqp=ref.planes is not None or ref.disks is not None)
+    en, sol = build_rollout(union, device, sqp=ref.planes is not None or ref.disks is not None,
+                            max_blocks=max_blocks)
     disks = []
     if ref.disks is not None:
         cen, nrm, rad, ptr, dsurf = [], [], [], [0], []
@@ -303,7 +309,7 @@ def build_union(batch, device: int = 0):
     return en, sol, slices, disks
 
 
-def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None):
+def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None, max_blocks: int = 0):
     """Energy and Solver for one request (the reference-style py_sors objects)."""
     s = ps.SimulationSettings()
     s.meshType = "Tetrahedron" if req.elements.shape[1] == 4 else "Hexahedron"
@@ -314,6 +320,7 @@ def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None)
     s.precision = req.precision
     s.newtonResidualTol = 0.0 if contact else req.newton_res_tol
     s.device = device
+    s.maxBlocksPerKernel = max_blocks
     cls = ps.EnergyTet if req.elements.shape[1] == 4 else ps.EnergyHex
     en = cls.from_arrays(req.vertices, req.elements, s, np.asarray(req.gravity, float), 0.0,
                          density=req.density, youngsModulus=req.youngs, poissonsRatio=req.poisson,

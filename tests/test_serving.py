@@ -16,12 +16,12 @@ def test_alone_equals_mix():
     reqs = _requests(6)
     alone = {}
     for r in _requests(6):
-        srv = RolloutServer(max_slots=1)
+        srv = RolloutServer(max_slots=1, max_blocks=296)
         srv.submit(r)
         res = srv.close()
         assert res[0].error is None, res[0].error
         alone[r.tag] = res[0].final
-    srv = RolloutServer(max_slots=4)
+    srv = RolloutServer(max_slots=4, max_blocks=296)
     for r in reqs:
         srv.submit(r)
     mixed = {r.tag: r for r in srv.close()}
