@@ -367,6 +367,8 @@ def run_c3(args):
         s = ps.SimulationSettings()
         s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
         s.precision = precision; s.newtonResidualTol = 1e-8
+        # static follower loads: no inertia term, exact Hessian indefinite -> always project
+        s.hessianProjection = True
         fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
         en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
                                       poissonsRatio=0.48, neumannBCmask=mask, neumannBCvalue=np.zeros(mask.size),

@@ -1580,7 +1580,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
     aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
     aa.H = (HT*)h->H; aa.nnzb = h->nnzb; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
-    aa.material = h->s.material; aa.project = h->s.project_spd != 0; aa.apply_mask = 1;
+    aa.material = h->s.material; aa.project = h->s.project_spd == 1; aa.apply_mask = 1;  // as a step assembles
     aa.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0; aa.want_hess = 1;
     aa.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0; aa.inertia_coef = inertia_coef(h, dt);
     CK(cudaEventRecord(a, h->stream));
