@@ -528,8 +528,9 @@ def run_serve(args):
             out.append(serving.poke_cube_request(r, n, tag=i, steps=args.rollout_steps, dt=1e-2, precision=precision))
         return out
 
-    def run(precision, slots, arrivals, batch=1):
-        reqs = make(precision)
+    def run(precision, slots, arrivals, batch=1, count=None):
+        reqs = make(precision)[:count]
+        arrivals = arrivals[:len(reqs)]
         srv = serving.RolloutServer(max_slots=slots, batch_max=batch)
         t0 = time.perf_counter()
         for req, at in zip(reqs, arrivals):
@@ -556,7 +557,11 @@ def run_serve(args):
     served, res_m, reqs = run("mixed", args.slots, arrivals, args.batch)
     saturated, _, _ = run("mixed", args.slots, np.zeros(args.rollouts), args.batch)
     unbatched, _, _ = run("mixed", args.slots, np.zeros(args.rollouts), 1)
-    plain, res_p, _ = run("fp64", 1, np.zeros(args.rollouts))
+    # the plain drop-in runs one rollout at a time, so its throughput is the
+    # inverse mean rollout time: measured on the first baseline_sample requests
+    nb = min(args.rollouts, args.baseline_sample) if args.baseline_sample > 0 else args.rollouts
+    plain, res_p, _ = run("fp64", 1, np.zeros(args.rollouts), 1, nb)
+    plain["requests_measured"] = nb
     # accuracy of the served form against the plain FP64 path, per rollout,
     # relative to that rollout's largest displacement
     by_tag = {r.tag: r.final for r in res_p}
@@ -613,6 +618,8 @@ def main():
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (rollouts/s)")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent handles")
     ap.add_argument("--batch", type=int, default=8, help="serve: rollouts packed into one union handle")
+    ap.add_argument("--baseline-sample", type=int, default=0,
+                    help="serve: measure the sequential FP64 baseline on the first K requests (0 = all)")
     ap.add_argument("--seeds", type=int, default=4, help="c4: rollouts differentiated concurrently")
     ap.add_argument("--c4-steps", type=int, default=100, help="c4: steps per rollout")
     ap.add_argument("--fd-dirs", type=int, default=4, help="c4: finite-difference directions checked")

@@ -201,11 +201,20 @@ class RolloutServer:
     def _run(self, batch, need: int):
         import torch
         torch.cuda.set_device(self.device)
-        started = time.perf_counter()
+        self._run_batch(batch, time.perf_counter())
+        with self._lock:
+            self._active -= 1
+            self._in_use -= need
+            self._lock.notify_all()
+
+    def _run_batch(self, batch, started):
+        """Steps one union; if it fails and holds several rollouts, each is run
+        again on its own so that one failing rollout does not fail the others."""
         steps_lat = []
         newton = pcg = 0
         finals = [None] * len(batch)
         err = None
+        en = sol = None
         try:
             en, sol, slices, disks = build_union(batch, self.device, self.max_blocks)
             ref = batch[0]
@@ -222,14 +231,15 @@ class RolloutServer:
             del en
         except Exception as ex:  # reported per rollout, the server keeps running
             err = str(ex)
+        en = sol = None  # release the union's device memory before any re-run
+        if err is not None and len(batch) > 1:
+            for r in batch:
+                self._run_batch([r], started)
+            return
         done = time.perf_counter()
         for r, f in zip(batch, finals):
             self._results.append(RolloutResult(r.tag, f, list(steps_lat), started - r.submitted, done - r.submitted,
                                                newton, pcg, err, batch=len(batch)))
-        with self._lock:
-            self._active -= 1
-            self._in_use -= need
-            self._lock.notify_all()
 
 
 def compatible(a: RolloutRequest, b: RolloutRequest) -> bool:
