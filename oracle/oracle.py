@@ -23,6 +23,7 @@ SCHEME = {"backward_euler": 0, "crank_nicolson": 1}
 METHOD = {"minimize_newton": 0, "minimize_newton_linesearch": 1, "minimize_frozenhessian": 2, "minimize_SQP": 3}
 MAT_NEOHOOKEAN = 0
 MAT_TEST_QUARTIC = 1
+MAT_STABLE_NEOHOOKEAN = 2
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
@@ -47,6 +48,8 @@ def lib():
         L.orc_elem_eval.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]
         L.orc_elem_eval_batch.argtypes = [C.c_int, C.c_int, _dp, _ip, _dp, _dp, _dp, C.c_int, _dp, _dp, _dp]
         L.orc_project_psd9.argtypes = [_dp]
+        L.orc_elem_eval_material.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp,
+                                              _dp]
         L.orc_elem_eval_muscle.argtypes = [C.c_int, _dp, _dp, C.c_double, C.c_double, C.c_double, _dp, C.c_double,
                                            C.c_int, C.c_int, _dp, _dp, _dp]
         L.orc_set_muscles.argtypes = [C.c_void_p, _ip, _dp, _dp, C.c_int, C.c_int]
@@ -116,6 +119,16 @@ def elem_eval(X, x, youngs, nu, project=False):
     n = 3 * nv
     psi = np.zeros(1); g = np.zeros(n); H = np.zeros((n, n))
     st = lib().orc_elem_eval(nv, _pd(X), _pd(x), float(youngs), float(nu), int(project), _pd(psi), _pd(g), _pd(H))
+    return float(psi[0]), g, H, st
+
+
+def elem_eval_material(X, x, youngs, nu, material, project=False):
+    """Psi*V, grad*V, hess*V of one element for a material model (MAT_*)."""
+    X = _d(X); x = _d(x)
+    n = 3 * X.shape[0]
+    psi = np.zeros(1); g = np.zeros(n); H = np.zeros((n, n))
+    st = lib().orc_elem_eval_material(X.shape[0], _pd(X), _pd(x), float(youngs), float(nu), int(material),
+                                      int(project), _pd(psi), _pd(g), _pd(H))
     return float(psi[0]), g, H, st
 
 

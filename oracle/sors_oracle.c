@@ -29,6 +29,11 @@
 #define ORC_ERR_SINGULAR 4
 #define ORC_ERR_ARG 5
 
+/* material models */
+#define ORC_MAT_NEOHOOKEAN 0
+#define ORC_MAT_TEST_QUARTIC 1
+#define ORC_MAT_STABLE_NEOHOOKEAN 2
+
 /* ------------------------------------------------------------------------- */
 /* 3x3 helpers (Eigen's fixed-size determinant()/inverse() use the cofactor   */
 /* expansion; restated here).                                                */
@@ -224,6 +229,15 @@ static void lame(double E, double nu, double* mu, double* lam) {
     *mu = E / (2 * (1 + nu));
 }
 
+/* stableNeoHookean.cpp:10-15 */
+static void lame_material(double E, double nu, int material, double* mu, double* lam) {
+    lame(E, nu, mu, lam);
+    if (material == ORC_MAT_STABLE_NEOHOOKEAN) {
+        *mu *= 4.0 / 3.0;
+        *lam += 5.0 / 8.0 * (*mu);
+    }
+}
+
 /* neoHookean.cpp:14-41 */
 static double nh_energy(const double* F, int nqp, double mu, double lam) {
     double e = 0;
@@ -311,6 +325,84 @@ static int nh_hessian(const double* F, const double* B, int nqp, int ncol, doubl
     return status;
 }
 
+/* Stable Neo-Hookean, cpp/src/energies/stableNeoHookean.cpp.  mu, lam arrive
+ * reparameterised (:10-15): mu_s = 4/3 mu, lam_s = lam + 5/8 mu_s; alpha =
+ * 1 + 3/4 mu_s / lam_s.  Energy :18-45, gradient :48-83, Hessian :86-140. */
+static double snh_energy(const double* F, int nqp, double mu, double lam) {
+    double e = 0, w = 1.0 / nqp, alpha = 1 + 0.75 * mu / lam;
+    for (int s = 0; s < nqp; s++) {
+        const double* f = F + 9 * s;
+        double J = det3(f), IC = 0;
+        for (int k = 0; k < 9; k++) IC += f[k] * f[k];
+        e += (0.5 * mu * (IC - 3) + 0.5 * lam * (J - alpha) * (J - alpha) - 0.5 * mu * log(IC + 1)) * w;
+    }
+    return e;
+}
+
+static void snh_gradient(const double* F, const double* B, int nqp, int ncol, double mu, double lam, double* g) {
+    double w = 1.0 / nqp, alpha = 1 + 0.75 * mu / lam;
+    for (int c = 0; c < ncol; c++) g[c] = 0;
+    for (int s = 0; s < nqp; s++) {
+        const double* f = F + 9 * s;
+        double inv[9], J = det3(f), IC = 0;
+        inv3(f, inv);
+        for (int k = 0; k < 9; k++) IC += f[k] * f[k];
+        double dEdF[9];
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++)
+                dEdF[r * 3 + c] = mu * f[r * 3 + c] + lam * (J - alpha) * J * inv[c * 3 + r] - mu * f[r * 3 + c] / (IC + 1);
+        const double* Bs = B + (size_t)s * 9 * ncol;
+        for (int c = 0; c < ncol; c++) {
+            double acc = 0;
+            for (int k = 0; k < 9; k++) acc += dEdF[k] * Bs[k * ncol + c];
+            g[c] += acc * w;
+        }
+    }
+}
+
+static int snh_hessian(const double* F, const double* B, int nqp, int ncol, double mu, double lam, int project,
+                       double* H) {
+    double w = 1.0 / nqp, alpha = 1 + 0.75 * mu / lam;
+    for (int i = 0; i < ncol * ncol; i++) H[i] = 0;
+    double* T = (double*)malloc(sizeof(double) * 9 * ncol);
+    for (int s = 0; s < nqp; s++) {
+        const double* f = F + 9 * s;
+        double inv[9], G[9], J = det3(f), IC = 0;
+        inv3(f, inv);
+        for (int r = 0; r < 3; r++)
+            for (int c = 0; c < 3; c++) G[r * 3 + c] = inv[c * 3 + r];
+        for (int k = 0; k < 9; k++) IC += f[k] * f[k];
+        double A[81];
+        for (int p = 0; p < 3; p++)
+            for (int q = 0; q < 3; q++)
+                for (int a = 0; a < 3; a++)
+                    for (int b = 0; b < 3; b++) {
+                        int row = p * 3 + q, col = a * 3 + b;
+                        double m = -G[p * 3 + b] * G[a * 3 + q];
+                        double v = (2 * J - alpha) * lam * J * G[row] * G[col] + lam * (J - alpha) * J * m +
+                                   2 * mu * f[row] * f[col] / ((IC + 1) * (IC + 1));
+                        if (row == col) v += mu - mu / (IC + 1);
+                        A[row * 9 + col] = v;
+                    }
+        if (project) project_psd(A);
+        const double* Bs = B + (size_t)s * 9 * ncol;
+        for (int r = 0; r < 9; r++)
+            for (int c = 0; c < ncol; c++) {
+                double acc = 0;
+                for (int k = 0; k < 9; k++) acc += A[k * 9 + r] * Bs[k * ncol + c];
+                T[r * ncol + c] = acc;
+            }
+        for (int i = 0; i < ncol; i++)
+            for (int j = 0; j < ncol; j++) {
+                double acc = 0;
+                for (int k = 0; k < 9; k++) acc += T[k * ncol + i] * Bs[k * ncol + j];
+                H[i * ncol + j] += acc * w;
+            }
+    }
+    free(T);
+    return ORC_OK;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Element evaluation (Element::compute_energy, Tetrahedron/Hexahedron::      */
 /* compute_gradient/hessian): material value x undeformed volume.            */
@@ -360,11 +452,10 @@ static void elem_F(const ElemGeom* g, const double* x, double* F) {
     }
 }
 
-/* Material models: 0 = Neo-Hookean; 1 = the reference's mock "Testahedron"
- * quartic energy sum x^2(x^2-0.5) over the element's coordinates, which is not
- * scaled by the volume (cpp/src/_test.cpp:8-66). */
-#define ORC_MAT_NEOHOOKEAN 0
-#define ORC_MAT_TEST_QUARTIC 1
+/* Material models (ORC_MAT_*): 0 = Neo-Hookean; 1 = the reference's mock
+ * "Testahedron" quartic energy sum x^2(x^2-0.5) over the element's
+ * coordinates, which is not scaled by the volume (cpp/src/_test.cpp:8-66);
+ * 2 = stable Neo-Hookean. */
 
 /* SoftCon fibre term of one element (cpp/src/energies/softconMuscle.cpp:12-132):
  * stiffness k, fibre direction m, activation e of the element's muscle group. */
@@ -453,9 +544,15 @@ static int elem_eval_geom(const ElemGeom* g, int material, const double* x, doub
     double F[72];
     elem_F(g, x, F);
     int st = ORC_OK;
-    if (psi) *psi = nh_energy(F, g->nqp, mu, lam);
-    if (grad) nh_gradient(F, g->B, g->nqp, n, mu, lam, grad);
-    if (hess) st = nh_hessian(F, g->B, g->nqp, n, mu, lam, project, hess);
+    if (material == ORC_MAT_STABLE_NEOHOOKEAN) {
+        if (psi) *psi = snh_energy(F, g->nqp, mu, lam);
+        if (grad) snh_gradient(F, g->B, g->nqp, n, mu, lam, grad);
+        if (hess) st = snh_hessian(F, g->B, g->nqp, n, mu, lam, project, hess);
+    } else {
+        if (psi) *psi = nh_energy(F, g->nqp, mu, lam);
+        if (grad) nh_gradient(F, g->B, g->nqp, n, mu, lam, grad);
+        if (hess) st = nh_hessian(F, g->B, g->nqp, n, mu, lam, project, hess);
+    }
     if (mm) muscle_eval(g, F, mm, mform, project, psi, grad, hess);
     if (psi) *psi *= g->vol;
     if (grad)
@@ -485,6 +582,16 @@ int orc_elem_eval_muscle(int nv, const double* X, const double* x, double youngs
     lame(youngs, nu, &mu, &lam);
     OrcMuscle mm = {k, {m[0], m[1], m[2]}, act};
     return elem_eval_geom(&g, ORC_MAT_NEOHOOKEAN, x, mu, lam, project, &mm, form, psi, grad, hess);
+}
+
+/* Element hook with a material model (ORC_MAT_*). */
+int orc_elem_eval_material(int nv, const double* X, const double* x, double youngs, double nu, int material,
+                           int project, double* psi, double* grad, double* hess) {
+    ElemGeom g;
+    elem_geom(nv, X, &g);
+    double mu, lam;
+    lame_material(youngs, nu, material, &mu, &lam);
+    return elem_eval_geom(&g, material, x, mu, lam, project, NULL, 0, psi, grad, hess);
 }
 
 /* Batched element evaluation over a mesh (OpenMP).  Outputs per element:
@@ -892,7 +999,7 @@ OrcSystem* orc_create(int nv, int N, const double* X, int E, const int32_t* conn
         for (int j = 0; j < nv; j++)
             for (int k = 0; k < 3; k++) Xe[j * 3 + k] = X[3 * conn[e * nv + j] + k];
         elem_geom(nv, Xe, &s->geom[e]);
-        lame(youngs[e], nu[e], &s->mu[e], &s->lam[e]);
+        lame_material(youngs[e], nu[e], material, &s->mu[e], &s->lam[e]);
     }
     /* lumped mass, energy.cpp:176-189: element mass rho*V split equally */
     for (int e = 0; e < E; e++) {

@@ -153,6 +153,20 @@ struct SorsHandle {
 namespace {
 
 bool mixed(const SorsHandle* h) { return h->s.precision == 1; }
+
+// (mu, lambda) of an element from Young's modulus and Poisson's ratio
+// (neoHookean.cpp:10-11); stable Neo-Hookean reparameterises them as
+// mu_s = 4/3 mu, lambda_s = lambda + 5/8 mu_s (stableNeoHookean.cpp:10-15).
+double2 lame_params(double Ey, double nu, int material) {
+    double2 m;
+    m.y = (Ey * nu) / ((1 + nu) * (1 - 2 * nu));
+    m.x = Ey / (2 * (1 + nu));
+    if (material == 2) {
+        m.x *= 4.0 / 3.0;
+        m.y += 5.0 / 8.0 * m.x;
+    }
+    return m;
+}
 MuscleArgs muscles(const SorsHandle* h) {
     MuscleArgs m;
     if (h->mgroup) { m.group = h->mgroup; m.param = h->mparam; m.act = h->mact; }
@@ -549,7 +563,8 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     }
     CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
     // element contractions with lam (zero on fixed DOFs and along held normals)
-    launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->adj_l, h->adj_e, h->stream);
+    launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->adj_l, h->adj_e,
+                        h->stream);
     std::vector<double> ge((size_t)2 * std::max(1, E));
     CK(d2h(h, ge.data(), h->adj_e, sizeof(double) * 2 * (size_t)E));
     std::vector<double> r(n, 0.0);
@@ -1080,9 +1095,7 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     std::vector<double2> mat(E > 0 ? E : 1);
     std::vector<double> mass(N, 0.0);
     for (int e = 0; e < E; e++) {
-        double Ey = youngs[e], nu = poisson[e];
-        mat[e].y = (Ey * nu) / ((1 + nu) * (1 - 2 * nu));
-        mat[e].x = Ey / (2 * (1 + nu));
+        mat[e] = lame_params(youngs[e], poisson[e], h->s.material);
         double m = density[e] * elem_volume(X, conn + (size_t)e * nv, nv);
         for (int v = 0; v < nv; v++) mass[conn[(size_t)e * nv + v]] += m / nv;
     }
@@ -1481,11 +1494,7 @@ int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson
     int st;
     if ((st = set_device(h))) return st;
     std::vector<double2> mat((size_t)std::max(1, h->E));
-    for (int e = 0; e < h->E; e++) {
-        const double Ey = youngs[e], nu = poisson[e];
-        mat[e].y = (Ey * nu) / ((1 + nu) * (1 - 2 * nu));
-        mat[e].x = Ey / (2 * (1 + nu));
-    }
+    for (int e = 0; e < h->E; e++) mat[e] = lame_params(youngs[e], poisson[e], h->s.material);
     h->youngs_h.assign(youngs, youngs + h->E);
     h->poisson_h.assign(poisson, poisson + h->E);
     if (h->E) CK(h2d(h, h->mat, mat.data(), sizeof(double2) * h->E));
@@ -1504,7 +1513,7 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (h->s.time_stepping != 0 && dt != 0.0)
         return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for backward Euler steps");
     if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
-    if (h->s.material != 0) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
+    if (h->s.material == 1) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
     if (stats) *stats = SorsStepStats{};
     return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
                                                  dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats)

@@ -337,6 +337,169 @@ __device__ __forceinline__ bool nh_qp_row(const double (&d)[NV][3], const double
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Stable Neo-Hookean (cpp/src/energies/stableNeoHookean.cpp, after Smith et al.
+// 2018): Psi = mu/2 (I_C - 3) + lam/2 (J - alpha)^2 - mu/2 log(I_C + 1), with
+// the reparameterised mu = 4/3 mu_L, lam = lam_L + 5/8 mu, alpha = 1 + 3/4 mu/lam
+// (stableNeoHookean.cpp:10-15; mu and lam arrive already reparameterised).
+// P = mu' F + c2 F^-T with mu' = mu (1 - 1/(I_C+1)), c2 = lam (J - alpha) J;
+// dP/dF = mu' I + c1 g g^T + c2 M + c4 f f^T (g = vec F^-T, f = vec F,
+// M = d F^-T / dF), c1 = lam (2J - alpha) J, c4 = 2 mu / (I_C+1)^2
+// (stableNeoHookean.cpp:90-135).  It stays finite for inverted elements.
+// In the rotation-variant SVD frame the twist / flip eigenvalues of pair (i,j)
+// are mu' +- (c2/J) s_k and the stretch block is
+// S_ij = mu' d_ij + c1/(s_i s_j) + c4 s_i s_j - c2 d_ij / s_i^2.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void snh_modes(const T* F, T J, T IC, T mu, T lam, T alpha, NhModes<T>& pm) {
+    T s[3];
+    svd3_rv(F, pm.U, s, pm.V);
+    const T mup = mu * (T(1) - T(1) / (IC + T(1)));
+    const T c2 = lam * (J - alpha) * J;
+    const T c1 = lam * (T(2) * J - alpha) * J;
+    const T c4 = T(2) * mu / ((IC + T(1)) * (IC + T(1)));
+    const T cj = c2 / J;
+    pm.lt[0] = mup + cj * s[2]; pm.lt[1] = mup + cj * s[1]; pm.lt[2] = mup + cj * s[0];
+    pm.lf[0] = mup - cj * s[2]; pm.lf[1] = mup - cj * s[1]; pm.lf[2] = mup - cj * s[0];
+    T S[9];
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            S[i * 3 + j] = c1 / (s[i] * s[j]) + c4 * s[i] * s[j] + ((i == j) ? mup - c2 / (s[i] * s[i]) : T(0));
+    sym3_eig(S, pm.ls, pm.Y);
+    pm.any = false;
+#pragma unroll
+    for (int m = 0; m < 3; m++) pm.any |= (pm.lt[m] < T(0)) | (pm.lf[m] < T(0)) | (pm.ls[m] < T(0));
+}
+
+// Row v of one quadrature point for the stable Neo-Hookean energy (same
+// contract as nh_qp_row); returns false only for a degenerate F (J == 0).
+template <typename HT, int NV, bool HESS>
+__device__ __forceinline__ bool snh_qp_row(const double (&d)[NV][3], const double (&x)[NV][3], const double (&dvd)[3],
+                                           double wV, double mu, double lam, bool project, double* g,
+                                           HT (&blk)[NV * 9]) {
+    double F[9];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int w = 0; w < NV; w++) acc += x[w][r] * d[w][c];
+            F[r * 3 + c] = acc;
+        }
+    double C[9];
+    cof3(F, C);
+    const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+    if (J == 0.0) return false;
+    double IC = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+    const double alpha = 1.0 + 0.75 * mu / lam;
+    const double iJ = 1.0 / J;
+    double G[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) G[k] = C[k] * iJ;
+    const double mup = mu * (1.0 - 1.0 / (IC + 1.0));
+    const double c2 = lam * (J - alpha) * J;
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        double pr = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) pr += (mup * F[r * 3 + c] + c2 * G[r * 3 + c]) * dvd[c];
+        g[r] += wV * pr;
+    }
+    if (!HESS) return true;
+    const double c1 = lam * (2.0 * J - alpha) * J;
+    const double c4 = 2.0 * mu / ((IC + 1.0) * (IC + 1.0));
+    HT Gh[9], Fh[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) { Gh[k] = (HT)G[k]; Fh[k] = (HT)F[k]; }
+    const HT dv[3] = {(HT)dvd[0], (HT)dvd[1], (HT)dvd[2]};
+    HT av[3], fv[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        av[r] = Gh[r * 3 + 0] * dv[0] + Gh[r * 3 + 1] * dv[1] + Gh[r * 3 + 2] * dv[2];
+        fv[r] = Fh[r * 3 + 0] * dv[0] + Fh[r * 3 + 1] * dv[1] + Fh[r * 3 + 2] * dv[2];
+    }
+    const HT hmu = (HT)(wV * mup), h1 = (HT)(wV * c1), h2 = (HT)(wV * c2), h4 = (HT)(wV * c4);
+#pragma unroll
+    for (int w = 0; w < NV; w++) {
+        const HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
+        HT aw[3], fw[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            aw[r] = Gh[r * 3 + 0] * dw[0] + Gh[r * 3 + 1] * dw[1] + Gh[r * 3 + 2] * dw[2];
+            fw[r] = Fh[r * 3 + 0] * dw[0] + Fh[r * 3 + 1] * dw[1] + Fh[r * 3 + 2] * dw[2];
+        }
+        const HT dd = dv[0] * dw[0] + dv[1] * dw[1] + dv[2] * dw[2];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+            for (int l = 0; l < 3; l++) {
+                HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l] + h4 * fv[k] * fw[l];
+                if (k == l) val += hmu * dd;
+                blk[w * 9 + k * 3 + l] += val;
+            }
+    }
+    if (project) {
+        NhModes<HT> pm;
+        snh_modes<HT>(Fh, (HT)J, (HT)IC, (HT)mu, (HT)lam, (HT)alpha, pm);
+        if (pm.any) {
+            const HT wv = (HT)wV;
+            HT dhv[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) dhv[c] = pm.V[0 * 3 + c] * dv[0] + pm.V[1 * 3 + c] * dv[1] + pm.V[2 * 3 + c] * dv[2];
+#pragma unroll
+            for (int w = 0; w < NV; w++) {
+                const HT dw[3] = {(HT)d[w][0], (HT)d[w][1], (HT)d[w][2]};
+                HT dhw[3];
+#pragma unroll
+                for (int c = 0; c < 3; c++) dhw[c] = pm.V[0 * 3 + c] * dw[0] + pm.V[1 * 3 + c] * dw[1] + pm.V[2 * 3 + c] * dw[2];
+                HT* b = blk + w * 9;
+                HT uv[3], uw[3];
+#define SORS_TF(M, I, JJ)                                      \
+    if (pm.lt[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(-1), uv);              \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(-1), uw);              \
+        add_outer(b, -pm.lt[M] * wv, uv, uw);                  \
+    }                                                          \
+    if (pm.lf[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(1), uv);               \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(1), uw);               \
+        add_outer(b, -pm.lf[M] * wv, uv, uw);                  \
+    }
+                SORS_TF(0, 0, 1)
+                SORS_TF(1, 0, 2)
+                SORS_TF(2, 1, 2)
+#undef SORS_TF
+#define SORS_SC(M)                                             \
+    if (pm.ls[M] < HT(0)) {                                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhv, uv);                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhw, uw);                    \
+        add_outer(b, -pm.ls[M] * wv, uv, uw);                  \
+    }
+                SORS_SC(0)
+                SORS_SC(1)
+                SORS_SC(2)
+#undef SORS_SC
+            }
+        }
+    }
+    return true;
+}
+
+// Stable Neo-Hookean energy density of one quadrature point (FP64).
+__device__ __forceinline__ double snh_qp_energy(const double* F, double mu, double lam) {
+    const double J = det3(F);
+    double IC = 0.0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+    const double alpha = 1.0 + 0.75 * mu / lam;
+    return 0.5 * mu * (IC - 3.0) + 0.5 * lam * (J - alpha) * (J - alpha) - 0.5 * mu * log(IC + 1.0);
+}
+
 // Energy density x weight of one quadrature point (FP64).
 __device__ __forceinline__ double nh_qp_energy(const double* F, double mu, double lam) {
     double J = det3(F);

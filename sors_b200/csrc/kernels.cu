@@ -107,7 +107,7 @@ static inline int red_grid(long long n, int per_thread = 1) {
 // ---------------------------------------------------------------------------
 // element row evaluation shared by the assembly and the parity hook
 // ---------------------------------------------------------------------------
-template <typename HT, int NV, bool HESS>
+template <typename HT, int NV, bool HESS, bool SNH = false>
 __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const double* __restrict__ qg,
                                          const int* __restrict__ conn, const double2* __restrict__ mat,
                                          const MuscleArgs& mus, int e, int v, int material, bool project, double* g,
@@ -151,7 +151,8 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
 #pragma unroll
         for (int w = 0; w < NV; w++)
             if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
-        ok = nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
+        ok = SNH ? snh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk)
+                 : nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
         if (grp >= 0) muscle_qp_row<HT, NV, HESS>(d, x, dv, V, mp, eact, project, g, blk);
     } else {
         const double V = hex_volume((const double(*)[3])X) * 0.125;
@@ -160,7 +161,8 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
 #pragma unroll
             for (int w = 0; w < NV; w++)
                 if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
-            ok &= nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
+            ok &= SNH ? snh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk)
+                      : nh_qp_row<HT, NV, HESS>(d, x, dv, V, m.x, m.y, project, g, blk);
             if (grp >= 0) muscle_qp_row<HT, NV, HESS>(d, x, dv, V, mp, eact, project, g, blk);
         }
     }
@@ -209,7 +211,7 @@ __device__ __forceinline__ double elem_energy(const double* __restrict__ Xg, con
                 for (int w = 0; w < NV; w++) t += x[w][r] * d[w][c];
                 F[r * 3 + c] = t;
             }
-        double qe = nh_qp_energy(F, m.x, m.y);
+        double qe = material == 2 ? snh_qp_energy(F, m.x, m.y) : nh_qp_energy(F, m.x, m.y);
         if (grp >= 0) qe += muscle_qp_energy(F, mp, eact);
         acc += (NV == 4) ? qe : qe * 0.125;
     }
@@ -224,7 +226,7 @@ __device__ __forceinline__ double elem_energy(const double* __restrict__ Xg, con
 template <int NV>
 __global__ void k_adjoint_elem(int E, const double* __restrict__ Xg, const double* __restrict__ qg,
                                const int* __restrict__ conn, const double2* __restrict__ mat, MuscleArgs mus,
-                               const double* __restrict__ lam, double* __restrict__ out) {
+                               int material, const double* __restrict__ lam, double* __restrict__ out) {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= E) return;
     double X[NV][3], x[NV][3], L[NV][3];
@@ -264,10 +266,22 @@ __global__ void k_adjoint_elem(int E, const double* __restrict__ Xg, const doubl
         double C[9];
         cof3(F, C);
         const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
-        const double cc = (m.y * log(J) - m.x) / J;
+        // P = a F + b cof(F): Neo-Hookean a = mu, b = (lam log J - mu) / J;
+        // stable Neo-Hookean a = mu (1 - 1/(I_C+1)), b = lam (J - alpha)
+        double pa, pb;
+        if (material == 2) {
+            double IC = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+            pa = m.x * (1.0 - 1.0 / (IC + 1.0));
+            pb = m.y * (J - (1.0 + 0.75 * m.x / m.y));
+        } else {
+            pa = m.x;
+            pb = (m.y * log(J) - m.x) / J;
+        }
         double pd = 0.0;
 #pragma unroll
-        for (int k = 0; k < 9; k++) pd += (m.x * F[k] + cc * C[k]) * LD[k];
+        for (int k = 0; k < 9; k++) pd += (pa * F[k] + pb * C[k]) * LD[k];
         acc_nh += wV * pd;
         if (grp >= 0) {
             double u[3], ls[3];
@@ -285,18 +299,18 @@ __global__ void k_adjoint_elem(int E, const double* __restrict__ Xg, const doubl
 }
 
 void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                         const MuscleArgs& mus, const double* lam, double* out, cudaStream_t st) {
+                         const MuscleArgs& mus, int material, const double* lam, double* out, cudaStream_t st) {
     if (E == 0) return;
     const int threads = 128, blocks = (E + threads - 1) / threads;
-    if (nv == 4) k_adjoint_elem<4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, lam, out);
-    else k_adjoint_elem<8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, lam, out);
+    if (nv == 4) k_adjoint_elem<4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, lam, out);
+    else k_adjoint_elem<8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, lam, out);
     counted();
 }
 
 // ---------------------------------------------------------------------------
 // Row-owner assembly of gradient rows and Hessian block-rows.
 // ---------------------------------------------------------------------------
-template <typename HT, int NV>
+template <typename HT, int NV, bool SNH>
 __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_assemble(AsmArgs<HT> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -313,12 +327,12 @@ __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_a
             const int e = ev >> 3, v = ev & 7;
             HT blk[NV * 9];
             if (a.want_hess) {
-                ok &= elem_row<HT, NV, true>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, a.project != 0, g, blk);
+                ok &= elem_row<HT, NV, true, SNH>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, a.project != 0, g, blk);
                 HT* dst = stage + (size_t)k * NV * 9;
 #pragma unroll
                 for (int t = 0; t < NV * 9; t++) dst[t] = blk[t];
             } else {
-                ok &= elem_row<HT, NV, false>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, false, g, blk);
+                ok &= elem_row<HT, NV, false, SNH>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, false, g, blk);
             }
         }
         if (!ok) atomicOr(a.status, kFlagInverted);
@@ -369,13 +383,16 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     long long blocks = (a.N + rows_per_block - 1) / rows_per_block;
     if (blocks > 148 * 64) blocks = 148 * 64;
     blocks = cap_grid(blocks);
+    const bool snh = a.material == 2;
     if (nv == 4) {
-        cudaFuncSetAttribute(k_assemble<HT, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_assemble<HT, 4><<<(int)blocks, threads, smem, st>>>(a);
+        auto k = snh ? k_assemble<HT, 4, true> : k_assemble<HT, 4, false>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
     } else {
-        cudaFuncSetAttribute(k_assemble<HT, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_assemble<HT, 8><<<(int)blocks, threads, smem, st>>>(a);
+        auto k = snh ? k_assemble<HT, 8, true> : k_assemble<HT, 8, false>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
     }
     (void)max_pairs;
@@ -391,7 +408,8 @@ __global__ void k_elem_rows(int E, const double* X, const double* q, const int* 
     int e = (int)(t / NV), v = (int)(t - (long long)e * NV);
     double g[3] = {0.0, 0.0, 0.0};
     HT blk[NV * 9];
-    bool ok = elem_row<HT, NV, true>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk);
+    bool ok = material == 2 ? elem_row<HT, NV, true, true>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk)
+                            : elem_row<HT, NV, true, false>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk);
     if (!ok) atomicOr(status, kFlagInverted);
     const int n = 3 * NV;
     if (grad)

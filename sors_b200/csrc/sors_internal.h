@@ -78,7 +78,7 @@ struct AsmArgs {
     double* g_int;          // 3N (masked element gradient)
     int* status;
     int stage_per_warp;     // HT elements per warp of staging
-    int material;           // 0 NH, 1 quartic test
+    int material;           // 0 NH, 1 quartic test, 2 stable NH
     int project;
     int apply_mask;         // drop masked DOFs from element terms (not SQP)
     int neumann_override;   // diag = 1 on masked DOFs ("minimize_newton")
@@ -117,7 +117,7 @@ void launch_elem_energy(int E, int nv, const double* X, const double* q, const i
                         const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
 void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                         const MuscleArgs& mus, const double* lam, double* out, cudaStream_t st);
+                         const MuscleArgs& mus, int material, const double* lam, double* out, cudaStream_t st);
 template <typename HT>
 void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* col, const uint8_t* node_mask,
                          double cscale, HT* H, long long nnzb, cudaStream_t st);

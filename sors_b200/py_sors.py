@@ -149,9 +149,12 @@ class _EnergyBase:
             for name in es:
                 if name not in _REF_ENERGIES:
                     raise RuntimeError(f"Unknown energy type: {name}")
-            if es - {"neohookean", "softconMuscle"}:
+            if es - {"neohookean", "stableneohookean", "softconMuscle"}:
                 raise NotImplementedError(
-                    f"element energies {sorted(es - {'neohookean', 'softconMuscle'})} are not built on the GPU path")
+                    f"element energies {sorted(es - {'neohookean', 'stableneohookean', 'softconMuscle'})} "
+                    "are not built on the GPU path")
+            if {"neohookean", "stableneohookean"} <= es:
+                raise NotImplementedError("an element with both Neo-Hookean energies is not supported")
             if "softconMuscle" in es:
                 # tetrahedron.cpp:82-88 / hexahedron.cpp:51-57
                 if mgroup is None:
@@ -160,15 +163,16 @@ class _EnergyBase:
                 mk[i] = float(pr.get_value("softconStiffness")[0, 0])
                 mdir[i] = np.asarray(pr.get_value("softconDirection"), dtype=np.float64).ravel()[:3]
             rho[i] = float(pr.get_value("density")[0, 0])
-            if "neohookean" in es:
+            if "neohookean" in es or "stableneohookean" in es:
                 E[i] = float(pr.get_value("youngsModulus")[0, 0])
                 nu[i] = float(pr.get_value("poissonsRatio")[0, 0])
-                material = 0 if material in (None, 0) else -1
+                kind = 2 if "stableneohookean" in es else 0
+                material = kind if material in (None, kind) else -1
             else:
                 E[i] = 0.0; nu[i] = 0.0
                 material = 1 if material in (None, 1) else -1
         if material == -1:
-            raise NotImplementedError("mixing elements with and without energies is not supported")
+            raise NotImplementedError("a mesh mixing elastic energy models (or elements without one) is not supported")
         if material == 1:
             # elements without energies only carry mass (Energy with empty sets)
             material = 0
@@ -280,14 +284,17 @@ class _EnergyBase:
     @classmethod
     def from_arrays(cls, undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha=0.0, *, density,
                     youngsModulus, poissonsRatio, neumannBCmask=None, neumannBCvalue=None, forceTypesList=(),
-                    forceParameterList=None, muscleGroup=None, softconStiffness=None, softconDirection=None):
+                    forceParameterList=None, muscleGroup=None, softconStiffness=None, softconDirection=None,
+                    energy="neohookean"):
         """Neo-Hookean mesh from per-element arrays instead of one Params per element.
 
         Same system as the reference-style constructor; meant for meshes with
         millions of elements where building Python Params objects dominates set-up."""
         obj = cls.__new__(cls)
+        if energy not in ("neohookean", "stableneohookean"):
+            raise NotImplementedError(f"element energy {energy} is not built on the GPU path")
         obj._init_arrays(undeformedVertices, eleIdx, settings, gravAcceleration, dampingAlpha, density,
-                         youngsModulus, poissonsRatio)
+                         youngsModulus, poissonsRatio, 2 if energy == "stableneohookean" else 0)
         if muscleGroup is not None:
             obj.set_muscles(muscleGroup, softconStiffness, softconDirection)
         ctypes_, cp = [], Params()

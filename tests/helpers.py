@@ -9,7 +9,7 @@ from sors_b200 import meshes
 def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha=0.0, dt=1e-3,
               scheme="backward_euler", method="minimize_newton", precision="fp64", project=True,
               clamp=True, res_tol=0.0, faces=None, groups=None, vertex_force=False, oracle_project=False,
-              muscles=None):
+              muscles=None, energy="neohookean"):
     """(gpu_energy, gpu_solver, oracle_system, X) on one mesh."""
     from oracle import oracle as orc
     from sors_b200 import py_sors as ps
@@ -28,14 +28,14 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     s.precision = precision
     s.hessianProjection = project
     s.newtonResidualTol = res_tol
-    energies = [{"neohookean"}] * ne
+    energies = [{energy}] * ne
     params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [rhov[i], Ev[i], nuv[i]]) for i in range(ne)]
     if muscles is not None:
         # per-element "softconMuscle" energies with their Params (tetrahedron.cpp:82-88)
         energies = list(energies)
         for i in range(ne):
             if muscles["group"][i] >= 0:
-                energies[i] = {"neohookean", "softconMuscle"}
+                energies[i] = {energy, "softconMuscle"}
                 params[i].set_param("muscleGroup", float(muscles["group"][i]))
                 params[i].set_param("softconStiffness", float(muscles["k"][i]))
                 params[i].set_param("softconDirection", np.asarray(muscles["dir"][i], float).reshape(1, 3))
@@ -56,7 +56,8 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     en = ps.Energy(X, T, s, np.asarray(grav, float), alpha, energies, params, ctypes_, cparams, ftypes, fparams)
     sol = ps.Solver(s)
     o = orc.System(X, T, rho=rhov, youngs=Ev, nu=nuv, grav=grav, alpha=alpha, scheme=scheme, method=method,
-                   project=oracle_project, dt=dt, substeps=1)
+                   project=oracle_project, dt=dt, substeps=1,
+                   material=orc.MAT_STABLE_NEOHOOKEAN if energy == "stableneohookean" else orc.MAT_NEOHOOKEAN)
     if clamp:
         o.set_neumann(mask, val)
     if faces is not None:

@@ -282,3 +282,52 @@ def test_softcon_contraction_oracle(oracle, golden):
         assert st == 0
     z = q.reshape(-1, 3)[:, 2]
     assert z.max() - z.min() < X[:, 2].max() - X[:, 2].min()
+
+
+# --- Stable Neo-Hookean (cpp/src/energies/stableNeoHookean.cpp) -------------
+
+def _torch_snh(X, x, E, nu):
+    """Psi*V of the stable Neo-Hookean energy with the reference's
+    reparameterisation (stableNeoHookean.cpp:10-15), as python/_autodiff_check.py."""
+    from oracle import oracle as orc
+    nv = X.shape[0]
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu)); mu = E / (2 * (1 + nu))
+    mu_s = 4.0 / 3.0 * mu; lam_s = lam + 5.0 / 8.0 * mu_s; alpha = 1 + 0.75 * mu_s / lam_s
+    xt = torch.tensor(x, dtype=torch.float64, requires_grad=True)
+    if nv == 4:
+        Dm = torch.tensor((X[:3] - X[3]).T)
+        Fs = [(xt[:3] - xt[3]).T @ torch.linalg.inv(Dm)]
+        V = abs(np.linalg.det(X[:3] - X[3])) / 6
+    else:
+        G, _, V = orc.hex_init(X)
+        Fs = [xt.T @ torch.tensor(G[s]) for s in range(8)]
+    psi = 0
+    for F in Fs:
+        J = torch.det(F); IC = (F * F).sum()
+        psi = psi + (0.5 * mu_s * (IC - 3) + 0.5 * lam_s * (J - alpha) ** 2 - 0.5 * mu_s * torch.log(IC + 1)) / len(Fs)
+    return psi * V, xt
+
+
+@pytest.mark.parametrize("nv", [4, 8])
+def test_stable_neohookean_vs_autograd(oracle, nv):
+    rng = np.random.default_rng(31 + nv)
+    if nv == 4:
+        X = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0], [0, 0, 1]], float) * 0.01
+    else:
+        from sors_b200.meshes import hex_grid_elements, grid_nodes
+        X = grid_nodes(1, 1, 1, (0.01, 0.012, 0.009))[hex_grid_elements(1, 1, 1)[0]]
+    for trial in range(5):
+        A = np.eye(3) + rng.uniform(-0.3, 0.3, (3, 3))
+        if trial == 4:
+            A[:, 0] *= -1.0   # an inverted element: the energy stays finite
+        x = X @ A.T
+        E, nu = 1e5 * (1 + trial), 0.3 + 0.04 * trial
+        psi, g, H, st = oracle.elem_eval_material(X, x, E, nu, oracle.MAT_STABLE_NEOHOOKEAN)
+        assert st == 0
+        tpsi, xt = _torch_snh(X, x, E, nu)
+        tg = torch.autograd.grad(tpsi, xt, create_graph=True)[0]
+        tH = torch.stack([torch.autograd.grad(tg.reshape(-1)[i], xt, retain_graph=True)[0].reshape(-1)
+                          for i in range(3 * nv)])
+        assert abs(psi - tpsi.item()) <= 1e-12 * abs(tpsi.item()) + 1e-18
+        np.testing.assert_allclose(g, tg.detach().numpy().ravel(), rtol=1e-10, atol=1e-10 * np.abs(g).max())
+        np.testing.assert_allclose(H, tH.numpy(), rtol=1e-9, atol=1e-10 * np.abs(H).max())
