@@ -535,6 +535,18 @@ class IO:
         return _meshes.extract_surfaces(np.asarray(vertices, float), np.asarray(eleIdx))
 
     @staticmethod
+    def read_tet_MSH(filename, verboseFlag=False):
+        """IO::read_tet_MSH (cpp/src/io.cpp:380-471): (vertices (N,3), tets (E,4)), MSH 4.1 / 2.2."""
+        from . import msh
+        return msh.read_tet_msh(filename)
+
+    @staticmethod
+    def read_hex_MSH(filename, verboseFlag=False):
+        """IO::read_hex_MSH (cpp/src/io.cpp:473-569): (vertices (N,3), hexes (E,8))."""
+        from . import msh
+        return msh.read_hex_msh(filename)
+
+    @staticmethod
     def hex_to_5_tets(hexElements):
         """cpp/src/io.cpp:899-929."""
         h = np.asarray(hexElements, dtype=np.int32)
