@@ -64,6 +64,9 @@ typedef struct SorsSettings {
     int32_t max_blocks;      /* largest grid of any kernel of this handle; 0 = the
                                 whole GPU (148 x 8 blocks).  Smaller grids let the
                                 kernels of several handles run side by side     */
+    int32_t newton_safeguard;/* 1 (with project_spd 2, "minimize_newton"): halve a
+                                Newton step that does not reduce ||g|| (no
+                                reference counterpart; off by default)            */
 } SorsSettings;
 
 typedef struct SorsStepStats {

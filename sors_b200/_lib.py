@@ -35,6 +35,7 @@ class SorsSettings(C.Structure):
         ("device", C.c_int32),
         ("newton_predictor", C.c_int32),
         ("max_blocks", C.c_int32),
+        ("newton_safeguard", C.c_int32),
     ]
 
 

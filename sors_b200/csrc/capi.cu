@@ -77,6 +77,7 @@ struct SorsHandle {
            *vforce = nullptr, *q_save = nullptr;
     int* conn = nullptr;
     double2* mat = nullptr;
+    double* tshape = nullptr;  // tets: shape gradients and volume per element
     int *row_ptr = nullptr, *col = nullptr, *diag_slot = nullptr, *pair_ptr = nullptr, *pair_ev = nullptr,
         *slot_item_ptr = nullptr;
     uint16_t* slot_items = nullptr;
@@ -384,6 +385,7 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
     if (st) return st;
     AsmArgs<HT> a;
     a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
+    a.tshape = h->tshape;
     a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
     a.H = (HT*)h->H; a.nnzb = h->nnzb; a.g_int = h->g_int; a.status = h->status;
@@ -642,6 +644,7 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
             if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
             if (stats) stats->pcg_iters += pit;
         }
+        double alpha = 1.0;
         if (m == 1) {
             // Armijo backtracking (solver.cpp:201-264): c = 0.1, beta = 0.5
             CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
@@ -649,7 +652,6 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
             double e0;
             if ((st = eval_energy(h, dt, &e0))) return st;
             double gdx = h->sc_host->gdx;
-            double alpha = 1.0;
             bool accepted = false;
             for (int ls = 0; ls < 64; ls++) {
                 launch_newton_update<VT>(n, (const VT*)h->x, alpha, h->q, h->q0, h->partials, h->sc, 6, h->stream);
@@ -662,10 +664,27 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         } else {
             CK(cudaMemcpyAsync(h->q0, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
             launch_newton_update<VT>(n, (const VT*)h->x, 1.0, h->q, h->q0, h->partials, h->sc, 6, h->stream);
+            if (m == 0 && h->s.project_spd == 2 && h->s.newton_safeguard) {
+                // Residual safeguard for the exact-Hessian Newton step: where the
+                // full step raises ||g|| (far from the solution, or where PCG
+                // met an indefinite Hessian without seeing it), halve it until
+                // ||g(q + a dx)|| <= (1 - 1e-4 a) ||g(q)||.  Full steps that
+                // decrease the residual are taken as the reference takes them.
+                for (int ls = 0; ls < 12; ls++) {
+                    if ((st = eval_system<HT>(h, dt, false))) return st;
+                    CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+                    CK(cudaStreamSynchronize(h->stream));
+                    const double gt = sqrt(h->sc_host->gnorm2);
+                    if (gt == gt && gt <= (1.0 - 1e-4 * alpha) * gn) break;
+                    alpha *= 0.5;
+                    launch_newton_update<VT>(n, (const VT*)h->x, alpha, h->q, h->q0, h->partials, h->sc, 6,
+                                             h->stream);
+                }
+            }
         }
         CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
-        double dxn = sqrt(h->sc_host->dxnorm2);
+        double dxn = sqrt(h->sc_host->dxnorm2) / alpha;
         if (stats) stats->dx_norm = dxn;
         if (verbose())
             fprintf(stderr, "[sors] newton %d |g|=%.3e eta=%.2e pcg=%d |r|/|b|=%.2e |dx|=%.3e\n", it, gn, eta, pit,
@@ -1060,6 +1079,7 @@ void sors_default_settings(SorsSettings* s) {
     s->device = 0;
     s->newton_predictor = 1;
     s->max_blocks = 0;
+    s->newton_safeguard = 0;
 }
 
 int sors_last_error(char* buf, size_t n) {
@@ -1106,6 +1126,11 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if ((st = upload(h, &h->conn, conn, (size_t)E * nv))) return bail(st);
     if ((st = upload(h, &h->mat, mat.data(), (size_t)E))) return bail(st);
     if ((st = upload(h, &h->mass, mass.data(), (size_t)N))) return bail(st);
+    if (nv == 4) {
+        if ((st = dalloc_t(h, &h->tshape, (size_t)10 * std::max(1, E)))) return bail(st);
+        launch_tet_shapes(E, h->X, h->conn, h->tshape, h->stream);
+        CK(cudaStreamSynchronize(h->stream));
+    }
     if ((st = build_pattern(h, conn))) return bail(st);
     const size_t nd = (size_t)3 * N;
     double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,
@@ -1359,10 +1384,10 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
     cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream);
     cudaMemsetAsync(h->status, 0, sizeof(int), h->stream);
     if (mixed(h))
-        launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
+        launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->tshape, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                 h->status, h->stream);
     else
-        launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
+        launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->tshape, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                  h->status, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
     if (e == cudaSuccess && psi) e = d2h(h, psi, dpsi, sizeof(double) * h->E);
@@ -1586,6 +1611,7 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     if (st) return st;
     AsmArgs<HT> aa;
     aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat; aa.mus = muscles(h);
+    aa.tshape = h->tshape;
     aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
     aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
     aa.H = (HT*)h->H; aa.nnzb = h->nnzb; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;

@@ -107,18 +107,21 @@ static inline int red_grid(long long n, int per_thread = 1) {
 // ---------------------------------------------------------------------------
 // element row evaluation shared by the assembly and the parity hook
 // ---------------------------------------------------------------------------
+// Tets read their shape gradients d_0..d_2 and volume from tsh (10 doubles per
+// element, written once by k_tet_shapes; d_3 = -(d_0 + d_1 + d_2)); hexes
+// recompute theirs from the undeformed positions at every quadrature point.
 template <typename HT, int NV, bool HESS, bool SNH = false>
 __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const double* __restrict__ qg,
                                          const int* __restrict__ conn, const double2* __restrict__ mat,
-                                         const MuscleArgs& mus, int e, int v, int material, bool project, double* g,
-                                         HT (&blk)[NV * 9]) {
+                                         const double* __restrict__ tsh, const MuscleArgs& mus, int e, int v,
+                                         int material, bool project, double* g, HT (&blk)[NV * 9]) {
     double X[NV][3], x[NV][3];
 #pragma unroll
     for (int w = 0; w < NV; w++) {
         const int n = __ldg(conn + (size_t)e * NV + w);
 #pragma unroll
         for (int r = 0; r < 3; r++) {
-            X[w][r] = __ldg(Xg + 3 * (size_t)n + r);
+            if (NV != 4) X[w][r] = __ldg(Xg + 3 * (size_t)n + r);
             x[w][r] = qg[3 * (size_t)n + r];
         }
     }
@@ -147,7 +150,19 @@ __device__ __forceinline__ bool elem_row(const double* __restrict__ Xg, const do
     double d[NV][3];
     double dv[3];
     if (NV == 4) {
-        const double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
+        const double2* ts = reinterpret_cast<const double2*>(tsh + (size_t)e * 10);
+        double t[10];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const double2 u = __ldg(ts + k);
+            t[2 * k] = u.x; t[2 * k + 1] = u.y;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            d[0][c] = t[c]; d[1][c] = t[3 + c]; d[2][c] = t[6 + c];
+            d[3][c] = -(t[c] + t[3 + c] + t[6 + c]);
+        }
+        const double V = t[9];
 #pragma unroll
         for (int w = 0; w < NV; w++)
             if (w == v) { dv[0] = d[w][0]; dv[1] = d[w][1]; dv[2] = d[w][2]; }
@@ -307,6 +322,34 @@ void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const 
     counted();
 }
 
+// Per-tet shape gradients d_0..d_2 (rows of Dm^-1) and undeformed volume,
+// computed once at mesh load (tetrahedron.cpp:11-15, :137-149).
+__global__ void k_tet_shapes(int E, const double* __restrict__ Xg, const int* __restrict__ conn,
+                             double* __restrict__ out) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    double X[4][3], d[4][3];
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const int n = conn[(size_t)e * 4 + w];
+#pragma unroll
+        for (int r = 0; r < 3; r++) X[w][r] = Xg[3 * (size_t)n + r];
+    }
+    const double V = tet_shape((const double(*)[3])X, (double(*)[3])d);
+    double* o = out + (size_t)e * 10;
+#pragma unroll
+    for (int w = 0; w < 3; w++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) o[w * 3 + c] = d[w][c];
+    o[9] = V;
+}
+
+void launch_tet_shapes(int E, const double* X, const int* conn, double* out, cudaStream_t st) {
+    if (E == 0) return;
+    k_tet_shapes<<<(E + 127) / 128, 128, 0, st>>>(E, X, conn, out);
+    counted();
+}
+
 // ---------------------------------------------------------------------------
 // Row-owner assembly of gradient rows and Hessian block-rows.
 // ---------------------------------------------------------------------------
@@ -327,12 +370,12 @@ __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_a
             const int e = ev >> 3, v = ev & 7;
             HT blk[NV * 9];
             if (a.want_hess) {
-                ok &= elem_row<HT, NV, true, SNH>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, a.project != 0, g, blk);
+                ok &= elem_row<HT, NV, true, SNH>(a.X, a.q, a.conn, a.mat, a.tshape, a.mus, e, v, a.material, a.project != 0, g, blk);
                 HT* dst = stage + (size_t)k * NV * 9;
 #pragma unroll
                 for (int t = 0; t < NV * 9; t++) dst[t] = blk[t];
             } else {
-                ok &= elem_row<HT, NV, false, SNH>(a.X, a.q, a.conn, a.mat, a.mus, e, v, a.material, false, g, blk);
+                ok &= elem_row<HT, NV, false, SNH>(a.X, a.q, a.conn, a.mat, a.tshape, a.mus, e, v, a.material, false, g, blk);
             }
         }
         if (!ok) atomicOr(a.status, kFlagInverted);
@@ -401,15 +444,16 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
 // Element-level parity hook: thread per (element, local vertex).
 template <typename HT, int NV>
 __global__ void k_elem_rows(int E, const double* X, const double* q, const int* conn, const double2* mat,
-                            MuscleArgs mus, int material, int project, double* psi, double* grad, double* hess,
-                            int* status) {
+                            const double* tsh, MuscleArgs mus, int material, int project, double* psi, double* grad,
+                            double* hess, int* status) {
     long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= (long long)E * NV) return;
     int e = (int)(t / NV), v = (int)(t - (long long)e * NV);
     double g[3] = {0.0, 0.0, 0.0};
     HT blk[NV * 9];
-    bool ok = material == 2 ? elem_row<HT, NV, true, true>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk)
-                            : elem_row<HT, NV, true, false>(X, q, conn, mat, mus, e, v, material, project != 0, g, blk);
+    bool ok = material == 2
+                  ? elem_row<HT, NV, true, true>(X, q, conn, mat, tsh, mus, e, v, material, project != 0, g, blk)
+                  : elem_row<HT, NV, true, false>(X, q, conn, mat, tsh, mus, e, v, material, project != 0, g, blk);
     if (!ok) atomicOr(status, kFlagInverted);
     const int n = 3 * NV;
     if (grad)
@@ -424,18 +468,18 @@ __global__ void k_elem_rows(int E, const double* X, const double* q, const int* 
 
 template <typename HT>
 void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                      const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
+                      const double* tsh, const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
                       cudaStream_t st) {
     long long n = (long long)E * nv;
     if (n == 0) return;
     int threads = 128;
     int blocks = (int)((n + threads - 1) / threads);
     if (nv == 4)
-        k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, project, psi, grad, hess,
-                                                       status);
+        k_elem_rows<HT, 4><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, tsh, mus, material, project, psi, grad,
+                                                       hess, status);
     else
-        k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, mus, material, project, psi, grad, hess,
-                                                       status);
+        k_elem_rows<HT, 8><<<blocks, threads, 0, st>>>(E, X, q, conn, mat, tsh, mus, material, project, psi, grad,
+                                                       hess, status);
     counted();
 }
 
@@ -1158,10 +1202,10 @@ template void launch_add_vec<float>(int, const double*, const float*, double*, c
 template void launch_assemble<double>(const AsmArgs<double>&, int, cudaStream_t);
 template void launch_assemble<float>(const AsmArgs<float>&, int, cudaStream_t);
 template void launch_elem_rows<double>(int, int, const double*, const double*, const int*, const double2*,
-                                       const MuscleArgs&, int, int,
+                                       const double*, const MuscleArgs&, int, int,
                                        double*, double*, double*, int*, cudaStream_t);
 template void launch_elem_rows<float>(int, int, const double*, const double*, const int*, const double2*,
-                                      const MuscleArgs&, int, int,
+                                      const double*, const MuscleArgs&, int, int,
                                       double*, double*, double*, int*, cudaStream_t);
 template void launch_pressure_jac<double>(const PressureArgs&, const int*, const int*, const uint8_t*, double, double*,
                                           long long, cudaStream_t);

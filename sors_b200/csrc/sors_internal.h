@@ -64,6 +64,7 @@ struct AsmArgs {
     const double* q;        // 3N current
     const int* conn;        // E*nv
     const double2* mat;     // (mu, lambda) per element
+    const double* tshape;   // tets: d_0..d_2 and volume per element (10 doubles)
     MuscleArgs mus;
     const int* pair_ptr;    // N+1
     const int* pair_ev;     // e*8 + v
@@ -111,11 +112,12 @@ template <typename HT>
 void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st);
 template <typename HT>
 void launch_elem_rows(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
-                      const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
+                      const double* tsh, const MuscleArgs& mus, int material, int project, double* psi, double* grad, double* hess, int* status,
                       cudaStream_t st);
 void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
                         const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
+void launch_tet_shapes(int E, const double* X, const int* conn, double* out, cudaStream_t st);
 void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
                          const MuscleArgs& mus, int material, const double* lam, double* out, cudaStream_t st);
 template <typename HT>
