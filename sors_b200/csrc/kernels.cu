@@ -353,7 +353,190 @@ void launch_tet_shapes(int E, const double* X, const int* conn, double* out, cud
 // ---------------------------------------------------------------------------
 // Row-owner assembly of gradient rows and Hessian block-rows.
 // ---------------------------------------------------------------------------
-template <typename HT, int NV, bool SNH>
+// Row v of tet e written straight into the warp's staging buffer (dst = 4
+// blocks of 9): the same terms as elem_row + nh_qp_row / snh_qp_row +
+// muscle_qp_row, rearranged for registers: F accumulates while the vertices
+// load, and each block is finished (base terms, projection corrections,
+// fibre term) and stored before the next is formed.
+template <typename HT, bool HESS, bool SNH, bool PROJ>
+__device__ __forceinline__ bool tet_row_stage(const AsmArgs<HT>& a, int e, int v, double* g, HT* dst) {
+    const double2* ts = reinterpret_cast<const double2*>(a.tshape + (size_t)e * 10);
+    double t[10];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const double2 u = __ldg(ts + k);
+        t[2 * k] = u.x; t[2 * k + 1] = u.y;
+    }
+    // d_w = t[3w .. 3w+2] for w < 3, d_3 = -(d_0 + d_1 + d_2)
+    auto dcomp = [&](int w, int c) -> double {
+        return w < 3 ? t[3 * w + c] : -(t[c] + t[3 + c] + t[6 + c]);
+    };
+    const double V = t[9];
+    double F[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) F[k] = 0.0;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const int n = __ldg(a.conn + (size_t)e * 4 + w);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const double xr = a.q[3 * (size_t)n + r];
+#pragma unroll
+            for (int c = 0; c < 3; c++) F[r * 3 + c] += xr * dcomp(w, c);
+        }
+    }
+    double dv[3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int w = 0; w < 4; w++)
+            if (w == v) acc = dcomp(w, c);
+        dv[c] = acc;
+    }
+    const double2 m = __ldg(a.mat + e);
+    const int grp = a.mus.group ? __ldg(a.mus.group + e) : -1;
+    double C[9];
+    cof3(F, C);
+    const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+    if (SNH ? (J == 0.0) : !(J > 0.0)) {
+        // the gradient row still follows the reference (NaN or inf as it gives)
+    }
+    const double iJ = 1.0 / J;
+    double IC = 0.0;
+    if (SNH) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+    }
+    const double alpha = SNH ? 1.0 + 0.75 * m.x / m.y : 0.0;
+    const double logJ = SNH ? 0.0 : log(J);
+    // P = pa F + pb G with G = C / J
+    const double pa = SNH ? m.x * (1.0 - 1.0 / (IC + 1.0)) : m.x;
+    const double pb = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        double pr = 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; c++) pr += (pa * F[r * 3 + c] + pb * C[r * 3 + c] * iJ) * dv[c];
+        g[r] += V * pr;
+    }
+    // fibre term (muscle_qp_row)
+    double4 mp = make_double4(0.0, 0.0, 0.0, 0.0);
+    double mu_u[3] = {0.0, 0.0, 0.0}, mu_c = 0.0, mu_hv = 0.0, mu_il2 = 0.0;
+    if (grp >= 0) {
+        mp = a.mus.param[e];
+        const double eact = __ldg(a.mus.act + grp);
+#pragma unroll
+        for (int r = 0; r < 3; r++) mu_u[r] = F[r * 3 + 0] * mp.x + F[r * 3 + 1] * mp.y + F[r * 3 + 2] * mp.z;
+        const double l = sqrt(mu_u[0] * mu_u[0] + mu_u[1] * mu_u[1] + mu_u[2] * mu_u[2]);
+        const double rr = (1.0 - eact) / l;
+        const double sv = dv[0] * mp.x + dv[1] * mp.y + dv[2] * mp.z;
+        const double gc = V * mp.w * (1.0 - rr) * sv;
+#pragma unroll
+        for (int r = 0; r < 3; r++) g[r] += gc * mu_u[r];
+        mu_c = 1.0 - rr;
+        if (PROJ && mu_c < 0.0) mu_c = 0.0;
+        mu_il2 = 1.0 / (l * l);
+        mu_hv = V * mp.w * sv;
+    }
+    const bool ok = SNH ? (J != 0.0) : (J > 0.0);
+    if (!HESS) return ok;
+    if (!ok) {
+#pragma unroll
+        for (int k = 0; k < 36; k++) dst[k] = HT(0);
+        return false;
+    }
+    HT Gh[9], Fh[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) { Gh[k] = (HT)(C[k] * iJ); Fh[k] = (HT)F[k]; }
+    const HT dvh[3] = {(HT)dv[0], (HT)dv[1], (HT)dv[2]};
+    HT av[3], fv[3];
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+        av[r] = Gh[r * 3 + 0] * dvh[0] + Gh[r * 3 + 1] * dvh[1] + Gh[r * 3 + 2] * dvh[2];
+        fv[r] = Fh[r * 3 + 0] * dvh[0] + Fh[r * 3 + 1] * dvh[1] + Fh[r * 3 + 2] * dvh[2];
+    }
+    // coefficients: block(v,w)[k][l] = hmu dd d_kl + h1 av_k aw_l - h2 aw_k av_l + h4 fv_k fw_l
+    const HT hmu = (HT)(V * pa);
+    const HT h1 = (HT)(SNH ? V * m.y * (2.0 * J - alpha) * J : V * m.y);
+    const HT h2 = (HT)(V * pb);
+    const HT h4 = (HT)(SNH ? V * 2.0 * m.x / ((IC + 1.0) * (IC + 1.0)) : 0.0);
+    NhModes<HT> pm;
+    HT dhv[3];
+    if (PROJ) {
+        if (SNH) snh_modes<HT>(Fh, (HT)J, (HT)IC, (HT)m.x, (HT)m.y, (HT)alpha, pm);
+        else nh_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)m.x, (HT)m.y, pm);
+#pragma unroll
+        for (int c = 0; c < 3; c++) dhv[c] = pm.V[0 * 3 + c] * dvh[0] + pm.V[1 * 3 + c] * dvh[1] + pm.V[2 * 3 + c] * dvh[2];
+    }
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        const HT dw[3] = {(HT)dcomp(w, 0), (HT)dcomp(w, 1), (HT)dcomp(w, 2)};
+        HT aw[3], fw[3];
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            aw[r] = Gh[r * 3 + 0] * dw[0] + Gh[r * 3 + 1] * dw[1] + Gh[r * 3 + 2] * dw[2];
+            fw[r] = Fh[r * 3 + 0] * dw[0] + Fh[r * 3 + 1] * dw[1] + Fh[r * 3 + 2] * dw[2];
+        }
+        const HT dd = dvh[0] * dw[0] + dvh[1] * dw[1] + dvh[2] * dw[2];
+        HT b[9];
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+#pragma unroll
+            for (int l = 0; l < 3; l++) {
+                HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
+                if (SNH) val += h4 * fv[k] * fw[l];
+                if (k == l) val += hmu * dd;
+                b[k * 3 + l] = val;
+            }
+        if (PROJ && pm.any) {
+            const HT wv = (HT)V;
+            HT dhw[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) dhw[c] = pm.V[0 * 3 + c] * dw[0] + pm.V[1 * 3 + c] * dw[1] + pm.V[2 * 3 + c] * dw[2];
+            HT uv[3], uw[3];
+#define SORS_TF(M, I, JJ)                                      \
+    if (pm.lt[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(-1), uv);              \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(-1), uw);              \
+        add_outer(b, -pm.lt[M] * wv, uv, uw);                  \
+    }                                                          \
+    if (pm.lf[M] < HT(0)) {                                    \
+        tf_vec<HT, I, JJ>(pm.U, dhv, HT(1), uv);               \
+        tf_vec<HT, I, JJ>(pm.U, dhw, HT(1), uw);               \
+        add_outer(b, -pm.lf[M] * wv, uv, uw);                  \
+    }
+            SORS_TF(0, 0, 1)
+            SORS_TF(1, 0, 2)
+            SORS_TF(2, 1, 2)
+#undef SORS_TF
+#define SORS_SC(M)                                             \
+    if (pm.ls[M] < HT(0)) {                                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhv, uv);                    \
+        sc_vec<HT, M>(pm.U, pm.Y, dhw, uw);                    \
+        add_outer(b, -pm.ls[M] * wv, uv, uw);                  \
+    }
+            SORS_SC(0)
+            SORS_SC(1)
+            SORS_SC(2)
+#undef SORS_SC
+        }
+        if (grp >= 0) {
+            const double sw = dcomp(w, 0) * mp.x + dcomp(w, 1) * mp.y + dcomp(w, 2) * mp.z;
+            const HT f = (HT)(mu_hv * sw);
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int l = 0; l < 3; l++)
+                    b[k * 3 + l] += f * (HT)((1.0 - mu_c) * mu_u[k] * mu_u[l] * mu_il2 + (k == l ? mu_c : 0.0));
+        }
+#pragma unroll
+        for (int k = 0; k < 9; k++) dst[w * 9 + k] = b[k];
+    }
+    return true;
+}
+
+template <typename HT, int NV, bool SNH, bool PROJ>
 __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_assemble(AsmArgs<HT> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
@@ -368,6 +551,27 @@ __global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? 2 : 1) k_a
         for (int k = lane; k < np; k += 32) {
             const int ev = __ldg(a.pair_ev + p0 + k);
             const int e = ev >> 3, v = ev & 7;
+            if (NV == 4) {
+                HT* dst = stage + (size_t)k * 36;
+                if (a.material == 1) {
+                    // quartic test element of the reference (cpp/src/_test.cpp:31-66)
+#pragma unroll
+                    for (int t = 0; t < 36; t++) dst[t] = HT(0);
+                    const int n = __ldg(a.conn + (size_t)e * 4 + v);
+#pragma unroll
+                    for (int r = 0; r < 3; r++) {
+                        const double xv = a.q[3 * (size_t)n + r];
+                        g[r] += (2 * xv - 1) * (2 * xv + 1) * xv;
+                        dst[v * 9 + r * 3 + r] = (HT)(12 * xv * xv - 1);
+                    }
+                } else if (a.want_hess) {
+                    ok &= (PROJ ? tet_row_stage<HT, true, SNH, true>(a, e, v, g, dst)
+                                : tet_row_stage<HT, true, SNH, false>(a, e, v, g, dst));
+                } else {
+                    ok &= tet_row_stage<HT, false, SNH, false>(a, e, v, g, dst);
+                }
+                continue;
+            }
             HT blk[NV * 9];
             if (a.want_hess) {
                 ok &= elem_row<HT, NV, true, SNH>(a.X, a.q, a.conn, a.mat, a.tshape, a.mus, e, v, a.material, a.project != 0, g, blk);
@@ -428,12 +632,15 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     blocks = cap_grid(blocks);
     const bool snh = a.material == 2;
     if (nv == 4) {
-        auto k = snh ? k_assemble<HT, 4, true> : k_assemble<HT, 4, false>;
+        // tets: projection selects the kernel variant (the exact Hessian keeps
+        // the projection's registers out of the common case)
+        auto k = snh ? (a.project ? k_assemble<HT, 4, true, true> : k_assemble<HT, 4, true, false>)
+                     : (a.project ? k_assemble<HT, 4, false, true> : k_assemble<HT, 4, false, false>);
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
     } else {
-        auto k = snh ? k_assemble<HT, 8, true> : k_assemble<HT, 8, false>;
+        auto k = snh ? k_assemble<HT, 8, true, false> : k_assemble<HT, 8, false, false>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
