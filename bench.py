@@ -61,6 +61,7 @@ def block_mesh(cells, seed=0):
 
 PROJECTION = {"true": True, "false": False, "adaptive": "adaptive"}
 _projection = "adaptive"
+_two_level = False
 
 
 def make_settings(precision):
@@ -73,6 +74,7 @@ def make_settings(precision):
     s.solverMethod = "minimize_newton"
     s.precision = precision
     s.hessianProjection = PROJECTION[_projection]
+    s.twoLevelPreconditioner = _two_level
     s.newtonResidualTol = 1e-8
     return s
 
@@ -320,6 +322,7 @@ def run_gpu(args, rank, world, local_rank):
                    "elements": ne, "nodes": nn, "dofs": 3 * nn, "precision": args.precision,
                    "newton": "||dx||<1e-9 or ||g||<1e-8, Eisenstat-Walker PCG forcing",
                    "hessian_projection": _projection,
+                   "preconditioner": "two-level" if _two_level else "block Jacobi",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (assembled system ~1 GB resident), no flush"},
         "newton_steps_per_s": world * args.steps / (ms / 1e3),
@@ -608,6 +611,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--two-level", action="store_true",
+                    help="two-level PCG preconditioner (block Jacobi + coarse rigid-body correction)")
     ap.add_argument("--projection", default="adaptive", choices=sorted(PROJECTION),
                     help="SPD projection of the element Hessians: always, never, or only where PCG meets "
                          "negative curvature")
@@ -630,8 +635,9 @@ def main():
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global _projection
+    global _projection, _two_level
     _projection = args.projection
+    _two_level = args.two_level
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

@@ -67,6 +67,9 @@ typedef struct SorsSettings {
     int32_t newton_safeguard;/* 1 (with project_spd 2, "minimize_newton"): halve a
                                 Newton step that does not reduce ||g|| (no
                                 reference counterpart; off by default)            */
+    int32_t two_level;       /* 1: precondition the Newton PCG with block Jacobi
+                                plus an exact coarse correction on per-aggregate
+                                rigid-body modes (no reference counterpart)     */
 } SorsSettings;
 
 typedef struct SorsStepStats {

@@ -36,6 +36,7 @@ class SorsSettings(C.Structure):
         ("newton_predictor", C.c_int32),
         ("max_blocks", C.c_int32),
         ("newton_safeguard", C.c_int32),
+        ("two_level", C.c_int32),
     ]
 
 

@@ -136,10 +136,22 @@ struct SorsHandle {
     int last_active = 0;
     std::vector<int> held_nodes;      // contacts held at the end of the last SQP step
     std::vector<double> held_normals;
+    // two-level preconditioner (settings.two_level): node aggregates, the
+    // Galerkin coarse matrix and its inverse (refreshed when PCG slows down)
+    bool tl_ready = false, tl_active = false;
+    double tl_ref_rate = 0.0;
+    CoarseArgs cargs;
+    int tl_npairs = 0;
+    int *tl_pair_ptr = nullptr;
+    int2 *tl_items = nullptr, *tl_ab = nullptr;
+    double *tl_Ac = nullptr, *tl_yc = nullptr, *tl_rowk = nullptr, *tl_colk = nullptr;
+    void *tl_Ainv = nullptr, *tl_zc = nullptr;
+    int tl_refreshes = 0;
+
     // projection used by the PCG kernels (null: none)
     const uint8_t* proj_flag = nullptr;
     const double4* proj_n = nullptr;
-    bool pcg_exec_proj = false;
+    int pcg_exec_mode = 0;  // 0 block Jacobi, 1 projected, 2 two-level
 
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
@@ -428,6 +440,20 @@ int eval_energy(SorsHandle* h, double dt, double* out) {
 template <typename HT, typename VT>
 void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
+    if (h->tl_active) {
+        for (int half = 0; half < 2; half++) {
+            VT* pin = (VT*)(half ? h->p1 : h->p0);
+            VT* pout = (VT*)(half ? h->p0 : h->p1);
+            launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, pin,
+                                    pout, (VT*)h->qv, h->partials, h->sc, h->stream);
+            launch_tl_update<VT>(h->N, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->sc, h->stream);
+            launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
+            launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
+            launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, z, 0, h->partials, h->sc,
+                            h->stream);
+        }
+        return;
+    }
     launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
                             h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
@@ -440,13 +466,14 @@ void pcg_iter_pair(SorsHandle* h) {
 
 template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
-    if (h->pcg_exec && h->pcg_exec_proj != (h->proj_flag != nullptr)) {
+    const int mode = h->proj_flag ? 1 : (h->tl_active ? 2 : 0);
+    if (h->pcg_exec && h->pcg_exec_mode != mode) {
         // the captured launches carry the projection pointers: capture again
         cudaGraphExecDestroy(h->pcg_exec);
         h->pcg_exec = nullptr;
     }
     if (!h->pcg_exec && !h->graph_failed) {
-        h->pcg_exec_proj = h->proj_flag != nullptr;
+        h->pcg_exec_mode = mode;
         cudaGraph_t graph = nullptr;
         const long long launches_before = g_kernel_launches.load();
         cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
@@ -479,9 +506,33 @@ int pcg_chunk(SorsHandle* h) {
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
+    // the two-level preconditioner serves the unconstrained Newton solves
+    h->tl_active = h->s.two_level && h->cargs.nc > 0 && !h->proj_flag;
+    bool refreshed = false;
+    if (h->tl_active && !h->tl_ready) {
+        const int nc = h->cargs.nc;
+        CK(cudaMemsetAsync(h->tl_Ac, 0, sizeof(double) * (size_t)nc * nc, h->stream));
+        if (sizeof(HT) == 4)
+            launch_coarse_galerkin_f(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col, (const float*)h->H,
+                                     h->nnzb, h->cargs, h->tl_Ac, h->stream);
+        else
+            launch_coarse_galerkin_d(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col,
+                                     (const double*)h->H, h->nnzb, h->cargs, h->tl_Ac, h->stream);
+        launch_coarse_invert(nc, h->tl_Ac, h->tl_rowk, h->tl_colk, h->stream);
+        launch_to_vt<VT>((long long)nc * nc, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
+        h->tl_ready = true;
+        h->tl_refreshes++;
+        refreshed = true;
+    }
     launch_pcg_init<HT, VT>(h->N, g ? g : h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0,
                             eta * eta, abs_tol * abs_tol, h->s.pcg_max_iter, h->proj_flag, h->proj_n, h->partials,
                             h->sc, h->stream);
+    if (h->tl_active) {
+        launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
+        launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
+        launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, (VT*)h->z, 1, h->partials,
+                        h->sc, h->stream);
+    }
     CK(cudaGetLastError());
     int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
     for (int c = 0; c < maxchunks; c++) {
@@ -492,6 +543,13 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
         if (h->sc_host->done) break;
     }
     *iters = h->sc_host->it;
+    if (h->tl_active && h->sc_host->it >= 8 && h->sc_host->rr > 0.0 && h->sc_host->bnorm2 > h->sc_host->rr) {
+        // iterations per decade of residual reduction: the coarse operator is
+        // rebuilt when that doubles against its value right after a rebuild
+        const double rate = h->sc_host->it / (0.5 * log10(h->sc_host->bnorm2 / h->sc_host->rr));
+        if (refreshed || h->tl_ref_rate <= 0.0) h->tl_ref_rate = rate;
+        else if (rate > 2.0 * h->tl_ref_rate) h->tl_ready = false;
+    }
     if (h->sc_host->breakdown && h->sc_host->it == 0 && !(h->s.project_spd == 2 && !h->proj_fallback))
         return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
     return SORS_OK;
@@ -782,6 +840,95 @@ void update_disk_group(SorsHandle* h, SorsHandle::DiskGroup& G, const double* q)
 
 void update_disk_contacts(SorsHandle* h, const double* q) {
     for (auto& G : h->disk_groups) update_disk_group(h, G, q);
+}
+
+// Two-level set-up: nodes binned into about N / 2000 (at most 256) boxes of
+// the undeformed bounding box, empty boxes dropped; each aggregate's coarse
+// unknowns are its 3 translations and 3 rotations about its centroid, the
+// rotations scaled by 1 / (box size).  The Galerkin matrix P^T H P is summed
+// per aggregate pair over a fixed list of Hessian blocks (deterministic).
+int setup_two_level(SorsHandle* h, const double* X) {
+    const int N = h->N;
+    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], X[3 * i + k]); hi[k] = std::max(hi[k], X[3 * i + k]); }
+    const int target = std::max(1, std::min(256, N / 2000));
+    double L[3], vol = 1.0;
+    for (int k = 0; k < 3; k++) { L[k] = std::max(hi[k] - lo[k], 1e-12); }
+    double lmax = std::max(L[0], std::max(L[1], L[2]));
+    for (int k = 0; k < 3; k++) vol *= std::max(L[k], 1e-3 * lmax);
+    const double hb = cbrt(vol / target);
+    int dim[3];
+    for (int k = 0; k < 3; k++) dim[k] = std::max(1, (int)llround(L[k] / hb));
+    std::vector<int> bin(N), remap((size_t)dim[0] * dim[1] * dim[2], -1);
+    for (int i = 0; i < N; i++) {
+        int c[3];
+        for (int k = 0; k < 3; k++) c[k] = std::min(dim[k] - 1, (int)((X[3 * i + k] - lo[k]) / L[k] * dim[k]));
+        bin[i] = c[0] + dim[0] * (c[1] + dim[1] * c[2]);
+    }
+    int nagg = 0;
+    for (int i = 0; i < N; i++)
+        if (remap[bin[i]] < 0) remap[bin[i]] = 0;
+    for (auto& r : remap)
+        if (r == 0) r = nagg++;
+    std::vector<int> aid(N), cnt(nagg + 1, 0);
+    for (int i = 0; i < N; i++) { aid[i] = remap[bin[i]]; cnt[aid[i] + 1]++; }
+    for (int a = 0; a < nagg; a++) cnt[a + 1] += cnt[a];
+    std::vector<int> nodes(N), fillp(cnt.begin(), cnt.end() - 1);
+    for (int i = 0; i < N; i++) nodes[fillp[aid[i]]++] = i;
+    std::vector<double4> cen(nagg);
+    for (int a = 0; a < nagg; a++) {
+        double c[3] = {0, 0, 0};
+        for (int k = cnt[a]; k < cnt[a + 1]; k++)
+            for (int d = 0; d < 3; d++) c[d] += X[3 * nodes[k] + d];
+        const double n = std::max(1, cnt[a + 1] - cnt[a]);
+        cen[a] = make_double4(c[0] / n, c[1] / n, c[2] / n, 1.0 / hb);
+    }
+    // aggregate pairs and their Hessian blocks (counting sort by pair key)
+    const long long nkeys = (long long)nagg * nagg;
+    std::vector<int> keycnt((size_t)nkeys + 1, 0);
+    const int64_t nnzb = h->nnzb;
+    for (int i = 0; i < N; i++)
+        for (int b = h->row_ptr_h[i]; b < h->row_ptr_h[i + 1]; b++) keycnt[(size_t)aid[i] * nagg + aid[h->col_h[b]] + 1]++;
+    std::vector<int> pair_ptr{0};
+    std::vector<int2> pair_ab;
+    std::vector<long long> keypos((size_t)nkeys, -1);
+    long long acc = 0;
+    for (long long k = 0; k < nkeys; k++) {
+        if (keycnt[k + 1] == 0) continue;
+        keypos[k] = acc;
+        acc += keycnt[k + 1];
+        pair_ab.push_back(make_int2((int)(k / nagg), (int)(k % nagg)));
+        pair_ptr.push_back((int)acc);
+    }
+    std::vector<int2> items((size_t)nnzb);
+    for (int i = 0; i < N; i++)
+        for (int b = h->row_ptr_h[i]; b < h->row_ptr_h[i + 1]; b++) {
+            const long long k = (long long)aid[i] * nagg + aid[h->col_h[b]];
+            items[(size_t)keypos[k]++] = make_int2(b, i);
+        }
+    int st;
+    h->tl_npairs = (int)pair_ab.size();
+    const int nc = 6 * nagg;
+    int* aid_d = nullptr; double4* cen_d = nullptr; int* aggptr_d = nullptr; int* nodes_d = nullptr;
+    if ((st = upload(h, &aid_d, aid.data(), (size_t)N))) return st;
+    if ((st = upload(h, &cen_d, cen.data(), (size_t)nagg))) return st;
+    if ((st = upload(h, &aggptr_d, cnt.data(), (size_t)nagg + 1))) return st;
+    if ((st = upload(h, &nodes_d, nodes.data(), (size_t)N))) return st;
+    if ((st = upload(h, &h->tl_pair_ptr, pair_ptr.data(), pair_ptr.size()))) return st;
+    if ((st = upload(h, &h->tl_ab, pair_ab.data(), pair_ab.size()))) return st;
+    if ((st = upload(h, &h->tl_items, items.data(), items.size()))) return st;
+    if ((st = dalloc_t(h, &h->tl_Ac, (size_t)nc * nc))) return st;
+    if ((st = dalloc_t(h, &h->tl_yc, (size_t)nc))) return st;
+    if ((st = dalloc_t(h, &h->tl_rowk, (size_t)nc))) return st;
+    if ((st = dalloc_t(h, &h->tl_colk, (size_t)nc))) return st;
+    if ((st = dalloc(h, &h->tl_Ainv, (size_t)nc * nc * hsize(h)))) return st;
+    if ((st = dalloc(h, &h->tl_zc, (size_t)nc * hsize(h)))) return st;
+    h->cargs.N = N; h->cargs.nagg = nagg; h->cargs.nc = nc;
+    h->cargs.aid = aid_d; h->cargs.agg_c = cen_d; h->cargs.agg_ptr = aggptr_d; h->cargs.agg_nodes = nodes_d;
+    h->cargs.fixed = h->node_mask; h->cargs.X = h->X;
+    h->tl_ready = false;
+    return SORS_OK;
 }
 
 int ensure_sqp_buffers(SorsHandle* h, int m) {
@@ -1080,6 +1227,7 @@ void sors_default_settings(SorsSettings* s) {
     s->newton_predictor = 1;
     s->max_blocks = 0;
     s->newton_safeguard = 0;
+    s->two_level = 0;
 }
 
 int sors_last_error(char* buf, size_t n) {
@@ -1144,6 +1292,7 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     CK(h2d(h, h->q, X, nd * sizeof(double)));
     h->mask_h.assign(N, 0);
     if ((st = upload(h, &h->node_mask, h->mask_h.data(), (size_t)N))) return bail(st);
+    if (h->s.two_level && (st = setup_two_level(h, X))) return bail(st);
     size_t hs = hsize(h);
     if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs + 64))) return bail(st);
     if ((st = dalloc(h, &h->Minv, (size_t)N * 9 * hs))) return bail(st);
@@ -1191,6 +1340,7 @@ int sors_set_neumann(SorsHandle* h, const int32_t* mask, const double* value) {
     CK(h2d(h, h->node_mask, h->mask_h.data(), h->N));
     CK(h2d(h, h->mval, value, sizeof(double) * h->ndof));
     h->has_neumann = true;
+    h->tl_ready = false;  // the coarse space drops held DOFs
     return SORS_OK;
 }
 

@@ -1404,6 +1404,287 @@ template void launch_add_vec<double>(int, const double*, const double*, double*,
 template void launch_add_vec<float>(int, const double*, const float*, double*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
+// Two-level preconditioner
+// ---------------------------------------------------------------------------
+// Column m of P_i (3 values): translation e_m (m < 3) or rotation
+// e_{m-3} x (X_i - c) s (m >= 3); rows of Neumann-held DOFs are zero.
+__device__ __forceinline__ void coarse_col(const CoarseArgs& c, int i, int m, double (&u)[3]) {
+    const int a = __ldg(c.aid + i);
+    const double4 cc = c.agg_c[a];
+    if (m < 3) {
+        u[0] = m == 0; u[1] = m == 1; u[2] = m == 2;
+    } else {
+        const double dx = (c.X[3 * (size_t)i] - cc.x) * cc.w, dy = (c.X[3 * (size_t)i + 1] - cc.y) * cc.w,
+                     dz = (c.X[3 * (size_t)i + 2] - cc.z) * cc.w;
+        if (m == 3) { u[0] = 0.0; u[1] = -dz; u[2] = dy; }
+        else if (m == 4) { u[0] = dz; u[1] = 0.0; u[2] = -dx; }
+        else { u[0] = -dy; u[1] = dx; u[2] = 0.0; }
+    }
+    if (c.fixed) {
+        const unsigned f = c.fixed[i];
+        if (f & 1u) u[0] = 0.0;
+        if (f & 2u) u[1] = 0.0;
+        if (f & 4u) u[2] = 0.0;
+    }
+}
+
+// Ac = P^T H P: one block per aggregate pair (a, b); thread (r, c) sums
+// P_i[:, r]^T H_ij P_j[:, c] over the Hessian blocks (i in a, j in b) in the
+// fixed order of the pair's item list.
+template <typename HT>
+__global__ void k_coarse_galerkin(int npairs, const int* __restrict__ cpair_ptr, const int2* __restrict__ items,
+                                  const int2* __restrict__ ab, const int* __restrict__ col,
+                                  const HT* __restrict__ H, long long nnzb, CoarseArgs c, double* __restrict__ Ac) {
+    const int pr = blockIdx.x;
+    const int t = threadIdx.x;
+    if (pr >= npairs || t >= 36) return;
+    const int r = t / 6, cc = t - 6 * (t / 6);
+    const int2 pab = ab[pr];
+    double acc = 0.0;
+    for (int it = cpair_ptr[pr]; it < cpair_ptr[pr + 1]; it++) {
+        const int2 bi = items[it];
+        const int bg = bi.x, i = bi.y, j = __ldg(col + bg);
+        double u[3], w[3];
+        coarse_col(c, i, r, u);
+        coarse_col(c, j, cc, w);
+        const HT* hb = H + hval((size_t)bg, 0, (size_t)nnzb);
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const double hw = (double)hb[k * 3] * w[0] + (double)hb[k * 3 + 1] * w[1] + (double)hb[k * 3 + 2] * w[2];
+            acc += u[k] * hw;
+        }
+    }
+    Ac[(size_t)(6 * pab.x + r) * c.nc + 6 * pab.y + cc] = acc;
+}
+
+void launch_coarse_galerkin_f(int npairs, const int* cpair_ptr, const int2* cpair_items, const int2* cpair_ab,
+                              const int* col, const float* H, long long nnzb, const CoarseArgs& c, double* Ac,
+                              cudaStream_t st) {
+    if (npairs == 0) return;
+    k_coarse_galerkin<float><<<npairs, 64, 0, st>>>(npairs, cpair_ptr, cpair_items, cpair_ab, col, H, nnzb, c, Ac);
+    counted();
+}
+void launch_coarse_galerkin_d(int npairs, const int* cpair_ptr, const int2* cpair_items, const int2* cpair_ab,
+                              const int* col, const double* H, long long nnzb, const CoarseArgs& c, double* Ac,
+                              cudaStream_t st) {
+    if (npairs == 0) return;
+    k_coarse_galerkin<double><<<npairs, 64, 0, st>>>(npairs, cpair_ptr, cpair_items, cpair_ab, col, H, nnzb, c, Ac);
+    counted();
+}
+
+// Coarse unknowns with (near-)zero diagonal (an aggregate held entirely by
+// Neumann DOFs) become identity rows, so the inverse exists.
+__global__ void k_coarse_fix(int nc, double* Ac) {
+    __shared__ double smax[256];
+    double m = 0.0;
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) m = fmax(m, fabs(Ac[(size_t)k * nc + k]));
+    smax[threadIdx.x] = m;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + o]);
+        __syncthreads();
+    }
+    const double tiny = 1e-12 * smax[0];
+    for (int k = 0; k < nc; k++) {
+        if (fabs(Ac[(size_t)k * nc + k]) > tiny) continue;
+        for (int j = threadIdx.x; j < nc; j += blockDim.x) {
+            Ac[(size_t)k * nc + j] = 0.0;
+            Ac[(size_t)j * nc + k] = 0.0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) Ac[(size_t)k * nc + k] = 1.0;
+        __syncthreads();
+    }
+}
+
+// In-place Gauss-Jordan inversion of the SPD coarse matrix, one pivot per pair
+// of launches: copy pivot row and column, then update every entry from the copies.
+__global__ void k_gj_copy(int nc, const double* __restrict__ A, int k, double* __restrict__ rowk,
+                          double* __restrict__ colk) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nc) return;
+    rowk[j] = A[(size_t)k * nc + j];
+    colk[j] = A[(size_t)j * nc + k];
+}
+
+__global__ void k_gj_update(int nc, double* __restrict__ A, int k, const double* __restrict__ rowk,
+                            const double* __restrict__ colk) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nc * nc) return;
+    const int i = (int)(t / nc), j = (int)(t - (long long)i * nc);
+    const double p = rowk[k];
+    double v;
+    if (i == k && j == k) v = 1.0 / p;
+    else if (i == k) v = rowk[j] / p;
+    else if (j == k) v = -colk[i] / p;
+    else v = A[t] - colk[i] * rowk[j] / p;
+    A[t] = v;
+}
+
+void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaStream_t st) {
+    if (nc == 0) return;
+    k_coarse_fix<<<1, 256, 0, st>>>(nc, Ac);
+    counted();
+    const long long n2 = (long long)nc * nc;
+    const int bu = (int)((n2 + 255) / 256), bc = (nc + 255) / 256;
+    for (int k = 0; k < nc; k++) {
+        k_gj_copy<<<bc, 256, 0, st>>>(nc, Ac, k, rowk, colk);
+        k_gj_update<<<bu, 256, 0, st>>>(nc, Ac, k, rowk, colk);
+    }
+    g_kernel_launches.fetch_add(2LL * nc);
+}
+
+template <typename VT>
+__global__ void k_to_vt(long long n, const double* __restrict__ in, VT* __restrict__ out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < n) out[t] = (VT)in[t];
+}
+template <typename VT>
+void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st) {
+    if (n == 0) return;
+    k_to_vt<VT><<<(int)((n + 255) / 256), 256, 0, st>>>(n, in, out);
+    counted();
+}
+
+// x += alpha p, r -= alpha q (the two-level iteration forms z afterwards)
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_tl_update(int N, const VT* __restrict__ p, const VT* __restrict__ qv,
+                                                            VT* __restrict__ x, VT* __restrict__ r, DevScalars* sc) {
+    if (*(volatile int*)&sc->done) return;
+    const VT alpha = (VT)sc->alpha;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * N; i += gridDim.x * blockDim.x) {
+        x[i] += alpha * p[i];
+        r[i] -= alpha * qv[i];
+    }
+}
+template <typename VT>
+void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, DevScalars* sc, cudaStream_t st) {
+    k_tl_update<VT><<<red_grid(3LL * N, 4), kRedThreads, 0, st>>>(N, p, qv, x, r, sc);
+    counted();
+}
+
+// yc = P^T r: one block per aggregate, a fixed-order tree sum.
+template <typename VT>
+__global__ void __launch_bounds__(256) k_coarse_restrict(CoarseArgs c, const VT* __restrict__ r,
+                                                         double* __restrict__ yc, const DevScalars* sc) {
+    if (sc && *(volatile const int*)&sc->done) return;
+    __shared__ double sh[6][256];
+    const int a = blockIdx.x;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
+        const int i = c.agg_nodes[k];
+        const double ri[3] = {(double)r[3 * (size_t)i], (double)r[3 * (size_t)i + 1], (double)r[3 * (size_t)i + 2]};
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            double u[3];
+            coarse_col(c, i, m, u);
+            acc[m] += u[0] * ri[0] + u[1] * ri[1] + u[2] * ri[2];
+        }
+    }
+#pragma unroll
+    for (int m = 0; m < 6; m++) sh[m][threadIdx.x] = acc[m];
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o)
+#pragma unroll
+            for (int m = 0; m < 6; m++) sh[m][threadIdx.x] += sh[m][threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x < 6) yc[6 * a + threadIdx.x] = sh[threadIdx.x][0];
+}
+template <typename VT>
+void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st) {
+    if (c.nagg == 0) return;
+    k_coarse_restrict<VT><<<c.nagg, 256, 0, st>>>(c, r, yc, nullptr);
+    counted();
+}
+
+// zc = Ainv yc: one warp per row.
+template <typename VT>
+__global__ void k_coarse_matvec(int nc, const VT* __restrict__ A, const double* __restrict__ yc, VT* __restrict__ zc) {
+    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (row >= nc) return;
+    double acc[1] = {0.0};
+    const VT* a = A + (size_t)row * nc;
+    for (int j = lane; j < nc; j += 32) acc[0] += (double)__ldg(a + j) * yc[j];
+    warp_sum<1>(acc);
+    if (lane == 0) zc[row] = (VT)acc[0];
+}
+template <typename VT>
+void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st) {
+    if (nc == 0) return;
+    k_coarse_matvec<VT><<<(nc + 7) / 8, 256, 0, st>>>(nc, Ainv, yc, zc);
+    counted();
+}
+
+// z = Minv r + P zc with the dots r.z and r.r.  init = 1: first z of a solve
+// (sets rz, rr, bnorm-based tolerance was set by k_pcg_init and is kept);
+// init = 0: one CG iteration's end (beta, it, done as k_pcg_update).
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __restrict__ r,
+                                                       const VT* __restrict__ Minv, const VT* __restrict__ zc,
+                                                       VT* __restrict__ z, int init, double* partials,
+                                                       DevScalars* sc) {
+    if (!init && *(volatile int*)&sc->done) return;
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+        VT rr[3], zz[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) rr[k] = r[3 * (size_t)i + k];
+        const VT* M = Minv + (size_t)i * 9;
+#pragma unroll
+        for (int k = 0; k < 3; k++) zz[k] = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
+        const int a = __ldg(c.aid + i);
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            double u[3];
+            coarse_col(c, i, m, u);
+            const VT zm = zc[6 * a + m];
+#pragma unroll
+            for (int k = 0; k < 3; k++) zz[k] += (VT)u[k] * zm;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            z[3 * (size_t)i + k] = zz[k];
+            acc[0] += (double)rr[k] * (double)zz[k];
+            acc[1] += (double)rr[k] * (double)rr[k];
+        }
+    }
+    double tot[2];
+    if (reduce_grid<2>(acc, partials, &sc->counters[init ? 8 : 9], tot) && threadIdx.x == 0) {
+        if (init) {
+            sc->rz = tot[0];
+        } else {
+            sc->beta = tot[0] / sc->rz;
+            sc->rz = tot[0];
+            sc->rr = tot[1];
+            sc->it += 1;
+            if (tot[1] <= sc->tol2 || sc->it >= sc->maxit || !(tot[1] == tot[1])) sc->done = 1;
+        }
+    }
+}
+template <typename VT>
+void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init, double* partials,
+                 DevScalars* sc, cudaStream_t st) {
+    k_tl_z<VT><<<red_grid(c.N, 2), kRedThreads, 0, st>>>(c, r, Minv, zc, z, init, partials, sc);
+    counted();
+}
+
+template void launch_to_vt<float>(long long, const double*, float*, cudaStream_t);
+template void launch_to_vt<double>(long long, const double*, double*, cudaStream_t);
+template void launch_tl_update<float>(int, const float*, const float*, float*, float*, DevScalars*, cudaStream_t);
+template void launch_tl_update<double>(int, const double*, const double*, double*, double*, DevScalars*,
+                                       cudaStream_t);
+template void launch_coarse_restrict<float>(const CoarseArgs&, const float*, double*, cudaStream_t);
+template void launch_coarse_restrict<double>(const CoarseArgs&, const double*, double*, cudaStream_t);
+template void launch_coarse_matvec<float>(int, const float*, const double*, float*, cudaStream_t);
+template void launch_coarse_matvec<double>(int, const double*, const double*, double*, cudaStream_t);
+template void launch_tl_z<float>(const CoarseArgs&, const float*, const float*, const float*, float*, int, double*,
+                                 DevScalars*, cudaStream_t);
+template void launch_tl_z<double>(const CoarseArgs&, const double*, const double*, const double*, double*, int,
+                                  double*, DevScalars*, cudaStream_t);
+
+// ---------------------------------------------------------------------------
 // explicit instantiations
 // ---------------------------------------------------------------------------
 template void launch_assemble<double>(const AsmArgs<double>&, int, cudaStream_t);

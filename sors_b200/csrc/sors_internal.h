@@ -104,7 +104,38 @@ struct PressureArgs {
 // Caps the grid of every kernel launched from this thread (kernels.cu).
 void set_grid_cap(int blocks);
 
-// Sets the message returned by sors_last_error on this thread (capi.cu).
+// Two-level preconditioner (no reference counterpart): block Jacobi plus an
+// exact correction on the coarse space spanned, per aggregate of nodes, by the
+// three translations and three rotations about the aggregate's centre.
+struct CoarseArgs {
+    int N = 0, nagg = 0, nc = 0;       // nodes, aggregates, coarse unknowns (6 nagg)
+    const int* aid = nullptr;          // aggregate of each node
+    const double4* agg_c = nullptr;    // centre (x, y, z), 1 / length scale
+    const int* agg_ptr = nullptr;      // nagg + 1
+    const int* agg_nodes = nullptr;    // nodes of each aggregate, ascending
+    const uint8_t* fixed = nullptr;    // Neumann bits per node (those rows of P are zero)
+    const double* X = nullptr;         // undeformed positions
+};
+void launch_coarse_galerkin_f(int npairs, const int* cpair_ptr, const int2* cpair_items, const int2* cpair_ab,
+                              const int* col, const float* H, long long nnzb, const CoarseArgs& c, double* Ac,
+                              cudaStream_t st);
+void launch_coarse_galerkin_d(int npairs, const int* cpair_ptr, const int2* cpair_items, const int2* cpair_ab,
+                              const int* col, const double* H, long long nnzb, const CoarseArgs& c, double* Ac,
+                              cudaStream_t st);
+void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaStream_t st);
+template <typename VT>
+void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st);
+template <typename VT>
+void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st);
+template <typename VT>
+void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st);
+template <typename VT>
+void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init, double* partials,
+                 DevScalars* sc, cudaStream_t st);
+
+// Sets the message returned by sors_last_error on this thread (capi.cu).// Sets the message returned by sors_last_error on this thread (capi.cu).
 void set_last_error(const std::string& msg);
 
 // Launchers (kernels.cu)

@@ -9,7 +9,7 @@ from sors_b200 import meshes
 def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha=0.0, dt=1e-3,
               scheme="backward_euler", method="minimize_newton", precision="fp64", project=True,
               clamp=True, res_tol=0.0, faces=None, groups=None, vertex_force=False, oracle_project=False,
-              muscles=None, energy="neohookean"):
+              muscles=None, energy="neohookean", two_level=False):
     """(gpu_energy, gpu_solver, oracle_system, X) on one mesh."""
     from oracle import oracle as orc
     from sors_b200 import py_sors as ps
@@ -28,6 +28,7 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     s.precision = precision
     s.hessianProjection = project
     s.newtonResidualTol = res_tol
+    s.twoLevelPreconditioner = two_level
     energies = [{energy}] * ne
     params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [rhov[i], Ev[i], nuv[i]]) for i in range(ne)]
     if muscles is not None:
