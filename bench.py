@@ -61,7 +61,7 @@ def block_mesh(cells, seed=0):
 
 PROJECTION = {"true": True, "false": False, "adaptive": "adaptive"}
 _projection = "adaptive"
-_two_level = False
+_two_level = True
 
 
 def make_settings(precision):
@@ -611,8 +611,8 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--cells", type=int, nargs=3, default=list(CELLS))
     ap.add_argument("--no-fp64", action="store_true")
-    ap.add_argument("--two-level", action="store_true",
-                    help="two-level PCG preconditioner (block Jacobi + coarse rigid-body correction)")
+    ap.add_argument("--no-two-level", dest="two_level", action="store_false",
+                    help="block Jacobi alone instead of the two-level PCG preconditioner")
     ap.add_argument("--projection", default="adaptive", choices=sorted(PROJECTION),
                     help="SPD projection of the element Hessians: always, never, or only where PCG meets "
                          "negative curvature")

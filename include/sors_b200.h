@@ -69,7 +69,9 @@ typedef struct SorsSettings {
                                 reference counterpart; off by default)            */
     int32_t two_level;       /* 1: precondition the Newton PCG with block Jacobi
                                 plus an exact coarse correction on per-aggregate
-                                rigid-body modes (no reference counterpart)     */
+                                rigid-body modes (no reference counterpart);
+                                0: block Jacobi; 2 (default): 1 for meshes of
+                                20,000 nodes or more                              */
 } SorsSettings;
 
 typedef struct SorsStepStats {

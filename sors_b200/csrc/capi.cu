@@ -1227,7 +1227,7 @@ void sors_default_settings(SorsSettings* s) {
     s->newton_predictor = 1;
     s->max_blocks = 0;
     s->newton_safeguard = 0;
-    s->two_level = 0;
+    s->two_level = 2;
 }
 
 int sors_last_error(char* buf, size_t n) {
@@ -1292,6 +1292,9 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     CK(h2d(h, h->q, X, nd * sizeof(double)));
     h->mask_h.assign(N, 0);
     if ((st = upload(h, &h->node_mask, h->mask_h.data(), (size_t)N))) return bail(st);
+    // two_level 2 ("auto"): on for meshes of 20,000 nodes or more, where the
+    // coarse correction's three extra kernels per iteration pay for themselves
+    if (h->s.two_level == 2) h->s.two_level = N >= 20000 ? 1 : 0;
     if (h->s.two_level && (st = setup_two_level(h, X))) return bail(st);
     size_t hs = hsize(h);
     if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs + 64))) return bail(st);

@@ -59,7 +59,9 @@ class SimulationSettings:
         self.hessianProjection = "adaptive"
         self.maxBlocksPerKernel = 0        # grid cap per kernel (0: whole GPU)
         self.newtonSafeguard = False       # halve Newton steps that raise ||g|| (adaptive Hessian only)
-        self.twoLevelPreconditioner = False  # block Jacobi + coarse rigid-body correction
+        # block Jacobi + coarse rigid-body correction: True, False or "auto"
+        # (on for meshes of 20,000 nodes or more)
+        self.twoLevelPreconditioner = "auto"
         self.newtonResidualTol = 0.0       # absolute ||gradient|| stop; 0 = reference dx test only
         self.newtonDxTol = 1e-9            # reference DX_TOL (cpp/headers/common.h:25)
         self.newtonMaxIter = 100           # reference MAX_ITER (cpp/headers/common.h:21)
@@ -275,7 +277,8 @@ class _EnergyBase:
         s.newton_predictor = int(bool(getattr(settings, "newtonPredictor", True)))
         s.max_blocks = int(getattr(settings, "maxBlocksPerKernel", 0))
         s.newton_safeguard = int(bool(getattr(settings, "newtonSafeguard", False)))
-        s.two_level = int(bool(getattr(settings, "twoLevelPreconditioner", False)))
+        tl = getattr(settings, "twoLevelPreconditioner", "auto")
+        s.two_level = 2 if (isinstance(tl, str) and tl == "auto") else int(bool(tl))
         self._settings_c = s
         h = C.c_void_p()
         _lib.check(L.sors_create(_p(X, C.c_double), X.shape[0], _p(T, C.c_int32), ne, self.NV, _p(rho, C.c_double),
