@@ -151,7 +151,7 @@ struct SorsHandle {
     // projection used by the PCG kernels (null: none)
     const uint8_t* proj_flag = nullptr;
     const double4* proj_n = nullptr;
-    int pcg_exec_mode = 0;  // 0 block Jacobi, 1 projected, 2 two-level
+    int pcg_exec_mode = 0;  // bit 0 projected, bit 1 two-level
 
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
@@ -446,11 +446,12 @@ void pcg_iter_pair(SorsHandle* h) {
             VT* pout = (VT*)(half ? h->p0 : h->p1);
             launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, pin,
                                     pout, (VT*)h->qv, h->partials, h->sc, h->stream);
-            launch_tl_update<VT>(h->N, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->sc, h->stream);
+            launch_tl_update<VT>(h->N, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag, h->proj_n, h->sc,
+                                 h->stream);
             launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
             launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
-            launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, z, 0, h->partials, h->sc,
-                            h->stream);
+            launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, z, 0, h->proj_flag,
+                            h->proj_n, h->partials, h->sc, h->stream);
         }
         return;
     }
@@ -466,7 +467,7 @@ void pcg_iter_pair(SorsHandle* h) {
 
 template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
-    const int mode = h->proj_flag ? 1 : (h->tl_active ? 2 : 0);
+    const int mode = (h->proj_flag ? 1 : 0) + (h->tl_active ? 2 : 0);
     if (h->pcg_exec && h->pcg_exec_mode != mode) {
         // the captured launches carry the projection pointers: capture again
         cudaGraphExecDestroy(h->pcg_exec);
@@ -506,8 +507,10 @@ int pcg_chunk(SorsHandle* h) {
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
-    // the two-level preconditioner serves the unconstrained Newton solves
-    h->tl_active = h->s.two_level && h->cargs.nc > 0 && !h->proj_flag;
+    // the two-level preconditioner: with a constraint projection (SQP, adjoint)
+    // the correction is projected too, so the preconditioner stays SPD on the
+    // free subspace (the coarse matrix itself is built without the projection)
+    h->tl_active = h->s.two_level && h->cargs.nc > 0;
     bool refreshed = false;
     if (h->tl_active && !h->tl_ready) {
         const int nc = h->cargs.nc;
@@ -530,8 +533,8 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
     if (h->tl_active) {
         launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
         launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
-        launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, (VT*)h->z, 1, h->partials,
-                        h->sc, h->stream);
+        launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, (VT*)h->z, 1, h->proj_flag,
+                        h->proj_n, h->partials, h->sc, h->stream);
     }
     CK(cudaGetLastError());
     int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;

@@ -1546,20 +1546,32 @@ void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st) {
     counted();
 }
 
-// x += alpha p, r -= alpha q (the two-level iteration forms z afterwards)
+// x += alpha p, r -= alpha P q (the two-level iteration forms z afterwards;
+// P the constraint projection when one is set)
 template <typename VT>
 __global__ void __launch_bounds__(kRedThreads) k_tl_update(int N, const VT* __restrict__ p, const VT* __restrict__ qv,
-                                                            VT* __restrict__ x, VT* __restrict__ r, DevScalars* sc) {
+                                                            VT* __restrict__ x, VT* __restrict__ r,
+                                                            const uint8_t* __restrict__ pflag,
+                                                            const double4* __restrict__ pn, DevScalars* sc) {
     if (*(volatile int*)&sc->done) return;
     const VT alpha = (VT)sc->alpha;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 3 * N; i += gridDim.x * blockDim.x) {
-        x[i] += alpha * p[i];
-        r[i] -= alpha * qv[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT qq[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t ii = 3 * (size_t)i + k;
+            x[ii] += alpha * p[ii];
+            qq[k] = qv[ii];
+        }
+        project3<VT>(pflag, pn, i, qq);
+#pragma unroll
+        for (int k = 0; k < 3; k++) r[3 * (size_t)i + k] -= alpha * qq[k];
     }
 }
 template <typename VT>
-void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, DevScalars* sc, cudaStream_t st) {
-    k_tl_update<VT><<<red_grid(3LL * N, 4), kRedThreads, 0, st>>>(N, p, qv, x, r, sc);
+void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag, const double4* pn,
+                      DevScalars* sc, cudaStream_t st) {
+    k_tl_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, x, r, pflag, pn, sc);
     counted();
 }
 
@@ -1623,7 +1635,8 @@ void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cuda
 template <typename VT>
 __global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __restrict__ r,
                                                        const VT* __restrict__ Minv, const VT* __restrict__ zc,
-                                                       VT* __restrict__ z, int init, double* partials,
+                                                       VT* __restrict__ z, int init, const uint8_t* __restrict__ pflag,
+                                                       const double4* __restrict__ pn, double* partials,
                                                        DevScalars* sc) {
     if (!init && *(volatile int*)&sc->done) return;
     double acc[2] = {0.0, 0.0};
@@ -1643,6 +1656,7 @@ __global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __
 #pragma unroll
             for (int k = 0; k < 3; k++) zz[k] += (VT)u[k] * zm;
         }
+        project3<VT>(pflag, pn, i, zz);
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             z[3 * (size_t)i + k] = zz[k];
@@ -1664,25 +1678,26 @@ __global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __
     }
 }
 template <typename VT>
-void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init, double* partials,
-                 DevScalars* sc, cudaStream_t st) {
-    k_tl_z<VT><<<red_grid(c.N, 2), kRedThreads, 0, st>>>(c, r, Minv, zc, z, init, partials, sc);
+void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init,
+                 const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc, cudaStream_t st) {
+    k_tl_z<VT><<<red_grid(c.N, 2), kRedThreads, 0, st>>>(c, r, Minv, zc, z, init, pflag, pn, partials, sc);
     counted();
 }
 
 template void launch_to_vt<float>(long long, const double*, float*, cudaStream_t);
 template void launch_to_vt<double>(long long, const double*, double*, cudaStream_t);
-template void launch_tl_update<float>(int, const float*, const float*, float*, float*, DevScalars*, cudaStream_t);
-template void launch_tl_update<double>(int, const double*, const double*, double*, double*, DevScalars*,
-                                       cudaStream_t);
+template void launch_tl_update<float>(int, const float*, const float*, float*, float*, const uint8_t*, const double4*,
+                                      DevScalars*, cudaStream_t);
+template void launch_tl_update<double>(int, const double*, const double*, double*, double*, const uint8_t*,
+                                       const double4*, DevScalars*, cudaStream_t);
 template void launch_coarse_restrict<float>(const CoarseArgs&, const float*, double*, cudaStream_t);
 template void launch_coarse_restrict<double>(const CoarseArgs&, const double*, double*, cudaStream_t);
 template void launch_coarse_matvec<float>(int, const float*, const double*, float*, cudaStream_t);
 template void launch_coarse_matvec<double>(int, const double*, const double*, double*, cudaStream_t);
-template void launch_tl_z<float>(const CoarseArgs&, const float*, const float*, const float*, float*, int, double*,
-                                 DevScalars*, cudaStream_t);
+template void launch_tl_z<float>(const CoarseArgs&, const float*, const float*, const float*, float*, int,
+                                 const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_tl_z<double>(const CoarseArgs&, const double*, const double*, const double*, double*, int,
-                                  double*, DevScalars*, cudaStream_t);
+                                  const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // explicit instantiations

@@ -126,14 +126,15 @@ void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaSt
 template <typename VT>
 void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st);
 template <typename VT>
-void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, DevScalars* sc, cudaStream_t st);
+void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag, const double4* pn,
+                      DevScalars* sc, cudaStream_t st);
 template <typename VT>
 void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st);
 template <typename VT>
 void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st);
 template <typename VT>
-void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init, double* partials,
-                 DevScalars* sc, cudaStream_t st);
+void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init,
+                 const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc, cudaStream_t st);
 
 // Sets the message returned by sors_last_error on this thread (capi.cu).// Sets the message returned by sors_last_error on this thread (capi.cu).
 void set_last_error(const std::string& msg);

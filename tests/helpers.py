@@ -83,7 +83,8 @@ def deform(X, rng, amp=0.05, scale=None):
 
 
 def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1e5, nu=0.45,
-                 grav=(0.0, 0.0, -9.81), dt=1e-3, precision="fp64", project=True, neumann=None, muscles=None):
+                 grav=(0.0, 0.0, -9.81), dt=1e-3, precision="fp64", project=True, neumann=None, muscles=None,
+                 two_level=False):
     """GPU Energy/Solver with minimize_SQP and the oracle's SQP on the same scene.
 
     planes: (points (k,3), normals (k,3)); disks: (centers, normals, radii);
@@ -107,6 +108,7 @@ def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1
     s.solverMethod = "minimize_SQP"
     s.precision = precision
     s.hessianProjection = project
+    s.twoLevelPreconditioner = two_level
     ctypes_, cp = [], ps.Params()
     if neumann is not None:
         ctypes_.append("neumannBC")

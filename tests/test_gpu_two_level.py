@@ -57,3 +57,22 @@ def test_two_level_deterministic():
 @pytest.fixture(scope="module")
 def c1_mesh():
     return meshes.cantilever_tets()
+
+
+def test_two_level_with_contact():
+    # SQP subproblems run the projected PCG; the two-level correction is
+    # projected as well and must give the same contact step as block Jacobi
+    X, H = meshes.hex_bar(12, 6, 6, (0.03, 0.015, 0.015))
+    X = X + np.array([0.0, 0.0, 0.0003])
+    from tests.helpers import contact_pair
+    out = {}
+    for tl in (False, True):
+        en, sol, sq, surf = contact_pair(X, H, planes=([[0, 0, 0]], [[0, 0, 1.0]]), dt=2e-3, two_level=tl)
+        x = X.ravel().copy()
+        pcg = 0
+        for _ in range(10):
+            x = sol.step(x, en)
+            pcg += sol.last_stats.pcg_iters
+        out[tl] = (x, pcg, en.active_contacts())
+    assert out[True][2] == out[False][2] and out[True][2] > 0
+    assert np.abs(out[True][0] - out[False][0]).max() < 1e-9
