@@ -446,9 +446,8 @@ void pcg_iter_pair(SorsHandle* h) {
             VT* pout = (VT*)(half ? h->p0 : h->p1);
             launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, pin,
                                     pout, (VT*)h->qv, h->partials, h->sc, h->stream);
-            launch_tl_update<VT>(h->N, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag, h->proj_n, h->sc,
-                                 h->stream);
-            launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
+            launch_tl_update_restrict<VT>(h->cargs, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag,
+                                          h->proj_n, h->tl_yc, h->sc, h->stream);
             launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
             launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, z, 0, h->proj_flag,
                             h->proj_n, h->partials, h->sc, h->stream);
@@ -887,6 +886,12 @@ int setup_two_level(SorsHandle* h, const double* X) {
         const double n = std::max(1, cnt[a + 1] - cnt[a]);
         cen[a] = make_double4(c[0] / n, c[1] / n, c[2] / n, 1.0 / hb);
     }
+    std::vector<float4> off(N);
+    for (int i = 0; i < N; i++) {
+        const double4 c = cen[aid[i]];
+        off[i] = make_float4((float)((X[3 * i] - c.x) * c.w), (float)((X[3 * i + 1] - c.y) * c.w),
+                             (float)((X[3 * i + 2] - c.z) * c.w), 0.0f);
+    }
     // aggregate pairs and their Hessian blocks (counting sort by pair key)
     const long long nkeys = (long long)nagg * nagg;
     std::vector<int> keycnt((size_t)nkeys + 1, 0);
@@ -916,6 +921,8 @@ int setup_two_level(SorsHandle* h, const double* X) {
     int* aid_d = nullptr; double4* cen_d = nullptr; int* aggptr_d = nullptr; int* nodes_d = nullptr;
     if ((st = upload(h, &aid_d, aid.data(), (size_t)N))) return st;
     if ((st = upload(h, &cen_d, cen.data(), (size_t)nagg))) return st;
+    float4* off_d = nullptr;
+    if ((st = upload(h, &off_d, off.data(), (size_t)N))) return st;
     if ((st = upload(h, &aggptr_d, cnt.data(), (size_t)nagg + 1))) return st;
     if ((st = upload(h, &nodes_d, nodes.data(), (size_t)N))) return st;
     if ((st = upload(h, &h->tl_pair_ptr, pair_ptr.data(), pair_ptr.size()))) return st;
@@ -929,7 +936,7 @@ int setup_two_level(SorsHandle* h, const double* X) {
     if ((st = dalloc(h, &h->tl_zc, (size_t)nc * hsize(h)))) return st;
     h->cargs.N = N; h->cargs.nagg = nagg; h->cargs.nc = nc;
     h->cargs.aid = aid_d; h->cargs.agg_c = cen_d; h->cargs.agg_ptr = aggptr_d; h->cargs.agg_nodes = nodes_d;
-    h->cargs.fixed = h->node_mask; h->cargs.X = h->X;
+    h->cargs.fixed = h->node_mask; h->cargs.off = off_d;
     h->tl_ready = false;
     return SORS_OK;
 }

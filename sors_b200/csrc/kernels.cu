@@ -1409,13 +1409,11 @@ template void launch_add_vec<float>(int, const double*, const float*, double*, c
 // Column m of P_i (3 values): translation e_m (m < 3) or rotation
 // e_{m-3} x (X_i - c) s (m >= 3); rows of Neumann-held DOFs are zero.
 __device__ __forceinline__ void coarse_col(const CoarseArgs& c, int i, int m, double (&u)[3]) {
-    const int a = __ldg(c.aid + i);
-    const double4 cc = c.agg_c[a];
     if (m < 3) {
         u[0] = m == 0; u[1] = m == 1; u[2] = m == 2;
     } else {
-        const double dx = (c.X[3 * (size_t)i] - cc.x) * cc.w, dy = (c.X[3 * (size_t)i + 1] - cc.y) * cc.w,
-                     dz = (c.X[3 * (size_t)i + 2] - cc.z) * cc.w;
+        const float4 o = c.off[i];
+        const double dx = o.x, dy = o.y, dz = o.z;
         if (m == 3) { u[0] = 0.0; u[1] = -dz; u[2] = dy; }
         else if (m == 4) { u[0] = dz; u[1] = 0.0; u[2] = -dx; }
         else { u[0] = -dy; u[1] = dx; u[2] = 0.0; }
@@ -1426,6 +1424,24 @@ __device__ __forceinline__ void coarse_col(const CoarseArgs& c, int i, int m, do
         if (f & 2u) u[1] = 0.0;
         if (f & 4u) u[2] = 0.0;
     }
+}
+
+// P_i^T v (6 values) and P_i w (3 values) for one node, from its offset.
+__device__ __forceinline__ void coarse_restrict_node(const CoarseArgs& c, int i, const double (&v)[3],
+                                                     double (&y)[6]) {
+    double w[3] = {v[0], v[1], v[2]};
+    if (c.fixed) {
+        const unsigned f = c.fixed[i];
+        if (f & 1u) w[0] = 0.0;
+        if (f & 2u) w[1] = 0.0;
+        if (f & 4u) w[2] = 0.0;
+    }
+    const float4 o = c.off[i];
+    const double dx = o.x, dy = o.y, dz = o.z;
+    y[0] = w[0]; y[1] = w[1]; y[2] = w[2];
+    y[3] = -dz * w[1] + dy * w[2];
+    y[4] = dz * w[0] - dx * w[2];
+    y[5] = -dy * w[0] + dx * w[1];
 }
 
 // Ac = P^T H P: one block per aggregate pair (a, b); thread (r, c) sums
@@ -1546,52 +1562,47 @@ void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st) {
     counted();
 }
 
-// x += alpha p, r -= alpha P q (the two-level iteration forms z afterwards;
-// P the constraint projection when one is set)
-template <typename VT>
-__global__ void __launch_bounds__(kRedThreads) k_tl_update(int N, const VT* __restrict__ p, const VT* __restrict__ qv,
-                                                            VT* __restrict__ x, VT* __restrict__ r,
-                                                            const uint8_t* __restrict__ pflag,
-                                                            const double4* __restrict__ pn, DevScalars* sc) {
-    if (*(volatile int*)&sc->done) return;
-    const VT alpha = (VT)sc->alpha;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
-        VT qq[3];
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            const size_t ii = 3 * (size_t)i + k;
-            x[ii] += alpha * p[ii];
-            qq[k] = qv[ii];
-        }
-        project3<VT>(pflag, pn, i, qq);
-#pragma unroll
-        for (int k = 0; k < 3; k++) r[3 * (size_t)i + k] -= alpha * qq[k];
-    }
-}
-template <typename VT>
-void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag, const double4* pn,
-                      DevScalars* sc, cudaStream_t st) {
-    k_tl_update<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, p, qv, x, r, pflag, pn, sc);
-    counted();
-}
-
-// yc = P^T r: one block per aggregate, a fixed-order tree sum.
-template <typename VT>
-__global__ void __launch_bounds__(256) k_coarse_restrict(CoarseArgs c, const VT* __restrict__ r,
-                                                         double* __restrict__ yc, const DevScalars* sc) {
-    if (sc && *(volatile const int*)&sc->done) return;
-    __shared__ double sh[6][256];
+// yc = P^T r: one block per aggregate, a fixed-order tree sum.  The fused
+// variant first applies the CG update x += alpha p, r -= alpha P q to the
+// aggregate's nodes (each node belongs to exactly one aggregate).
+template <typename VT, bool UPDATE>
+__global__ void __launch_bounds__(512) k_coarse_restrict(CoarseArgs c, const VT* __restrict__ p,
+                                                         const VT* __restrict__ qv, VT* __restrict__ x,
+                                                         VT* __restrict__ r, const uint8_t* __restrict__ pflag,
+                                                         const double4* __restrict__ pn, double* __restrict__ yc,
+                                                         const DevScalars* sc) {
+    if (UPDATE && *(volatile const int*)&sc->done) return;
+    __shared__ double sh[6][512];
     const int a = blockIdx.x;
+    const VT alpha = UPDATE ? (VT)sc->alpha : VT(0);
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
         const int i = c.agg_nodes[k];
-        const double ri[3] = {(double)r[3 * (size_t)i], (double)r[3 * (size_t)i + 1], (double)r[3 * (size_t)i + 2]};
+        double ri[3];
+        if (UPDATE) {
+            VT qq[3], rr[3];
 #pragma unroll
-        for (int m = 0; m < 6; m++) {
-            double u[3];
-            coarse_col(c, i, m, u);
-            acc[m] += u[0] * ri[0] + u[1] * ri[1] + u[2] * ri[2];
+            for (int d = 0; d < 3; d++) {
+                const size_t ii = 3 * (size_t)i + d;
+                x[ii] += alpha * p[ii];
+                qq[d] = qv[ii];
+            }
+            project3<VT>(pflag, pn, i, qq);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                const size_t ii = 3 * (size_t)i + d;
+                rr[d] = r[ii] - alpha * qq[d];
+                r[ii] = rr[d];
+                ri[d] = (double)rr[d];
+            }
+        } else {
+#pragma unroll
+            for (int d = 0; d < 3; d++) ri[d] = (double)r[3 * (size_t)i + d];
         }
+        double y[6];
+        coarse_restrict_node(c, i, ri, y);
+#pragma unroll
+        for (int m = 0; m < 6; m++) acc[m] += y[m];
     }
 #pragma unroll
     for (int m = 0; m < 6; m++) sh[m][threadIdx.x] = acc[m];
@@ -1607,25 +1618,35 @@ __global__ void __launch_bounds__(256) k_coarse_restrict(CoarseArgs c, const VT*
 template <typename VT>
 void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st) {
     if (c.nagg == 0) return;
-    k_coarse_restrict<VT><<<c.nagg, 256, 0, st>>>(c, r, yc, nullptr);
+    k_coarse_restrict<VT, false><<<c.nagg, 512, 0, st>>>(c, nullptr, nullptr, nullptr, const_cast<VT*>(r), nullptr,
+                                                          nullptr, yc, nullptr);
+    counted();
+}
+template <typename VT>
+void launch_tl_update_restrict(const CoarseArgs& c, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag,
+                               const double4* pn, double* yc, DevScalars* sc, cudaStream_t st) {
+    k_coarse_restrict<VT, true><<<c.nagg, 512, 0, st>>>(c, p, qv, x, r, pflag, pn, yc, sc);
     counted();
 }
 
-// zc = Ainv yc: one warp per row.
+// zc = Ainv yc: one 128-thread block per row.
 template <typename VT>
-__global__ void k_coarse_matvec(int nc, const VT* __restrict__ A, const double* __restrict__ yc, VT* __restrict__ zc) {
-    const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (row >= nc) return;
+__global__ void __launch_bounds__(128) k_coarse_matvec(int nc, const VT* __restrict__ A,
+                                                        const double* __restrict__ yc, VT* __restrict__ zc) {
+    __shared__ double sh[4];
+    const int row = blockIdx.x;
     double acc[1] = {0.0};
     const VT* a = A + (size_t)row * nc;
-    for (int j = lane; j < nc; j += 32) acc[0] += (double)__ldg(a + j) * yc[j];
+    for (int j = threadIdx.x; j < nc; j += blockDim.x) acc[0] += (double)__ldg(a + j) * yc[j];
     warp_sum<1>(acc);
-    if (lane == 0) zc[row] = (VT)acc[0];
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc[0];
+    __syncthreads();
+    if (threadIdx.x == 0) zc[row] = (VT)(sh[0] + sh[1] + sh[2] + sh[3]);
 }
 template <typename VT>
 void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st) {
     if (nc == 0) return;
-    k_coarse_matvec<VT><<<(nc + 7) / 8, 256, 0, st>>>(nc, Ainv, yc, zc);
+    k_coarse_matvec<VT><<<nc, 128, 0, st>>>(nc, Ainv, yc, zc);
     counted();
 }
 
@@ -1647,14 +1668,22 @@ __global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __
         const VT* M = Minv + (size_t)i * 9;
 #pragma unroll
         for (int k = 0; k < 3; k++) zz[k] = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
-        const int a = __ldg(c.aid + i);
+        {
+            // P_i zc(a): translation + rotation x offset, held DOFs dropped
+            const int a = __ldg(c.aid + i);
+            const float4 o = c.off[i];
+            const VT t0 = zc[6 * a], t1 = zc[6 * a + 1], t2 = zc[6 * a + 2];
+            const VT w0 = zc[6 * a + 3], w1 = zc[6 * a + 4], w2 = zc[6 * a + 5];
+            const VT ox = (VT)o.x, oy = (VT)o.y, oz = (VT)o.z;
+            VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
+            if (c.fixed) {
+                const unsigned f = c.fixed[i];
+                if (f & 1u) add[0] = VT(0);
+                if (f & 2u) add[1] = VT(0);
+                if (f & 4u) add[2] = VT(0);
+            }
 #pragma unroll
-        for (int m = 0; m < 6; m++) {
-            double u[3];
-            coarse_col(c, i, m, u);
-            const VT zm = zc[6 * a + m];
-#pragma unroll
-            for (int k = 0; k < 3; k++) zz[k] += (VT)u[k] * zm;
+            for (int k = 0; k < 3; k++) zz[k] += add[k];
         }
         project3<VT>(pflag, pn, i, zz);
 #pragma unroll
@@ -1686,10 +1715,10 @@ void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc,
 
 template void launch_to_vt<float>(long long, const double*, float*, cudaStream_t);
 template void launch_to_vt<double>(long long, const double*, double*, cudaStream_t);
-template void launch_tl_update<float>(int, const float*, const float*, float*, float*, const uint8_t*, const double4*,
-                                      DevScalars*, cudaStream_t);
-template void launch_tl_update<double>(int, const double*, const double*, double*, double*, const uint8_t*,
-                                       const double4*, DevScalars*, cudaStream_t);
+template void launch_tl_update_restrict<float>(const CoarseArgs&, const float*, const float*, float*, float*,
+                                               const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
+template void launch_tl_update_restrict<double>(const CoarseArgs&, const double*, const double*, double*, double*,
+                                                const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_coarse_restrict<float>(const CoarseArgs&, const float*, double*, cudaStream_t);
 template void launch_coarse_restrict<double>(const CoarseArgs&, const double*, double*, cudaStream_t);
 template void launch_coarse_matvec<float>(int, const float*, const double*, float*, cudaStream_t);

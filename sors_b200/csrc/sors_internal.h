@@ -114,7 +114,7 @@ struct CoarseArgs {
     const int* agg_ptr = nullptr;      // nagg + 1
     const int* agg_nodes = nullptr;    // nodes of each aggregate, ascending
     const uint8_t* fixed = nullptr;    // Neumann bits per node (those rows of P are zero)
-    const double* X = nullptr;         // undeformed positions
+    const float4* off = nullptr;       // (X_i - centre) / length scale, per node
 };
 void launch_coarse_galerkin_f(int npairs, const int* cpair_ptr, const int2* cpair_items, const int2* cpair_ab,
                               const int* col, const float* H, long long nnzb, const CoarseArgs& c, double* Ac,
@@ -126,10 +126,10 @@ void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaSt
 template <typename VT>
 void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st);
 template <typename VT>
-void launch_tl_update(int N, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag, const double4* pn,
-                      DevScalars* sc, cudaStream_t st);
-template <typename VT>
 void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st);
+template <typename VT>
+void launch_tl_update_restrict(const CoarseArgs& c, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag,
+                               const double4* pn, double* yc, DevScalars* sc, cudaStream_t st);
 template <typename VT>
 void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st);
 template <typename VT>

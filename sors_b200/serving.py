@@ -290,8 +290,10 @@ def build_union(batch, device: int = 0, max_blocks: int = 0):
     union = RolloutRequest(X, T, rho, E, nu, ref.steps, ref.dt, gravity=ref.gravity, neumann_mask=mask,
                            neumann_value=val, precision=ref.precision, scheme=ref.scheme,
                            newton_res_tol=ref.newton_res_tol, planes=ref.planes, disks=None, surface=surf)
+    # the meshes of a union overlap in space: aggregates would mix them, so the
+    # union runs block Jacobi (its members are small)
     en, sol = build_rollout(union, device, sqp=ref.planes is not None or ref.disks is not None,
-                            max_blocks=max_blocks)
+                            max_blocks=max_blocks, two_level=len(batch) == 1 and "auto")
     disks = []
     if ref.disks is not None:
         cen, nrm, rad, ptr, dsurf = [], [], [], [0], []
@@ -319,7 +321,8 @@ def build_union(batch, device: int = 0, max_blocks: int = 0):
     return en, sol, slices, disks
 
 
-def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None, max_blocks: int = 0):
+def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None, max_blocks: int = 0,
+                  two_level="auto"):
     """Energy and Solver for one request (the reference-style py_sors objects)."""
     s = ps.SimulationSettings()
     s.meshType = "Tetrahedron" if req.elements.shape[1] == 4 else "Hexahedron"
@@ -331,6 +334,7 @@ def build_rollout(req: RolloutRequest, device: int = 0, sqp: bool | None = None,
     s.newtonResidualTol = 0.0 if contact else req.newton_res_tol
     s.device = device
     s.maxBlocksPerKernel = max_blocks
+    s.twoLevelPreconditioner = two_level
     cls = ps.EnergyTet if req.elements.shape[1] == 4 else ps.EnergyHex
     en = cls.from_arrays(req.vertices, req.elements, s, np.asarray(req.gravity, float), 0.0,
                          density=req.density, youngsModulus=req.youngs, poissonsRatio=req.poisson,
