@@ -854,7 +854,7 @@ int setup_two_level(SorsHandle* h, const double* X) {
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
     for (int i = 0; i < N; i++)
         for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], X[3 * i + k]); hi[k] = std::max(hi[k], X[3 * i + k]); }
-    const int target = std::max(1, std::min(256, N / 2000));
+    const int target = std::max(1, std::min(512, N / 1000));
     double L[3], vol = 1.0;
     for (int k = 0; k < 3; k++) { L[k] = std::max(hi[k] - lo[k], 1e-12); }
     double lmax = std::max(L[0], std::max(L[1], L[2]));
