@@ -189,7 +189,9 @@ def run_reference(args, rank, world):
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(SAMPLE_CELLS, "FP64 (CPU restatement of the reference path)")},
+            "config": {"workload": workload_name(tuple(args.cells), "FP64 CPU restatement of the reference path, "
+                                                 "each step timed on the bounded sample in cpu_baseline.sample"),
+                       "elements": 6 * int(np.prod(args.cells)), "precision": "fp64", "parallelism": "host cores"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
