@@ -224,6 +224,16 @@ def timed_device_steps(torch, L, en, sol, q_dev, steps, stream):
     return ev0.elapsed_time(ev1), newton, pcg
 
 
+def max_over_ranks(value, dist, device=None):
+    """The largest of each rank's value (every rank calls it, same order)."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def run_gpu(args, rank, world, local_rank):
     import torch
     from sors_b200 import _lib
@@ -254,9 +264,7 @@ def run_gpu(args, rank, world, local_rank):
     launches = L.sors_kernel_launch_count() - launches0
     torch.cuda.synchronize()
     if dist:
-        t = torch.tensor([ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+        ms = max_over_ranks(ms, dist, f"cuda:{local_rank}")
         dist.barrier()
     value = world * ne * args.steps / (ms / 1e3)
     # kernel roofline on the final assembled system
@@ -288,9 +296,7 @@ def run_gpu(args, rank, world, local_rank):
     ev1.synchronize()
     e2e_ms = ev0.elapsed_time(ev1)
     if dist:
-        t = torch.tensor([e2e_ms], device=f"cuda:{local_rank}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+        e2e_ms = max_over_ranks(e2e_ms, dist, f"cuda:{local_rank}")
     e2e_value = world * ne * e2e_steps / (e2e_ms / 1e3)
     # plain FP64 drop-in beside it (same trajectory length)
     fp64 = None
