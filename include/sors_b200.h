@@ -154,6 +154,24 @@ int sors_set_disk_contact_groups(SorsHandle* h, const double* centers, const dou
 /* DiskContact::set_disk (cpp/py_sors.cpp:231-245): moves disk disk_idx. */
 int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const double* normal, double radius);
 
+/* maxDistance constraint (cpp/src/energy.cpp:109-120, constraints/
+ * maxDistance.cpp:4-80): |q_vertex1[k] - q_vertex2[k]| <= max_distance[k] for
+ * every pair, always active, an inequality row of the SQP subproblem
+ * (solver_method 3).  n_pairs == 0 removes the constraint. */
+int sors_set_max_distance(SorsHandle* h, const int32_t* vertex1, const int32_t* vertex2, const double* max_distance,
+                          int32_t n_pairs);
+
+/* Max-distance pairs held (at their bound) when the last SQP step converged:
+ * indices into the sors_set_max_distance list and their multipliers (>= 0;
+ * grad E = sum mu_k grad g_k at the solution).  Writes min(count, cap) entries
+ * of either array (may be NULL); returns the count. */
+int32_t sors_held_pairs(SorsHandle* h, int32_t* pairs, double* multipliers, int32_t cap);
+
+/* Held max-distance pairs (indices and multipliers, as sors_held_pairs gave
+ * them right after the step) for the following sors_adjoint_step calls, until
+ * set again; n == 0 clears.  No reference counterpart. */
+int sors_adjoint_set_pairs(SorsHandle* h, const int32_t* pairs, const double* multipliers, int32_t n);
+
 /* Number of contact constraints active in the last SQP step. */
 int32_t sors_active_contacts(SorsHandle* h);
 
@@ -208,10 +226,12 @@ int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32
  * differentiation).  A step took the state (q_n, v_n) to q_next with this
  * handle's materials and the activations set at the time; call this with the
  * same activations set.  held_nodes / held_normals (n_held, may be 0) are the
- * contacts the step held (sors_held_contacts right after it).  Given
- * dL/dq_next (3N) it solves the transpose system of the step's residual at
- * q_next (exact, unprojected Hessian) on the subspace the Neumann DOFs and the
- * held contacts leave free, and writes (any output may be NULL):
+ * contacts the step held (sors_held_contacts right after it); held
+ * max-distance pairs come from sors_adjoint_set_pairs.  Given dL/dq_next (3N)
+ * it solves the transpose system of the step's residual at q_next (exact,
+ * unprojected Hessian, plus the held pairs' constraint curvature mu_k / L_k
+ * (I - u u^T)) on the subspace the Neumann DOFs, the held contacts and the held
+ * pairs leave free, and writes (any output may be NULL):
  *   dL/dq_n (3N), dL/dv_n (3N)  through the residual's old-state terms and the
  *                                Neumann targets q_n + dt val,
  *   dL/dyoungs (E)               per element,

@@ -114,6 +114,28 @@ class DiskContact:
         return [(int(self.surf[i]), self.c[d], self.n[d]) for i, d in enumerate(self.mask) if d >= 0]
 
 
+class MaxDistance:
+    """MaxDistance (cpp/src/constraints/maxDistance.cpp:4-80): g_k = d_k - |x_i - x_j| >= 0 for every
+    pair, always active (fixed constraint flag, maxDistance.h:26-33); QP row -u.dx_i + u.dx_j >= |x_i - x_j| - d_k
+    with u = (x_i - x_j) / |x_i - x_j| (a zero u when the vertices coincide, as Eigen's normalized())."""
+
+    def __init__(self, vertex1, vertex2, max_distance):
+        self.i = np.asarray(vertex1, int).ravel()
+        self.j = np.asarray(vertex2, int).ravel()
+        self.d = np.asarray(max_distance, float).ravel()
+
+    def rows(self, x, n):
+        xs = x.reshape(-1, 3)
+        diff = xs[self.i] - xs[self.j]
+        L = np.linalg.norm(diff, axis=1)
+        u = np.where(L[:, None] > 0.0, diff / np.where(L > 0.0, L, 1.0)[:, None], 0.0)
+        ri, ci, vi = [], [], []
+        for r in range(self.d.size):
+            for k in range(3):
+                ri += [r, r]; ci += [3 * self.i[r] + k, 3 * self.j[r] + k]; vi += [-u[r, k], u[r, k]]
+        return sp.csr_matrix((vi, (ri, ci)), shape=(self.d.size, n)), L - self.d
+
+
 def solve_qp(H, g, Aeq, beq, Ain, bin_, max_iter=50):
     """min 1/2 dx'H dx + g'dx s.t. Aeq dx = beq, Ain dx >= bin_ (exact, active set)."""
     n = H.shape[0]
@@ -142,10 +164,12 @@ def solve_qp(H, g, Aeq, beq, Ain, bin_, max_iter=50):
 class SQPOracle:
     """One rollout of Solver::step with minimize_SQP (backward Euler)."""
 
-    def __init__(self, system, planes=None, disks=None, neumann=None):
+    def __init__(self, system, planes=None, disks=None, neumann=None, max_distance=None):
         self.s = system
         self.planes = planes
         self.disks = disks
+        self.max_distance = max_distance
+        self.held_pairs = np.zeros(0, int)
         self.mask = None if neumann is None else np.asarray(neumann[0]).ravel().astype(bool)
         self.val = None if neumann is None else np.asarray(neumann[1], float).ravel()
         self.last_iters = 0
@@ -183,7 +207,13 @@ class SQPOracle:
             assert st == 0, "inverted element"
             beq = -(x[eq] - qPrev[eq] - dt * self.val[eq]) if eq.size else np.zeros(0)
             bin_ = np.array([-(nn @ (x[3 * v:3 * v + 3] - p)) for v, p, nn in rows])
-            dx, _, _ = solve_qp(H, g, Aeq, beq, Ain, bin_)
+            A_all, b_all = Ain, bin_
+            if self.max_distance is not None:
+                Ap, bp = self.max_distance.rows(x, n)
+                A_all = sp.vstack([Ain, Ap]).tocsr()
+                b_all = np.concatenate([bin_, bp])
+            dx, work, _ = solve_qp(H, g, Aeq, beq, A_all, b_all)
+            self.held_pairs = np.nonzero(work[len(rows):])[0]
             x += dx
             if np.isnan(dx).any():
                 raise RuntimeError("SQP method diverged")

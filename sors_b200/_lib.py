@@ -75,6 +75,9 @@ SIGNATURES = [
     ("sors_set_disk_contact", C.c_int, [_h, _dp, _dp, _dp, C.c_int32, _ip, C.c_int32]),
     ("sors_set_disk_contact_groups", C.c_int, [_h, _dp, _dp, _dp, C.c_int32, _ip, _ip]),
     ("sors_set_disk", C.c_int, [_h, C.c_int32, _dp, _dp, C.c_double]),
+    ("sors_set_max_distance", C.c_int, [_h, _ip, _ip, _dp, C.c_int32]),
+    ("sors_held_pairs", C.c_int32, [_h, _ip, _dp, C.c_int32]),
+    ("sors_adjoint_set_pairs", C.c_int, [_h, _ip, _dp, C.c_int32]),
     ("sors_active_contacts", C.c_int32, [_h]),
     ("sors_held_contacts", C.c_int32, [_h, _ip, _dp, C.c_int32]),
     ("sors_get_contact_state", C.c_int32, [_h, _ip, C.c_int32]),

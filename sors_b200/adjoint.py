@@ -13,7 +13,10 @@ States are checkpointed every `checkpoint_every` steps during the forward pass
 (positions, velocities and the disk contacts' state); the backward pass
 recomputes each segment from its checkpoint (the GPU path is deterministic, so
 the recomputed states equal the forward ones bit for bit).  Contact steps
-(minimize_SQP) are differentiated with the contacts they held as equalities.
+(minimize_SQP) are differentiated with the contacts they held as equalities;
+held maxDistance pairs enter as equalities too, with their constraint
+curvature (the multiplier times the Hessian of |x_i - x_j|) in the transpose
+system.
 
 `rollout(...)` is the torch entry point: a torch.autograd.Function whose inputs
 are float64 tensors E (E,) and act (T, G).
@@ -85,7 +88,11 @@ class RolloutAdjoint:
         nodes = np.zeros(max(k, 1), np.int32); normals = np.zeros((max(k, 1), 3))
         if k:
             L.sors_held_contacts(self.en._h, _p(nodes, C.c_int32), _p(normals), k)
-        return nodes[:k].copy(), normals[:k].copy()
+        kp = L.sors_held_pairs(self.en._h, None, None, 0)
+        pairs = np.zeros(max(kp, 1), np.int32); mu = np.zeros(max(kp, 1))
+        if kp:
+            L.sors_held_pairs(self.en._h, _p(pairs, C.c_int32), _p(mu), kp)
+        return nodes[:k].copy(), normals[:k].copy(), pairs[:kp].copy(), mu[:kp].copy()
 
     def _step(self, q, t):
         if self.before_step is not None:
@@ -142,8 +149,10 @@ class RolloutAdjoint:
             for t in range(e - 1, s - 1, -1):
                 self._set_act(None if self._act is None else self._act[t])
                 b = Qb + Vb / self.dt
-                hn, hv = self._held[t]
+                hn, hv, hp, hmu = self._held[t]
                 hv = np.ascontiguousarray(hv)
+                _lib.check(L.sors_adjoint_set_pairs(self.en._h, _p(hp, C.c_int32) if hp.size else None,
+                                                    _p(hmu) if hp.size else None, hp.size))
                 _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b),
                                                _p(hn, C.c_int32) if hn.size else None, _p(hv) if hn.size else None,
                                                hn.size, _p(dq), _p(dv), _p(dE), _p(dA) if G else None, None,

@@ -136,6 +136,22 @@ struct SorsHandle {
     int last_active = 0;
     std::vector<int> held_nodes;      // contacts held at the end of the last SQP step
     std::vector<double> held_normals;
+    // maxDistance pairs |x_i - x_j| <= d (always active); in the SQP subproblem
+    // the held pairs enter through a Schur complement on the node-projected
+    // system: one projected solve w_k per held pair, cached in md_w
+    std::vector<int> md_i, md_j;
+    std::vector<double> md_d;
+    std::vector<char> md_work;        // pair working set (persists over the Newton iterations)
+    std::vector<int> held_pairs;      // pairs held at the end of the last SQP step
+    std::vector<double> held_mu;      // and their multipliers
+    std::vector<int> adj_pairs;       // held pairs and multipliers for the next adjoint steps
+    std::vector<double> adj_mu;
+    int* md_nodes_d = nullptr;        // i_0, j_0, i_1, j_1, ...
+    double* md_pos_d = nullptr;       // gather buffer, 6 per pair
+    int2* md_ij_d = nullptr;
+    double4* md_coef_d = nullptr;
+    int md_cap = 0;
+    std::vector<double*> md_w;        // pool of n-vectors
     // two-level preconditioner (settings.two_level): node aggregates, the
     // Galerkin coarse matrix and its inverse (refreshed when PCG slows down)
     bool tl_ready = false, tl_active = false;
@@ -558,6 +574,8 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
 }
 
 int ensure_sqp_buffers(SorsHandle* h, int m);
+template <typename HT, typename VT>
+int adjoint_pairs(SorsHandle* h, double eta, std::vector<double>& lam, std::vector<double>& extra, int* iters);
 
 // Adjoint of one backward-Euler step (see sors_adjoint_step).  At the step's
 // solution q the residual g = grad Psi(q) - f + m (v - v_n)/dt - m grav +
@@ -624,6 +642,12 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         for (int i = 0; i < n; i++) lam[i] = lf[i];
     }
     CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
+    std::vector<double> extra;  // forces of the held pairs' columns (empty: none)
+    if (!h->adj_pairs.empty()) {
+        int pp = 0;
+        if ((st = adjoint_pairs<HT, VT>(h, eta, lam, extra, &pp))) return st;
+        if (stats) stats->pcg_iters += pp;
+    }
     // element contractions with lam (zero on fixed DOFs and along held normals)
     launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->adj_l, h->adj_e,
                         h->stream);
@@ -633,7 +657,7 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     if (h->has_neumann) {
         launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->adj_l, h->adj_y, h->stream);
         CK(d2h(h, r.data(), h->adj_y, sizeof(double) * n));
-        for (int i = 0; i < n; i++) r[i] = b[i] - r[i];
+        for (int i = 0; i < n; i++) r[i] = b[i] - r[i] + (extra.empty() ? 0.0 : extra[i]);
     }
     const double a = h->s.damping_alpha;
     for (int i = 0; i < n; i++) {
@@ -963,6 +987,259 @@ int ensure_sqp_buffers(SorsHandle* h, int m) {
     return SORS_OK;
 }
 
+// Rows of the maxDistance pairs at the linearisation point x (maxDistance.cpp:
+// 4-80): g_k = d_k - |x_i - x_j| >= 0, gradient -u at i and +u at j with
+// u = (x_i - x_j) / |x_i - x_j|, so the QP row is a_k . dx >= l_k = |x_i - x_j| - d_k.
+struct PairRows {
+    std::vector<double> u, l;  // 3 per pair, 1 per pair
+};
+
+PairRows pair_rows(const SorsHandle* h, const std::vector<double>& xp) {
+    const int np = (int)h->md_d.size();
+    PairRows r;
+    r.u.assign(3 * (size_t)np, 0.0);
+    r.l.assign(np, 0.0);
+    for (int k = 0; k < np; k++) {
+        double d[3], L2 = 0.0;
+        for (int c = 0; c < 3; c++) { d[c] = xp[6 * (size_t)k + c] - xp[6 * (size_t)k + 3 + c]; L2 += d[c] * d[c]; }
+        const double L = sqrt(L2);
+        if (L > 0.0)  // Eigen's normalized() leaves a zero vector unchanged
+            for (int c = 0; c < 3; c++) r.u[3 * (size_t)k + c] = d[c] / L;
+        r.l[k] = L - h->md_d[k];
+    }
+    return r;
+}
+
+// a_k . v with v given at the pair nodes (6 values per pair: v_i, v_j)
+double pair_dot(const PairRows& R, int k, const double* v) {
+    const double* u = &R.u[3 * (size_t)k];
+    return -(u[0] * v[0] + u[1] * v[1] + u[2] * v[2]) + (u[0] * v[3] + u[1] * v[4] + u[2] * v[5]);
+}
+
+int ensure_pair_buffers(SorsHandle* h, int np) {
+    if (np <= h->md_cap) return SORS_OK;
+    int st;
+    if ((st = dalloc_t(h, &h->md_nodes_d, 2 * (size_t)np))) return st;
+    if ((st = dalloc_t(h, &h->md_pos_d, 6 * (size_t)np))) return st;
+    if ((st = dalloc_t(h, &h->md_ij_d, (size_t)np))) return st;
+    if ((st = dalloc_t(h, &h->md_coef_d, (size_t)np))) return st;
+    h->md_cap = np;
+    return SORS_OK;
+}
+
+// Small dense solve (Gaussian elimination, partial pivoting); false if singular.
+bool dense_solve(int m, std::vector<double> A, std::vector<double>& b) {
+    for (int c = 0; c < m; c++) {
+        int piv = c;
+        for (int r = c + 1; r < m; r++)
+            if (fabs(A[(size_t)r * m + c]) > fabs(A[(size_t)piv * m + c])) piv = r;
+        if (!(fabs(A[(size_t)piv * m + c]) > 0.0)) return false;
+        if (piv != c) {
+            for (int k = 0; k < m; k++) std::swap(A[(size_t)c * m + k], A[(size_t)piv * m + k]);
+            std::swap(b[c], b[piv]);
+        }
+        for (int r = c + 1; r < m; r++) {
+            const double f = A[(size_t)r * m + c] / A[(size_t)c * m + c];
+            for (int k = c; k < m; k++) A[(size_t)r * m + k] -= f * A[(size_t)c * m + k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int c = m - 1; c >= 0; c--) {
+        double s = b[c];
+        for (int k = c + 1; k < m; k++) s -= A[(size_t)c * m + k] * b[k];
+        b[c] = s / A[(size_t)c * m + c];
+    }
+    return true;
+}
+
+// The held maxDistance pairs on top of the node-projected QP solution dx0 (in
+// qp_dx).  With P the projection of the held nodes, w_k = (P H P)^+ P a_k (one
+// projected PCG solve per held pair) and dx = dx0 + sum_k mu_k w_k satisfies
+// P (H dx + g - sum_k mu_k a_k) = 0; the held rows a_j . dx = l_j give the
+// small system S mu = l - A dx0, S_jk = a_j . w_k.  Violated pairs join the
+// working set, held pairs with mu < 0 leave.  On return qp_dx holds dx and
+// mu[k] the multiplier of pair k (0 when not held).  Returns -1 when a solve met
+// negative curvature with the exact Hessian (the caller falls back to the
+// projected one).
+template <typename HT, typename VT>
+int solve_pairs(SorsHandle* h, const PairRows& R, double eta, std::vector<double>& mu, int* pcg_iters) {
+    const int np = (int)h->md_d.size(), n = h->ndof;
+    mu.assign(np, 0.0);
+    std::vector<double> D0(6 * (size_t)np), Wh;   // dx0 and the w_k at the pair nodes
+    launch_gather_nodes(2 * np, h->md_nodes_d, h->qp_dx, h->md_pos_d, h->stream);
+    CK(d2h(h, D0.data(), h->md_pos_d, sizeof(double) * 6 * np));
+    std::vector<int> slot(np, -1);  // pool index of w_k
+    int used = 0;
+    double l_scale = 0.0;
+    for (int k = 0; k < np; k++) l_scale = std::max(l_scale, fabs(R.l[k]));
+    const double tol_s = 1e-12 + 1e-9 * l_scale;
+    std::vector<int> wl;
+    for (int round = 0; round < 25; round++) {
+        wl.clear();
+        for (int k = 0; k < np; k++)
+            if (h->md_work[k]) wl.push_back(k);
+        for (int k : wl) {
+            if (slot[k] >= 0) continue;
+            if (used == (int)h->md_w.size()) {
+                double* w = nullptr;
+                int st;
+                if ((st = dalloc_t(h, &w, (size_t)n))) return st;
+                h->md_w.push_back(w);
+            }
+            // g = -a_k: the PCG solves P H P x = -P g
+            const double4 coef = make_double4(R.u[3 * (size_t)k], R.u[3 * (size_t)k + 1], R.u[3 * (size_t)k + 2], -1.0);
+            const int2 ij = make_int2(h->md_i[k], h->md_j[k]);
+            CK(h2d(h, h->md_coef_d, &coef, sizeof(double4)));
+            CK(h2d(h, h->md_ij_d, &ij, sizeof(int2)));
+            CK(cudaMemsetAsync(h->qp_g2, 0, sizeof(double) * n, h->stream));
+            launch_pair_axpy(1, h->md_ij_d, h->md_coef_d, h->qp_g2, h->stream);
+            int pit = 0, st;
+            if ((st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2))) return st;
+            *pcg_iters += pit;
+            if (h->s.project_spd == 2 && !h->proj_fallback && h->sc_host->breakdown) return -1;
+            double* w = h->md_w[used];
+            CK(cudaMemsetAsync(w, 0, sizeof(double) * n, h->stream));
+            launch_add_vec<VT>(n, w, (const VT*)h->x, w, h->stream);
+            Wh.resize(6 * (size_t)np * (used + 1));
+            launch_gather_nodes(2 * np, h->md_nodes_d, w, h->md_pos_d, h->stream);
+            CK(d2h(h, &Wh[6 * (size_t)np * used], h->md_pos_d, sizeof(double) * 6 * np));
+            slot[k] = used++;
+        }
+        const int m = (int)wl.size();
+        std::vector<double> S((size_t)m * m), rhs(m);
+        for (int a = 0; a < m; a++) {
+            rhs[a] = R.l[wl[a]] - pair_dot(R, wl[a], &D0[6 * (size_t)wl[a]]);
+            for (int b = 0; b < m; b++)
+                S[(size_t)a * m + b] = pair_dot(R, wl[a], &Wh[6 * (size_t)np * slot[wl[b]] + 6 * (size_t)wl[a]]);
+        }
+        for (int a = 0; a < m; a++)
+            for (int b = 0; b < a; b++) S[(size_t)a * m + b] = S[(size_t)b * m + a] = 0.5 * (S[(size_t)a * m + b] + S[(size_t)b * m + a]);
+        std::vector<double> sol = rhs;
+        if (m && !dense_solve(m, S, sol)) return fail(SORS_ERR_NOT_CONVERGED, "max-distance pairs are dependent");
+        mu.assign(np, 0.0);
+        double mu_scale = 0.0;
+        for (int a = 0; a < m; a++) { mu[wl[a]] = sol[a]; mu_scale = std::max(mu_scale, fabs(sol[a])); }
+        const double tol_mu = 1e-14 + 1e-8 * mu_scale;
+        bool changed = false;
+        for (int k = 0; k < np; k++) {
+            if (h->md_work[k]) {
+                if (mu[k] < -tol_mu) { h->md_work[k] = 0; changed = true; }
+                continue;
+            }
+            double v[6];
+            for (int c = 0; c < 6; c++) {
+                v[c] = D0[6 * (size_t)k + c];
+                for (int a = 0; a < m; a++) v[c] += sol[a] * Wh[6 * (size_t)np * slot[wl[a]] + 6 * (size_t)k + c];
+            }
+            if (pair_dot(R, k, v) - R.l[k] < -tol_s) { h->md_work[k] = 1; changed = true; }
+        }
+        if (!changed) break;
+    }
+    for (int k = 0; k < np; k++) {
+        if (!h->md_work[k] || slot[k] < 0) mu[k] = 0.0;
+        if (mu[k] != 0.0) launch_axpy(n, mu[k], h->md_w[slot[k]], h->qp_dx, h->stream);
+    }
+    return SORS_OK;
+}
+
+// Held maxDistance pairs in the adjoint.  At a converged SQP step
+// grad E(q) = sum_k mu_k grad g_k(q), so the step's sensitivity sees the
+// Lagrangian Hessian H_L = H + sum_k (mu_k / L_k) (I - u_k u_k^T) on (x_i - x_j)
+// (g_k = d_k - |x_i - x_j| has Hessian -(1/L)(I - u u^T) there) and the held
+// rows a_k . lam = 0.  Both enter as columns c_q = (w at i, -w at j) on top of
+// the node-projected solve lam0 = K^+ P b (K = P H P): the curvature as two
+// columns per pair (w = t1, t2 spanning u-perp, weight mu/L), the row as one
+// (w = -u).  With Y_q = K^+ P c_q, lam = lam0 + sum_q sigma_q z_q Y_q (sigma = -1
+// for curvature columns, z = their force; +1 for rows, z = the multiplier) and a
+// small dense system for z.  On return lam holds the result (host and adj_l)
+// and extra (3N) the columns' forces sum_q sigma_q z_q c_q, which the
+// reactions at fixed DOFs include.
+template <typename HT, typename VT>
+int adjoint_pairs(SorsHandle* h, double eta, std::vector<double>& lam, std::vector<double>& extra, int* iters) {
+    const int n = h->ndof, np = (int)h->md_d.size();
+    const int nh = (int)h->adj_pairs.size();
+    std::vector<double> xp(6 * (size_t)np);
+    launch_gather_nodes(2 * np, h->md_nodes_d, h->q, h->md_pos_d, h->stream);
+    CK(d2h(h, xp.data(), h->md_pos_d, sizeof(double) * 6 * np));
+    const PairRows R = pair_rows(h, xp);
+    struct Col { int pair; double w[3]; double c; double sigma; };
+    std::vector<Col> cols;
+    for (int a = 0; a < nh; a++) {
+        const int k = h->adj_pairs[a];
+        const double* u = &R.u[3 * (size_t)k];
+        const double L = R.l[k] + h->md_d[k];
+        const double c = L > 0.0 ? h->adj_mu[a] / L : 0.0;
+        if (c != 0.0) {
+            double e[3] = {0, 0, 0};
+            e[fabs(u[0]) < 0.9 ? 0 : 1] = 1.0;
+            const double eu = e[0] * u[0] + e[1] * u[1] + e[2] * u[2];
+            double t1[3] = {e[0] - eu * u[0], e[1] - eu * u[1], e[2] - eu * u[2]};
+            const double tn = sqrt(t1[0] * t1[0] + t1[1] * t1[1] + t1[2] * t1[2]);
+            for (double& v : t1) v /= tn;
+            const double t2[3] = {u[1] * t1[2] - u[2] * t1[1], u[2] * t1[0] - u[0] * t1[2], u[0] * t1[1] - u[1] * t1[0]};
+            cols.push_back({k, {t1[0], t1[1], t1[2]}, c, -1.0});
+            cols.push_back({k, {t2[0], t2[1], t2[2]}, c, -1.0});
+        }
+        cols.push_back({k, {-u[0], -u[1], -u[2]}, 0.0, 1.0});
+    }
+    const int m = (int)cols.size();
+    while ((int)h->md_w.size() < m) {
+        double* w = nullptr;
+        int st;
+        if ((st = dalloc_t(h, &w, (size_t)n))) return st;
+        h->md_w.push_back(w);
+    }
+    // the columns at the pair nodes: col_p . v for v given there
+    auto dot = [&](const Col& c, const double* v) {
+        const double* vi = v + 6 * (size_t)c.pair;
+        return c.w[0] * (vi[0] - vi[3]) + c.w[1] * (vi[1] - vi[4]) + c.w[2] * (vi[2] - vi[5]);
+    };
+    std::vector<double> y0(6 * (size_t)np), Y(6 * (size_t)np * m);
+    launch_gather_nodes(2 * np, h->md_nodes_d, h->adj_l, h->md_pos_d, h->stream);
+    CK(d2h(h, y0.data(), h->md_pos_d, sizeof(double) * 6 * np));
+    h->proj_flag = h->pflag_d;
+    h->proj_n = h->pn_d;
+    for (int q = 0; q < m; q++) {
+        // g = -c_q: the PCG solves K x = -P g
+        const double4 coef = make_double4(cols[q].w[0], cols[q].w[1], cols[q].w[2], 1.0);
+        const int2 ij = make_int2(h->md_i[cols[q].pair], h->md_j[cols[q].pair]);
+        CK(h2d(h, h->md_coef_d, &coef, sizeof(double4)));
+        CK(h2d(h, h->md_ij_d, &ij, sizeof(int2)));
+        CK(cudaMemsetAsync(h->qp_g2, 0, sizeof(double) * n, h->stream));
+        launch_pair_axpy(1, h->md_ij_d, h->md_coef_d, h->qp_g2, h->stream);
+        int pit = 0, st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
+        if (st) { h->proj_flag = nullptr; h->proj_n = nullptr; return st; }
+        *iters += pit;
+        CK(cudaMemsetAsync(h->md_w[q], 0, sizeof(double) * n, h->stream));
+        launch_add_vec<VT>(n, h->md_w[q], (const VT*)h->x, h->md_w[q], h->stream);
+        launch_gather_nodes(2 * np, h->md_nodes_d, h->md_w[q], h->md_pos_d, h->stream);
+        CK(d2h(h, &Y[6 * (size_t)np * q], h->md_pos_d, sizeof(double) * 6 * np));
+    }
+    h->proj_flag = nullptr;
+    h->proj_n = nullptr;
+    std::vector<double> A((size_t)m * m), z(m);
+    for (int p = 0; p < m; p++) {
+        const bool curv = cols[p].sigma < 0.0;
+        for (int q = 0; q < m; q++) {
+            const double v = cols[q].sigma * dot(cols[p], &Y[6 * (size_t)np * q]);
+            A[(size_t)p * m + q] = curv ? (p == q) - cols[p].c * v : v;
+        }
+        z[p] = curv ? cols[p].c * dot(cols[p], y0.data()) : -dot(cols[p], y0.data());
+    }
+    if (m && !dense_solve(m, A, z)) return fail(SORS_ERR_NOT_CONVERGED, "held max-distance pairs are dependent");
+    extra.assign(n, 0.0);
+    for (int q = 0; q < m; q++) {
+        launch_axpy(n, cols[q].sigma * z[q], h->md_w[q], h->adj_l, h->stream);
+        const int i = h->md_i[cols[q].pair], j = h->md_j[cols[q].pair];
+        for (int c = 0; c < 3; c++) {
+            extra[3 * (size_t)i + c] += cols[q].sigma * z[q] * cols[q].w[c];
+            extra[3 * (size_t)j + c] -= cols[q].sigma * z[q] * cols[q].w[c];
+        }
+    }
+    CK(d2h(h, lam.data(), h->adj_l, sizeof(double) * n));
+    return SORS_OK;
+}
+
 // Solver::minimize_SQP (solver.cpp:109-197): at each iteration the QP
 //   min 1/2 dx^T H dx + g^T dx  s.t.  dx_i = -(x_i - qPrev_i - dt val_i) (Neumann),
 //                                     n_c . dx_v >= -n_c . (x_v - p_c)   (contact)
@@ -997,8 +1274,12 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
         for (size_t i = 0; i < G.mask.size(); i++)
             if (G.mask[i] >= 0) add(G.surf[i], h->disks[G.mask[i]].c, h->disks[G.mask[i]].n);
     const int m = (int)cnode.size();
+    const int np = (int)h->md_d.size();
     h->last_active = m;
     if ((st = ensure_sqp_buffers(h, m))) return st;
+    std::vector<double> xpair(6 * (size_t)np), mu_pair;
+    PairRows R;
+    h->md_work.assign(np, 0);
     if (m) CK(h2d(h, h->cnode_d, cnode.data(), sizeof(int) * m));
     std::vector<char> inW(m, 0);
     std::vector<double> b(m), xc(3 * (size_t)m), chk(2 * (size_t)m);
@@ -1035,6 +1316,13 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
             if (it == 0) inW[c] = b[c] > 0.0;  // start with the constraints violated now
         }
         if (m) CK(h2d(h, h->cnb_d, cnb.data(), sizeof(double4) * m));
+        if (np) {
+            launch_gather_nodes(2 * np, h->md_nodes_d, h->q, h->md_pos_d, h->stream);
+            CK(d2h(h, xpair.data(), h->md_pos_d, sizeof(double) * 6 * np));
+            R = pair_rows(h, xpair);
+            if (it == 0)
+                for (int k = 0; k < np; k++) h->md_work[k] = R.l[k] > 0.0;  // violated now
+        }
         if (stats) { stats->newton_iters++; stats->residual_norm = sqrt(h->sc_host->gnorm2); }
         int inner_used = 0, pcg_used = 0, adds = 0, drops = 0;
         for (int inner = 0; inner < 25; inner++) {
@@ -1071,8 +1359,41 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
                 continue;
             }
             launch_add_vec<VT>(n, h->qp_x0, (const VT*)h->x, h->qp_dx, h->stream);
+            if (np) {
+                h->proj_flag = h->pflag_d;
+                h->proj_n = h->pn_d;
+                int pp = 0;
+                st = solve_pairs<HT, VT>(h, R, eta, mu_pair, &pp);
+                h->proj_flag = nullptr;
+                h->proj_n = nullptr;
+                if (stats) stats->pcg_iters += pp;
+                pcg_used += pp;
+                if (st == -1) {
+                    h->proj_fallback = true;
+                    if ((st = eval_system<HT>(h, dt, true, kAsmFull))) return st;
+                    inner--;
+                    continue;
+                }
+                if (st) return st;
+            }
             if (m == 0) break;
             launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->qp_dx, h->qp_y, h->stream);
+            if (np) {
+                // the held pairs' forces: y = H dx - sum_k mu_k a_k
+                std::vector<int2> ij;
+                std::vector<double4> coef;
+                for (int k = 0; k < np; k++)
+                    if (mu_pair[k] != 0.0) {
+                        ij.push_back(make_int2(h->md_i[k], h->md_j[k]));
+                        coef.push_back(make_double4(R.u[3 * (size_t)k], R.u[3 * (size_t)k + 1], R.u[3 * (size_t)k + 2],
+                                                    -mu_pair[k]));
+                    }
+                if (!ij.empty()) {
+                    CK(h2d(h, h->md_ij_d, ij.data(), sizeof(int2) * ij.size()));
+                    CK(h2d(h, h->md_coef_d, coef.data(), sizeof(double4) * coef.size()));
+                    launch_pair_axpy((int)ij.size(), h->md_ij_d, h->md_coef_d, h->qp_y, h->stream);
+                }
+            }
             launch_qp_check(m, h->cnode_d, h->cnb_d, h->qp_dx, h->qp_y, h->g, h->cout_d, h->stream);
             CK(d2h(h, chk.data(), h->cout_d, sizeof(double) * 2 * m));
             double mu_scale = 0.0, b_scale = 0.0;
@@ -1128,6 +1449,13 @@ int minimize_sqp(SorsHandle* h, double dt, SorsStepStats* stats) {
         if (dxn < h->s.newton_dx_tol) { converged = true; break; }
     }
     if (!converged) return fail(SORS_ERR_NOT_CONVERGED, "SQP method did not converge");
+    h->held_pairs.clear();
+    h->held_mu.clear();
+    for (int k = 0; k < np; k++)
+        if (h->md_work[k]) {
+            h->held_pairs.push_back(k);
+            h->held_mu.push_back(k < (int)mu_pair.size() ? mu_pair[k] : 0.0);
+        }
     h->held_nodes.clear();
     h->held_normals.clear();
     for (int c = 0; c < m; c++)
@@ -1634,6 +1962,46 @@ int sors_set_disk(SorsHandle* h, int32_t disk_idx, const double* center, const d
     if (!(nn > 0)) return fail(SORS_ERR_ARG, "zero disk normal");
     for (int c = 0; c < 3; c++) { D.c[c] = center[c]; D.n[c] = normal[c] / nn; }
     D.r = radius;
+    return SORS_OK;
+}
+
+int sors_set_max_distance(SorsHandle* h, const int32_t* vertex1, const int32_t* vertex2, const double* max_distance,
+                          int32_t n_pairs) {
+    if (!h || (n_pairs > 0 && (!vertex1 || !vertex2 || !max_distance))) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_pairs < 0) return fail(SORS_ERR_ARG, "negative count");
+    for (int k = 0; k < n_pairs; k++)
+        if (vertex1[k] < 0 || vertex1[k] >= h->N || vertex2[k] < 0 || vertex2[k] >= h->N)
+            return fail(SORS_ERR_ARG, "max-distance vertex out of range");
+    int st;
+    if ((st = ensure_pair_buffers(h, n_pairs))) return st;
+    h->md_i.assign(vertex1, vertex1 + n_pairs);
+    h->md_j.assign(vertex2, vertex2 + n_pairs);
+    h->md_d.assign(max_distance, max_distance + n_pairs);
+    h->md_work.assign(n_pairs, 0);
+    h->held_pairs.clear();
+    std::vector<int> nodes(2 * (size_t)n_pairs);
+    for (int k = 0; k < n_pairs; k++) { nodes[2 * k] = vertex1[k]; nodes[2 * k + 1] = vertex2[k]; }
+    if (n_pairs) CK(h2d(h, h->md_nodes_d, nodes.data(), sizeof(int) * nodes.size()));
+    return SORS_OK;
+}
+
+int32_t sors_held_pairs(SorsHandle* h, int32_t* pairs, double* multipliers, int32_t cap) {
+    if (!h) return 0;
+    const int k = (int)h->held_pairs.size();
+    for (int c = 0; c < k && c < cap; c++) {
+        if (pairs) pairs[c] = h->held_pairs[c];
+        if (multipliers) multipliers[c] = h->held_mu[c];
+    }
+    return k;
+}
+
+int sors_adjoint_set_pairs(SorsHandle* h, const int32_t* pairs, const double* multipliers, int32_t n) {
+    if (!h || (n > 0 && (!pairs || !multipliers))) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n < 0) return fail(SORS_ERR_ARG, "negative count");
+    for (int c = 0; c < n; c++)
+        if (pairs[c] < 0 || pairs[c] >= (int)h->md_d.size()) return fail(SORS_ERR_ARG, "held pair out of range");
+    h->adj_pairs.assign(pairs, pairs + n);
+    h->adj_mu.assign(multipliers, multipliers + n);
     return SORS_OK;
 }
 

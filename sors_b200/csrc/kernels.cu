@@ -1379,6 +1379,37 @@ __global__ void k_gather_nodes(int m, const int* __restrict__ node, const double
     out[t] = q[3 * (size_t)node[c] + k];
 }
 
+// Max-distance rows a_p = (-n_p at node i_p, +n_p at node j_p): y += s_p a_p for
+// every listed pair, coef[p] = (n_p, s_p).  Pairs may share nodes, so one
+// thread walks them in order (a handful of pairs; deterministic).
+__global__ void k_pair_axpy(int np, const int2* __restrict__ ij, const double4* __restrict__ coef,
+                            double* __restrict__ y) {
+    if (blockIdx.x || threadIdx.x) return;
+    for (int p = 0; p < np; p++) {
+        const int2 e = ij[p];
+        const double4 c = coef[p];
+        const size_t a = 3 * (size_t)e.x, b = 3 * (size_t)e.y;
+        y[a] -= c.w * c.x; y[a + 1] -= c.w * c.y; y[a + 2] -= c.w * c.z;
+        y[b] += c.w * c.x; y[b + 1] += c.w * c.y; y[b + 2] += c.w * c.z;
+    }
+}
+
+// y += alpha x
+__global__ void k_axpy(int n, double alpha, const double* __restrict__ x, double* __restrict__ y) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] += alpha * x[i];
+}
+
+void launch_pair_axpy(int np, const int2* ij, const double4* coef, double* y, cudaStream_t st) {
+    if (np == 0) return;
+    k_pair_axpy<<<1, 1, 0, st>>>(np, ij, coef, y);
+    counted();
+}
+void launch_axpy(int n, double alpha, const double* x, double* y, cudaStream_t st) {
+    k_axpy<<<(n + 255) / 256, 256, 0, st>>>(n, alpha, x, y);
+    counted();
+}
+
 void launch_qp_x0(int N, const uint8_t* pflag, const double4* pn, const double* q, const double* qPrev,
                   const double* mval, double dt, double* x0, cudaStream_t st) {
     k_qp_x0<<<(N + 255) / 256, 256, 0, st>>>(N, pflag, pn, q, qPrev, mval, dt, x0);

@@ -186,6 +186,8 @@ void launch_add_vec(int n, const double* a, const VT* b, double* out, cudaStream
 void launch_qp_check(int m, const int* cnode, const double4* cnb, const double* dx, const double* y,
                      const double* g, double* out, cudaStream_t st);
 void launch_gather_nodes(int m, const int* node, const double* q, double* out, cudaStream_t st);
+void launch_pair_axpy(int np, const int2* ij, const double4* coef, double* y, cudaStream_t st);
+void launch_axpy(int n, double alpha, const double* x, double* y, cudaStream_t st);
 template <typename VT>
 void launch_newton_update(int n, const VT* dx, double alpha, double* q, const double* q0, double* partials,
                           DevScalars* sc, int counter, cudaStream_t st);

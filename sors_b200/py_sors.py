@@ -222,6 +222,17 @@ class _EnergyBase:
                     raise ValueError("DiskContact: centers/normals must be same length and multiples of 3")
                 _lib.check(L.sors_set_disk_contact(self._h, _p(cen, C.c_double), _p(nrm, C.c_double),
                                                    _p(rad, C.c_double), rad.size, _p(surf, C.c_int32), surf.size))
+            elif c == "maxDistance":
+                # energy.cpp:109-120
+                v1 = np.ascontiguousarray(cp.get_value("maxDistanceVertex1Indices").ravel().astype(np.int32))
+                v2 = np.ascontiguousarray(cp.get_value("maxDistanceVertex2Indices").ravel().astype(np.int32))
+                dm = np.ascontiguousarray(cp.get_value("maxDistanceList").ravel().astype(np.float64))
+                if not (v1.size == v2.size == dm.size):
+                    raise ValueError("MaxDistance constraint parameters must have the same size.")
+                if v1.size == 0:
+                    raise ValueError("MaxDistance constraint pair is empty. Remove this constraint.")
+                _lib.check(L.sors_set_max_distance(self._h, _p(v1, C.c_int32), _p(v2, C.c_int32),
+                                                   _p(dm, C.c_double), v1.size))
             else:
                 raise NotImplementedError(f"constraint {c} is not built on the GPU path")
         for f in forceTypesList:
@@ -424,6 +435,14 @@ class _EnergyBase:
     def active_contacts(self):
         """Contact constraints active in the last SQP step."""
         return int(_lib.load().sors_active_contacts(self._h))
+
+    def held_pairs(self):
+        """Indices of the maxDistance pairs held at their bound by the last SQP step."""
+        L = _lib.load()
+        k = int(L.sors_held_pairs(self._h, None, None, 0))
+        out = np.zeros(max(k, 1), np.int32)
+        L.sors_held_pairs(self._h, _p(out, C.c_int32), None, k)
+        return out[:k]
 
     def handle(self):
         return self._h

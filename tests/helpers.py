@@ -84,10 +84,11 @@ def deform(X, rng, amp=0.05, scale=None):
 
 def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1e5, nu=0.45,
                  grav=(0.0, 0.0, -9.81), dt=1e-3, precision="fp64", project=True, neumann=None, muscles=None,
-                 two_level=False):
+                 two_level=False, max_distance=None):
     """GPU Energy/Solver with minimize_SQP and the oracle's SQP on the same scene.
 
     planes: (points (k,3), normals (k,3)); disks: (centers, normals, radii);
+    max_distance: (vertex1, vertex2, distances);
     surface: candidate contact vertices (all surface vertices when None);
     neumann: (mask 3N, value 3N) or None."""
     from oracle import oracle as orc
@@ -125,6 +126,11 @@ def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1
         cp.set_param("diskRadiusList", np.asarray(disks[2], float).ravel())
     if planes is not None or disks is not None:
         cp.set_param("surfaceVerticesIdx", surface.astype(float))
+    if max_distance is not None:
+        ctypes_.append("maxDistance")
+        cp.set_param("maxDistanceVertex1Indices", np.asarray(max_distance[0], float))
+        cp.set_param("maxDistanceVertex2Indices", np.asarray(max_distance[1], float))
+        cp.set_param("maxDistanceList", np.asarray(max_distance[2], float))
     en = ps.EnergyTet.from_arrays if T.shape[1] == 4 else ps.EnergyHex.from_arrays
     en = en(X, T, s, np.asarray(grav, float), 0.0, density=rho, youngsModulus=Ev, poissonsRatio=nu,
             muscleGroup=None if muscles is None else muscles["group"],
@@ -138,5 +144,20 @@ def contact_pair(X, T, *, planes=None, disks=None, surface=None, rho=1070.0, E=1
         o.set_muscles(muscles["group"], muscles["k"], muscles["dir"], int(max(muscles["group"])) + 1)
     pl = None if planes is None else oc.PlaneContact(planes[0], planes[1], surface)
     dk = None if disks is None else oc.DiskContact(disks[0], disks[1], disks[2], surface)
-    sq = oc.SQPOracle(o, pl, dk, neumann)
+    md = None if max_distance is None else oc.MaxDistance(*max_distance)
+    sq = oc.SQPOracle(o, pl, dk, neumann, max_distance=md)
     return en, sol, sq, surface
+
+
+def two_cubes(n=2, s=0.004, gap=0.002, kind="hex"):
+    """Two n^3-cell cubes of side s, gap apart along x; returns (X, T, a, b, n1) with
+    a the max-x vertex of the first cube and b the min-x vertex of the second, both at
+    mid height and mid depth (the pair of a maxDistance rope), n1 the first cube's
+    vertex count."""
+    X, H = meshes.hex_bar(n, n, n, (s, s, s))
+    T = H if kind == "hex" else meshes.kuhn_tet_elements(n, n, n)
+    X2 = X + np.array([s + gap, 0.0, 0.0])
+    off = 1e-3 * (np.abs(X[:, 1] - s / 2) + np.abs(X[:, 2] - s / 2))
+    a = int(np.argmax(X[:, 0] - off))
+    b = X.shape[0] + int(np.argmin(X[:, 0] + off))
+    return np.vstack([X, X2]), np.vstack([T, T + X.shape[0]]).astype(np.int32), a, b, X.shape[0]

@@ -38,3 +38,47 @@ def test_cube_drop_kkt():
         touched |= sq.last_active > 0
         assert x.reshape(-1, 3)[surf, 2].min() > -1e-9
     assert touched
+
+
+def test_max_distance_rope_oracle():
+    # two cubes flying apart (+-0.2 m/s) joined by a maxDistance pair of 2.5 mm
+    # (the two-sphere rope of cpp/demos/08_multiple_constraints_sphere.cpp): the
+    # pair goes taut, holds at its bound with a non-negative multiplier, then
+    # releases when the bodies rebound.
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    from tests.helpers import two_cubes
+    X, T, a, b, n1 = two_cubes()
+    dt = 5e-4
+    o = orc.System(X, T, rho=1000.0, youngs=np.full(T.shape[0], 2e4), nu=0.4, grav=(0, 0, -9.81),
+                   scheme="backward_euler", method="minimize_SQP", dt=dt, substeps=1, nthreads=1)
+    v = np.zeros_like(X); v[:n1, 0] = -0.2; v[n1:, 0] = 0.2
+    o.set_initial_velocity(v.ravel())
+    sq = oc.SQPOracle(o, max_distance=oc.MaxDistance([a], [b], [0.0025]))
+    x = X.ravel().copy()
+    held = []
+    for _ in range(14):
+        x = sq.step(x, dt)
+        L = np.linalg.norm(x.reshape(-1, 3)[a] - x.reshape(-1, 3)[b])
+        assert L <= 0.0025 + 1e-12
+        held.append(len(sq.held_pairs))
+        if held[-1]:
+            assert abs(L - 0.0025) < 1e-12
+    assert held[0] == 0 and max(held) == 1 and held[-1] == 0
+
+
+def test_max_distance_qp_kkt():
+    # one QP with a pair row: stationarity H dx + g = mu a, mu >= 0, a.dx = l
+    from oracle import contact as oc
+    import scipy.sparse as sp
+    rng = np.random.default_rng(3)
+    n = 12
+    M = rng.standard_normal((n, n)); H = sp.csr_matrix(M @ M.T + n * np.eye(n))
+    g = rng.standard_normal(n)
+    x = rng.standard_normal(n)
+    md = oc.MaxDistance([0, 1], [2, 3], [0.1, 50.0])
+    A, l = md.rows(x, n)
+    dx, work, mu = oc.solve_qp(H, g, sp.csr_matrix((0, n)), np.zeros(0), A, l)
+    assert work[0] and not work[1]
+    assert mu[0] >= 0.0 and abs((A @ dx)[0] - l[0]) < 1e-10
+    assert np.abs(H @ dx + g - A.T @ mu).max() < 1e-9
