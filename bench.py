@@ -270,14 +270,17 @@ def run_gpu(args, rank, world, local_rank):
     # kernel roofline on the final assembled system
     prof = _lib.SorsKernelProfile()
     _lib.check(L.sors_profile_kernels(en.handle(), 20, __import__("ctypes").byref(prof)))
-    per_step = {
-        "pcg_spmv": (pcg / args.steps) * prof.spmv_ms,
-        "pcg_update": (pcg / args.steps) * prof.pcg_update_ms,
-        "assemble": (newton / args.steps) * prof.assemble_ms,
-    }
+    # per PCG iteration: the SpMV and either the block-Jacobi update or the two
+    # two-level kernels (update + restriction, coarse solve + prolongation)
+    two_level = prof.tl_restrict_ms > 0.0
+    it_kernels = {"tl_restrict": (prof.tl_restrict_ms, prof.tl_restrict_bytes),
+                  "tl_coarse_z": (prof.tl_coarse_z_ms, prof.tl_coarse_z_bytes)} if two_level else \
+        {"pcg_update": (prof.pcg_update_ms, prof.pcg_update_bytes)}
+    kern = {"pcg_spmv": (prof.spmv_ms, prof.spmv_bytes), **it_kernels,
+            "assemble": (prof.assemble_ms, prof.assemble_bytes)}
+    per_step = {k: (newton if k == "assemble" else pcg) / args.steps * v[0] for k, v in kern.items()}
     dom = max(per_step, key=per_step.get)
-    bytes_ = {"pcg_spmv": prof.spmv_bytes, "pcg_update": prof.pcg_update_bytes, "assemble": prof.assemble_bytes}[dom]
-    dur = {"pcg_spmv": prof.spmv_ms, "pcg_update": prof.pcg_update_ms, "assemble": prof.assemble_ms}[dom]
+    dur, bytes_ = kern[dom]
     peak, peak_src = measured_peak_hbm()
     achieved = bytes_ / (dur / 1e3) / 1e9
     traffic = ncu_traffic(f"{dom}_{args.precision}", nn)
@@ -336,9 +339,8 @@ def run_gpu(args, rank, world, local_rank):
         "newton_steps_per_s": world * args.steps / (ms / 1e3),
         "newton_iters_per_step": newton / args.steps, "pcg_iters_per_step": pcg / args.steps,
         "assembly_gbs": prof.assemble_bytes / (prof.assemble_ms / 1e3) / 1e9,
-        "kernels": {"assemble_ms": prof.assemble_ms, "spmv_ms": prof.spmv_ms, "pcg_update_ms": prof.pcg_update_ms,
-                    "spmv_gbs": prof.spmv_bytes / (prof.spmv_ms / 1e3) / 1e9,
-                    "pcg_update_gbs": prof.pcg_update_bytes / (prof.pcg_update_ms / 1e3) / 1e9,
+        "kernels": {**{f"{k}_ms": v[0] for k, v in kern.items()},
+                    **{f"{k}_gbs": v[1] / (v[0] / 1e3) / 1e9 for k, v in kern.items()},
                     "share_ms_per_step": per_step},
         "roofline": {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_src, "traffic": traffic,

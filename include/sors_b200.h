@@ -265,6 +265,10 @@ int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t*
 typedef struct SorsKernelProfile {
     double assemble_ms, spmv_ms, pcg_update_ms, energy_ms;
     double assemble_bytes, spmv_bytes, pcg_update_bytes, energy_bytes;
+    /* two-level PCG iteration kernels (0 without the two-level preconditioner):
+     * the x / r update fused with the restriction, and the coarse solve fused
+     * with the prolongation and z = Minv r */
+    double tl_restrict_ms, tl_coarse_z_ms, tl_restrict_bytes, tl_coarse_z_bytes;
 } SorsKernelProfile;
 int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
 

@@ -161,7 +161,8 @@ struct SorsHandle {
     int *tl_pair_ptr = nullptr;
     int2 *tl_items = nullptr, *tl_ab = nullptr;
     double *tl_Ac = nullptr, *tl_yc = nullptr, *tl_rowk = nullptr, *tl_colk = nullptr;
-    void *tl_Ainv = nullptr, *tl_zc = nullptr;
+    void* tl_Ainv = nullptr;
+    int tl_ld = 0;                    // leading dimension of tl_Ainv (nc rounded up to 16 bytes)
     int tl_refreshes = 0;
 
     // projection used by the PCG kernels (null: none)
@@ -464,9 +465,8 @@ void pcg_iter_pair(SorsHandle* h) {
                                     pout, (VT*)h->qv, h->partials, h->sc, h->stream);
             launch_tl_update_restrict<VT>(h->cargs, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag,
                                           h->proj_n, h->tl_yc, h->sc, h->stream);
-            launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
-            launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, z, 0, h->proj_flag,
-                            h->proj_n, h->partials, h->sc, h->stream);
+            launch_tl_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->r,
+                                   (const VT*)h->Minv, z, 0, h->proj_flag, h->proj_n, h->partials, h->sc, h->stream);
         }
         return;
     }
@@ -537,7 +537,7 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
             launch_coarse_galerkin_d(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col,
                                      (const double*)h->H, h->nnzb, h->cargs, h->tl_Ac, h->stream);
         launch_coarse_invert(nc, h->tl_Ac, h->tl_rowk, h->tl_colk, h->stream);
-        launch_to_vt<VT>((long long)nc * nc, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
+        launch_to_vt_pad<VT>(nc, h->tl_ld, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
         h->tl_ready = true;
         h->tl_refreshes++;
         refreshed = true;
@@ -547,9 +547,8 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
                             h->sc, h->stream);
     if (h->tl_active) {
         launch_coarse_restrict<VT>(h->cargs, (VT*)h->r, h->tl_yc, h->stream);
-        launch_coarse_matvec<VT>(h->cargs.nc, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->tl_zc, h->stream);
-        launch_tl_z<VT>(h->cargs, (VT*)h->r, (const VT*)h->Minv, (const VT*)h->tl_zc, (VT*)h->z, 1, h->proj_flag,
-                        h->proj_n, h->partials, h->sc, h->stream);
+        launch_tl_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->r, (const VT*)h->Minv,
+                               (VT*)h->z, 1, h->proj_flag, h->proj_n, h->partials, h->sc, h->stream);
     }
     CK(cudaGetLastError());
     int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
@@ -953,11 +952,14 @@ int setup_two_level(SorsHandle* h, const double* X) {
     if ((st = upload(h, &h->tl_ab, pair_ab.data(), pair_ab.size()))) return st;
     if ((st = upload(h, &h->tl_items, items.data(), items.size()))) return st;
     if ((st = dalloc_t(h, &h->tl_Ac, (size_t)nc * nc))) return st;
-    if ((st = dalloc_t(h, &h->tl_yc, (size_t)nc))) return st;
+    // Ainv rows padded to a multiple of 16 bytes (zero padding, and zero tail in yc)
+    const int w16 = 16 / (int)hsize(h);
+    h->tl_ld = (nc + w16 - 1) / w16 * w16;
+    if ((st = dalloc_t(h, &h->tl_yc, (size_t)h->tl_ld))) return st;
+    CK(dzero(h, h->tl_yc, sizeof(double) * (size_t)h->tl_ld));
     if ((st = dalloc_t(h, &h->tl_rowk, (size_t)nc))) return st;
     if ((st = dalloc_t(h, &h->tl_colk, (size_t)nc))) return st;
-    if ((st = dalloc(h, &h->tl_Ainv, (size_t)nc * nc * hsize(h)))) return st;
-    if ((st = dalloc(h, &h->tl_zc, (size_t)nc * hsize(h)))) return st;
+    if ((st = dalloc(h, &h->tl_Ainv, (size_t)nc * h->tl_ld * hsize(h)))) return st;
     h->cargs.N = N; h->cargs.nagg = nagg; h->cargs.nc = nc;
     h->cargs.aid = aid_d; h->cargs.agg_c = cen_d; h->cargs.agg_ptr = aggptr_d; h->cargs.agg_nodes = nodes_d;
     h->cargs.fixed = h->node_mask; h->cargs.off = off_d;
@@ -2184,6 +2186,31 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     out->pcg_update_ms = ms / iters;
     // p, q, Minv read; x, r read+written; z written
     out->pcg_update_bytes = 3 * N * vs * 2 + 9 * N * vs + 3 * N * vs * 4 + 3 * N * vs;
+    if (h->cargs.nc > 0) {
+        // two-level iteration kernels (their values are not used: timing only)
+        CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
+        CK(cudaEventRecord(a, h->stream));
+        for (int i = 0; i < iters; i++)
+            launch_tl_update_restrict<VT>(h->cargs, (VT*)h->p1, (VT*)h->qv, (VT*)h->x, (VT*)h->r, nullptr, nullptr,
+                                          h->tl_yc, h->sc, h->stream);
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        CK(cudaEventElapsedTime(&ms, a, b));
+        out->tl_restrict_ms = ms / iters;
+        // p, q, x, r read; x, r written; offsets (16 B) and node list (4 B) per node
+        out->tl_restrict_bytes = 18 * N * vs + 20 * N;
+        CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
+        CK(cudaEventRecord(a, h->stream));
+        for (int i = 0; i < iters; i++)
+            launch_tl_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->r, (const VT*)h->Minv,
+                                   (VT*)h->z, 1, nullptr, nullptr, h->partials, h->sc, h->stream);
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        CK(cudaEventElapsedTime(&ms, a, b));
+        out->tl_coarse_z_ms = ms / iters;
+        // the coarse inverse once, r and Minv read, z written, offsets and node list
+        out->tl_coarse_z_bytes = (double)h->cargs.nc * h->tl_ld * vs + 15 * N * vs + 20 * N;
+    }
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
         launch_elem_energy(h->E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->partials, h->sc, h->stream);

@@ -31,6 +31,29 @@ __device__ __forceinline__ void warp_sum(double (&v)[NS]) {
         for (int s = 0; s < NS; s++) v[s] += __shfl_xor_sync(0xffffffffu, v[s], o);
 }
 
+// Block sum of NS values (fixed order: lanes, then warps); every thread gets
+// the totals.  sh: 32 x NS shared doubles.
+template <int NS>
+__device__ __forceinline__ void block_sum(double (&v)[NS], double (*sh)[NS]) {
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    warp_sum<NS>(v);
+    if (l == 0)
+#pragma unroll
+        for (int s = 0; s < NS; s++) sh[w][s] = v[s];
+    __syncthreads();
+    if (w == 0) {
+#pragma unroll
+        for (int s = 0; s < NS; s++) v[s] = (l < nw) ? sh[l][s] : 0.0;
+        warp_sum<NS>(v);
+        if (l == 0)
+#pragma unroll
+            for (int s = 0; s < NS; s++) sh[0][s] = v[s];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NS; s++) v[s] = sh[0][s];
+}
+
 // Block sum of v into partials[blockIdx.x*NS + s]; then the last block to
 // arrive sums all partials in grid order and returns true with totals in tot.
 template <int NS>
@@ -1581,29 +1604,19 @@ void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaSt
     g_kernel_launches.fetch_add(2LL * nc);
 }
 
-template <typename VT>
-__global__ void k_to_vt(long long n, const double* __restrict__ in, VT* __restrict__ out) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t < n) out[t] = (VT)in[t];
-}
-template <typename VT>
-void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st) {
-    if (n == 0) return;
-    k_to_vt<VT><<<(int)((n + 255) / 256), 256, 0, st>>>(n, in, out);
-    counted();
-}
-
 // yc = P^T r: one block per aggregate, a fixed-order tree sum.  The fused
 // variant first applies the CG update x += alpha p, r -= alpha P q to the
 // aggregate's nodes (each node belongs to exactly one aggregate).
+constexpr int kAggThreads = 256;  // threads per aggregate block
+
 template <typename VT, bool UPDATE>
-__global__ void __launch_bounds__(512) k_coarse_restrict(CoarseArgs c, const VT* __restrict__ p,
-                                                         const VT* __restrict__ qv, VT* __restrict__ x,
-                                                         VT* __restrict__ r, const uint8_t* __restrict__ pflag,
-                                                         const double4* __restrict__ pn, double* __restrict__ yc,
-                                                         const DevScalars* sc) {
+__global__ void __launch_bounds__(kAggThreads) k_coarse_restrict(CoarseArgs c, const VT* __restrict__ p,
+                                                                 const VT* __restrict__ qv, VT* __restrict__ x,
+                                                                 VT* __restrict__ r, const uint8_t* __restrict__ pflag,
+                                                                 const double4* __restrict__ pn,
+                                                                 double* __restrict__ yc, const DevScalars* sc) {
     if (UPDATE && *(volatile const int*)&sc->done) return;
-    __shared__ double sh[6][512];
+    __shared__ double sh[32][6];
     const int a = blockIdx.x;
     const VT alpha = UPDATE ? (VT)sc->alpha : VT(0);
     double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -1635,93 +1648,98 @@ __global__ void __launch_bounds__(512) k_coarse_restrict(CoarseArgs c, const VT*
 #pragma unroll
         for (int m = 0; m < 6; m++) acc[m] += y[m];
     }
+    block_sum<6>(acc, sh);
+    if (threadIdx.x == 0)
 #pragma unroll
-    for (int m = 0; m < 6; m++) sh[m][threadIdx.x] = acc[m];
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-        if (threadIdx.x < o)
-#pragma unroll
-            for (int m = 0; m < 6; m++) sh[m][threadIdx.x] += sh[m][threadIdx.x + o];
-        __syncthreads();
-    }
-    if (threadIdx.x < 6) yc[6 * a + threadIdx.x] = sh[threadIdx.x][0];
+        for (int m = 0; m < 6; m++) yc[6 * a + m] = acc[m];
 }
 template <typename VT>
 void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st) {
     if (c.nagg == 0) return;
-    k_coarse_restrict<VT, false><<<c.nagg, 512, 0, st>>>(c, nullptr, nullptr, nullptr, const_cast<VT*>(r), nullptr,
-                                                          nullptr, yc, nullptr);
+    k_coarse_restrict<VT, false><<<c.nagg, kAggThreads, 0, st>>>(c, nullptr, nullptr, nullptr, const_cast<VT*>(r),
+                                                                  nullptr, nullptr, yc, nullptr);
     counted();
 }
 template <typename VT>
 void launch_tl_update_restrict(const CoarseArgs& c, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag,
                                const double4* pn, double* yc, DevScalars* sc, cudaStream_t st) {
-    k_coarse_restrict<VT, true><<<c.nagg, 512, 0, st>>>(c, p, qv, x, r, pflag, pn, yc, sc);
+    k_coarse_restrict<VT, true><<<c.nagg, kAggThreads, 0, st>>>(c, p, qv, x, r, pflag, pn, yc, sc);
     counted();
 }
 
-// zc = Ainv yc: one 128-thread block per row.
+// 16-byte loads of the coarse inverse: 4 floats or 2 doubles
 template <typename VT>
-__global__ void __launch_bounds__(128) k_coarse_matvec(int nc, const VT* __restrict__ A,
-                                                        const double* __restrict__ yc, VT* __restrict__ zc) {
-    __shared__ double sh[4];
-    const int row = blockIdx.x;
-    double acc[1] = {0.0};
-    const VT* a = A + (size_t)row * nc;
-    for (int j = threadIdx.x; j < nc; j += blockDim.x) acc[0] += (double)__ldg(a + j) * yc[j];
-    warp_sum<1>(acc);
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc[0];
-    __syncthreads();
-    if (threadIdx.x == 0) zc[row] = (VT)(sh[0] + sh[1] + sh[2] + sh[3]);
-}
-template <typename VT>
-void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st) {
-    if (nc == 0) return;
-    k_coarse_matvec<VT><<<nc, 128, 0, st>>>(nc, Ainv, yc, zc);
-    counted();
+__device__ __forceinline__ void load16(const VT* p, VT (&v)[16 / sizeof(VT)]) {
+    if constexpr (sizeof(VT) == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p));
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else {
+        const double2 t = __ldg(reinterpret_cast<const double2*>(p));
+        v[0] = t.x; v[1] = t.y;
+    }
 }
 
-// z = Minv r + P zc with the dots r.z and r.r.  init = 1: first z of a solve
-// (sets rz, rr, bnorm-based tolerance was set by k_pcg_init and is kept);
-// init = 0: one CG iteration's end (beta, it, done as k_pcg_update).
+// z = Minv r + P zc, zc = Ainv yc, with the dots r.z and r.r.  One block per
+// aggregate: it forms its own six coarse values (rows 6a..6a+5 of Ainv, leading
+// dimension ld, zero padded, times yc) and prolongs them to its nodes, so the
+// coarse matvec needs no launch of its own and Ainv is read once in all.
+// init = 1: first z of a solve (sets rz); init = 0: one CG iteration's end
+// (beta, it, done as k_pcg_update).
 template <typename VT>
-__global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __restrict__ r,
-                                                       const VT* __restrict__ Minv, const VT* __restrict__ zc,
-                                                       VT* __restrict__ z, int init, const uint8_t* __restrict__ pflag,
-                                                       const double4* __restrict__ pn, double* partials,
-                                                       DevScalars* sc) {
+__global__ void __launch_bounds__(kAggThreads) k_tl_coarse_z(CoarseArgs c, int ld, const VT* __restrict__ Ainv,
+                                                             const double* __restrict__ yc, const VT* __restrict__ r,
+                                                             const VT* __restrict__ Minv, VT* __restrict__ z, int init,
+                                                             const uint8_t* __restrict__ pflag,
+                                                             const double4* __restrict__ pn, double* partials,
+                                                             DevScalars* sc) {
     if (!init && *(volatile int*)&sc->done) return;
+    __shared__ double sh[32][6];
+    constexpr int W = 16 / sizeof(VT);
+    const int a = blockIdx.x;
+    double zc[6] = {0, 0, 0, 0, 0, 0};
+    const VT* A = Ainv + (size_t)(6 * a) * ld;
+    for (int j = threadIdx.x * W; j < ld; j += blockDim.x * W) {
+        double y[W];
+#pragma unroll
+        for (int w = 0; w < W; w++) y[w] = yc[j + w];
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            VT v[W];
+            load16<VT>(A + (size_t)m * ld + j, v);
+#pragma unroll
+            for (int w = 0; w < W; w++) zc[m] += (double)v[w] * y[w];
+        }
+    }
+    block_sum<6>(zc, sh);
+    const VT t0 = (VT)zc[0], t1 = (VT)zc[1], t2 = (VT)zc[2];
+    const VT w0 = (VT)zc[3], w1 = (VT)zc[4], w2 = (VT)zc[5];
     double acc[2] = {0.0, 0.0};
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < c.N; i += gridDim.x * blockDim.x) {
+    for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
+        const int i = c.agg_nodes[k];
         VT rr[3], zz[3];
 #pragma unroll
-        for (int k = 0; k < 3; k++) rr[k] = r[3 * (size_t)i + k];
+        for (int d = 0; d < 3; d++) rr[d] = r[3 * (size_t)i + d];
         const VT* M = Minv + (size_t)i * 9;
 #pragma unroll
-        for (int k = 0; k < 3; k++) zz[k] = M[k * 3 + 0] * rr[0] + M[k * 3 + 1] * rr[1] + M[k * 3 + 2] * rr[2];
-        {
-            // P_i zc(a): translation + rotation x offset, held DOFs dropped
-            const int a = __ldg(c.aid + i);
-            const float4 o = c.off[i];
-            const VT t0 = zc[6 * a], t1 = zc[6 * a + 1], t2 = zc[6 * a + 2];
-            const VT w0 = zc[6 * a + 3], w1 = zc[6 * a + 4], w2 = zc[6 * a + 5];
-            const VT ox = (VT)o.x, oy = (VT)o.y, oz = (VT)o.z;
-            VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
-            if (c.fixed) {
-                const unsigned f = c.fixed[i];
-                if (f & 1u) add[0] = VT(0);
-                if (f & 2u) add[1] = VT(0);
-                if (f & 4u) add[2] = VT(0);
-            }
-#pragma unroll
-            for (int k = 0; k < 3; k++) zz[k] += add[k];
+        for (int d = 0; d < 3; d++) zz[d] = M[d * 3 + 0] * rr[0] + M[d * 3 + 1] * rr[1] + M[d * 3 + 2] * rr[2];
+        // P_i zc: translation + rotation x offset, held DOFs dropped
+        const float4 o = c.off[i];
+        const VT ox = (VT)o.x, oy = (VT)o.y, oz = (VT)o.z;
+        VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
+        if (c.fixed) {
+            const unsigned f = c.fixed[i];
+            if (f & 1u) add[0] = VT(0);
+            if (f & 2u) add[1] = VT(0);
+            if (f & 4u) add[2] = VT(0);
         }
+#pragma unroll
+        for (int d = 0; d < 3; d++) zz[d] += add[d];
         project3<VT>(pflag, pn, i, zz);
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-            z[3 * (size_t)i + k] = zz[k];
-            acc[0] += (double)rr[k] * (double)zz[k];
-            acc[1] += (double)rr[k] * (double)rr[k];
+        for (int d = 0; d < 3; d++) {
+            z[3 * (size_t)i + d] = zz[d];
+            acc[0] += (double)rr[d] * (double)zz[d];
+            acc[1] += (double)rr[d] * (double)rr[d];
         }
     }
     double tot[2];
@@ -1738,26 +1756,44 @@ __global__ void __launch_bounds__(kRedThreads) k_tl_z(CoarseArgs c, const VT* __
     }
 }
 template <typename VT>
-void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init,
-                 const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc, cudaStream_t st) {
-    k_tl_z<VT><<<red_grid(c.N, 2), kRedThreads, 0, st>>>(c, r, Minv, zc, z, init, pflag, pn, partials, sc);
+void launch_tl_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const VT* r, const VT* Minv,
+                        VT* z, int init, const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc,
+                        cudaStream_t st) {
+    if (c.nagg == 0) return;
+    k_tl_coarse_z<VT><<<c.nagg, kAggThreads, 0, st>>>(c, ld, Ainv, yc, r, Minv, z, init, pflag, pn, partials, sc);
     counted();
 }
 
-template void launch_to_vt<float>(long long, const double*, float*, cudaStream_t);
-template void launch_to_vt<double>(long long, const double*, double*, cudaStream_t);
+// out (nc rows, leading dimension ld >= nc, padding zero) = in (nc x nc), symmetrised
+template <typename VT>
+__global__ void k_to_vt_pad(int nc, int ld, const double* __restrict__ in, VT* __restrict__ out) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)nc * ld) return;
+    const int i = (int)(t / ld), j = (int)(t - (long long)i * ld);
+    out[t] = j < nc ? (VT)(0.5 * (in[(size_t)i * nc + j] + in[(size_t)j * nc + i])) : VT(0);
+}
+template <typename VT>
+void launch_to_vt_pad(int nc, int ld, const double* in, VT* out, cudaStream_t st) {
+    if (nc == 0) return;
+    const long long n = (long long)nc * ld;
+    k_to_vt_pad<VT><<<(int)((n + 255) / 256), 256, 0, st>>>(nc, ld, in, out);
+    counted();
+}
+
+template void launch_to_vt_pad<float>(int, int, const double*, float*, cudaStream_t);
+template void launch_to_vt_pad<double>(int, int, const double*, double*, cudaStream_t);
 template void launch_tl_update_restrict<float>(const CoarseArgs&, const float*, const float*, float*, float*,
                                                const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_tl_update_restrict<double>(const CoarseArgs&, const double*, const double*, double*, double*,
                                                 const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_coarse_restrict<float>(const CoarseArgs&, const float*, double*, cudaStream_t);
 template void launch_coarse_restrict<double>(const CoarseArgs&, const double*, double*, cudaStream_t);
-template void launch_coarse_matvec<float>(int, const float*, const double*, float*, cudaStream_t);
-template void launch_coarse_matvec<double>(int, const double*, const double*, double*, cudaStream_t);
-template void launch_tl_z<float>(const CoarseArgs&, const float*, const float*, const float*, float*, int,
-                                 const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
-template void launch_tl_z<double>(const CoarseArgs&, const double*, const double*, const double*, double*, int,
-                                  const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
+template void launch_tl_coarse_z<float>(const CoarseArgs&, int, const float*, const double*, const float*,
+                                        const float*, float*, int, const uint8_t*, const double4*, double*,
+                                        DevScalars*, cudaStream_t);
+template void launch_tl_coarse_z<double>(const CoarseArgs&, int, const double*, const double*, const double*,
+                                         const double*, double*, int, const uint8_t*, const double4*, double*,
+                                         DevScalars*, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // explicit instantiations

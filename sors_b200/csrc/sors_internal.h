@@ -124,19 +124,18 @@ void launch_coarse_galerkin_d(int npairs, const int* cpair_ptr, const int2* cpai
                               cudaStream_t st);
 void launch_coarse_invert(int nc, double* Ac, double* rowk, double* colk, cudaStream_t st);
 template <typename VT>
-void launch_to_vt(long long n, const double* in, VT* out, cudaStream_t st);
+void launch_to_vt_pad(int nc, int ld, const double* in, VT* out, cudaStream_t st);
 template <typename VT>
 void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaStream_t st);
 template <typename VT>
 void launch_tl_update_restrict(const CoarseArgs& c, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag,
                                const double4* pn, double* yc, DevScalars* sc, cudaStream_t st);
 template <typename VT>
-void launch_coarse_matvec(int nc, const VT* Ainv, const double* yc, VT* zc, cudaStream_t st);
-template <typename VT>
-void launch_tl_z(const CoarseArgs& c, const VT* r, const VT* Minv, const VT* zc, VT* z, int init,
-                 const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc, cudaStream_t st);
+void launch_tl_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const VT* r, const VT* Minv,
+                        VT* z, int init, const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc,
+                        cudaStream_t st);
 
-// Sets the message returned by sors_last_error on this thread (capi.cu).// Sets the message returned by sors_last_error on this thread (capi.cu).
+// Sets the message returned by sors_last_error on this thread (capi.cu).
 void set_last_error(const std::string& msg);
 
 // Launchers (kernels.cu)
