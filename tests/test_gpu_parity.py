@@ -288,3 +288,53 @@ def test_c3_chamber_pressure_static(c3_reference, precision):
     assert np.abs(u).max() > 1e-5
     tol = 1e-8 if precision == "fp64" else 1e-6 * np.abs(u).max()
     assert np.abs(q - qo).max() < tol, np.abs(q - qo).max()
+
+
+def _fan_ball(r=0.01):
+    """Tets fanned from a centre vertex to a once-subdivided icosahedron (42
+    surface vertices, 80 tets): the centre's block-row has 43 blocks, more
+    than the widest SpMV lane group (32 lanes), which then loops over the row."""
+    t = (1 + 5 ** 0.5) / 2
+    V = [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t], [0, 1, -t],
+         [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]]
+    F = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+         [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5], [2, 4, 11],
+         [6, 2, 10], [8, 6, 7], [9, 8, 1]]
+    V = [list(np.asarray(v, float) / np.linalg.norm(v)) for v in V]
+    mid = {}
+
+    def m(a, b):
+        k = (min(a, b), max(a, b))
+        if k not in mid:
+            v = np.asarray(V[a]) + np.asarray(V[b])
+            V.append(list(v / np.linalg.norm(v)))
+            mid[k] = len(V) - 1
+        return mid[k]
+    F2 = []
+    for a, b, c in F:
+        ab, bc, ca = m(a, b), m(b, c), m(c, a)
+        F2 += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+    X = np.vstack([np.asarray(V) * r, [[0.0, 0.0, 0.0]]])
+    c = X.shape[0] - 1
+    T = []
+    for a, b, d in F2:
+        # positive orientation, the centre as vertex 3
+        v = np.dot(np.cross(X[b] - X[a], X[d] - X[a]), X[c] - X[a])
+        T.append([a, b, d, c] if v > 0 else [a, d, b, c])
+    return X, np.asarray(T, np.int32)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_long_block_rows(oracle, precision):
+    # a block-row longer than 32 blocks (several blocks per SpMV lane, and a
+    # long assembly row); the trajectory still matches the oracle
+    X, T = _fan_ball()
+    en, sol, o, _ = make_pair(X, T, E=5e4, nu=0.4, dt=2e-3, precision=precision)
+    q = X.ravel().copy(); qo = q.copy()
+    for _ in range(8):
+        q = sol.step(q, en)
+        qo, st = o.step(qo)
+        assert st == 0
+    disp = np.abs(qo - X.ravel()).max()
+    assert disp > 1e-6
+    assert np.abs(q - qo).max() < (1e-9 if precision == "fp64" else 1e-6 * disp)
