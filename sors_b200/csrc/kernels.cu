@@ -1686,11 +1686,14 @@ __device__ __forceinline__ void load16(const VT* p, VT (&v)[16 / sizeof(VT)]) {
 // z = Minv r + P zc, zc = Ainv yc, with the dots r.z and r.r.  One block per
 // aggregate: it forms its own six coarse values (rows 6a..6a+5 of Ainv, leading
 // dimension ld, zero padded, times yc) and prolongs them to its nodes, so the
-// coarse matvec needs no launch of its own and Ainv is read once in all.
+// coarse matvec needs no launch of its own and Ainv is read once in all.  Each
+// thread loads two nodes before using either (8 % faster than one at a time;
+// four, at 108 registers, was slower), held to 64 registers so that 4 blocks
+// fit an SM and every aggregate block is resident at once.
 // init = 1: first z of a solve (sets rz); init = 0: one CG iteration's end
 // (beta, it, done as k_pcg_update).
 template <typename VT>
-__global__ void __launch_bounds__(kAggThreads) k_tl_coarse_z(CoarseArgs c, int ld, const VT* __restrict__ Ainv,
+__global__ void __launch_bounds__(kAggThreads, 4) k_tl_coarse_z(CoarseArgs c, int ld, const VT* __restrict__ Ainv,
                                                              const double* __restrict__ yc, const VT* __restrict__ r,
                                                              const VT* __restrict__ Minv, VT* __restrict__ z, int init,
                                                              const uint8_t* __restrict__ pflag,
@@ -1718,32 +1721,52 @@ __global__ void __launch_bounds__(kAggThreads) k_tl_coarse_z(CoarseArgs c, int l
     const VT t0 = (VT)zc[0], t1 = (VT)zc[1], t2 = (VT)zc[2];
     const VT w0 = (VT)zc[3], w1 = (VT)zc[4], w2 = (VT)zc[5];
     double acc[2] = {0.0, 0.0};
-    for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
-        const int i = c.agg_nodes[k];
-        VT rr[3], zz[3];
+    constexpr int U = 2;  // nodes per thread in flight
+    const int k0 = c.agg_ptr[a], k1 = c.agg_ptr[a + 1];
+    for (int kb = k0 + threadIdx.x; kb < k1; kb += U * blockDim.x) {
+        int id[U];
 #pragma unroll
-        for (int d = 0; d < 3; d++) rr[d] = r[3 * (size_t)i + d];
-        const VT* M = Minv + (size_t)i * 9;
+        for (int u = 0; u < U; u++) {
+            const int k = kb + u * blockDim.x;
+            id[u] = k < k1 ? __ldg(c.agg_nodes + k) : -1;
+        }
+        VT rv[U][3], Mv[U][9];
+        float4 o[U];
+        unsigned f[U];
 #pragma unroll
-        for (int d = 0; d < 3; d++) zz[d] = M[d * 3 + 0] * rr[0] + M[d * 3 + 1] * rr[1] + M[d * 3 + 2] * rr[2];
-        // P_i zc: translation + rotation x offset, held DOFs dropped
-        const float4 o = c.off[i];
-        const VT ox = (VT)o.x, oy = (VT)o.y, oz = (VT)o.z;
-        VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
-        if (c.fixed) {
-            const unsigned f = c.fixed[i];
-            if (f & 1u) add[0] = VT(0);
-            if (f & 2u) add[1] = VT(0);
-            if (f & 4u) add[2] = VT(0);
+        for (int u = 0; u < U; u++) {
+            if (id[u] < 0) continue;
+            const size_t b = 3 * (size_t)id[u];
+#pragma unroll
+            for (int d = 0; d < 3; d++) rv[u][d] = r[b + d];
+#pragma unroll
+            for (int e = 0; e < 9; e++) Mv[u][e] = __ldg(Minv + 9 * (size_t)id[u] + e);
+            o[u] = __ldg(c.off + id[u]);
+            f[u] = c.fixed ? (unsigned)__ldg(c.fixed + id[u]) : 0u;
         }
 #pragma unroll
-        for (int d = 0; d < 3; d++) zz[d] += add[d];
-        project3<VT>(pflag, pn, i, zz);
+        for (int u = 0; u < U; u++) {
+            if (id[u] < 0) continue;
+            const int i = id[u];
+            VT zz[3];
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            z[3 * (size_t)i + d] = zz[d];
-            acc[0] += (double)rr[d] * (double)zz[d];
-            acc[1] += (double)rr[d] * (double)rr[d];
+            for (int d = 0; d < 3; d++)
+                zz[d] = Mv[u][d * 3 + 0] * rv[u][0] + Mv[u][d * 3 + 1] * rv[u][1] + Mv[u][d * 3 + 2] * rv[u][2];
+            // P_i zc: translation + rotation x offset, held DOFs dropped
+            const VT ox = (VT)o[u].x, oy = (VT)o[u].y, oz = (VT)o[u].z;
+            VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
+            if (f[u] & 1u) add[0] = VT(0);
+            if (f[u] & 2u) add[1] = VT(0);
+            if (f[u] & 4u) add[2] = VT(0);
+#pragma unroll
+            for (int d = 0; d < 3; d++) zz[d] += add[d];
+            project3<VT>(pflag, pn, i, zz);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                z[3 * (size_t)i + d] = zz[d];
+                acc[0] += (double)rv[u][d] * (double)zz[d];
+                acc[1] += (double)rv[u][d] * (double)rv[u][d];
+            }
         }
     }
     double tot[2];
