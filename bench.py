@@ -276,7 +276,7 @@ def run_gpu(args, rank, world, local_rank):
     it_kernels = {"tl_restrict": (prof.tl_restrict_ms, prof.tl_restrict_bytes),
                   "tl_coarse_z": (prof.tl_coarse_z_ms, prof.tl_coarse_z_bytes)} if two_level else \
         {"pcg_update": (prof.pcg_update_ms, prof.pcg_update_bytes)}
-    kern = {"pcg_spmv": (prof.spmv_ms, prof.spmv_bytes), **it_kernels,
+    kern = {"form_p": (prof.form_p_ms, prof.form_p_bytes), "pcg_spmv": (prof.spmv_ms, prof.spmv_bytes), **it_kernels,
             "assemble": (prof.assemble_ms, prof.assemble_bytes)}
     per_step = {k: (newton if k == "assemble" else pcg) / args.steps * v[0] for k, v in kern.items()}
     dom = max(per_step, key=per_step.get)

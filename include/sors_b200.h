@@ -269,6 +269,8 @@ typedef struct SorsKernelProfile {
      * the x / r update fused with the restriction, and the coarse solve fused
      * with the prolongation and z = Minv r */
     double tl_restrict_ms, tl_coarse_z_ms, tl_restrict_bytes, tl_coarse_z_bytes;
+    /* p = z + beta p_old, formed before the SpMV (padded, 4 values per node) */
+    double form_p_ms, form_p_bytes;
 } SorsKernelProfile;
 int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
 

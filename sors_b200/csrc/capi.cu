@@ -172,6 +172,7 @@ struct SorsHandle {
 
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
+    long long pcg_graph_kernels = 0;  // kernel nodes of the captured chunk
     bool graph_failed = false;
 
     double prev_gnorm = -1.0;
@@ -461,8 +462,9 @@ void pcg_iter_pair(SorsHandle* h) {
         for (int half = 0; half < 2; half++) {
             VT* pin = (VT*)(half ? h->p1 : h->p0);
             VT* pout = (VT*)(half ? h->p0 : h->p1);
-            launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, pin,
-                                    pout, (VT*)h->qv, h->partials, h->sc, h->stream);
+            launch_form_p<VT>(h->N, z, pin, pout, h->sc, h->stream);
+            launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, pout,
+                                    (VT*)h->qv, h->partials, h->sc, h->stream);
             launch_tl_update_restrict<VT>(h->cargs, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag,
                                           h->proj_n, h->tl_yc, h->sc, h->stream);
             launch_tl_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->r,
@@ -470,12 +472,14 @@ void pcg_iter_pair(SorsHandle* h) {
         }
         return;
     }
-    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, (VT*)h->p0, (VT*)h->p1, (VT*)h->qv,
-                            h->partials, h->sc, h->stream);
+    launch_form_p<VT>(h->N, z, (VT*)h->p0, (VT*)h->p1, h->sc, h->stream);
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, (VT*)h->p1,
+                            (VT*)h->qv, h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p1, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
                           h->proj_n, h->partials, h->sc, h->stream);
-    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, z, (VT*)h->p1, (VT*)h->p0, (VT*)h->qv,
-                            h->partials, h->sc, h->stream);
+    launch_form_p<VT>(h->N, z, (VT*)h->p1, (VT*)h->p0, h->sc, h->stream);
+    launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, (VT*)h->p0,
+                            (VT*)h->qv, h->partials, h->sc, h->stream);
     launch_pcg_update<VT>(h->N, (VT*)h->p0, (VT*)h->qv, (VT*)h->Minv, (VT*)h->x, (VT*)h->r, z, h->proj_flag,
                           h->proj_n, h->partials, h->sc, h->stream);
 }
@@ -497,6 +501,7 @@ int pcg_chunk(SorsHandle* h) {
             for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
             e = cudaStreamEndCapture(h->stream, &graph);
         }
+        h->pcg_graph_kernels = g_kernel_launches.load() - launches_before;
         g_kernel_launches.store(launches_before);  // captured launches run when the graph runs
         if (e == cudaSuccess) e = cudaGraphInstantiate(&h->pcg_exec, graph, 0);
         if (graph) cudaGraphDestroy(graph);
@@ -508,7 +513,7 @@ int pcg_chunk(SorsHandle* h) {
     }
     if (h->pcg_exec) {
         CK(cudaGraphLaunch(h->pcg_exec, h->stream));
-        g_kernel_launches.fetch_add(2 * kPcgChunk);
+        g_kernel_launches.fetch_add(h->pcg_graph_kernels);
     } else {
         for (int k = 0; k < kPcgChunk / 2; k++) pcg_iter_pair<HT, VT>(h);
         CK(cudaGetLastError());
@@ -1641,8 +1646,10 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if ((st = dalloc(h, &h->Minv, (size_t)N * 9 * hs))) return bail(st);
     void** vv[] = {&h->x, &h->r, &h->z, &h->p0, &h->p1, &h->qv};
     for (void** p : vv) {
-        if ((st = dalloc(h, p, nd * hs))) return bail(st);
-        CK(dzero(h, *p, nd * hs));
+        // the search directions p0, p1 are padded to 4 values per node
+        const size_t bytes = (p == &h->p0 || p == &h->p1) ? (size_t)N * 4 * hs : nd * hs;
+        if ((st = dalloc(h, p, bytes))) return bail(st);
+        CK(dzero(h, *p, bytes));
     }
     if ((st = dalloc_t(h, &h->partials, (size_t)kRedBlocks * kMaxScalars))) return bail(st);
     if ((st = dalloc_t(h, &h->sc, 1))) return bail(st);
@@ -2167,14 +2174,25 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
-        launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0),
-                                (VT*)(i & 1 ? h->p0 : h->p1), (VT*)h->qv, h->partials, h->sc, h->stream);
+        launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, (VT*)h->p1,
+                                (VT*)h->qv, h->partials, h->sc, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&ms, a, b));
     out->spmv_ms = ms / iters;
-    // values + block columns + row pointers + z and p_old (read) + p_new and q (written)
-    out->spmv_bytes = nnzb * 9 * hs + nnzb * 4 + (N + 1) * 4 + 2 * 3 * N * vs + 2 * 3 * N * vs;
+    // values + block columns + row pointers + p (padded, read) + q (written)
+    out->spmv_bytes = nnzb * 9 * hs + nnzb * 4 + (N + 1) * 4 + 4 * N * vs + 3 * N * vs;
+    CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
+    CK(cudaEventRecord(a, h->stream));
+    for (int i = 0; i < iters; i++)
+        launch_form_p<VT>(h->N, (VT*)h->z, (VT*)(i & 1 ? h->p1 : h->p0), (VT*)(i & 1 ? h->p0 : h->p1), h->sc,
+                          h->stream);
+    CK(cudaEventRecord(b, h->stream));
+    CK(cudaEventSynchronize(b));
+    CK(cudaEventElapsedTime(&ms, a, b));
+    out->form_p_ms = ms / iters;
+    // z and p_old read, p_new written (padded)
+    out->form_p_bytes = 3 * N * vs + 8 * N * vs;
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)

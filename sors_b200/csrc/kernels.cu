@@ -1030,8 +1030,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_init(int N, const double* g
         for (int k = 0; k < 3; k++) {
             rr[k] = (VT)(-g[3 * (size_t)i + k]);
             x[3 * (size_t)i + k] = VT(0);
-            p0[3 * (size_t)i + k] = VT(0);
+            p0[4 * (size_t)i + k] = VT(0);
         }
+        p0[4 * (size_t)i + 3] = VT(0);
         project3<VT>(pflag, pn, i, rr);
         for (int k = 0; k < 3; k++) r[3 * (size_t)i + k] = rr[k];
         const VT* M = Minv + (size_t)i * 9;
@@ -1078,19 +1079,59 @@ __device__ __forceinline__ void load_block(const HT* __restrict__ H, size_t b, s
     for (int k = 0; k < 9; k++) h[k] = (VT)__ldg(v + k);
 }
 
-// q = A p_new with p_new = z + beta p_old built on the fly; dot p_new.q.
-// A group of LPR lanes owns one block-row: lane b of the group takes block b
-// of the row, loads its column and 9 values and gathers p_new(col) at once,
-// so a row costs one dependent load chain; groups are reduced with shuffles.
-template <typename HT, typename VT, int LPR>
-__global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __restrict__ row_ptr,
-                                                           const int* __restrict__ col, const HT* __restrict__ H,
-                                                           long long nnzb,
-                                                           const VT* __restrict__ z, const VT* __restrict__ p_old,
-                                                           VT* __restrict__ p_new, VT* __restrict__ qv,
-                                                           double* partials, DevScalars* sc) {
-    if (*(volatile int*)&sc->done) return;
+// The search direction p is stored padded, four values per node (the fourth
+// zero), so that a gather of p at a column is one 16-byte load (two for doubles).
+template <typename VT>
+__device__ __forceinline__ void ld_p4(const VT* __restrict__ p4, size_t i, VT& a, VT& b, VT& c) {
+    if constexpr (sizeof(VT) == 4) {
+        const float4 t = __ldg(reinterpret_cast<const float4*>(p4) + i);
+        a = t.x; b = t.y; c = t.z;
+    } else {
+        const double2* d = reinterpret_cast<const double2*>(p4) + 2 * i;
+        const double2 t0 = __ldg(d), t1 = __ldg(d + 1);
+        a = t0.x; b = t0.y; c = t1.x;
+    }
+}
+
+// p_new = z + beta p_old (padded layout), before the SpMV gathers it.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_form_p(int N, const VT* __restrict__ z, const VT* __restrict__ p_old,
+                                                         VT* __restrict__ p_new, const DevScalars* sc) {
+    if (*(volatile const int*)&sc->done) return;
     const VT beta = (VT)sc->beta;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT a, b, c;
+        ld_p4<VT>(p_old, i, a, b, c);
+        const size_t k = 3 * (size_t)i;
+        a = z[k] + beta * a;
+        b = z[k + 1] + beta * b;
+        c = z[k + 2] + beta * c;
+        if constexpr (sizeof(VT) == 4) {
+            reinterpret_cast<float4*>(p_new)[i] = make_float4(a, b, c, 0.0f);
+        } else {
+            double2* d = reinterpret_cast<double2*>(p_new) + 2 * i;
+            d[0] = make_double2(a, b);
+            d[1] = make_double2(c, 0.0);
+        }
+    }
+}
+template <typename VT>
+void launch_form_p(int N, const VT* z, const VT* p_old, VT* p_new, const DevScalars* sc, cudaStream_t st) {
+    k_form_p<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, z, p_old, p_new, sc);
+    counted();
+}
+
+// q = A p with the dot p.q (p formed by k_form_p, padded layout).
+// A group of LPR lanes owns one block-row: lane b of the group takes block b
+// of the row, loads its column and 9 values and gathers p(col) with one
+// 16-byte load, so a row costs one dependent load chain; groups are reduced
+// with shuffles.
+template <typename HT, typename VT, int LPR>
+__global__ void __launch_bounds__(kRedThreads, sizeof(HT) == 4 ? 8 : 6) k_pcg_spmv(int N, const int* __restrict__ row_ptr,
+                                                           const int* __restrict__ col, const HT* __restrict__ H,
+                                                           long long nnzb, const VT* __restrict__ p4,
+                                                           VT* __restrict__ qv, double* partials, DevScalars* sc) {
+    if (*(volatile int*)&sc->done) return;
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPR, sl = lane % LPR;
     constexpr int RPW = 32 / LPR;
@@ -1106,15 +1147,11 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
                 const int j = __ldg(col + b0 + s);
                 VT hb[9];
                 load_block<HT, VT>(H, (size_t)(b0 + s), (size_t)nnzb, hb);
-                const VT h0 = hb[0], h1 = hb[1], h2 = hb[2], h3 = hb[3], h4 = hb[4], h5 = hb[5];
-                const VT h6 = hb[6], h7 = hb[7], h8 = hb[8];
-                const size_t jj = 3 * (size_t)j;
-                const VT p0 = __ldg(z + jj) + beta * __ldg(p_old + jj);
-                const VT p1 = __ldg(z + jj + 1) + beta * __ldg(p_old + jj + 1);
-                const VT p2 = __ldg(z + jj + 2) + beta * __ldg(p_old + jj + 2);
-                a0 += h0 * p0 + h1 * p1 + h2 * p2;
-                a1 += h3 * p0 + h4 * p1 + h5 * p2;
-                a2 += h6 * p0 + h7 * p1 + h8 * p2;
+                VT p0, p1, p2;
+                ld_p4<VT>(p4, (size_t)j, p0, p1, p2);
+                a0 += hb[0] * p0 + hb[1] * p1 + hb[2] * p2;
+                a1 += hb[3] * p0 + hb[4] * p1 + hb[5] * p2;
+                a2 += hb[6] * p0 + hb[7] * p1 + hb[8] * p2;
             }
         }
 #pragma unroll
@@ -1124,12 +1161,9 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
             a2 += __shfl_xor_sync(0xffffffffu, a2, o);
         }
         if (row < N && sl < 3) {
-            const size_t ii = 3 * (size_t)row + sl;
             const VT qi = sl == 0 ? a0 : (sl == 1 ? a1 : a2);
-            const VT pi = z[ii] + beta * p_old[ii];
-            p_new[ii] = pi;
-            qv[ii] = qi;
-            acc[0] += (double)pi * (double)qi;
+            qv[3 * (size_t)row + sl] = qi;
+            acc[0] += (double)p4[4 * (size_t)row + sl] * (double)qi;
         }
     }
     double tot[1];
@@ -1147,8 +1181,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_spmv(int N, const int* __re
 
 template <typename HT, typename VT>
 void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
-                     const VT* z, const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc,
-                     cudaStream_t st) {
+                     const VT* p4, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
     const int lpr = max_row_blocks <= 4 ? 4 : (max_row_blocks <= 8 ? 8 : (max_row_blocks <= 16 ? 16 : 32));
     const int rows_per_block = (kRedThreads / 32) * (32 / lpr);
     long long blocks = (N + rows_per_block - 1) / rows_per_block;
@@ -1156,10 +1189,10 @@ void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* c
     if (blocks < 1) blocks = 1;
     blocks = cap_grid(blocks);
     switch (lpr) {
-        case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
-        case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
-        case 16: k_pcg_spmv<HT, VT, 16><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
-        default: k_pcg_spmv<HT, VT, 32><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, z, p_old, p_new, qv, partials, sc); break;
+        case 4: k_pcg_spmv<HT, VT, 4><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
+        case 8: k_pcg_spmv<HT, VT, 8><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
+        case 16: k_pcg_spmv<HT, VT, 16><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
+        default: k_pcg_spmv<HT, VT, 32><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
     }
     counted();
 }
@@ -1179,7 +1212,7 @@ __global__ void __launch_bounds__(kRedThreads) k_pcg_update(int N, const VT* __r
 #pragma unroll
         for (int k = 0; k < 3; k++) {
             const size_t ii = 3 * (size_t)i + k;
-            x[ii] += alpha * p[ii];
+            x[ii] += alpha * p[4 * (size_t)i + k];
             qq[k] = qv[ii];
         }
         project3<VT>(pflag, pn, i, qq);
@@ -1632,7 +1665,7 @@ __global__ void __launch_bounds__(kAggThreads) k_coarse_restrict(CoarseArgs c, c
 #pragma unroll
             for (int d = 0; d < 3; d++) {
                 const size_t ii = 3 * (size_t)i + d;
-                x[ii] += alpha * p[ii];
+                x[ii] += alpha * p[4 * (size_t)i + d];
                 qq[d] = qv[ii];
             }
             project3<VT>(pflag, pn, i, qq);
@@ -1848,10 +1881,11 @@ template void launch_pcg_init<float, float>(int, const double*, const float*, fl
                                             double, int, const uint8_t*, const double4*, double*, DevScalars*,
                                             cudaStream_t);
 template void launch_pcg_spmv<double, double>(int, int, const int*, const int*, const double*, long long,
-                                              const double*, const double*, double*, double*, double*, DevScalars*,
-                                              cudaStream_t);
+                                              const double*, double*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_spmv<float, float>(int, int, const int*, const int*, const float*, long long, const float*,
-                                            const float*, float*, float*, double*, DevScalars*, cudaStream_t);
+                                            float*, double*, DevScalars*, cudaStream_t);
+template void launch_form_p<double>(int, const double*, const double*, double*, const DevScalars*, cudaStream_t);
+template void launch_form_p<float>(int, const float*, const float*, float*, const DevScalars*, cudaStream_t);
 template void launch_pcg_update<double>(int, const double*, const double*, const double*, double*, double*, double*,
                                         const uint8_t*, const double4*, double*, DevScalars*, cudaStream_t);
 template void launch_pcg_update<float>(int, const float*, const float*, const float*, float*, float*, float*,

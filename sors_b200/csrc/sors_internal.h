@@ -171,8 +171,9 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
                      DevScalars* sc, cudaStream_t st);
 template <typename HT, typename VT>
 void launch_pcg_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
-                     const VT* z, const VT* p_old, VT* p_new, VT* qv, double* partials, DevScalars* sc,
-                     cudaStream_t st);
+                     const VT* p4, VT* qv, double* partials, DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_form_p(int N, const VT* z, const VT* p_old, VT* p_new, const DevScalars* sc, cudaStream_t st);
 template <typename VT>
 void launch_pcg_update(int N, const VT* p, const VT* qv, const VT* Minv, VT* x, VT* r, VT* z, const uint8_t* pflag,
                        const double4* pn, double* partials, DevScalars* sc, cudaStream_t st);
