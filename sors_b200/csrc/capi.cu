@@ -368,7 +368,13 @@ int build_pattern(SorsHandle* h, const int32_t* conn) {
     if ((st = upload(h, &h->pair_ptr, pair_ptr.data(), pair_ptr.size()))) return st;
     if ((st = upload(h, &h->pair_ev, pair_ev.data(), pair_ev.size()))) return st;
     if ((st = upload(h, &h->row_ptr, row_ptr.data(), row_ptr.size()))) return st;
-    if ((st = upload(h, &h->col, cols_all.data(), cols_all.size()))) return st;
+    {
+        // 4 ints of zero padding: the SpMV reads column indices 4 at a time
+        // from 16-byte aligned groups, the last of which may run past nnzb
+        std::vector<int> col_pad(cols_all.size() + 4, 0);
+        std::copy(cols_all.begin(), cols_all.end(), col_pad.begin());
+        if ((st = upload(h, &h->col, col_pad.data(), col_pad.size()))) return st;
+    }
     if ((st = upload(h, &h->diag_slot, diag.data(), diag.size()))) return st;
     if ((st = upload(h, &h->slot_item_ptr, slot_cnt.data(), slot_cnt.size()))) return st;
     if ((st = upload(h, &h->slot_items, items.data(), items.size()))) return st;
@@ -1642,7 +1648,10 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if (h->s.two_level == 2) h->s.two_level = N >= 20000 ? 1 : 0;
     if (h->s.two_level && (st = setup_two_level(h, X))) return bail(st);
     size_t hs = hsize(h);
-    if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs + 64))) return bail(st);
+    // 160 bytes of padding: the SpMV reads values in 144-byte groups, the last of
+    // which may run past the last block
+    if ((st = dalloc(h, &h->H, (size_t)h->nnzb * 9 * hs + 160))) return bail(st);
+    CK(dzero(h, (char*)h->H + (size_t)h->nnzb * 9 * hs, 160));
     if ((st = dalloc(h, &h->Minv, (size_t)N * 9 * hs))) return bail(st);
     void** vv[] = {&h->x, &h->r, &h->z, &h->p0, &h->p1, &h->qv};
     for (void** p : vv) {
