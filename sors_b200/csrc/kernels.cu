@@ -1784,10 +1784,12 @@ __device__ __forceinline__ void load16(const VT* p, VT (&v)[16 / sizeof(VT)]) {
 // z = Minv r + P zc, zc = Ainv yc, with the dots r.z and r.r.  One block per
 // aggregate: it forms its own six coarse values (rows 6a..6a+5 of Ainv, leading
 // dimension ld, zero padded, times yc) and prolongs them to its nodes, so the
-// coarse matvec needs no launch of its own and Ainv is read once in all.  Each
-// thread loads two nodes before using either (8 % faster than one at a time;
-// four, at 108 registers, was slower), held to 64 registers so that 4 blocks
-// fit an SM and every aggregate block is resident at once.
+// coarse matvec needs no launch of its own and Ainv is read once in all.  In
+// FP32 each thread loads two nodes before using either (8 % faster than one at
+// a time; four, at 108 registers, was slower); FP64 takes one (two spill).
+// Held to 64 registers so that 4 blocks fit an SM and every aggregate block
+// is resident at once.  (Storing Ainv in FP16 with a symmetric diagonal
+// scaling halved its bytes but measured slower, 18.9 -> 21.8 us.)
 // init = 1: first z of a solve (sets rz); init = 0: one CG iteration's end
 // (beta, it, done as k_pcg_update).
 template <typename VT>
@@ -1819,7 +1821,7 @@ __global__ void __launch_bounds__(kAggThreads, 4) k_tl_coarse_z(CoarseArgs c, in
     const VT t0 = (VT)zc[0], t1 = (VT)zc[1], t2 = (VT)zc[2];
     const VT w0 = (VT)zc[3], w1 = (VT)zc[4], w2 = (VT)zc[5];
     double acc[2] = {0.0, 0.0};
-    constexpr int U = 2;  // nodes per thread in flight
+    constexpr int U = sizeof(VT) == 4 ? 2 : 1;  // nodes per thread in flight
     const int k0 = c.agg_ptr[a], k1 = c.agg_ptr[a + 1];
     for (int kb = k0 + threadIdx.x; kb < k1; kb += U * blockDim.x) {
         int id[U];
