@@ -634,7 +634,7 @@ def main():
     ap.add_argument("--rollout-steps", type=int, default=20)
     ap.add_argument("--rate", type=float, default=20.0, help="serve: Poisson arrival rate (rollouts/s)")
     ap.add_argument("--slots", type=int, default=8, help="serve: concurrent handles")
-    ap.add_argument("--batch", type=int, default=8, help="serve: rollouts packed into one union handle")
+    ap.add_argument("--batch", type=int, default=1, help="serve: rollouts packed into one union handle (1: none; unions measured slower on the poke mix)")
     ap.add_argument("--baseline-sample", type=int, default=0,
                     help="serve: measure the sequential FP64 baseline on the first K requests (0 = all)")
     ap.add_argument("--seeds", type=int, default=4, help="c4: rollouts differentiated concurrently")
