@@ -559,11 +559,12 @@ __device__ __forceinline__ bool tet_row_stage(const AsmArgs<HT>& a, int e, int v
     return true;
 }
 
-// FP32 tet rows of the exact Neo-Hookean Hessian: 3 blocks per SM (80
+// Tet rows of the exact Neo-Hookean Hessian: FP32 at 3 blocks per SM (80
 // registers, a few hundred bytes of spills) measured 18 % faster than 2 blocks
-// at 128 registers; the projected and stable variants spill more and keep 2.
+// at 128 registers, and FP64 fits 2 blocks (128 registers, no spills; 156
+// unbounded); the projected and stable variants spill more and keep 2 / 1.
 template <typename HT, int NV, bool SNH, bool PROJ>
-__global__ void __launch_bounds__(256, (sizeof(HT) == 4 && NV == 4) ? ((SNH || PROJ) ? 2 : 3) : 1)
+__global__ void __launch_bounds__(256, NV == 4 ? (sizeof(HT) == 4 ? ((SNH || PROJ) ? 2 : 3) : ((SNH || PROJ) ? 1 : 2)) : 1)
     k_assemble(AsmArgs<HT> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int lane = threadIdx.x & 31;
