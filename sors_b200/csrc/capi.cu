@@ -703,8 +703,12 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     for (int it = 0; it < h->s.newton_max_iter; it++) {
         bool want_hess = (m != 2) || !have_hess;  // frozen Hessian: assemble once
         if (want_hess) h->proj_fallback = (m == 2);  // adaptive: the frozen Hessian is the projected one
-        if ((st = eval_system<HT>(h, dt, want_hess))) return st;
-        if (want_hess) have_hess = true;
+        // When the inexact-Newton bound eta |g| of the last solve predicts a
+        // residual below res_tol, evaluate the gradient alone first: the
+        // Hessian is assembled only if that iteration does not stop.
+        const bool probe = want_hess && res_tol > 0.0 && prev_g > 0.0 && prev_eta * prev_g <= res_tol;
+        if ((st = eval_system<HT>(h, dt, want_hess && !probe))) return st;
+        if (want_hess && !probe) have_hess = true;
         CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         if (h->sc_host->status & kFlagInverted)
@@ -713,6 +717,12 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         if (stats) { stats->newton_iters++; stats->residual_norm = gn; }
         if (!(gn == gn)) break;  // NaN gradient: diverged
         if (res_tol > 0.0 && gn < res_tol) { converged = true; break; }
+        if (probe) {
+            if ((st = eval_system<HT>(h, dt, true))) return st;
+            have_hess = true;
+            CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+            CK(cudaStreamSynchronize(h->stream));
+        }
         // forcing term: Eisenstat-Walker choice 2 with its safeguard, never
         // solving below what the residual target needs, floored at pcg_rel_tol
         // (and at 1e-6 for FP32 PCG vectors)
