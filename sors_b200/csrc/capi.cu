@@ -571,11 +571,14 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
         if (h->sc_host->done) break;
     }
     *iters = h->sc_host->it;
-    if (h->tl_active && h->sc_host->it >= 8 && h->sc_host->rr > 0.0 && h->sc_host->bnorm2 > h->sc_host->rr) {
-        // iterations per decade of residual reduction: the coarse operator is
-        // rebuilt when that doubles against its value right after a rebuild
+    if (refreshed) h->tl_ref_rate = -1.0;
+    if (h->tl_active && h->sc_host->it >= 8 && h->sc_host->rr > 0.0 && h->sc_host->bnorm2 >= 1e4 * h->sc_host->rr) {
+        // iterations per decade of residual reduction, over solves of two
+        // decades or more (loose solves converge faster per decade and would
+        // skew it): the coarse operator is rebuilt when that doubles against
+        // the first such solve after the last rebuild
         const double rate = h->sc_host->it / (0.5 * log10(h->sc_host->bnorm2 / h->sc_host->rr));
-        if (refreshed || h->tl_ref_rate <= 0.0) h->tl_ref_rate = rate;
+        if (h->tl_ref_rate <= 0.0) h->tl_ref_rate = rate;
         else if (rate > 2.0 * h->tl_ref_rate) h->tl_ready = false;
     }
     if (h->sc_host->breakdown && h->sc_host->it == 0 && !(h->s.project_spd == 2 && !h->proj_fallback))
