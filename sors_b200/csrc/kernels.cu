@@ -1072,14 +1072,6 @@ void launch_pcg_init(int N, const double* g, const VT* Minv, VT* x, VT* r, VT* z
     counted();
 }
 
-// One 3x3 block (hval layout): nine scalar loads.
-template <typename HT, typename VT>
-__device__ __forceinline__ void load_block(const HT* __restrict__ H, size_t b, size_t nnzb, VT (&h)[9]) {
-    const HT* v = H + hval(b, 0, nnzb);
-#pragma unroll
-    for (int k = 0; k < 9; k++) h[k] = (VT)__ldg(v + k);
-}
-
 // The search direction p is stored padded, four values per node (the fourth
 // zero), so that a gather of p at a column is one 16-byte load (two for doubles).
 template <typename VT>

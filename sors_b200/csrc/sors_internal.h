@@ -49,8 +49,9 @@ struct MuscleArgs {
 
 // Hessian value storage: nnzb 3x3 blocks in CSR order, each block's 9 values
 // contiguous and row-major.  (Splitting entries 0-7 from entry 8 for 16-byte
-// vector loads was measured slower in the SpMV.)  nnzb is carried so the
-// layout can change in one place.
+// vector loads was measured slower in the SpMV.)  The PCG SpMV also reads
+// this layout directly, two blocks (18 values) at a time in nine vector loads;
+// the allocation carries 160 bytes of padding for its last group.
 __host__ __device__ __forceinline__ size_t hval(size_t b, int rc, size_t nnzb) {
     (void)nnzb;
     return 9 * b + (size_t)rc;
