@@ -706,10 +706,14 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     for (int it = 0; it < h->s.newton_max_iter; it++) {
         bool want_hess = (m != 2) || !have_hess;  // frozen Hessian: assemble once
         if (want_hess) h->proj_fallback = (m == 2);  // adaptive: the frozen Hessian is the projected one
-        // When the inexact-Newton bound eta |g| of the last solve predicts a
-        // residual below res_tol, evaluate the gradient alone first: the
-        // Hessian is assembled only if that iteration does not stop.
-        const bool probe = want_hess && res_tol > 0.0 && prev_g > 0.0 && prev_eta * prev_g <= res_tol;
+        // Near convergence (the inexact-Newton bound eta |g| of the last solve
+        // within 1e3 res_tol) the gradient is evaluated alone first: the
+        // iteration may stop there, and if it does not but |g| fell tenfold,
+        // the step reuses the Hessian of the last assembly (a chord step, whose
+        // error is second order in the last update); otherwise the Hessian is
+        // assembled as usual.
+        const bool probe = want_hess && have_hess && m != 2 && res_tol > 0.0 && prev_g > 0.0 &&
+                           prev_eta * prev_g <= 1e3 * res_tol;
         if ((st = eval_system<HT>(h, dt, want_hess && !probe))) return st;
         if (want_hess && !probe) have_hess = true;
         CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
@@ -720,9 +724,8 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         if (stats) { stats->newton_iters++; stats->residual_norm = gn; }
         if (!(gn == gn)) break;  // NaN gradient: diverged
         if (res_tol > 0.0 && gn < res_tol) { converged = true; break; }
-        if (probe) {
+        if (probe && gn > 0.1 * prev_g) {
             if ((st = eval_system<HT>(h, dt, true))) return st;
-            have_hess = true;
             CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
             CK(cudaStreamSynchronize(h->stream));
         }
