@@ -278,6 +278,11 @@ int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
  * launches count every kernel node).  Diagnostic only. */
 int64_t sors_kernel_launch_count(void);
 
+/* Number of system evaluations (gradient rows, and the Hessian when
+ * with_hessian != 0) this handle has made since it was created; with_hessian
+ * == 0 counts the gradient-only ones.  Diagnostic only. */
+int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian);
+
 /* Sum of the Neo-Hookean element energies (volume x Psi, the element part of
  * sors_energy) of a tet (nodes_per_elem = 4) or hex (8) mesh, computed from
  * caller-owned DEVICE arrays, without any device allocation.  No counterpart

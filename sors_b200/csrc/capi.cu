@@ -173,6 +173,7 @@ struct SorsHandle {
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
     long long pcg_graph_kernels = 0;  // kernel nodes of the captured chunk
+    int64_t n_hess_evals = 0, n_grad_evals = 0;  // system evaluations with / without the Hessian
     bool graph_failed = false;
 
     double prev_gnorm = -1.0;
@@ -419,6 +420,7 @@ template <typename HT>
 int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmStep) {
     int st = compute_external(h);
     if (st) return st;
+    (want_hess ? h->n_hess_evals : h->n_grad_evals)++;
     AsmArgs<HT> a;
     a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.tshape = h->tshape;
@@ -2158,6 +2160,11 @@ int sors_sizes(const SorsHandle* h, int64_t* n_nodes, int64_t* n_elems, int64_t*
 void* sors_stream(SorsHandle* h) { return h ? (void*)h->stream : nullptr; }
 
 int64_t sors_kernel_launch_count(void) { return (int64_t)g_kernel_launches.load(); }
+
+int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian) {
+    if (!h) return 0;
+    return with_hessian ? h->n_hess_evals : h->n_grad_evals;
+}
 
 }  // extern "C"
 
