@@ -85,7 +85,7 @@ def estimate_device_bytes(n_nodes: int, n_elems: int, nodes_per_elem: int, preci
     nnzb = int((2.7 if nv == 4 else 3.6) * n_elems + n_nodes)
     b = 0
     b += 8 * 3 * n_nodes * 12             # FP64 state vectors
-    b += 3 * n_nodes * hs * 6 + 9 * n_nodes * hs   # PCG vectors + block-Jacobi
+    b += (3 * 4 + 4 * 2) * n_nodes * hs + 9 * n_nodes * hs   # PCG vectors (p padded) + block-Jacobi
     b += 9 * nnzb * hs                     # Hessian values
     b += 4 * nnzb * 2 + 4 * n_nodes * 4    # pattern + slot pointers
     b += 4 * n_elems * nv * 2 + 2 * n_elems * nv * nv + 16 * n_elems  # conn, pairs, slot items, materials
