@@ -82,3 +82,70 @@ def test_max_distance_qp_kkt():
     assert work[0] and not work[1]
     assert mu[0] >= 0.0 and abs((A @ dx)[0] - l[0]) < 1e-10
     assert np.abs(H @ dx + g - A.T @ mu).max() < 1e-9
+
+
+def test_max_distance_adjoint_needs_constraint_curvature():
+    # One SQP step of the rope scene with the pair held: the step's sensitivity
+    # to the Young's moduli, from the KKT system with the Lagrangian Hessian
+    # H + (mu / L)(I - u u^T) on (x_i - x_j), matches central differences of
+    # the oracle's step; the energy Hessian alone is off by about 1 %.  (This
+    # is the transpose system sors_adjoint_step solves for held pairs.)
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    from tests.helpers import two_cubes
+    X, T, a, b, n1 = two_cubes(kind="tet")
+    ne = T.shape[0]
+    rng = np.random.default_rng(5)
+    E = np.exp(rng.uniform(np.log(1e4), np.log(4e4), ne))
+    dt = 5e-4
+    v0 = np.zeros_like(X); v0[:n1, 0] = -0.2; v0[n1:, 0] = 0.2
+
+    def system(Ev):
+        return orc.System(X, T, rho=1000.0, youngs=Ev, nu=0.4, grav=(0, 0, -9.81), scheme="backward_euler",
+                          method="minimize_SQP", dt=dt, substeps=1, nthreads=1)
+
+    o = system(E)
+    o.set_initial_velocity(v0.ravel())
+    sq = oc.SQPOracle(o, max_distance=oc.MaxDistance([a], [b], [0.0025]))
+    q = X.ravel().copy()
+    for _ in range(3):
+        q = sq.step(q, dt)
+    qP, vP, _ = o.state()
+
+    def one_step(Ev):
+        s = system(Ev)
+        s.set_initial_deformation(qP); s.set_initial_velocity(vP)
+        sqs = oc.SQPOracle(s, max_distance=oc.MaxDistance([a], [b], [0.0025]))
+        return sqs.step(qP.copy(), dt), sqs
+
+    q1, sq1 = one_step(E)
+    assert list(sq1.held_pairs) == [0]
+    s0 = system(E); s0.set_initial_deformation(qP); s0.set_initial_velocity(vP)
+    H = s0.hessian_csr(q1, dt)[0].toarray()
+    g = s0.gradient(q1, dt)
+    n = q1.size
+    xs = q1.reshape(-1, 3); d = xs[a] - xs[b]; L = np.linalg.norm(d); u = d / L
+    arow = np.zeros(n); arow[3 * a:3 * a + 3] = -u; arow[3 * b:3 * b + 3] = u
+    mu = (arow @ g) / (arow @ arow)
+    assert mu > 0 and np.abs(g - mu * arow).max() < 1e-6 * np.abs(g).max()
+    C = np.zeros((n, n)); M = (np.eye(3) - np.outer(u, u)) * mu / L
+    for p, sp_ in ((a, 1), (b, -1)):
+        for r, sr in ((a, 1), (b, -1)):
+            C[3 * p:3 * p + 3, 3 * r:3 * r + 3] += sp_ * sr * M
+    c = rng.standard_normal(n)
+    r = rng.standard_normal(ne)
+    h = 1e-6
+
+    def grad_at(Ev):
+        s = system(Ev); s.set_initial_deformation(qP); s.set_initial_velocity(vP)
+        return s.gradient(q1, dt)
+
+    dg = (grad_at(E * (1 + h * r)) - grad_at(E * (1 - h * r))) / (2 * h)
+    d_fd = c @ (one_step(E * (1 + h * r))[0] - one_step(E * (1 - h * r))[0]) / (2 * h)
+    errs = []
+    for HL in (H + C, H):
+        K = np.block([[HL, arow[:, None]], [arow[None, :], np.zeros((1, 1))]])
+        lam = np.linalg.solve(K, np.concatenate([c, [0.0]]))[:n]
+        errs.append(abs(-lam @ dg - d_fd) / abs(d_fd))
+    assert errs[0] < 1e-5, errs
+    assert errs[1] > 1e-3, errs
