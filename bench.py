@@ -180,20 +180,49 @@ def cpu_sample_run(steps, warmup, threads=None):
             "ms_per_step": 1e3 * dt_wall / steps, "elements": ne}
 
 
+def cpu_phases(threads=None):
+    """The reference's element and assembly phases at full size, on the host
+    cores: one Energy::compute_gradient (cpp/src/energy.cpp:252-308) and one
+    Energy::compute_hessian with triplets -> CSR (cpp/src/energy.cpp:312-390)
+    of the whole 3.0M-tet block, by the CPU restatement (FP64, OpenMP)."""
+    from oracle import oracle as orc
+    X, T, E, mask, val = block_mesh(CELLS, seed=0)
+    nthreads = threads or os.cpu_count() or 1
+    o = orc.System(X, T, rho=1070.0, youngs=E, nu=0.45, grav=(0, 0, -9.81), scheme="backward_euler",
+                   method="minimize_newton", dt=DT, substeps=1, nthreads=nthreads)
+    o.set_neumann(mask, val)
+    q = X.ravel().copy()
+    t0 = time.perf_counter()
+    o.gradient(q, DT)
+    t1 = time.perf_counter()
+    H, st = o.hessian_csr(q, DT)
+    t2 = time.perf_counter()
+    nnz = int(H.nnz)
+    del H, o
+    return {"workload": workload_name(CELLS, "FP64"), "cores": nthreads, "kind": "port",
+            "gradient_s": t1 - t0, "hessian_csr_s": t2 - t1, "hessian_nnz": nnz,
+            "what": "one full-size gradient assembly and one Hessian assembly (element Hessians, triplets, "
+                    "triplets -> CSR with duplicate sums), FP64, all host threads"}
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 6))
-    warmup = 1
+    steps, warmup = args.steps, args.warmup
     cb = cpu_sample_run(steps, warmup)
+    ne = cb["elements"]
     line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": world, "steps": steps,
             "warmup": warmup, "ms_per_step": cb["ms_per_step"], "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-            "config": {"workload": workload_name(tuple(args.cells), "FP64 CPU restatement of the reference path, "
-                                                 "each step timed on the bounded sample in cpu_baseline.sample"),
-                       "elements": 6 * int(np.prod(args.cells)), "precision": "fp64", "parallelism": "host cores"},
+            "config": {"workload": workload_name(SAMPLE_CELLS, "FP64 CPU restatement of the reference path "
+                                                 "(sparse LDL^T Newton)") +
+                       f"; a bounded sample of the {workload_name(CELLS, 'GPU')} workload, same spacing, jitter "
+                       "and material distribution, compared per element",
+                       "elements": ne, "precision": "fp64", "parallelism": "host cores"},
             "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_phases:
+        line["cpu_baseline"]["phases"] = cpu_phases()
     print(json.dumps(line), flush=True)
 
 
@@ -287,23 +316,25 @@ def run_gpu(args, rank, world, local_rank):
     achieved = bytes_ / (dur / 1e3) / 1e9
     traffic = ncu_traffic(f"{dom}_{args.precision}", nn)
     # end-to-end through Solver.step with pinned host buffers
+    # the solver steps the pinned host solution in place (q_in == q_out)
     q_host = torch.empty(3 * nn, dtype=torch.float64, pin_memory=True).numpy()
-    q_out = torch.empty(3 * nn, dtype=torch.float64, pin_memory=True).numpy()
     q_host[:] = q_dev.cpu().numpy()
     e2e_steps = args.steps
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True); ev1 = torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(e2e_steps):
-        sol.step(q_host, en, out=q_out)
-        q_host[:] = q_out
+        sol.step(q_host, en, out=q_host)
     ev1.record(stream)
     ev1.synchronize()
     e2e_ms = ev0.elapsed_time(ev1)
     if dist:
         e2e_ms = max_over_ranks(e2e_ms, dist, f"cuda:{local_rank}")
     e2e_value = world * ne * e2e_steps / (e2e_ms / 1e3)
-    # plain FP64 drop-in beside it (same trajectory length)
+    steps_done = args.warmup + args.steps + e2e_steps
+    q_mixed = q_host.copy()
+    # plain FP64 drop-in beside it, then advanced untimed to the same step count
+    # from the same start, for the mixed-precision error
     fp64 = None
     if not args.no_fp64 and args.precision == "mixed":
         del en  # free the mixed handle's memory first
@@ -313,16 +344,24 @@ def run_gpu(args, rank, world, local_rank):
             sol64.step_device(q64.data_ptr(), en64)
         stream64 = torch.cuda.ExternalStream(L.sors_stream(en64.handle()), device=local_rank)
         ms64, n64, p64 = timed_device_steps(torch, L, en64, sol64, q64, args.steps, stream64)
-        # the mixed run advanced W + K + K(e2e) steps; compare at equal step counts
-        qm = torch.tensor(X.ravel(), dtype=torch.float64, device=f"cuda:{local_rank}")
         prof64 = _lib.SorsKernelProfile()
         _lib.check(L.sors_profile_kernels(en64.handle(), 20, __import__("ctypes").byref(prof64)))
+        for _ in range(steps_done - args.warmup - args.steps):
+            sol64.step_device(q64.data_ptr(), en64)
+        torch.cuda.synchronize()
+        q64h = q64.cpu().numpy()
+        disp64 = float(np.abs(q64h - X.ravel()).max())
         fp64 = {"value": ne * args.steps / (ms64 / 1e3), "ms_per_step": ms64 / args.steps,
                 "newton_iters_per_step": n64 / args.steps, "pcg_iters_per_step": p64 / args.steps,
                 "spmv_gbs": prof64.spmv_bytes / (prof64.spmv_ms / 1e3) / 1e9,
                 "assemble_gbs": prof64.assemble_bytes / (prof64.assemble_ms / 1e3) / 1e9,
-                "final_disp_max": float((q64 - torch.tensor(X.ravel(), device=q64.device)).abs().max())}
-        del qm
+                "assemble_ms": prof64.assemble_ms,
+                "final_disp_max": disp64}
+        error_vs_fp64 = {"steps": steps_done, "max_abs_m": float(np.abs(q_mixed - q64h).max()),
+                         "rel_to_max_disp": float(np.abs(q_mixed - q64h).max()) / max(disp64, 1e-300),
+                         "what": "max |q_mixed - q_fp64| over all DOFs after the same number of steps from "
+                                 "the same start, relative to the FP64 run's largest displacement"}
+        del en64
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -354,6 +393,7 @@ def run_gpu(args, rank, world, local_rank):
     }
     if fp64:
         line["fp64"] = fp64
+        line["error_vs_fp64"] = error_vs_fp64
     if world == 1 and not args.no_cpu:
         try:
             cb = cpu_sample_run(steps=3, warmup=1)
@@ -361,6 +401,15 @@ def run_gpu(args, rank, world, local_rank):
         except Exception as ex:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
                                     "sample": f"failed: {ex}"}
+        if not args.no_phases:
+            try:
+                ph = cpu_phases()
+                # the GPU does both phases in one assembly launch (gradient rows and Hessian)
+                ph["gpu_assemble_ms"] = {"mixed": prof.assemble_ms,
+                                         "fp64": fp64["assemble_ms"] if fp64 else None}
+                line["cpu_baseline"]["phases"] = ph
+            except Exception as ex:
+                line["cpu_baseline"]["phases"] = {"failed": str(ex)}
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
@@ -630,6 +679,8 @@ def main():
                     help="SPD projection of the element Hessians: always, never, or only where PCG meets "
                          "negative curvature")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-phases", action="store_true",
+                    help="skip the full-size CPU gradient / Hessian assembly timing (about 30 s of host work)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "serve"],
                     help="c2: the 3.0M-tet block (default); c3: pressure-actuated hex arm, static load ramp; "
                          "serve: Poisson stream of poke rollouts")

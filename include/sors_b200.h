@@ -9,7 +9,7 @@
  * Each entry point names the reference interface it replaces (paths relative
  * to the SORS project root).  The reference's Python module py_sors
  * (cpp/py_sors.cpp) binds the C++ classes Energy<3,E> and Solver<3,E>; a
- * maintainer binds these functions instead (INTEGRATION.md).
+ * maintainer binds these functions instead.
  */
 #ifndef SORS_B200_H
 #define SORS_B200_H
@@ -294,8 +294,11 @@ int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian);
  * stream) and asynchronous to the host.  The kernel's scratch is a fixed
  * 64 KiB array inside the library, shared by all calls: n_elems above
  * 8,388,608 is rejected (SORS_ERR_ARG), and calls that overlap on the GPU
- * race and must be serialised by the caller.  The first call on each device
- * looks up the array's device address; make it before any stream capture. */
+ * race and must be serialised by the caller.  A call on a stream that is not
+ * capturing looks up the array's device address and remembers it; a call on a
+ * capturing stream uses the remembered one.  So make the first call on each
+ * device before any stream capture, and after a device reset (which may move
+ * the array) make one uncaptured call before the next capture. */
 int sors_elem_energy_noalloc(const double* X_device, const double* q_device, const int32_t* conn_device,
                              int32_t n_elems, int32_t nodes_per_elem, const double* youngs_device,
                              const double* poisson_device, double* out_device, void* stream);

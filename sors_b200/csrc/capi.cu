@@ -1503,26 +1503,14 @@ int run_minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
     return minimize<double, double>(h, dt, stats);
 }
 
-// CFL time step (solver.cpp:300-331), host side
+// CFL time step (solver.cpp:300-331): the shortest element edge at q and
+// max |vPrev| reduced on the device, dt_CFL = l_min / v_max, at most dt.
 int cfl_dt(SorsHandle* h, double dt, double* out) {
-    std::vector<double> q(h->ndof), v(h->ndof);
-    std::vector<int> conn((size_t)h->E * h->nv);
-    CK(cudaMemcpyAsync(q.data(), h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(v.data(), h->vPrev, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
-    CK(cudaMemcpyAsync(conn.data(), h->conn, sizeof(int) * conn.size(), cudaMemcpyDeviceToHost, h->stream));
+    launch_cfl(h->E, h->nv, h->q, h->conn, h->ndof, h->vPrev, h->partials, h->sc, h->stream);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    double vmax = 0;
-    for (double a : v) vmax = std::max(vmax, fabs(a));
-    double lmin = -1;
-    for (int e = 0; e < h->E; e++)
-        for (int i = 0; i < h->nv; i++)
-            for (int j = i + 1; j < h->nv; j++) {
-                const double* a = &q[3 * conn[(size_t)e * h->nv + i]];
-                const double* b = &q[3 * conn[(size_t)e * h->nv + j]];
-                double l = sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
-                if (lmin < 0 || l < lmin) lmin = l;
-            }
-    double dtc = lmin / vmax;
+    const double dtc = h->sc_host->minedge / h->sc_host->vmax;
     *out = dtc < dt ? dtc : dt;
     return SORS_OK;
 }

@@ -422,9 +422,8 @@ __device__ __forceinline__ bool tet_row_stage(const AsmArgs<HT>& a, int e, int v
     double C[9];
     cof3(F, C);
     const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
-    if (SNH ? (J == 0.0) : !(J > 0.0)) {
-        // the gradient row still follows the reference (NaN or inf as it gives)
-    }
+    // an inverted element still gets the reference's gradient row (NaN or inf
+    // as log J and 1/J give); the caller reports it through `ok`
     const double iJ = 1.0 / J;
     double IC = 0.0;
     if (SNH) {
@@ -1366,6 +1365,65 @@ void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, d
 }
 
 // Newton predictor q += dt v_prev
+// CFL time step inputs (cpp/src/solver.cpp:300-331): the shortest edge of any
+// element at q, over every vertex pair (Element::compute_minimal_edge_length,
+// cpp/headers/geometries/element.h:131-142), and max |vPrev|.  Minimum and
+// maximum do not depend on the order of evaluation, so the result is the
+// reference loop's exactly.  sc->minedge, sc->vmax.
+__global__ void __launch_bounds__(kRedThreads) k_cfl(int E, int nv, const double* __restrict__ q,
+                                                     const int* __restrict__ conn, int n,
+                                                     const double* __restrict__ vPrev, double* partials,
+                                                     DevScalars* sc) {
+    __shared__ double sh[32][2];
+    __shared__ bool am_last;
+    double lmin = INFINITY, vmax = 0.0;
+    const int stride = gridDim.x * blockDim.x;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < E; e += stride) {
+        double x[8][3];
+        for (int w = 0; w < nv; w++) {
+            const int v = __ldg(conn + (size_t)e * nv + w);
+#pragma unroll
+            for (int r = 0; r < 3; r++) x[w][r] = q[3 * (size_t)v + r];
+        }
+        for (int i = 0; i < nv; i++)
+            for (int j = i + 1; j < nv; j++) {
+                const double d0 = x[i][0] - x[j][0], d1 = x[i][1] - x[j][1], d2 = x[i][2] - x[j][2];
+                lmin = fmin(lmin, sqrt(d0 * d0 + d1 * d1 + d2 * d2));
+            }
+    }
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) vmax = fmax(vmax, fabs(vPrev[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lmin = fmin(lmin, __shfl_xor_sync(0xffffffffu, lmin, o));
+        vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    }
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+    if (l == 0) { sh[w][0] = lmin; sh[w][1] = vmax; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < nw; k++) { lmin = fmin(lmin, sh[k][0]); vmax = fmax(vmax, sh[k][1]); }
+        partials[2 * blockIdx.x] = lmin;
+        partials[2 * blockIdx.x + 1] = vmax;
+        __threadfence();
+        am_last = (atomicAdd(&sc->counters[10], 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!am_last || threadIdx.x != 0) return;
+    __threadfence();
+    const volatile double* vp = partials;
+    double a = INFINITY, b = 0.0;
+    for (int k = 0; k < (int)gridDim.x; k++) { a = fmin(a, vp[2 * k]); b = fmax(b, vp[2 * k + 1]); }
+    sc->minedge = a;
+    sc->vmax = b;
+    sc->counters[10] = 0u;
+}
+
+void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const double* vPrev, double* partials,
+                DevScalars* sc, cudaStream_t st) {
+    k_cfl<<<red_grid(E > n ? E : n), kRedThreads, 0, st>>>(E, nv, q, conn, n, vPrev, partials, sc);
+    counted();
+}
+
 __global__ void k_predict(int n, double* q, const double* vPrev, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) q[i] += dt * vPrev[i];

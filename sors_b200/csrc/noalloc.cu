@@ -18,9 +18,13 @@
 // and its kernel leaves it at zero again.
 //
 // In host code the array's name only stands for the variable; its device
-// address is looked up once per device with cudaGetSymbolAddress, on the first
-// call made while that device is current.  That first call on each device
-// should come before any stream capture.
+// address comes from cudaGetSymbolAddress with the caller's device current.
+// A call on a stream that is not being captured looks the address up afresh
+// (so a device reset, which reloads the library's module at a possibly
+// different address, is picked up by the next call) and remembers it per
+// device; a call on a capturing stream uses the remembered address.  So the
+// first call on each device should come before any stream capture, and after
+// a device reset one uncaptured call must precede the next capture.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -145,17 +149,26 @@ __global__ void __launch_bounds__(kNoAllocThreads) k_elem_energy_noalloc(int E, 
     }
 }
 
-// Device address of the scratch array on the current device (looked up once).
-int scratch_address(int device, unsigned char** ptr) {
+// Device address of the scratch array on the current device: looked up afresh
+// unless `stream` is capturing, in which case the address remembered from the
+// last uncaptured call on this device is used.
+int scratch_address(int device, cudaStream_t stream, unsigned char** ptr) {
     if (device < 0 || device >= kMaxDevices) return noalloc_fail(SORS_ERR_ARG, "device ordinal out of range");
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(stream, &cap);
+    if (e != cudaSuccess)
+        return noalloc_fail(SORS_ERR_CUDA, std::string("cudaStreamIsCapturing: ") + cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[device]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
             return noalloc_fail(SORS_ERR_CUDA,
                                 std::string("cudaGetSymbolAddress of the scratch array failed: ") + cudaGetErrorString(e));
         g_noalloc_addr[device] = p;
+    } else if (!g_noalloc_addr[device]) {
+        return noalloc_fail(SORS_ERR_ARG,
+                            "sors_elem_energy_noalloc: the first call on a device must come before any stream capture");
     }
     *ptr = static_cast<unsigned char*>(g_noalloc_addr[device]);
     return SORS_OK;
@@ -179,10 +192,10 @@ int sors_elem_energy_noalloc(const double* X_device, const double* q_device, con
     int device = 0;
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return noalloc_fail(SORS_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-    unsigned char* scratch = nullptr;
-    int st = scratch_address(device, &scratch);
-    if (st) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    unsigned char* scratch = nullptr;
+    int st = scratch_address(device, s, &scratch);
+    if (st) return st;
     if (n_elems == 0) {
         e = cudaMemsetAsync(out_device, 0, sizeof(double), s);
         if (e != cudaSuccess) return noalloc_fail(SORS_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));

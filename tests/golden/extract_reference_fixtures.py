@@ -117,7 +117,10 @@ def extract(ref_root: str) -> dict:
 
 
 def main() -> None:
-    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SORS_REFERENCE_ROOT", "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SORS_REFERENCE_ROOT")
+    if not ref:
+        sys.exit("usage: extract_reference_fixtures.py <reference project root> "
+                 "(or set SORS_REFERENCE_ROOT)")
     data = extract(ref)
     dst = os.path.join(HERE, "reference_known_answers.json")
     with open(dst, "w") as f:

@@ -9,7 +9,7 @@ from sors_b200 import meshes
 def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha=0.0, dt=1e-3,
               scheme="backward_euler", method="minimize_newton", precision="fp64", project=True,
               clamp=True, res_tol=0.0, faces=None, groups=None, vertex_force=False, oracle_project=False,
-              muscles=None, energy="neohookean", two_level=False):
+              muscles=None, energy="neohookean", two_level=False, substeps=1, cfl=False):
     """(gpu_energy, gpu_solver, oracle_system, X) on one mesh."""
     from oracle import oracle as orc
     from sors_b200 import py_sors as ps
@@ -22,7 +22,8 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     s = ps.SimulationSettings()
     s.meshType = "Tetrahedron" if T.shape[1] == 4 else "Hexahedron"
     s.dt = dt
-    s.substeps = 1
+    s.substeps = substeps
+    s.CFLtimeSteppingFlag = cfl
     s.timeSteppingScheme = scheme
     s.solverMethod = method
     s.precision = precision
@@ -57,7 +58,7 @@ def make_pair(X, T, *, rho=1070.0, E=1e5, nu=0.45, grav=(0.0, 0.0, -9.81), alpha
     en = ps.Energy(X, T, s, np.asarray(grav, float), alpha, energies, params, ctypes_, cparams, ftypes, fparams)
     sol = ps.Solver(s)
     o = orc.System(X, T, rho=rhov, youngs=Ev, nu=nuv, grav=grav, alpha=alpha, scheme=scheme, method=method,
-                   project=oracle_project, dt=dt, substeps=1,
+                   project=oracle_project, dt=dt, substeps=substeps, cfl=cfl,
                    material=orc.MAT_STABLE_NEOHOOKEAN if energy == "stableneohookean" else orc.MAT_NEOHOOKEAN)
     if clamp:
         o.set_neumann(mask, val)

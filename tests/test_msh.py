@@ -6,7 +6,10 @@ import pytest
 
 from sors_b200 import meshes, msh
 
-REF_MESHES = "/root/reference/cpp/demos/meshes"
+# The reference project's root, when a checkout is available (no default):
+# its demo meshes live under cpp/demos/meshes.
+_REF_ROOT = os.environ.get("SORS_REFERENCE_ROOT", "")
+REF_MESHES = os.path.join(_REF_ROOT, "cpp", "demos", "meshes") if _REF_ROOT else ""
 
 
 @pytest.mark.parametrize("version", ["4.1", "2.2"])
@@ -34,7 +37,8 @@ def test_tag_mapping_and_type_filter(tmp_path):
     np.testing.assert_array_equal(T, [[0, 1, 2, 3], [1, 2, 3, 4]])
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_MESHES), reason="reference meshes not present")
+@pytest.mark.skipif(not REF_MESHES or not os.path.isdir(REF_MESHES),
+                    reason="SORS_REFERENCE_ROOT not set to a reference checkout")
 def test_reference_demo_meshes():
     # the MSH 4.1 binary meshes that ship with the reference's demos
     for name in ("duck.msh", "sphere1.msh"):
