@@ -283,6 +283,18 @@ int64_t sors_kernel_launch_count(void);
  * == 0 counts the gradient-only ones.  Diagnostic only. */
 int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian);
 
+/* Assembly kernel of the handle's tet Hessian and gradient evaluations:
+ * 0 (default) the element-owner kernel over node chunks wherever it applies
+ * (exact Neo-Hookean or stable Neo-Hookean tets without fibre terms; the
+ * projected Hessian, fibres, the quartic test element and hexes always use
+ * the row-owner kernel), 1 the row-owner kernel everywhere.  Both give the
+ * same Hessian values; no counterpart in the reference.  Diagnostic only. */
+int sors_set_assembly_variant(SorsHandle* h, int32_t variant);
+
+/* Node chunks of the element-owner assembly (0: the mesh uses the row-owner
+ * kernel only).  Diagnostic only. */
+int64_t sors_assembly_chunks(SorsHandle* h);
+
 /* Sum of the Neo-Hookean element energies (volume x Psi, the element part of
  * sors_energy) of a tet (nodes_per_elem = 4) or hex (8) mesh, computed from
  * caller-owned DEVICE arrays, without any device allocation.  No counterpart

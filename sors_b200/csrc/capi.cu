@@ -81,6 +81,10 @@ struct SorsHandle {
     int *row_ptr = nullptr, *col = nullptr, *diag_slot = nullptr, *pair_ptr = nullptr, *pair_ev = nullptr,
         *slot_item_ptr = nullptr;
     uint16_t* slot_items = nullptr;
+    // element-owner tet assembly: node chunks (build_tet_chunks)
+    ChunkArgs chunks;
+    long long chunk_elem_total = 0;  // sum over chunks of their element counts
+    int asm_variant = 0;  // 0: chunked element-owner where it applies, 1: row-owner
     uint8_t* node_mask = nullptr;
     std::vector<uint8_t> mask_h;
     std::vector<int> row_ptr_h, col_h;
@@ -282,8 +286,14 @@ void parallel_for(int n, F&& f) {
     for (auto& t : ts) t.join();
 }
 
+// Host copies of the pattern's pair lists and slot items (set-up only).
+struct PatternHost {
+    std::vector<int> pair_ptr, pair_ev, slot_cnt;
+    std::vector<uint16_t> items;
+};
+
 // Builds pattern, pair lists and slot-item lists (host), then uploads.
-int build_pattern(SorsHandle* h, const int32_t* conn) {
+int build_pattern(SorsHandle* h, const int32_t* conn, PatternHost* keep) {
     const int N = h->N, E = h->E, nv = h->nv;
     std::vector<int> pair_ptr(N + 1, 0);
     for (long long t = 0; t < (long long)E * nv; t++) pair_ptr[conn[t] + 1]++;
@@ -381,6 +391,171 @@ int build_pattern(SorsHandle* h, const int32_t* conn) {
     if ((st = upload(h, &h->slot_items, items.data(), items.size()))) return st;
     h->row_ptr_h = std::move(row_ptr);
     h->col_h = std::move(cols_all);
+    if (keep) {
+        keep->pair_ptr = std::move(pair_ptr);
+        keep->pair_ev = std::move(pair_ev);
+        keep->slot_cnt = std::move(slot_cnt);
+        keep->items = std::move(items);
+    }
+    return SORS_OK;
+}
+
+// Node chunks of the element-owner tet assembly.  Nodes are taken in Morton
+// order of their undeformed positions and cut greedily into chunks of at most
+// chunk_limits(...) rows, incident elements and (element, vertex) pairs; each
+// chunk lists its incident elements once, in first-seen order.  Meshes where
+// a single node exceeds the limits keep the row-owner assembly only.
+int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const PatternHost& ph) {
+    h->chunks = ChunkArgs{};
+    if (h->nv != 4 || !(h->s.material == 0 || h->s.material == 2) || h->N == 0) return SORS_OK;
+    const int N = h->N, E = h->E;
+    const ChunkLimits lim = chunk_limits(mixed(h) ? 4 : 8, h->s.material);
+    for (int i = 0; i < N; i++) {
+        const int np = ph.pair_ptr[i + 1] - ph.pair_ptr[i];
+        if (np > lim.pairs || np > lim.elems) return SORS_OK;
+    }
+    // Morton order of the undeformed positions (21 bits per axis)
+    double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], X[3 * (size_t)i + k]);
+            hi[k] = std::max(hi[k], X[3 * (size_t)i + k]);
+        }
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<std::pair<uint64_t, int>> key(N);
+    parallel_for(N, [&](int a, int b) {
+        for (int i = a; i < b; i++) {
+            uint64_t code = 0;
+            for (int k = 0; k < 3; k++) {
+                const double ext = hi[k] - lo[k];
+                const double u = ext > 0 ? (X[3 * (size_t)i + k] - lo[k]) / ext : 0.0;
+                const uint64_t c = (uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0));
+                code |= spread(c) << k;
+            }
+            key[i] = {code, i};
+        }
+    });
+    std::sort(key.begin(), key.end());
+    // greedy cut
+    std::vector<int> ch_ptr{0}, ch_rows, ch_eptr{0}, ch_elems;
+    ch_rows.reserve(N);
+    ch_elems.reserve((size_t)E * 3 / 2);
+    std::vector<int> mark(E, -1);
+    int cur = 0, nr = 0, ne = 0, np = 0;
+    for (int o = 0; o < N; o++) {
+        const int i = key[o].second;
+        const int p0 = ph.pair_ptr[i], p1 = ph.pair_ptr[i + 1];
+        int fresh = 0;
+        for (int t = p0; t < p1; t++) fresh += mark[ph.pair_ev[t] >> 3] != cur;
+        if (nr > 0 && (nr + 1 > lim.rows || ne + fresh > lim.elems || np + (p1 - p0) > lim.pairs)) {
+            cur++;
+            ch_ptr.push_back((int)ch_rows.size());
+            ch_eptr.push_back((int)ch_elems.size());
+            nr = ne = np = 0;
+        }
+        ch_rows.push_back(i);
+        nr++;
+        np += p1 - p0;
+        for (int t = p0; t < p1; t++) {
+            const int e = ph.pair_ev[t] >> 3;
+            if (mark[e] != cur) {
+                mark[e] = cur;
+                ch_elems.push_back(e);
+                ne++;
+            }
+        }
+    }
+    ch_ptr.push_back((int)ch_rows.size());
+    ch_eptr.push_back((int)ch_elems.size());
+    const int nch = (int)ch_ptr.size() - 1;
+    // per chunk: pair slots of owned vertices, and the (element, v) of every pair
+    std::vector<uint16_t> eslot(ch_elems.size() * 4, 0xffff);
+    std::vector<uint32_t> pair_sv(ph.pair_ev.size());
+    parallel_for(nch, [&](int a, int b) {
+        std::vector<std::pair<int, int>> loc;
+        for (int c = a; c < b; c++) {
+            loc.clear();
+            for (int k = ch_eptr[c]; k < ch_eptr[c + 1]; k++) loc.push_back({ch_elems[k], k - ch_eptr[c]});
+            std::sort(loc.begin(), loc.end());
+            int slot = 0;
+            for (int p = ch_ptr[c]; p < ch_ptr[c + 1]; p++) {
+                const int r = ch_rows[p];
+                for (int t = ph.pair_ptr[r]; t < ph.pair_ptr[r + 1]; t++, slot++) {
+                    const int e = ph.pair_ev[t] >> 3, v = ph.pair_ev[t] & 7;
+                    const int sidx = std::lower_bound(loc.begin(), loc.end(), std::make_pair(e, -1))->second;
+                    eslot[(size_t)(ch_eptr[c] + sidx) * 4 + v] = (uint16_t)slot;
+                    pair_sv[t] = (uint32_t)(sidx << 2 | v);
+                }
+            }
+        }
+    });
+    // items in slot_items' order: (pair k of row r, vertex w) -> (element slot, v, w)
+    std::vector<uint16_t> items(ph.items.size());
+    const std::vector<int>& rp = h->row_ptr_h;
+    parallel_for(N, [&](int a, int b) {
+        for (int r = a; r < b; r++)
+            for (int bk = rp[r]; bk < rp[r + 1]; bk++)
+                for (int it = ph.slot_cnt[bk]; it < ph.slot_cnt[bk + 1]; it++) {
+                    const int o = ph.items[it], k = o / 4, w = o % 4;
+                    const uint32_t sv = pair_sv[ph.pair_ptr[r] + k];
+                    items[it] = (uint16_t)(sv << 2 | (uint32_t)w);
+                }
+    });
+    // every index the kernel derives from these tables stays inside its
+    // shared-memory arrays: check them all here, before any upload
+    std::vector<int> chunk_of_row(N, -1);
+    for (int c = 0; c < nch; c++) {
+        const int nrc = ch_ptr[c + 1] - ch_ptr[c], nec = ch_eptr[c + 1] - ch_eptr[c];
+        if (nrc < 1 || nrc > lim.rows || nec < 0 || nec > lim.elems || nec > 4095)
+            return fail(SORS_ERR_ARG, "internal: node chunk exceeds its limits");
+        int npc = 0;
+        for (int p = ch_ptr[c]; p < ch_ptr[c + 1]; p++) {
+            const int r = ch_rows[p];
+            if (r < 0 || r >= N || chunk_of_row[r] != -1) return fail(SORS_ERR_ARG, "internal: bad chunk row");
+            chunk_of_row[r] = c;
+            npc += ph.pair_ptr[r + 1] - ph.pair_ptr[r];
+        }
+        if (npc > lim.pairs) return fail(SORS_ERR_ARG, "internal: node chunk exceeds its pair limit");
+        int owned = 0;
+        for (size_t k = (size_t)ch_eptr[c] * 4; k < (size_t)ch_eptr[c + 1] * 4; k++) {
+            if (eslot[k] == 0xffff) continue;
+            if (eslot[k] >= npc) return fail(SORS_ERR_ARG, "internal: chunk pair slot out of range");
+            owned++;
+        }
+        if (owned != npc) return fail(SORS_ERR_ARG, "internal: chunk pair slots incomplete");
+    }
+    for (int r = 0; r < N; r++) {
+        if (chunk_of_row[r] < 0) return fail(SORS_ERR_ARG, "internal: node missing from the chunks");
+        const int c = chunk_of_row[r], nec = ch_eptr[c + 1] - ch_eptr[c];
+        for (int bk = rp[r]; bk < rp[r + 1]; bk++)
+            for (int it = ph.slot_cnt[bk]; it < ph.slot_cnt[bk + 1]; it++)
+                if ((int)(items[it] >> 4) >= nec) return fail(SORS_ERR_ARG, "internal: chunk item out of range");
+    }
+    if ((long long)nch > 0x7fffffffLL) return fail(SORS_ERR_ARG, "internal: too many node chunks");
+    int st;
+    ChunkArgs& c = h->chunks;
+    int *d_ptr = nullptr, *d_rows = nullptr, *d_eptr = nullptr, *d_elems = nullptr;
+    uint16_t *d_eslot = nullptr, *d_items = nullptr;
+    if ((st = upload(h, &d_ptr, ch_ptr.data(), ch_ptr.size()))) return st;
+    if ((st = upload(h, &d_rows, ch_rows.data(), ch_rows.size()))) return st;
+    if ((st = upload(h, &d_eptr, ch_eptr.data(), ch_eptr.size()))) return st;
+    if ((st = upload(h, &d_elems, ch_elems.data(), ch_elems.size()))) return st;
+    if ((st = upload(h, &d_eslot, eslot.data(), eslot.size()))) return st;
+    if ((st = upload(h, &d_items, items.data(), items.size()))) return st;
+    c.ch_ptr = d_ptr; c.ch_rows = d_rows; c.ch_eptr = d_eptr; c.ch_elems = d_elems;
+    c.ch_eslot = reinterpret_cast<const ushort4*>(d_eslot);
+    c.items = d_items;
+    c.rows_max = lim.rows; c.elems_max = lim.elems; c.pairs_max = lim.pairs;
+    c.nchunks = nch;
+    h->chunk_elem_total = (long long)ch_elems.size();
     return SORS_OK;
 }
 
@@ -416,11 +591,9 @@ int compute_external(SorsHandle* h) {
 // unmasked system.
 enum AsmMode { kAsmStep = 0, kAsmMaskedIdentity = 1, kAsmFull = 2 };
 
+// Assembly arguments of the handle at h->q for one evaluation.
 template <typename HT>
-int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmStep) {
-    int st = compute_external(h);
-    if (st) return st;
-    (want_hess ? h->n_hess_evals : h->n_grad_evals)++;
+AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int project) {
     AsmArgs<HT> a;
     a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.tshape = h->tshape;
@@ -428,13 +601,24 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
     a.H = (HT*)h->H; a.nnzb = h->nnzb; a.g_int = h->g_int; a.status = h->status;
     a.stage_per_warp = h->max_pairs * h->nv * 9;
-    a.material = h->s.material; a.project = h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd;
+    a.material = h->s.material; a.project = project;
     a.apply_mask = mode == kAsmFull ? 0 : 1;
     a.neumann_override = mode == kAsmFull ? 0
                          : ((mode == kAsmMaskedIdentity || method(h) == 0) && h->has_neumann) ? 1 : 0;
     a.want_hess = want_hess ? 1 : 0;
     a.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0;
     a.inertia_coef = inertia_coef(h, dt);
+    if (h->asm_variant == 0) a.ch = h->chunks;
+    return a;
+}
+
+template <typename HT>
+int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmStep) {
+    int st = compute_external(h);
+    if (st) return st;
+    (want_hess ? h->n_hess_evals : h->n_grad_evals)++;
+    const int project = h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd;
+    AsmArgs<HT> a = asm_args<HT>(h, dt, want_hess, mode, project);
     launch_assemble<HT>(a, h->max_pairs, h->stream);
     if (want_hess && h->has_pressure && method(h) == 0) {
         PressureArgs p;
@@ -1636,7 +1820,11 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
         launch_tet_shapes(E, h->X, h->conn, h->tshape, h->stream);
         CK(cudaStreamSynchronize(h->stream));
     }
-    if ((st = build_pattern(h, conn))) return bail(st);
+    {
+        PatternHost ph;
+        if ((st = build_pattern(h, conn, &ph))) return bail(st);
+        if ((st = build_tet_chunks(h, conn, X, ph))) return bail(st);
+    }
     const size_t nd = (size_t)3 * N;
     double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,
                        &h->mval, &h->vforce, &h->q_save};
@@ -2149,6 +2337,15 @@ void* sors_stream(SorsHandle* h) { return h ? (void*)h->stream : nullptr; }
 
 int64_t sors_kernel_launch_count(void) { return (int64_t)g_kernel_launches.load(); }
 
+int sors_set_assembly_variant(SorsHandle* h, int32_t variant) {
+    if (!h) return fail(SORS_ERR_ARG, "NULL handle");
+    if (variant != 0 && variant != 1) return fail(SORS_ERR_ARG, "assembly variant must be 0 or 1");
+    h->asm_variant = variant;
+    return SORS_OK;
+}
+
+int64_t sors_assembly_chunks(SorsHandle* h) { return h ? (int64_t)h->chunks.nchunks : 0; }
+
 int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian) {
     if (!h) return 0;
     return with_hessian ? h->n_hess_evals : h->n_grad_evals;
@@ -2169,24 +2366,28 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     // assembly of gradient rows + Hessian block-rows at the current iterate
     int st = eval_system<HT>(h, dt, true);
     if (st) return st;
-    AsmArgs<HT> aa;
-    aa.N = h->N; aa.nv = h->nv; aa.X = h->X; aa.q = h->q; aa.conn = h->conn; aa.mat = h->mat; aa.mus = muscles(h);
-    aa.tshape = h->tshape;
-    aa.pair_ptr = h->pair_ptr; aa.pair_ev = h->pair_ev; aa.row_ptr = h->row_ptr; aa.col = h->col;
-    aa.slot_item_ptr = h->slot_item_ptr; aa.slot_items = h->slot_items; aa.node_mask = h->node_mask; aa.mass = h->mass;
-    aa.H = (HT*)h->H; aa.nnzb = h->nnzb; aa.g_int = h->g_int; aa.status = h->status; aa.stage_per_warp = h->max_pairs * h->nv * 9;
-    aa.material = h->s.material; aa.project = h->s.project_spd == 1; aa.apply_mask = 1;  // as a step assembles
-    aa.neumann_override = (method(h) == 0 && h->has_neumann) ? 1 : 0; aa.want_hess = 1;
-    aa.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0; aa.inertia_coef = inertia_coef(h, dt);
+    // as a step assembles (the adaptive projection's first try is the exact Hessian)
+    AsmArgs<HT> aa = asm_args<HT>(h, dt, true, kAsmStep, h->s.project_spd == 1);
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++) launch_assemble<HT>(aa, h->max_pairs, h->stream);
     CK(cudaEventRecord(b, h->stream));
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&ms, a, b));
     out->assemble_ms = ms / iters;
-    // compulsory bytes: conn, (mu,lambda), X, q, mask, mass, pair lists, slot maps, pattern; H and gradient out
-    out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
-                          (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
+    if (aa.ch.nchunks > 0 && nv == 4 && !aa.project && !aa.mus.group) {
+        // chunked element-owner kernel, each compulsory input and output once:
+        // conn, shape gradients + volume, (mu, lambda); q, mask, mass; chunk rows
+        // and element lists with their owned-vertex slots; pair counts, pattern
+        // and slot items; H and gradient out
+        const double ch_elems = (double)h->chunk_elem_total;
+        out->assemble_bytes = E * (16 + 80 + 16) + N * (24 + 1 + 8) + (N + 4 * (double)h->chunks.nchunks) * 4 +
+                              ch_elems * (4 + 8) + (N + 1) * 4 * 2 + (nnzb + 1) * 4 + nnzb * 4 + E * nv * nv * 2 +
+                              nnzb * 9 * hs + N * 24;
+    } else {
+        // compulsory bytes: conn, (mu,lambda), X, q, mask, mass, pair lists, slot maps, pattern; H and gradient out
+        out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
+                              (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
+    }
     // PCG kernels on the assembled system
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,

@@ -120,6 +120,19 @@ static inline long long cap_grid(long long b) {
     return b < 1 ? 1 : b;
 }
 
+// Streaming multiprocessors of the current device (looked up once per device).
+static int sm_count() {
+    static std::atomic<int> cache[kMaxDevices];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n <= 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+        cache[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
+}
+
 static inline int red_grid(long long n, int per_thread = 1) {
     long long b = (n + (long long)kRedThreads * per_thread - 1) / ((long long)kRedThreads * per_thread);
     if (b < 1) b = 1;
@@ -644,6 +657,294 @@ __global__ void __launch_bounds__(256, NV == 4 ? (sizeof(HT) == 4 ? ((SNH || PRO
     }
 }
 
+// ---------------------------------------------------------------------------
+// Element-owner tet assembly over node chunks (exact Neo-Hookean and stable
+// Neo-Hookean Hessians).  One block per chunk of nearby nodes:
+//   A. each element incident to the chunk is evaluated once (F, cofactor, J,
+//      log J and P in FP64, as tet_row_stage) into a Hessian generator in
+//      shared memory, and V P d_v is stored for every vertex v the chunk owns;
+//   B. one thread per CSR block of the chunk's rows sums the block's items in
+//      their fixed order, expanding block (v, w) of element e from its
+//      generator:  hmu (d_v . d_w) I + h1 a_v a_w^T - h2 a_w a_v^T
+//      [+ h4 f_v f_w^T], a_v = F^-T d_v, f_v = F d_v (the same terms, in the
+//      same Hessian type, as the row-owner kernel), and writes it once;
+//   C. one thread per row sums its gradient pairs in their fixed order.
+// No atomics, a fixed order everywhere: bit-reproducible.
+// ---------------------------------------------------------------------------
+constexpr int kChunkThreads = 256;
+
+// generator fields per element: hmu, h1, h2, a_v (12), d_v . d_w (10, v <= w);
+// stable Neo-Hookean adds h4 and f_v (12)
+template <bool SNH>
+struct ChunkGen {
+    static constexpr int kA = 3, kDD = 15, kH4 = 25, kF = 26;
+    static constexpr int kFields = SNH ? 38 : 25;
+};
+
+__device__ __forceinline__ int dd_index(int v, int w) {
+    // v <= w: (0,0..3) -> 0..3, (1,1..3) -> 4..6, (2,2..3) -> 7..8, (3,3) -> 9
+    return v * 4 - (v * (v - 1)) / 2 + (w - v);
+}
+
+ChunkLimits chunk_limits(int hsize, int material) {
+    const bool snh = material == 2;
+    if (hsize == 4) return snh ? ChunkLimits{64, 384, 1152} : ChunkLimits{64, 512, 1536};
+    return snh ? ChunkLimits{32, 192, 576} : ChunkLimits{32, 256, 768};
+}
+
+size_t chunk_smem_bytes(int hsize, int material) {
+    const ChunkLimits l = chunk_limits(hsize, material);
+    const int nf = material == 2 ? ChunkGen<true>::kFields : ChunkGen<false>::kFields;
+    return (size_t)l.pairs * 3 * sizeof(double) + (size_t)nf * l.elems * hsize + (size_t)(4 * l.rows + 2) * sizeof(int);
+}
+
+template <typename HT, bool SNH>
+__global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT> a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using G = ChunkGen<SNH>;
+    const int EM = a.ch.elems_max;
+    double* gslot = reinterpret_cast<double*>(smem_raw);
+    HT* gen = reinterpret_cast<HT*>(gslot + 3 * (size_t)a.ch.pairs_max);
+    int* srow = reinterpret_cast<int*>(gen + (size_t)G::kFields * EM);
+    int* srp0 = srow + a.ch.rows_max;
+    int* spair0 = srp0 + a.ch.rows_max;
+    int* sblk0 = spair0 + a.ch.rows_max + 1;
+    const int chunk = blockIdx.x;
+    const int r0 = __ldg(a.ch.ch_ptr + chunk), nr = __ldg(a.ch.ch_ptr + chunk + 1) - r0;
+    const int e0 = __ldg(a.ch.ch_eptr + chunk), ne = __ldg(a.ch.ch_eptr + chunk + 1) - e0;
+    const int lane = threadIdx.x & 31;
+    // chunk rows: node id, first CSR block, and chunk-local pair / block offsets
+    if (threadIdx.x < 32) {
+        int pacc = 0, bacc = 0;
+        for (int base = 0; base < nr; base += 32) {
+            const int p = base + lane;
+            int r = 0, rp = 0, np = 0, nb = 0;
+            if (p < nr) {
+                r = __ldg(a.ch.ch_rows + r0 + p);
+                np = __ldg(a.pair_ptr + r + 1) - __ldg(a.pair_ptr + r);
+                rp = __ldg(a.row_ptr + r);
+                nb = __ldg(a.row_ptr + r + 1) - rp;
+            }
+            int ip = np, ib = nb;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int tp = __shfl_up_sync(0xffffffffu, ip, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
+                if (lane >= o) { ip += tp; ib += tb; }
+            }
+            if (p < nr) { srow[p] = r; srp0[p] = rp; spair0[p] = pacc + ip - np; sblk0[p] = bacc + ib - nb; }
+            pacc += __shfl_sync(0xffffffffu, ip, 31);
+            bacc += __shfl_sync(0xffffffffu, ib, 31);
+        }
+        if (lane == 0) { spair0[nr] = pacc; sblk0[nr] = bacc; }
+    }
+    // A. element generators and gradient pairs
+    bool ok = true;
+    for (int s = threadIdx.x; s < ne; s += blockDim.x) {
+        const int e = __ldg(a.ch.ch_elems + e0 + s);
+        const ushort4 sl = a.ch.ch_eslot[e0 + s];
+        const double2* ts = reinterpret_cast<const double2*>(a.tshape + (size_t)e * 10);
+        double t[10];
+#pragma unroll
+        for (int k = 0; k < 5; k++) {
+            const double2 u = __ldg(ts + k);
+            t[2 * k] = u.x; t[2 * k + 1] = u.y;
+        }
+        const int4 cn = __ldg(reinterpret_cast<const int4*>(a.conn) + e);
+        const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
+        double d[4][3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            d[0][c] = t[c]; d[1][c] = t[3 + c]; d[2][c] = t[6 + c];
+            d[3][c] = -(t[c] + t[3 + c] + t[6 + c]);
+        }
+        const double V = t[9];
+        double F[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) F[k] = 0.0;
+#pragma unroll
+        for (int w = 0; w < 4; w++) {
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                const double xr = a.q[3 * (size_t)nodes[w] + r];
+#pragma unroll
+                for (int c = 0; c < 3; c++) F[r * 3 + c] += xr * d[w][c];
+            }
+        }
+        const double2 m = __ldg(a.mat + e);
+        double C[9];
+        cof3(F, C);
+        const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+        const double iJ = 1.0 / J;
+        double IC = 0.0;
+        if (SNH) {
+#pragma unroll
+            for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+        }
+        const double alpha = SNH ? 1.0 + 0.75 * m.x / m.y : 0.0;
+        const double logJ = SNH ? 0.0 : log(J);
+        const double pa = SNH ? m.x * (1.0 - 1.0 / (IC + 1.0)) : m.x;
+        const double pb = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
+        double P[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) P[k] = pa * F[k] + pb * C[k] * iJ;
+        const unsigned short slots[4] = {sl.x, sl.y, sl.z, sl.w};
+#pragma unroll
+        for (int v = 0; v < 4; v++) {
+            if (slots[v] == 0xffff) continue;
+#pragma unroll
+            for (int r = 0; r < 3; r++) {
+                double pr = 0.0;
+#pragma unroll
+                for (int c = 0; c < 3; c++) pr += P[r * 3 + c] * d[v][c];
+                gslot[3 * slots[v] + r] = V * pr;
+            }
+        }
+        const bool eok = SNH ? (J != 0.0) : (J > 0.0);
+        ok &= eok;
+        if (!a.want_hess) continue;
+        if (!eok) {
+#pragma unroll
+            for (int f = 0; f < G::kFields; f++) gen[f * EM + s] = HT(0);
+            continue;
+        }
+        HT Gh[9], dh[4][3];
+#pragma unroll
+        for (int k = 0; k < 9; k++) Gh[k] = (HT)(C[k] * iJ);
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+#pragma unroll
+            for (int c = 0; c < 3; c++) dh[v][c] = (HT)d[v][c];
+        gen[0 * EM + s] = (HT)(V * pa);
+        gen[1 * EM + s] = (HT)(SNH ? V * m.y * (2.0 * J - alpha) * J : V * m.y);
+        gen[2 * EM + s] = (HT)(V * pb);
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                gen[(G::kA + v * 3 + r) * EM + s] = Gh[r * 3 + 0] * dh[v][0] + Gh[r * 3 + 1] * dh[v][1] + Gh[r * 3 + 2] * dh[v][2];
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+#pragma unroll
+            for (int w = v; w < 4; w++)
+                gen[(G::kDD + dd_index(v, w)) * EM + s] = dh[v][0] * dh[w][0] + dh[v][1] * dh[w][1] + dh[v][2] * dh[w][2];
+        if (SNH) {
+            gen[G::kH4 * EM + s] = (HT)(V * 2.0 * m.x / ((IC + 1.0) * (IC + 1.0)));
+            HT Fh[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
+#pragma unroll
+            for (int v = 0; v < 4; v++)
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+                    gen[(G::kF + v * 3 + r) * EM + s] = Fh[r * 3 + 0] * dh[v][0] + Fh[r * 3 + 1] * dh[v][1] + Fh[r * 3 + 2] * dh[v][2];
+        }
+    }
+    if (!ok) atomicOr(a.status, kFlagInverted);
+    __syncthreads();
+    // B. Hessian blocks of the chunk's rows
+    if (a.want_hess) {
+        const int total = sblk0[nr];
+        for (int lb = threadIdx.x; lb < total; lb += blockDim.x) {
+            int lo = 0, hi = nr - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sblk0[mid] <= lb) lo = mid; else hi = mid - 1;
+            }
+            const int row = srow[lo];
+            const int bg = srp0[lo] + (lb - sblk0[lo]);
+            const int i0 = __ldg(a.slot_item_ptr + bg), i1 = __ldg(a.slot_item_ptr + bg + 1);
+            HT acc[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) acc[k] = HT(0);
+            for (int it = i0; it < i1; ++it) {
+                const unsigned item = __ldg(a.ch.items + it);
+                const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
+                const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
+                const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
+                HT av[3], aw[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                    aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
+                }
+                HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
+                if (SNH) {
+                    h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
+                        fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+#pragma unroll
+                    for (int l = 0; l < 3; l++) {
+                        HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
+                        if (SNH) val += h4 * fv[k] * fw[l];
+                        if (k == l) val += hmu * dd;
+                        acc[k * 3 + l] += val;
+                    }
+            }
+            const int j = __ldg(a.col + bg);
+            const unsigned mrow = a.node_mask[row], mcol = a.node_mask[j];
+            const double md = a.inertia_coef * a.mass[row];
+#pragma unroll
+            for (int rc = 0; rc < 9; rc++) {
+                const int r = rc / 3, c = rc - 3 * (rc / 3);
+                const bool rmask = (mrow >> r) & 1u;
+                double val = (double)acc[rc] * a.hscale;
+                if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
+                if (j == row && r == c) {
+                    val += md;
+                    if (a.neumann_override && rmask) val = 1.0;
+                }
+                a.H[hval(bg, rc, a.nnzb)] = (HT)val;
+            }
+        }
+    }
+    // C. gradient rows
+    for (int p = threadIdx.x; p < nr; p += blockDim.x) {
+        const int row = srow[p];
+        double g0 = 0.0, g1 = 0.0, g2 = 0.0;
+        for (int k = spair0[p]; k < spair0[p + 1]; k++) {
+            g0 += gslot[3 * k]; g1 += gslot[3 * k + 1]; g2 += gslot[3 * k + 2];
+        }
+        const unsigned mrow = a.node_mask[row];
+        if (a.apply_mask) {
+            if (mrow & 1u) g0 = 0.0;
+            if (mrow & 2u) g1 = 0.0;
+            if (mrow & 4u) g2 = 0.0;
+        }
+        a.g_int[3 * (size_t)row + 0] = g0;
+        a.g_int[3 * (size_t)row + 1] = g1;
+        a.g_int[3 * (size_t)row + 2] = g2;
+    }
+}
+
+// Raises a kernel's dynamic shared-memory limit to `smem` once per device
+// (the attribute is per device; `done` remembers the largest size set on each).
+template <typename K>
+static void set_smem_limit(K kernel, size_t smem, std::atomic<int>* done) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) dev = 0;
+    if (done[dev].load(std::memory_order_relaxed) >= (int)smem) return;
+    cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int cur = done[dev].load(std::memory_order_relaxed);
+    while (cur < (int)smem && !done[dev].compare_exchange_weak(cur, (int)smem)) {
+    }
+}
+
+template <typename HT, bool SNH>
+static void launch_assemble_chunk(const AsmArgs<HT>& a, cudaStream_t st) {
+    static std::atomic<int> limit[kMaxDevices];
+    auto k = k_assemble_chunk<HT, SNH>;
+    const size_t smem = chunk_smem_bytes(sizeof(HT), SNH ? 2 : 0);
+    set_smem_limit(k, smem, limit);
+    k<<<a.ch.nchunks, kChunkThreads, smem, st>>>(a);
+    counted();
+}
+
 template <typename HT>
 void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     if (a.N == 0) return;
@@ -655,20 +956,28 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     int threads = wpb * 32;
     long long rows_per_block = wpb;
     long long blocks = (a.N + rows_per_block - 1) / rows_per_block;
-    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks > (long long)sm_count() * 64) blocks = (long long)sm_count() * 64;
     blocks = cap_grid(blocks);
     const bool snh = a.material == 2;
+    if (nv == 4 && a.ch.nchunks > 0 && !a.project && !a.mus.group && (a.material == 0 || snh)) {
+        if (snh) launch_assemble_chunk<HT, true>(a, st);
+        else launch_assemble_chunk<HT, false>(a, st);
+        return;
+    }
     if (nv == 4) {
         // tets: projection selects the kernel variant (the exact Hessian keeps
         // the projection's registers out of the common case)
+        static std::atomic<int> limit[4][kMaxDevices];
+        const int variant = (snh ? 2 : 0) + (a.project ? 1 : 0);
         auto k = snh ? (a.project ? k_assemble<HT, 4, true, true> : k_assemble<HT, 4, true, false>)
                      : (a.project ? k_assemble<HT, 4, false, true> : k_assemble<HT, 4, false, false>);
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_limit(k, smem, limit[variant]);
         k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
     } else {
+        static std::atomic<int> limit[2][kMaxDevices];
         auto k = snh ? k_assemble<HT, 8, true, false> : k_assemble<HT, 8, false, false>;
-        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_limit(k, smem, limit[snh ? 1 : 0]);
         k<<<(int)blocks, threads, smem, st>>>(a);
         counted();
     }

@@ -21,6 +21,7 @@ enum : int { kFlagInverted = 1, kFlagPcgBreakdown = 2, kFlagNaN = 4, kFlagTimeou
 constexpr int kRedBlocks = 1184;      // 148 SMs x 8
 constexpr int kRedThreads = 256;
 constexpr int kMaxScalars = 4;
+constexpr int kMaxDevices = 64;  // per-device caches of launch attributes
 
 struct DevScalars {
     // Newton / energy reductions
@@ -57,6 +58,32 @@ __host__ __device__ __forceinline__ size_t hval(size_t b, int rc, size_t nnzb) {
     return 9 * b + (size_t)rc;
 }
 
+// Element-owner tet assembly over node chunks (kernels.cu k_assemble_chunk).
+// At mesh load the nodes are cut into chunks of nearby nodes (Morton order of
+// the undeformed positions); a chunk lists the elements incident to any of its
+// nodes, each once, and for each of those elements the chunk-local pair slot
+// of every vertex the chunk owns.  The Hessian items (one per element block
+// that sums into a CSR block) follow slot_item_ptr's order, re-encoded as
+// (chunk-local element << 4 | v << 2 | w).
+struct ChunkArgs {
+    int nchunks = 0;
+    const int* ch_ptr = nullptr;        // nchunks+1: positions in ch_rows
+    const int* ch_rows = nullptr;       // node ids, chunk by chunk
+    const int* ch_eptr = nullptr;       // nchunks+1: positions in ch_elems
+    const int* ch_elems = nullptr;      // element ids, chunk by chunk
+    const ushort4* ch_eslot = nullptr;  // chunk-local pair slot of local vertex v (0xffff: not owned)
+    const uint16_t* items = nullptr;    // one per slot item, same order as slot_items
+    int rows_max = 0, elems_max = 0, pairs_max = 0;
+};
+
+// Chunk limits and shared-memory size of the chunked assembly for a Hessian
+// type size (4 or 8 bytes) and material (0 Neo-Hookean, 2 stable Neo-Hookean).
+struct ChunkLimits {
+    int rows, elems, pairs;
+};
+ChunkLimits chunk_limits(int hsize, int material);
+size_t chunk_smem_bytes(int hsize, int material);
+
 // Row-owner assembly arguments (tet or hex).
 template <typename HT>
 struct AsmArgs {
@@ -87,6 +114,7 @@ struct AsmArgs {
     int want_hess;
     double hscale;          // 0.5 for Crank-Nicolson with dt != 0
     double inertia_coef;    // diag m * coef
+    ChunkArgs ch;           // element-owner tet assembly (used when ch.nchunks > 0)
 };
 
 struct PressureArgs {

@@ -89,6 +89,10 @@ def estimate_device_bytes(n_nodes: int, n_elems: int, nodes_per_elem: int, preci
     b += 9 * nnzb * hs                     # Hessian values
     b += 4 * nnzb * 2 + 4 * n_nodes * 4    # pattern + slot pointers
     b += 4 * n_elems * nv * 2 + 2 * n_elems * nv * nv + 16 * n_elems  # conn, pairs, slot items, materials
+    if nv == 4:
+        # element-owner assembly: tet shapes, node chunks (chunk element lists
+        # hold each element ~1.5 times with its owned-vertex slots) and items
+        b += 80 * n_elems + 4 * n_nodes + int(1.5 * n_elems) * 12 + 2 * n_elems * nv * nv
     return int(b * 1.1) + (1 << 20)
 
 
