@@ -50,11 +50,25 @@ def workload_name(cells, precision):
             f"x=0 clamped, gravity, backward Euler dt 5e-3, {precision}")
 
 
-def block_mesh(cells, seed=0):
+_shuffle = False
+
+
+def block_mesh(cells, seed=0, shuffle=None):
+    """The jittered block; with shuffle, its nodes and elements renumbered by a
+    seeded random permutation (the numbering of a mesh read from a file)."""
     from sors_b200 import meshes
     nx, ny, nz = cells
     h = SIZE[0] / CELLS[0]
     X, T, E = meshes.jittered_block_tets(nx, ny, nz, (nx * h, ny * h, nz * h), jitter=0.1, seed=seed)
+    if _shuffle if shuffle is None else shuffle:
+        rng = np.random.default_rng(seed + 1000)
+        perm = rng.permutation(X.shape[0])
+        inv = np.empty_like(perm)
+        inv[perm] = np.arange(perm.size)
+        eperm = rng.permutation(T.shape[0])
+        X = X[perm]
+        T = inv[T[eperm]].astype(np.int32)
+        E = E[eperm]
     mask, val = meshes.clamp_mask(X)
     return X, T, E, mask, val
 
@@ -156,7 +170,7 @@ def ncu_traffic(kernel_key, units):
 # ---------------------------------------------------------------------------
 def cpu_sample_run(steps, warmup, threads=None):
     from oracle import oracle as orc
-    X, T, E, mask, val = block_mesh(SAMPLE_CELLS, seed=0)
+    X, T, E, mask, val = block_mesh(SAMPLE_CELLS, seed=0, shuffle=False)
     nthreads = threads or os.cpu_count() or 1
     o = orc.System(X, T, rho=1070.0, youngs=E, nu=0.45, grav=(0, 0, -9.81), scheme="backward_euler",
                    method="minimize_newton", dt=DT, substeps=1, nthreads=nthreads)
@@ -186,7 +200,7 @@ def cpu_phases(threads=None):
     Energy::compute_hessian with triplets -> CSR (cpp/src/energy.cpp:312-390)
     of the whole 3.0M-tet block, by the CPU restatement (FP64, OpenMP)."""
     from oracle import oracle as orc
-    X, T, E, mask, val = block_mesh(CELLS, seed=0)
+    X, T, E, mask, val = block_mesh(CELLS, seed=0, shuffle=False)
     nthreads = threads or os.cpu_count() or 1
     o = orc.System(X, T, rho=1070.0, youngs=E, nu=0.45, grav=(0, 0, -9.81), scheme="backward_euler",
                    method="minimize_newton", dt=DT, substeps=1, nthreads=nthreads)
@@ -375,6 +389,7 @@ def run_gpu(args, rank, world, local_rank):
                    "newton": "||dx||<1e-9 or ||g||<1e-8, Eisenstat-Walker PCG forcing",
                    "hessian_projection": _projection,
                    "preconditioner": "two-level" if _two_level else "block Jacobi",
+                   "numbering": "random permutation" if _shuffle else "grid order (x fastest)",
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (assembled system ~1 GB resident), no flush"},
         "newton_steps_per_s": world * args.steps / (ms / 1e3),
@@ -418,44 +433,52 @@ def run_gpu(args, rank, world, local_rank):
 def run_c3(args):
     """Pressure-actuated arm: voxelised cylinder (R 20 mm, L 200 mm, h 1.25 mm) with
     three closed chambers, base clamped, E 3e5, nu 0.48; static Newton solve per
-    load level, 10 levels 0 -> 50 kPa on one chamber.  One line per precision."""
+    load level, 10 levels 0 -> 50 kPa, on one chamber and on all three.  As in
+    python/d04_sopra.py:73-85 the largest surface group (the outer skin) is
+    dropped and the remaining groups (the chamber walls) are the pressure
+    groups.  One line per (load case, precision)."""
     import torch
     from sors_b200 import meshes
     from sors_b200 import py_sors as ps
     torch.cuda.set_device(0)
     X, H = meshes.voxel_cylinder(radius=0.02, length=0.2, h=1.25e-3, cap_layers=2)
     groups, _ = meshes.extract_surfaces(X, H)
+    groups.pop(int(np.argmax([len(g) for g in groups])))
     faces = np.concatenate(groups)
     gid = np.concatenate([np.full(len(g), k) for k, g in enumerate(groups)])
     mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
-    for precision in ("mixed", "fp64"):
-        s = ps.SimulationSettings()
-        s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
-        s.precision = precision; s.newtonResidualTol = 1e-8
-        # static follower loads: with the exact Hessian (adaptive) the inexact
-        # Newton stalls on this arm; the always-projected Hessian converges
-        s.hessianProjection = True
-        fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
-        en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
-                                      poissonsRatio=0.48, neumannBCmask=mask, neumannBCvalue=np.zeros(mask.size),
-                                      forceTypesList=["pressure"], forceParameterList=fp)
-        sol = ps.Solver(s)
-        q = X.ravel().copy()
-        levels, newton, pcg = 10, 0, 0
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for lvl in range(1, levels + 1):
-            pr = np.zeros((len(groups), 1)); pr[1, 0] = 5e3 * lvl
-            q = sol.step(q, en, ps.Params(["pressure"], [pr]), 0.0)
-            newton += sol.last_stats.newton_iters; pcg += sol.last_stats.pcg_iters
-        wall = time.perf_counter() - t0
-        print(json.dumps({"workload": "c3 pressure-actuated hex arm, static 10-level ramp to 50 kPa (one chamber)",
-                          "precision": precision, "hessian_projection": "true",
-                          "hexes": int(H.shape[0]), "nodes": int(X.shape[0]),
-                          "surface_groups": len(groups), "s_per_load_level": wall / levels,
-                          "newton_iters_per_level": newton / levels, "pcg_iters_per_level": pcg / levels,
-                          "tip_displacement_max_m": float(np.abs(q - X.ravel()).max())}), flush=True)
-        del en
+    for case, chambers in (("one chamber", [0]), ("all three chambers", list(range(len(groups))))):
+        for precision in ("mixed", "fp64"):
+            s = ps.SimulationSettings()
+            s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
+            s.precision = precision; s.newtonResidualTol = 1e-8
+            s.hessianProjection = PROJECTION[args.c3_projection]
+            fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
+            en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
+                                          poissonsRatio=0.48, neumannBCmask=mask,
+                                          neumannBCvalue=np.zeros(mask.size), forceTypesList=["pressure"],
+                                          forceParameterList=fp)
+            sol = ps.Solver(s)
+            q = X.ravel().copy()
+            levels, newton, pcg = 10, 0, 0
+            err = None
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            try:
+                for lvl in range(1, levels + 1):
+                    pr = np.zeros((len(groups), 1)); pr[chambers, 0] = 5e3 * lvl
+                    q = sol.step(q, en, ps.Params(["pressure"], [pr]), 0.0)
+                    newton += sol.last_stats.newton_iters; pcg += sol.last_stats.pcg_iters
+            except RuntimeError as ex:
+                err = f"level {lvl}: {ex}"
+            wall = time.perf_counter() - t0
+            print(json.dumps({"workload": f"c3 pressure-actuated hex arm, static 10-level ramp to 50 kPa ({case})",
+                              "precision": precision, "hessian_projection": args.c3_projection,
+                              "hexes": int(H.shape[0]), "nodes": int(X.shape[0]), "chambers": len(groups),
+                              "s_per_load_level": wall / levels, "newton_iters_per_level": newton / levels,
+                              "pcg_iters_per_level": pcg / levels, "error": err,
+                              "tip_displacement_max_m": float(np.abs(q - X.ravel()).max())}), flush=True)
+            del en
 
 
 def c4_case(seed, steps):
@@ -475,19 +498,28 @@ def c4_case(seed, steps):
     return X, H, E, act, surf
 
 
-def c4_energy(X, H, E, surf, precision="fp64"):
+def c4_energy(X, H, E, surf, precision="fp64", members=1):
+    """Energy/Solver of `members` copies of the C4 bar in one handle (a union:
+    the copies share no element, so the system, its contacts and its adjoint
+    are the direct sum of the copies'; every kernel launch serves all of them).
+    Each element is its own muscle group."""
     from sors_b200 import py_sors as ps
     s = ps.SimulationSettings()
     s.meshType = "Hexahedron"; s.dt = 2e-3; s.timeSteppingScheme = "backward_euler"
     s.solverMethod = "minimize_SQP"; s.precision = precision
-    ne = H.shape[0]
-    en = ps.EnergyHex.from_arrays(X, H, s, np.array([0.0, 0.0, -9.81]), 0.0, density=1070.0, youngsModulus=E,
+    n1, e1 = X.shape[0], H.shape[0]
+    Xu = np.tile(X, (members, 1))
+    Hu = np.concatenate([H + k * n1 for k in range(members)]).astype(np.int32)
+    su = np.concatenate([surf + k * n1 for k in range(members)])
+    ne = e1 * members
+    Eu = np.broadcast_to(np.asarray(E, float), (ne,)).copy() if np.size(E) in (1, ne) else np.tile(E, members)
+    en = ps.EnergyHex.from_arrays(Xu, Hu, s, np.array([0.0, 0.0, -9.81]), 0.0, density=1070.0, youngsModulus=Eu,
                                   poissonsRatio=0.45, muscleGroup=np.arange(ne), softconStiffness=np.full(ne, 5e4),
                                   softconDirection=np.tile([1.0, 0.0, 0.0], (ne, 1)))
     cp = ps.Params()
     cp.set_param("positionVectorListPlanes", np.zeros(3))
     cp.set_param("normalVectorListPlanes", np.array([0.0, 0.0, 1.0]))
-    cp.set_param("surfaceVerticesIdx", surf.astype(float))
+    cp.set_param("surfaceVerticesIdx", su.astype(float))
     en._setup_constraints_forces(["planeContact"], cp, (), None)
     return en, ps.Solver(s)
 
@@ -500,79 +532,66 @@ def c4_mass(X, H):
 
 
 def run_c4(args):
-    """Gradient of the C4 loss w.r.t. per-element E and a_e(t) by the adjoint:
-    seeds run concurrently (one handle and stream each); the directional
-    derivative is checked against central differences (h = 1e-6) of the GPU
-    FP64 forward along seeded directions."""
-    import threading
-
+    """Gradient of the C4 loss w.r.t. per-element E and a_e(t) by the adjoint,
+    for `seeds` activation seeds in one union handle (one forward and one
+    backward pass serve all of them).  The directional derivative of seed 0
+    along `fd_dirs` seeded directions is checked against central differences
+    (h = 1e-6) of the GPU FP64 forward, all directions in one union of
+    2 x fd_dirs perturbed copies."""
     import torch
     from sors_b200.adjoint import RolloutAdjoint
     torch.cuda.set_device(0)
-    steps = args.c4_steps
-    dt = 2e-3
-    cases = [c4_case(sd, steps) for sd in range(args.seeds)]
-    runners = []
-    for X, H, E, act, surf in cases:
-        en, sol = c4_energy(X, H, E, surf)
-        runners.append((RolloutAdjoint(en, sol, steps, dt, poisson=0.45, checkpoint_every=args.checkpoint_every),
-                        en))
-    m = c4_mass(cases[0][0], cases[0][1])
+    steps, dt, S = args.c4_steps, 2e-3, args.seeds
+    X, H, E, _, surf = c4_case(0, steps)
+    n1, e1 = X.shape[0], H.shape[0]
+    acts = [c4_case(sd, steps)[3] for sd in range(S)]
+    act_u = np.concatenate(acts, axis=1)                      # (T, S * e1): group = union element
+    E_u = np.tile(E, S)
+    m = c4_mass(X, H)
 
-    def loss_grad(k, out):
-        try:
-            r, en = runners[k]
-            _, H, E, act, _ = cases[k]
-            t0 = time.perf_counter()
-            qT = r.forward(E, act)
-            t1 = time.perf_counter()
-            z = (qT[2::3] * m).sum() / m.sum()
-            dq = np.zeros_like(qT)
-            dq[2::3] = 2 * (z - 0.08) * m / m.sum()
-            gE, gA, _, _ = r.backward(dq)
-            t2 = time.perf_counter()
-            out[k] = ((z - 0.08) ** 2, gE, gA, t1 - t0, t2 - t1, r.last_pcg_iters)
-        except Exception as ex:  # reported below
-            out[k] = ex
+    def losses(qT, members):
+        z = (qT.reshape(members, n1, 3)[:, :, 2] * m).sum(axis=1) / m.sum()
+        return (z - 0.08) ** 2, z
 
-    res = {}
-    threads = [threading.Thread(target=loss_grad, args=(k, res)) for k in range(len(cases))]
+    en, sol = c4_energy(X, H, E, surf, members=S)
+    r = RolloutAdjoint(en, sol, steps, dt, poisson=0.45, checkpoint_every=args.checkpoint_every)
+    torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for th in threads:
-        th.start()
-    for th in threads:
-        th.join()
-    wall = time.perf_counter() - t0
-    errors = [str(v) for v in res.values() if isinstance(v, Exception)]
-    if errors:
-        print(json.dumps({"workload": "c4", "errors": errors}), flush=True)
-        return
-    r, en = runners[0]
-    _, H, E, act, _ = cases[0]
-
-    def L(Ev, Av):
-        q = r.forward(Ev, Av)
-        return ((q[2::3] * m).sum() / m.sum() - 0.08) ** 2
-
-    loss0, gE, gA = res[0][0], res[0][1], res[0][2]
+    qT = r.forward(E_u, act_u)
+    t1 = time.perf_counter()
+    Ls, z = losses(qT, S)
+    dq = np.zeros((S, n1, 3))
+    dq[:, :, 2] = (2 * (z - 0.08))[:, None] * m[None, :] / m.sum()
+    gE, gA, _, _ = r.backward(dq.ravel())
+    t2 = time.perf_counter()
+    fwd_iters = r.last_pcg_iters
+    del r, en, sol
+    # central differences for seed 0: member 2d = +h r_d, member 2d + 1 = -h r_d
+    D, h = args.fd_dirs, 1e-6
     rng = np.random.default_rng(99)
-    errs = []
-    h = 1e-6
-    for _ in range(args.fd_dirs):
-        rE = rng.standard_normal(E.size); rA = rng.standard_normal(act.shape)
-        d_adj = gE @ (E * rE) + (gA * rA).sum()
-        d_fd = (L(E * (1 + h * rE), act + h * rA) - L(E * (1 - h * rE), act - h * rA)) / (2 * h)
-        errs.append(abs(d_adj - d_fd) / max(abs(d_fd), 1e-300))
-    X = cases[0][0]
-    print(json.dumps({"workload": "c4 SoftCon hex bar 40x8x8 dropped from 0.05 m on z=0, adjoint of E and a_e(t), "
-                                  "FP64", "hexes": int(H.shape[0]), "nodes": int(X.shape[0]), "steps": steps,
-                      "seeds": len(cases), "gradients_per_s": len(cases) / wall, "wall_s": wall,
-                      "forward_ms_per_step": 1e3 * float(np.mean([v[3] for v in res.values()])) / steps,
-                      "backward_ms_per_step": 1e3 * float(np.mean([v[4] for v in res.values()])) / steps,
-                      "adjoint_pcg_iters_per_step": float(np.mean([v[5] for v in res.values()])) / steps,
-                      "checkpoint_every": args.checkpoint_every, "loss_seed0": loss0,
-                      "fd_directions": args.fd_dirs, "fd_h": h, "fd_max_rel_err": max(errs) if errs else None,
-                      "active_contacts_last_step": en.active_contacts()}), flush=True)
+    dirs = [(rng.standard_normal(e1), rng.standard_normal((steps, e1))) for _ in range(D)]
+    d_adj = np.array([gE[:e1] @ (E * rE) + (gA[:, :e1] * rA).sum() for rE, rA in dirs])
+    Efd = np.concatenate([E * (1 + sg * h * rE) for rE, _ in dirs for sg in (1, -1)])
+    Afd = np.concatenate([acts[0] + sg * h * rA for _, rA in dirs for sg in (1, -1)], axis=1)
+    en2, sol2 = c4_energy(X, H, Efd, surf, members=2 * D)
+    r2 = RolloutAdjoint(en2, sol2, steps, dt, poisson=0.45, checkpoint_every=steps)
+    t3 = time.perf_counter()
+    qfd = r2.forward(Efd, Afd)
+    t4 = time.perf_counter()
+    Lfd, _ = losses(qfd, 2 * D)
+    d_fd = (Lfd[0::2] - Lfd[1::2]) / (2 * h)
+    errs = np.abs(d_adj - d_fd) / np.maximum(np.abs(d_fd), 1e-300)
+    print(json.dumps({"workload": f"c4 SoftCon hex bar 40x8x8 dropped from 0.05 m on z=0, adjoint of E and a_e(t), "
+                                  f"FP64, {S} seeds in one union handle",
+                      "hexes_per_seed": int(e1), "nodes_per_seed": int(n1), "hexes_total": int(e1 * S),
+                      "steps": steps, "seeds": S, "gradients_per_s": S / (t2 - t0), "wall_s": t2 - t0,
+                      "forward_ms_per_step": 1e3 * (t1 - t0) / steps, "backward_ms_per_step": 1e3 * (t2 - t1) / steps,
+                      "adjoint_pcg_iters_per_step": fwd_iters / steps, "checkpoint_every": args.checkpoint_every,
+                      "loss_seed0": float(Ls[0]), "loss_mean": float(Ls.mean()),
+                      "fd_directions": D, "fd_h": h, "fd_forward_s": t4 - t3,
+                      "fd_max_rel_err": float(errs.max()) if D else None,
+                      "fd_vs": "central differences of the GPU FP64 forward (union of 2 x fd_directions copies)",
+                      "directional_derivatives": d_adj.tolist()}), flush=True)
 
 
 def run_serve(args):
@@ -679,6 +698,8 @@ def main():
                     help="SPD projection of the element Hessians: always, never, or only where PCG meets "
                          "negative curvature")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--shuffle", action="store_true",
+                    help="renumber the block's nodes and elements by a seeded random permutation")
     ap.add_argument("--no-phases", action="store_true",
                     help="skip the full-size CPU gradient / Hessian assembly timing (about 30 s of host work)")
     ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4", "serve"],
@@ -691,17 +712,20 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="serve: rollouts packed into one union handle (1: none; unions measured slower on the poke mix)")
     ap.add_argument("--baseline-sample", type=int, default=0,
                     help="serve: measure the sequential FP64 baseline on the first K requests (0 = all)")
-    ap.add_argument("--seeds", type=int, default=4, help="c4: rollouts differentiated concurrently")
+    ap.add_argument("--c3-projection", default="true", choices=sorted(PROJECTION),
+                    help="c3: SPD projection of the element Hessians")
+    ap.add_argument("--seeds", type=int, default=64, help="c4: activation seeds differentiated in one union handle")
     ap.add_argument("--c4-steps", type=int, default=100, help="c4: steps per rollout")
-    ap.add_argument("--fd-dirs", type=int, default=4, help="c4: finite-difference directions checked")
+    ap.add_argument("--fd-dirs", type=int, default=20, help="c4: finite-difference directions checked")
     ap.add_argument("--checkpoint-every", type=int, default=10, help="c4: checkpoint interval (steps)")
     ap.add_argument("--profile-only", action="store_true",
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global _projection, _two_level
+    global _projection, _two_level, _shuffle
     _projection = args.projection
     _two_level = args.two_level
+    _shuffle = args.shuffle
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
