@@ -11,10 +11,22 @@ cpp/src/energy.cpp:275,:337):
       Neumann rows  dx_i = -(x_i - qPrev_i - dt val_i)            (neumannBC.cpp:4-21)
       contact rows  n . dx_v >= -n . (x_v - p)                      (planeContact.cpp:4-42)
   - Solver::minimize_SQP (cpp/src/solver.cpp:109-197): x += dx until ||dx|| < 1e-9, at most 100 iterations.
-The reference solves each QP with OSQP (max_iter 250, eps 1e-3); OSQP is not in
-the container, so this oracle solves each QP exactly (primal-dual active set on
-the KKT system, SuperLU): parity with OSQP's own iterates is unpinned, the
-converged step is the KKT point both approximate.
+The reference solves each QP with OSQP (cpp/src/solver.cpp:116-176: scaling
+off, max_iter = MAX_ITER_QP = 250, verbose off, other settings default).  OSQP
+is an un-vendored submodule (external/osqp, v1.x API; its pinned commit is not
+recorded in the mounted tree), so two QP solvers are restated here:
+  - qp="exact": the KKT point itself (primal-dual active set on the KKT
+    system, SuperLU), the point OSQP approximates;
+  - qp="osqp": the published OSQP algorithm (B. Stellato, G. Banjac,
+    P. Goulart, A. Bemporad, S. Boyd, "OSQP: an operator splitting solver for
+    quadratic programs", Math. Prog. Comp. 12, 2020: Algorithm 1 with the
+    direct KKT solve, termination of section 3.4, step-size update of
+    section 5.2) with OSQP's default parameters and the reference's settings,
+    including OSQP's rejection of a non-convex problem at set-up (the KKT
+    matrix must have n positive and m negative pivots), which minimize_SQP
+    turns into "OSQP solver failed" (solver.cpp:160-163).  OSQP schedules its
+    step-size updates by measured run time (not reproducible); this
+    restatement updates at each termination check (every 25 iterations).
 """
 from __future__ import annotations
 
@@ -161,10 +173,94 @@ def solve_qp(H, g, Aeq, beq, Ain, bin_, max_iter=50):
     return dx, work, mu
 
 
+# OSQP defaults (published with the solver) and the reference's settings
+OSQP_RHO = 0.1
+OSQP_SIGMA = 1e-6
+OSQP_ALPHA = 1.6
+OSQP_EPS_ABS = 1e-3
+OSQP_EPS_REL = 1e-3
+OSQP_CHECK_TERMINATION = 25
+OSQP_RHO_EQ_OVER_INEQ = 1e3     # equality rows (|u - l| < 1e-4) get a 1e3 times larger step size
+OSQP_RHO_TOL = 1e-4
+OSQP_ADAPTIVE_RHO_TOLERANCE = 5.0
+OSQP_RHO_MIN, OSQP_RHO_MAX = 1e-6, 1e6
+MAX_ITER_QP = 250               # cpp/headers/common.h:23
+
+
+class OSQPNonConvex(RuntimeError):
+    """OSQP's set-up rejects the problem: P + sigma I + A' diag(rho) A is not
+    positive definite (the KKT matrix lacks n positive pivots)."""
+
+
+def _osqp_factor(P, A, rho_vec):
+    n = P.shape[0]
+    M = (P + OSQP_SIGMA * sp.identity(n) + (A.T @ sp.diags(rho_vec) @ A if A.shape[0] else 0)).tocsc()
+    lu = spla.splu(M, permc_spec="MMD_AT_PLUS_A", diag_pivot_thresh=0.0, options={"SymmetricMode": True})
+    # symmetric pivoting: the signs of U's diagonal are the inertia of M
+    if not (lu.U.diagonal() > 0.0).all():
+        raise OSQPNonConvex("non-convex problem")
+    return lu
+
+
+def osqp_solve(P, q, A, l, u, max_iter=MAX_ITER_QP):
+    """min 1/2 x'Px + q'x s.t. l <= Ax <= u by OSQP's ADMM (cold start, no
+    scaling, no polishing).  Returns (x, iterations, converged)."""
+    P = sp.csr_matrix(P)
+    A = sp.csr_matrix(A) if A is not None and A.shape[0] else sp.csr_matrix((0, P.shape[0]))
+    n, m = P.shape[0], A.shape[0]
+    l = np.asarray(l, float); u = np.asarray(u, float)
+    eq = np.abs(u - l) < OSQP_RHO_TOL
+    rho = OSQP_RHO
+
+    def rho_vec(r):
+        v = np.full(m, r)
+        v[eq] *= OSQP_RHO_EQ_OVER_INEQ
+        return v
+
+    rv = rho_vec(rho)
+    lu = _osqp_factor(P, A, rv)
+    x = np.zeros(n); z = np.zeros(m); y = np.zeros(m)
+    converged = False
+    it = 0
+    for it in range(1, max_iter + 1):
+        # KKT solve with nu eliminated: (P + sigma I + A' R A) xt = sigma x - q + A'(R z - y), zt = A xt
+        xt = lu.solve(OSQP_SIGMA * x - q + (A.T @ (rv * z - y) if m else 0.0))
+        zt = A @ xt if m else np.zeros(0)
+        x = OSQP_ALPHA * xt + (1.0 - OSQP_ALPHA) * x
+        zr = OSQP_ALPHA * zt + (1.0 - OSQP_ALPHA) * z
+        z_new = np.clip(zr + y / rv, l, u) if m else z
+        y = y + rv * (zr - z_new) if m else y
+        z = z_new
+        if it % OSQP_CHECK_TERMINATION == 0 or it == max_iter:
+            Ax = A @ x if m else np.zeros(0)
+            Px = P @ x
+            Aty = A.T @ y if m else np.zeros(n)
+            r_prim = np.abs(Ax - z).max(initial=0.0)
+            r_dual = np.abs(Px + q + Aty).max(initial=0.0)
+            s_prim = max(np.abs(Ax).max(initial=0.0), np.abs(z).max(initial=0.0))
+            s_dual = max(np.abs(Px).max(initial=0.0), np.abs(Aty).max(initial=0.0), np.abs(q).max(initial=0.0))
+            if r_prim <= OSQP_EPS_ABS + OSQP_EPS_REL * s_prim and r_dual <= OSQP_EPS_ABS + OSQP_EPS_REL * s_dual:
+                converged = True
+                break
+            if m:
+                num = r_prim / (s_prim + 1e-30)
+                den = r_dual / (s_dual + 1e-30)
+                new = min(max(rho * np.sqrt(num / (den + 1e-30)), OSQP_RHO_MIN), OSQP_RHO_MAX)
+                if new > OSQP_ADAPTIVE_RHO_TOLERANCE * rho or new < rho / OSQP_ADAPTIVE_RHO_TOLERANCE:
+                    rho = new
+                    rv = rho_vec(rho)
+                    lu = _osqp_factor(P, A, rv)
+    return x, it, converged
+
+
 class SQPOracle:
     """One rollout of Solver::step with minimize_SQP (backward Euler)."""
 
-    def __init__(self, system, planes=None, disks=None, neumann=None, max_distance=None):
+    def __init__(self, system, planes=None, disks=None, neumann=None, max_distance=None, qp="exact"):
+        if qp not in ("exact", "osqp"):
+            raise ValueError(qp)
+        self.qp = qp
+        self.qp_unconverged = 0   # OSQP solves that stopped at MAX_ITER_QP (the reference uses them anyway)
         self.s = system
         self.planes = planes
         self.disks = disks
@@ -212,6 +308,23 @@ class SQPOracle:
                 Ap, bp = self.max_distance.rows(x, n)
                 A_all = sp.vstack([Ain, Ap]).tocsr()
                 b_all = np.concatenate([bin_, bp])
+            if self.qp == "osqp":
+                # rows as Energy::compute_constraint_bounds: equalities l = u, inequalities [l, inf)
+                A_q = sp.vstack([Aeq, A_all]).tocsr()
+                l_q = np.concatenate([beq, b_all])
+                u_q = np.concatenate([beq, np.full(b_all.size, np.inf)])
+                try:
+                    dx, _, ok = osqp_solve(H, g, A_q, l_q, u_q)
+                except OSQPNonConvex:
+                    raise RuntimeError("OSQP solver failed")
+                self.qp_unconverged += not ok
+                x += dx
+                if np.isnan(dx).any():
+                    raise RuntimeError("SQP method diverged")
+                if np.linalg.norm(dx) < DX_TOL:
+                    self.last_iters = it + 1
+                    return x
+                continue
             dx, work, _ = solve_qp(H, g, Aeq, beq, A_all, b_all)
             self.held_pairs = np.nonzero(work[len(rows):])[0]
             x += dx

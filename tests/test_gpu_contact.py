@@ -68,3 +68,27 @@ def test_disk_poke_on_ground():
     assert np.abs(x - xo).max() < 1e-8
     # the disk pushed the top down
     assert x.reshape(-1, 3)[:, 2].max() < top
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_drop_within_osqp_tolerance_of_reference_qp(kind):
+    # The reference solves each SQP subproblem with OSQP (max_iter 250, absolute
+    # tolerance 1e-3, solver.cpp:116-176), restated in oracle/contact.py.  The
+    # device solves the subproblem exactly: its contacts stay on the plane, the
+    # OSQP-restated step leaves them up to the tolerance below it, and the two
+    # trajectories differ by less than that tolerance.
+    from oracle import contact as oc
+    X, H = meshes.hex_bar(4, 3, 3, (0.012, 0.009, 0.009))
+    T = H if kind == "hex" else meshes.kuhn_tet_elements(4, 3, 3)
+    X = X + np.array([0.0, 0.0, 0.0003])
+    en, sol, sq, surf = contact_pair(X, T, planes=([[0, 0, 0]], [[0, 0, 1.0]]), dt=2e-3)
+    sq.qp = "osqp"
+    x = X.ravel().copy(); xo = x.copy()
+    worst = 0.0
+    for step in range(20):
+        x = sol.step(x, en)
+        xo = sq.step(xo, 2e-3)
+        worst = max(worst, float(np.abs(x - xo).max()))
+        assert x.reshape(-1, 3)[surf, 2].min() > -1e-9
+        assert xo.reshape(-1, 3)[surf, 2].min() > -oc.OSQP_EPS_ABS
+    assert worst < oc.OSQP_EPS_ABS

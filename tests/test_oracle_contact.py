@@ -149,3 +149,79 @@ def test_max_distance_adjoint_needs_constraint_curvature():
         errs.append(abs(-lam @ dg - d_fd) / abs(d_fd))
     assert errs[0] < 1e-5, errs
     assert errs[1] > 1e-3, errs
+
+
+# --- OSQP restatement (oracle/contact.py osqp_solve) -------------------------
+
+def test_osqp_restatement_solves_a_convex_qp():
+    # well-scaled convex QP with equality and one-sided rows: OSQP's ADMM meets
+    # its termination test and lands on the exact KKT point
+    import scipy.sparse as sp
+    from oracle import contact as oc
+    rng = np.random.default_rng(0)
+    n = 30
+    B = rng.standard_normal((n, n))
+    P = sp.csr_matrix(B @ B.T + n * np.eye(n)); q = rng.standard_normal(n)
+    A = sp.csr_matrix(rng.standard_normal((8, n))); lo = rng.standard_normal(8) - 1
+    up = np.full(8, np.inf); up[:2] = lo[:2]
+    x, it, conv = oc.osqp_solve(P, q, A, lo, up)
+    dx, _, _ = oc.solve_qp(P, q, A[:2], lo[:2], A[2:], lo[2:])
+    assert conv and it <= oc.MAX_ITER_QP
+    assert np.abs(x - dx).max() <= 1e-6 * np.abs(dx).max()
+
+
+def test_osqp_restatement_rejects_nonconvex():
+    # OSQP's set-up refuses an indefinite P; minimize_SQP turns that into "OSQP solver failed"
+    import scipy.sparse as sp
+    from oracle import contact as oc
+    n = 6
+    P = sp.diags([1.0, 2.0, -3.0, 1.0, 1.0, 1.0]).tocsr()
+    A = sp.csr_matrix(np.eye(n)[:2])
+    with pytest.raises(oc.OSQPNonConvex):
+        oc.osqp_solve(P, np.ones(n), A, np.zeros(2), np.full(2, np.inf))
+
+
+def test_plane_contact_no_penetration_osqp(golden):
+    # the reference's contact test with the QP solved as the reference does
+    # (OSQP, max_iter 250): within the test's 1e-4 tolerance, but not exactly
+    # on the plane, as OSQP's 1e-3 absolute tolerance allows
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    d = golden["test_constraint"]
+    X = np.array(d["vertices"]); T = np.array([[0, 1, 2, 3]])
+    o = orc.System(X, T, rho=1.0, youngs=1e5, nu=0.3, grav=(0, 0, -9.81), scheme="backward_euler",
+                   method="minimize_SQP", dt=1e-2, substeps=1, nthreads=1)
+    sq = oc.SQPOracle(o, oc.PlaneContact([[0, 0, 0]], [[0, 0, 1.0]], [0, 1, 2, 3]), qp="osqp")
+    z = sq.step(X.ravel(), 1e-2).reshape(-1, 3)[:, 2]
+    assert z.min() >= -d["tol"]
+
+
+@pytest.mark.parametrize("kind", ["hex", "tet"])
+def test_osqp_and_exact_contact_steps_agree_to_osqp_tolerance(kind):
+    # a small body dropped onto z = 0: the exact QP keeps every contact on the
+    # plane; OSQP stops at its first termination check with up to
+    # eps_abs = 1e-3 m of primal residual, so its contacts sink slightly and the
+    # two trajectories differ by less than that tolerance
+    from oracle import oracle as orc
+    from oracle import contact as oc
+    from sors_b200 import meshes
+    if kind == "hex":
+        X, T = meshes.hex_bar(3, 3, 3, (0.01, 0.01, 0.01))
+    else:
+        X, T = meshes.cantilever_tets(6, 3, 3, (0.012, 0.006, 0.006))
+    X = X + np.array([0, 0, 0.0004])
+    groups, _ = meshes.extract_surfaces(X, T)
+    surf = np.unique(np.concatenate([g.ravel() for g in groups]))
+    out = {}
+    for qp in ("exact", "osqp"):
+        o = orc.System(X, T, rho=1070.0, youngs=1e5, nu=0.45, grav=(0, 0, -9.81), scheme="backward_euler",
+                       method="minimize_SQP", dt=2e-3, substeps=1, nthreads=2)
+        sq = oc.SQPOracle(o, oc.PlaneContact([[0, 0, 0]], [[0, 0, 1.0]], surf), qp=qp)
+        x = X.ravel().copy(); tr = []
+        for _ in range(20):
+            x = sq.step(x, 2e-3); tr.append(x.copy())
+        out[qp] = np.array(tr)
+    zmin = lambda tr: tr[:, 2::3].reshape(len(tr), -1)[:, surf].min()
+    assert zmin(out["exact"]) > -1e-12
+    assert -oc.OSQP_EPS_ABS < zmin(out["osqp"]) < 0.0
+    assert np.abs(out["exact"] - out["osqp"]).max() < oc.OSQP_EPS_ABS
