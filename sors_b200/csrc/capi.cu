@@ -409,7 +409,10 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     h->chunks = ChunkArgs{};
     if (h->nv != 4 || !(h->s.material == 0 || h->s.material == 2) || h->N == 0) return SORS_OK;
     const int N = h->N, E = h->E;
-    const ChunkLimits lim = chunk_limits(mixed(h) ? 4 : 8, h->s.material);
+    const int hsz = mixed(h) ? 4 : 8;
+    const ChunkLimits lim = chunk_limits(hsz, h->s.material);
+    // two blocks per SM must fit (227 KB of shared memory per SM)
+    if (chunk_smem_bytes(hsz, h->s.material, h->max_pairs) > 113 * 1024) return SORS_OK;
     for (int i = 0; i < N; i++) {
         const int np = ph.pair_ptr[i + 1] - ph.pair_ptr[i];
         if (np > lim.pairs || np > lim.elems) return SORS_OK;
@@ -554,6 +557,9 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     c.ch_eslot = reinterpret_cast<const ushort4*>(d_eslot);
     c.items = d_items;
     c.rows_max = lim.rows; c.elems_max = lim.elems; c.pairs_max = lim.pairs;
+    c.stage_per_warp = h->max_pairs * 4 * 9;
+    c.region_bytes = (int)chunk_region_bytes(hsz, h->s.material, h->max_pairs);
+    c.smem_bytes = (int)chunk_smem_bytes(hsz, h->s.material, h->max_pairs);
     c.nchunks = nch;
     h->chunk_elem_total = (long long)ch_elems.size();
     return SORS_OK;

@@ -692,10 +692,22 @@ ChunkLimits chunk_limits(int hsize, int material) {
     return snh ? ChunkLimits{32, 192, 576} : ChunkLimits{32, 256, 768};
 }
 
-size_t chunk_smem_bytes(int hsize, int material) {
+// Shared memory of one chunk block: a region holding first the gradient pairs
+// (3 doubles per pair) and then, per warp, the staged Hessian items of one row
+// (9 values per item, 4 items per incident pair), the element generators, and
+// the chunk's row table.
+size_t chunk_region_bytes(int hsize, int material, int max_pairs) {
+    const ChunkLimits l = chunk_limits(hsize, material);
+    const size_t grad = (size_t)l.pairs * 3 * sizeof(double);
+    const size_t stage = (size_t)(kChunkThreads / 32) * max_pairs * 4 * 9 * hsize;
+    return ((grad > stage ? grad : stage) + 15) / 16 * 16;
+}
+
+size_t chunk_smem_bytes(int hsize, int material, int max_pairs) {
     const ChunkLimits l = chunk_limits(hsize, material);
     const int nf = material == 2 ? ChunkGen<true>::kFields : ChunkGen<false>::kFields;
-    return (size_t)l.pairs * 3 * sizeof(double) + (size_t)nf * l.elems * hsize + (size_t)(4 * l.rows + 2) * sizeof(int);
+    return chunk_region_bytes(hsize, material, max_pairs) + (size_t)nf * l.elems * hsize +
+           (size_t)(4 * l.rows + 2) * sizeof(int);
 }
 
 template <typename HT, bool SNH>
@@ -704,7 +716,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
     using G = ChunkGen<SNH>;
     const int EM = a.ch.elems_max;
     double* gslot = reinterpret_cast<double*>(smem_raw);
-    HT* gen = reinterpret_cast<HT*>(gslot + 3 * (size_t)a.ch.pairs_max);
+    HT* gen = reinterpret_cast<HT*>(smem_raw + a.ch.region_bytes);
     int* srow = reinterpret_cast<int*>(gen + (size_t)G::kFields * EM);
     int* srp0 = srow + a.ch.rows_max;
     int* spair0 = srp0 + a.ch.rows_max;
@@ -841,68 +853,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
     }
     if (!ok) atomicOr(a.status, kFlagInverted);
     __syncthreads();
-    // B. Hessian blocks of the chunk's rows
-    if (a.want_hess) {
-        const int total = sblk0[nr];
-        for (int lb = threadIdx.x; lb < total; lb += blockDim.x) {
-            int lo = 0, hi = nr - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (sblk0[mid] <= lb) lo = mid; else hi = mid - 1;
-            }
-            const int row = srow[lo];
-            const int bg = srp0[lo] + (lb - sblk0[lo]);
-            const int i0 = __ldg(a.slot_item_ptr + bg), i1 = __ldg(a.slot_item_ptr + bg + 1);
-            HT acc[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) acc[k] = HT(0);
-            for (int it = i0; it < i1; ++it) {
-                const unsigned item = __ldg(a.ch.items + it);
-                const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
-                const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
-                const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
-                HT av[3], aw[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    av[k] = gen[(G::kA + v * 3 + k) * EM + es];
-                    aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
-                }
-                HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
-                if (SNH) {
-                    h4 = gen[G::kH4 * EM + es];
-#pragma unroll
-                    for (int k = 0; k < 3; k++) {
-                        fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
-                        fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < 3; k++)
-#pragma unroll
-                    for (int l = 0; l < 3; l++) {
-                        HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
-                        if (SNH) val += h4 * fv[k] * fw[l];
-                        if (k == l) val += hmu * dd;
-                        acc[k * 3 + l] += val;
-                    }
-            }
-            const int j = __ldg(a.col + bg);
-            const unsigned mrow = a.node_mask[row], mcol = a.node_mask[j];
-            const double md = a.inertia_coef * a.mass[row];
-#pragma unroll
-            for (int rc = 0; rc < 9; rc++) {
-                const int r = rc / 3, c = rc - 3 * (rc / 3);
-                const bool rmask = (mrow >> r) & 1u;
-                double val = (double)acc[rc] * a.hscale;
-                if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
-                if (j == row && r == c) {
-                    val += md;
-                    if (a.neumann_override && rmask) val = 1.0;
-                }
-                a.H[hval(bg, rc, a.nnzb)] = (HT)val;
-            }
-        }
-    }
     // C. gradient rows
     for (int p = threadIdx.x; p < nr; p += blockDim.x) {
         const int row = srow[p];
@@ -919,6 +869,71 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
         a.g_int[3 * (size_t)row + 0] = g0;
         a.g_int[3 * (size_t)row + 1] = g1;
         a.g_int[3 * (size_t)row + 2] = g2;
+    }
+    if (!a.want_hess) return;
+    __syncthreads();  // the gradient pairs' memory becomes the warps' item stages
+    // B. Hessian rows, one warp per row: the lanes expand the row's items (in
+    // slot order they are contiguous) into the warp's stage, then each lane sums
+    // (block, entry) values over the block's items in order and writes them
+    const int warp = threadIdx.x >> 5;
+    HT* stage = reinterpret_cast<HT*>(smem_raw) + (size_t)warp * a.ch.stage_per_warp;
+    for (int p = warp; p < nr; p += blockDim.x >> 5) {
+        const int row = srow[p];
+        const int b0 = srp0[p], nb = sblk0[p + 1] - sblk0[p];
+        const int base = __ldg(a.slot_item_ptr + b0);
+        const int nit = __ldg(a.slot_item_ptr + b0 + nb) - base;
+        for (int it = lane; it < nit; it += 32) {
+            const unsigned item = __ldg(a.ch.items + base + it);
+            const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
+            const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
+            const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
+            HT av[3], aw[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
+            }
+            HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
+            if (SNH) {
+                h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
+                    fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
+                }
+            }
+            HT* dst = stage + (size_t)it * 9;
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int l = 0; l < 3; l++) {
+                    HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
+                    if (SNH) val += h4 * fv[k] * fw[l];
+                    if (k == l) val += hmu * dd;
+                    dst[k * 3 + l] = val;
+                }
+        }
+        __syncwarp();
+        const unsigned mrow = a.node_mask[row];
+        const double md = a.inertia_coef * a.mass[row];
+        for (int t = lane; t < nb * 9; t += 32) {
+            const int sb = t / 9, rc = t - 9 * sb, r = rc / 3, c = rc - 3 * r;
+            const int bg = b0 + sb;
+            const int i0 = __ldg(a.slot_item_ptr + bg) - base, i1 = __ldg(a.slot_item_ptr + bg + 1) - base;
+            HT acc = HT(0);
+            for (int i = i0; i < i1; ++i) acc += stage[i * 9 + rc];
+            const int j = __ldg(a.col + bg);
+            const unsigned mcol = a.node_mask[j];
+            const bool rmask = (mrow >> r) & 1u;
+            double val = (double)acc * a.hscale;
+            if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
+            if (j == row && r == c) {
+                val += md;
+                if (a.neumann_override && rmask) val = 1.0;
+            }
+            a.H[hval(bg, rc, a.nnzb)] = (HT)val;
+        }
+        __syncwarp();
     }
 }
 
@@ -939,7 +954,7 @@ template <typename HT, bool SNH>
 static void launch_assemble_chunk(const AsmArgs<HT>& a, cudaStream_t st) {
     static std::atomic<int> limit[kMaxDevices];
     auto k = k_assemble_chunk<HT, SNH>;
-    const size_t smem = chunk_smem_bytes(sizeof(HT), SNH ? 2 : 0);
+    const size_t smem = a.ch.smem_bytes;
     set_smem_limit(k, smem, limit);
     k<<<a.ch.nchunks, kChunkThreads, smem, st>>>(a);
     counted();

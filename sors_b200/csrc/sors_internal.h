@@ -74,6 +74,9 @@ struct ChunkArgs {
     const ushort4* ch_eslot = nullptr;  // chunk-local pair slot of local vertex v (0xffff: not owned)
     const uint16_t* items = nullptr;    // one per slot item, same order as slot_items
     int rows_max = 0, elems_max = 0, pairs_max = 0;
+    int stage_per_warp = 0;     // HT values of one row's staged items (max_pairs * 4 * 9)
+    int region_bytes = 0;       // gradient pairs, then the warps' item stages
+    int smem_bytes = 0;         // dynamic shared memory of one chunk block
 };
 
 // Chunk limits and shared-memory size of the chunked assembly for a Hessian
@@ -82,7 +85,8 @@ struct ChunkLimits {
     int rows, elems, pairs;
 };
 ChunkLimits chunk_limits(int hsize, int material);
-size_t chunk_smem_bytes(int hsize, int material);
+size_t chunk_region_bytes(int hsize, int material, int max_pairs);
+size_t chunk_smem_bytes(int hsize, int material, int max_pairs);
 
 // Row-owner assembly arguments (tet or hex).
 template <typename HT>
