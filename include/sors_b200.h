@@ -295,6 +295,15 @@ int sors_set_assembly_variant(SorsHandle* h, int32_t variant);
  * kernel only).  Diagnostic only. */
 int64_t sors_assembly_chunks(SorsHandle* h);
 
+/* Linear solves of the last sors_step / sors_step_device whose PCG met a
+ * direction p of non-positive curvature, on the subspace the step's
+ * constraints leave free (the exact Hessian is indefinite there), and the most
+ * negative Rayleigh quotient p'Hp / p'p among them (+inf when none).  The
+ * reference's OSQP rejects a QP as non-convex when H + sigma I + A' rho A has a
+ * negative pivot (sigma = 1e-6, rho = 0.1 on contact rows), which a quotient
+ * below -(sigma + rho) certifies.  Diagnostic; no counterpart in the reference. */
+int sors_last_step_curvature(SorsHandle* h, double* min_rayleigh, int32_t* indefinite_solves);
+
 /* Sum of the Neo-Hookean element energies (volume x Psi, the element part of
  * sors_energy) of a tet (nodes_per_elem = 4) or hex (8) mesh, computed from
  * caller-owned DEVICE arrays, without any device allocation.  No counterpart

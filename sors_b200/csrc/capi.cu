@@ -181,6 +181,10 @@ struct SorsHandle {
     bool graph_failed = false;
 
     double prev_gnorm = -1.0;
+    // PCG directions with non-positive curvature met during the last step:
+    // count and the most negative Rayleigh quotient p'Hp / p'p
+    int step_indefinite = 0;
+    double step_min_rq = INFINITY;
     // project_spd == 2: the exact Hessian first, the projected one for this
     // iteration after PCG met negative curvature
     bool proj_fallback = false;
@@ -719,6 +723,24 @@ int pcg_chunk(SorsHandle* h) {
     return SORS_OK;
 }
 
+// Records the curvature of the PCG direction that broke down: iteration `it`
+// multiplied p1 (it even) or p0 (it odd), padded to 4 values per node, and no
+// kernel wrote either after the breakdown.
+template <typename VT>
+int record_curvature(SorsHandle* h) {
+    const int it = h->sc_host->it;
+    const VT* pb = (const VT*)((it & 1) ? h->p0 : h->p1);
+    std::vector<VT> p((size_t)4 * h->N);
+    CK(cudaMemcpyAsync(p.data(), pb, sizeof(VT) * p.size(), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    double pp = 0.0;
+    for (int i = 0; i < h->N; i++)
+        for (int k = 0; k < 3; k++) pp += (double)p[4 * (size_t)i + k] * (double)p[4 * (size_t)i + k];
+    h->step_indefinite++;
+    if (pp > 0.0) h->step_min_rq = std::min(h->step_min_rq, h->sc_host->pq / pp);
+    return SORS_OK;
+}
+
 // Solves H dx = -g (dx in h->x), g = h->g unless given.  With h->proj_flag set
 // the solve runs on the subspace the constraint projection leaves free.
 // Returns PCG iterations in *iters.
@@ -763,6 +785,10 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
         if (h->sc_host->done) break;
     }
     *iters = h->sc_host->it;
+    if (h->sc_host->breakdown) {
+        int st = record_curvature<VT>(h);
+        if (st) return st;
+    }
     if (refreshed) h->tl_ref_rate = -1.0;
     if (h->tl_active && h->sc_host->it >= 8 && h->sc_host->rr > 0.0 && h->sc_host->bnorm2 >= 1e4 * h->sc_host->rr) {
         // iterations per decade of residual reduction, over solves of two
@@ -1706,6 +1732,8 @@ int cfl_dt(SorsHandle* h, double dt, double* out) {
 }
 
 int step_resident(SorsHandle* h, double dt, int substeps, SorsStepStats* stats) {
+    h->step_indefinite = 0;
+    h->step_min_rq = INFINITY;
     if (dt == 0.0) dt = h->s.dt;
     if (substeps == 0) substeps = h->s.substeps;
     if (h->s.cfl) {
@@ -2351,6 +2379,13 @@ int sors_set_assembly_variant(SorsHandle* h, int32_t variant) {
 }
 
 int64_t sors_assembly_chunks(SorsHandle* h) { return h ? (int64_t)h->chunks.nchunks : 0; }
+
+int sors_last_step_curvature(SorsHandle* h, double* min_rayleigh, int32_t* indefinite_solves) {
+    if (!h || !min_rayleigh || !indefinite_solves) return fail(SORS_ERR_ARG, "NULL argument");
+    *min_rayleigh = h->step_min_rq;
+    *indefinite_solves = h->step_indefinite;
+    return SORS_OK;
+}
 
 int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian) {
     if (!h) return 0;

@@ -235,6 +235,8 @@ class RolloutServer:
             del en
         except Exception as ex:  # reported per rollout, the server keeps running
             err = str(ex)
+            if en is not None:
+                err += curvature_note(en)
         en = sol = None  # release the union's device memory before any re-run
         if err is not None and len(batch) > 1:
             for r in batch:
@@ -244,6 +246,19 @@ class RolloutServer:
         for r, f in zip(batch, finals):
             self._results.append(RolloutResult(r.tag, f, list(steps_lat), started - r.submitted, done - r.submitted,
                                                newton, pcg, err, batch=len(batch)))
+
+
+def curvature_note(en) -> str:
+    """' (exact Hessian indefinite: ...)' when the last step's PCG met
+    non-positive curvature, else ''.  A Rayleigh quotient below -0.1 (OSQP's
+    default step size on contact rows, plus sigma) means the reference's OSQP
+    set-up would reject that step's QP as non-convex."""
+    import ctypes as C
+    from . import _lib
+    rq = C.c_double(); n = C.c_int32()
+    if _lib.load().sors_last_step_curvature(en._h, C.byref(rq), C.byref(n)) != 0 or n.value == 0:
+        return ""
+    return f" (exact Hessian indefinite in {n.value} solves of the step, min p'Hp/p'p = {rq.value:.3e})"
 
 
 def compatible(a: RolloutRequest, b: RolloutRequest) -> bool:
