@@ -561,7 +561,6 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     c.ch_eslot = reinterpret_cast<const ushort4*>(d_eslot);
     c.items = d_items;
     c.rows_max = lim.rows; c.elems_max = lim.elems; c.pairs_max = lim.pairs;
-    c.stage_per_warp = h->max_pairs * 4 * 9;
     c.region_bytes = (int)chunk_region_bytes(hsz, h->s.material, h->max_pairs);
     c.smem_bytes = (int)chunk_smem_bytes(hsz, h->s.material, h->max_pairs);
     c.nchunks = nch;
@@ -608,6 +607,7 @@ AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int
     a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.tshape = h->tshape;
     a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
+    a.diag_slot = h->diag_slot;
     a.slot_item_ptr = h->slot_item_ptr; a.slot_items = h->slot_items; a.node_mask = h->node_mask; a.mass = h->mass;
     a.H = (HT*)h->H; a.nnzb = h->nnzb; a.g_int = h->g_int; a.status = h->status;
     a.stage_per_warp = h->max_pairs * h->nv * 9;

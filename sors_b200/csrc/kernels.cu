@@ -692,22 +692,19 @@ ChunkLimits chunk_limits(int hsize, int material) {
     return snh ? ChunkLimits{32, 192, 576} : ChunkLimits{32, 256, 768};
 }
 
-// Shared memory of one chunk block: a region holding first the gradient pairs
-// (3 doubles per pair) and then, per warp, the staged Hessian items of one row
-// (9 values per item, 4 items per incident pair), the element generators, and
-// the chunk's row table.
+// Shared memory of one chunk block: the gradient pairs (3 doubles per pair),
+// the element generators, and the chunk's row table.
 size_t chunk_region_bytes(int hsize, int material, int max_pairs) {
+    (void)max_pairs;
     const ChunkLimits l = chunk_limits(hsize, material);
-    const size_t grad = (size_t)l.pairs * 3 * sizeof(double);
-    const size_t stage = (size_t)(kChunkThreads / 32) * max_pairs * 4 * 9 * hsize;
-    return ((grad > stage ? grad : stage) + 15) / 16 * 16;
+    return ((size_t)l.pairs * 3 * sizeof(double) + 15) / 16 * 16;
 }
 
 size_t chunk_smem_bytes(int hsize, int material, int max_pairs) {
     const ChunkLimits l = chunk_limits(hsize, material);
     const int nf = material == 2 ? ChunkGen<true>::kFields : ChunkGen<false>::kFields;
     return chunk_region_bytes(hsize, material, max_pairs) + (size_t)nf * l.elems * hsize +
-           (size_t)(4 * l.rows + 2) * sizeof(int);
+           (size_t)(5 * l.rows + 2) * sizeof(int);
 }
 
 template <typename HT, bool SNH>
@@ -721,6 +718,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
     int* srp0 = srow + a.ch.rows_max;
     int* spair0 = srp0 + a.ch.rows_max;
     int* sblk0 = spair0 + a.ch.rows_max + 1;
+    int* sdiag = sblk0 + a.ch.rows_max + 1;  // position of the diagonal block in each row
     const int chunk = blockIdx.x;
     const int r0 = __ldg(a.ch.ch_ptr + chunk), nr = __ldg(a.ch.ch_ptr + chunk + 1) - r0;
     const int e0 = __ldg(a.ch.ch_eptr + chunk), ne = __ldg(a.ch.ch_eptr + chunk + 1) - e0;
@@ -743,7 +741,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
                 const int tp = __shfl_up_sync(0xffffffffu, ip, o), tb = __shfl_up_sync(0xffffffffu, ib, o);
                 if (lane >= o) { ip += tp; ib += tb; }
             }
-            if (p < nr) { srow[p] = r; srp0[p] = rp; spair0[p] = pacc + ip - np; sblk0[p] = bacc + ib - nb; }
+            if (p < nr) {
+                srow[p] = r; srp0[p] = rp; spair0[p] = pacc + ip - np; sblk0[p] = bacc + ib - nb;
+                sdiag[p] = __ldg(a.diag_slot + r) - rp;
+            }
             pacc += __shfl_sync(0xffffffffu, ip, 31);
             bacc += __shfl_sync(0xffffffffu, ib, 31);
         }
@@ -871,61 +872,100 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
         a.g_int[3 * (size_t)row + 2] = g2;
     }
     if (!a.want_hess) return;
-    __syncthreads();  // the gradient pairs' memory becomes the warps' item stages
-    // B. Hessian rows, one warp per row: the lanes expand the row's items (in
-    // slot order they are contiguous) into the warp's stage, then each lane sums
-    // (block, entry) values over the block's items in order and writes them
-    const int warp = threadIdx.x >> 5;
-    HT* stage = reinterpret_cast<HT*>(smem_raw) + (size_t)warp * a.ch.stage_per_warp;
-    for (int p = warp; p < nr; p += blockDim.x >> 5) {
-        const int row = srow[p];
-        const int b0 = srp0[p], nb = sblk0[p + 1] - sblk0[p];
-        const int base = __ldg(a.slot_item_ptr + b0);
-        const int nit = __ldg(a.slot_item_ptr + b0 + nb) - base;
-        for (int it = lane; it < nit; it += 32) {
-            const unsigned item = __ldg(a.ch.items + base + it);
-            const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
-            const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
-            const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
-            HT av[3], aw[3];
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                av[k] = gen[(G::kA + v * 3 + k) * EM + es];
-                aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
+    // B. Hessian blocks, one thread per block, the chunk's diagonal blocks
+    // first: a diagonal block sums one item per incident pair (about four
+    // times an off-diagonal block's), so grouping them keeps warps balanced.
+    // Diagonal items use the symmetric form hmu (d_v . d_v) I + (h1 - h2) a_v a_v^T
+    // [+ h4 f_v f_v^T].
+    const int total = sblk0[nr];
+    for (int lb = threadIdx.x; lb < total; lb += blockDim.x) {
+        int pos, bg;
+        const bool diag = lb < nr;
+        if (diag) {
+            pos = lb;
+            bg = srp0[pos] + sdiag[pos];
+        } else {
+            const int j = lb - nr;  // j-th off-diagonal block of the chunk
+            int lo = 0, hi = nr - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (sblk0[mid] - mid <= j) lo = mid; else hi = mid - 1;
             }
-            HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
-            if (SNH) {
-                h4 = gen[G::kH4 * EM + es];
+            pos = lo;
+            const int k = j - (sblk0[pos] - pos);
+            bg = srp0[pos] + k + (k >= sdiag[pos] ? 1 : 0);
+        }
+        const int row = srow[pos];
+        const int i0 = __ldg(a.slot_item_ptr + bg), i1 = __ldg(a.slot_item_ptr + bg + 1);
+        HT acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) acc[k] = HT(0);
+        if (diag) {
+            for (int it = i0; it < i1; ++it) {
+                const unsigned item = __ldg(a.ch.items + it);
+                const int es = (int)(item >> 4), v = (item >> 2) & 3;
+                const HT hmu = gen[0 * EM + es], c1 = gen[1 * EM + es] - gen[2 * EM + es];
+                const HT dd = gen[(G::kDD + dd_index(v, v)) * EM + es];
+                HT av[3], fv[3] = {HT(0), HT(0), HT(0)};
+#pragma unroll
+                for (int k = 0; k < 3; k++) av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                HT h4 = HT(0);
+                if (SNH) {
+                    h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+#pragma unroll
+                    for (int l = k; l < 3; l++) {
+                        HT val = c1 * av[k] * av[l];
+                        if (SNH) val += h4 * fv[k] * fv[l];
+                        if (k == l) val += hmu * dd;
+                        acc[k * 3 + l] += val;
+                    }
+            }
+            acc[3] = acc[1]; acc[6] = acc[2]; acc[7] = acc[5];
+        } else {
+            for (int it = i0; it < i1; ++it) {
+                const unsigned item = __ldg(a.ch.items + it);
+                const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
+                const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
+                const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
+                HT av[3], aw[3];
 #pragma unroll
                 for (int k = 0; k < 3; k++) {
-                    fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
-                    fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
+                    av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                    aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
                 }
+                HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
+                if (SNH) {
+                    h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
+                        fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < 3; k++)
+#pragma unroll
+                    for (int l = 0; l < 3; l++) {
+                        HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
+                        if (SNH) val += h4 * fv[k] * fw[l];
+                        if (k == l) val += hmu * dd;
+                        acc[k * 3 + l] += val;
+                    }
             }
-            HT* dst = stage + (size_t)it * 9;
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int l = 0; l < 3; l++) {
-                    HT val = h1 * av[k] * aw[l] - h2 * aw[k] * av[l];
-                    if (SNH) val += h4 * fv[k] * fw[l];
-                    if (k == l) val += hmu * dd;
-                    dst[k * 3 + l] = val;
-                }
         }
-        __syncwarp();
-        const unsigned mrow = a.node_mask[row];
+        const int j = __ldg(a.col + bg);
+        const unsigned mrow = a.node_mask[row], mcol = a.node_mask[j];
         const double md = a.inertia_coef * a.mass[row];
-        for (int t = lane; t < nb * 9; t += 32) {
-            const int sb = t / 9, rc = t - 9 * sb, r = rc / 3, c = rc - 3 * r;
-            const int bg = b0 + sb;
-            const int i0 = __ldg(a.slot_item_ptr + bg) - base, i1 = __ldg(a.slot_item_ptr + bg + 1) - base;
-            HT acc = HT(0);
-            for (int i = i0; i < i1; ++i) acc += stage[i * 9 + rc];
-            const int j = __ldg(a.col + bg);
-            const unsigned mcol = a.node_mask[j];
+#pragma unroll
+        for (int rc = 0; rc < 9; rc++) {
+            const int r = rc / 3, c = rc - 3 * (rc / 3);
             const bool rmask = (mrow >> r) & 1u;
-            double val = (double)acc * a.hscale;
+            double val = (double)acc[rc] * a.hscale;
             if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
             if (j == row && r == c) {
                 val += md;
@@ -933,7 +973,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             }
             a.H[hval(bg, rc, a.nnzb)] = (HT)val;
         }
-        __syncwarp();
     }
 }
 

@@ -74,8 +74,7 @@ struct ChunkArgs {
     const ushort4* ch_eslot = nullptr;  // chunk-local pair slot of local vertex v (0xffff: not owned)
     const uint16_t* items = nullptr;    // one per slot item, same order as slot_items
     int rows_max = 0, elems_max = 0, pairs_max = 0;
-    int stage_per_warp = 0;     // HT values of one row's staged items (max_pairs * 4 * 9)
-    int region_bytes = 0;       // gradient pairs, then the warps' item stages
+    int region_bytes = 0;       // gradient pairs
     int smem_bytes = 0;         // dynamic shared memory of one chunk block
 };
 
@@ -101,6 +100,7 @@ struct AsmArgs {
     const int* pair_ptr;    // N+1
     const int* pair_ev;     // e*8 + v
     const int* row_ptr;     // N+1 (blocks)
+    const int* diag_slot;   // N: the diagonal block of each row
     const int* col;         // nnzb
     const int* slot_item_ptr;   // nnzb+1
     const uint16_t* slot_items; // k*nv + w
