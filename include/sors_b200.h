@@ -295,6 +295,17 @@ int sors_set_assembly_variant(SorsHandle* h, int32_t variant);
  * kernel only).  Diagnostic only. */
 int64_t sors_assembly_chunks(SorsHandle* h);
 
+/* Declares the handle's mesh to be n_members independent meshes: member k
+ * owns nodes [node_offsets[k], node_offsets[k+1]) (node_offsets[0] = 0,
+ * node_offsets[n_members] = the node count) and no element joins two members,
+ * which is checked.  Every linear solve then runs one preconditioned CG per
+ * member, with its own step lengths, tolerance and convergence, in the same
+ * kernel launches (the block-Jacobi preconditioner; the two-level one is not
+ * used).  A rollout server packs small meshes into one handle this way.
+ * n_members <= 1 returns to one CG over the whole system.  No counterpart in
+ * the reference (it steps one mesh per Energy). */
+int sors_set_members(SorsHandle* h, const int32_t* node_offsets, int32_t n_members);
+
 /* Linear solves of the last sors_step / sors_step_device whose PCG met a
  * direction p of non-positive curvature, on the subspace the step's
  * constraints leave free (the exact Hessian is indefinite there), and the most

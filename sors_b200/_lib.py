@@ -105,6 +105,7 @@ SIGNATURES = [
     ("sors_set_assembly_variant", C.c_int, [_h, C.c_int32]),
     ("sors_assembly_chunks", C.c_int64, [_h]),
     ("sors_last_step_curvature", C.c_int, [_h, C.POINTER(C.c_double), C.POINTER(C.c_int32)]),
+    ("sors_set_members", C.c_int, [_h, C.POINTER(C.c_int32), C.c_int32]),
     ("sors_elem_energy_noalloc", C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32, C.c_int32, C.c_void_p,
                                            C.c_void_p, C.c_void_p, C.c_void_p]),
     ("sors_stream", C.c_void_p, [_h]),

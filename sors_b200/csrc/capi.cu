@@ -172,7 +172,11 @@ struct SorsHandle {
     // projection used by the PCG kernels (null: none)
     const uint8_t* proj_flag = nullptr;
     const double4* proj_n = nullptr;
-    int pcg_exec_mode = 0;  // bit 0 projected, bit 1 two-level
+    int pcg_exec_mode = 0;  // bit 0 projected, bit 1 two-level, bit 2 member-segmented
+    // several independent meshes in one handle (sors_set_members): one PCG per member
+    BatchArgs batch;
+    std::vector<int> mem_node0_h;
+    std::vector<MemberScalars> ms_h;
 
     // PCG chunk graph
     cudaGraphExec_t pcg_exec = nullptr;
@@ -660,6 +664,15 @@ int eval_energy(SorsHandle* h, double dt, double* out) {
 template <typename HT, typename VT>
 void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
+    if (h->batch.nmem > 1) {
+        for (int half = 0; half < 2; half++) {
+            VT* pin = (VT*)(half ? h->p1 : h->p0);
+            VT* pout = (VT*)(half ? h->p0 : h->p1);
+            launch_bpcg_iter<HT, VT>(h->batch, h->row_ptr, h->col, (const HT*)h->H, (const VT*)h->Minv, z, pin, pout,
+                                     (VT*)h->qv, (VT*)h->x, (VT*)h->r, z, h->proj_flag, h->proj_n, h->stream);
+        }
+        return;
+    }
     if (h->tl_active) {
         for (int half = 0; half < 2; half++) {
             VT* pin = (VT*)(half ? h->p1 : h->p0);
@@ -688,7 +701,7 @@ void pcg_iter_pair(SorsHandle* h) {
 
 template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
-    const int mode = (h->proj_flag ? 1 : 0) + (h->tl_active ? 2 : 0);
+    const int mode = (h->proj_flag ? 1 : 0) + (h->tl_active ? 2 : 0) + (h->batch.nmem > 1 ? 4 : 0);
     if (h->pcg_exec && h->pcg_exec_mode != mode) {
         // the captured launches carry the projection pointers: capture again
         cudaGraphExecDestroy(h->pcg_exec);
@@ -744,13 +757,70 @@ int record_curvature(SorsHandle* h) {
 // Solves H dx = -g (dx in h->x), g = h->g unless given.  With h->proj_flag set
 // the solve runs on the subspace the constraint projection leaves free.
 // Returns PCG iterations in *iters.
+// Member-segmented solve (sors_set_members): one PCG per member in the same
+// launches.  Tolerances per member: eta relative to its own residual, or the
+// absolute target of the call, or (a re-solve: eta 0, absolute target set)
+// eta^2 ||b_k||^2 remembered from its last relative solve.  Summaries for the
+// callers: the most iterations of any member, breakdown if any member broke
+// down, squared norms summed over members.
+template <typename HT, typename VT>
+int pcg_solve_members(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g) {
+    const int tol_mode = (eta > 0.0 && abs_tol == 0.0) ? 1 : ((eta == 0.0 && abs_tol > 0.0) ? 2 : 0);
+    launch_bpcg_init<VT>(h->batch, g ? g : h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0,
+                         eta * eta, abs_tol * abs_tol, tol_mode, h->s.pcg_max_iter, h->proj_flag, h->proj_n,
+                         h->stream);
+    CK(cudaGetLastError());
+    const int nm = h->batch.nmem;
+    const int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
+    for (int c = 0; c < maxchunks; c++) {
+        CK(cudaMemcpyAsync(h->ms_h.data(), h->batch.ms, sizeof(MemberScalars) * nm, cudaMemcpyDeviceToHost,
+                           h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        bool all = true;
+        for (int k = 0; k < nm && all; k++) all = h->ms_h[k].done != 0;
+        if (all) break;
+        int st = pcg_chunk<HT, VT>(h);
+        if (st) return st;
+    }
+    CK(cudaMemcpyAsync(h->ms_h.data(), h->batch.ms, sizeof(MemberScalars) * nm, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    DevScalars& sh = *h->sc_host;
+    sh.it = 0; sh.breakdown = 0; sh.done = 1; sh.bnorm2 = 0.0; sh.rr = 0.0; sh.rz = 0.0;
+    bool first_iteration_breakdown = false;
+    for (int k = 0; k < nm; k++) {
+        const MemberScalars& m = h->ms_h[k];
+        sh.it = std::max(sh.it, m.it);
+        sh.bnorm2 += m.bnorm2;
+        sh.rr += m.rr;
+        if (!m.breakdown) continue;
+        sh.breakdown = 1;
+        first_iteration_breakdown |= m.it == 0;
+        // this member's breaking direction: its nodes of p1 (it even) or p0 (it odd)
+        const int n0 = h->mem_node0_h[k], n1 = h->mem_node0_h[k + 1];
+        const VT* pb = (const VT*)((m.it & 1) ? h->p0 : h->p1) + 4 * (size_t)n0;
+        std::vector<VT> pv((size_t)4 * (n1 - n0));
+        CK(cudaMemcpyAsync(pv.data(), pb, sizeof(VT) * pv.size(), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        double pp = 0.0;
+        for (size_t i = 0; i < pv.size(); i++)
+            if ((i & 3) != 3) pp += (double)pv[i] * (double)pv[i];
+        h->step_indefinite++;
+        if (pp > 0.0) h->step_min_rq = std::min(h->step_min_rq, m.pq / pp);
+    }
+    *iters = sh.it;
+    if (first_iteration_breakdown && !(h->s.project_spd == 2 && !h->proj_fallback))
+        return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
+    return SORS_OK;
+}
+
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
+    if (h->batch.nmem > 1) return pcg_solve_members<HT, VT>(h, eta, abs_tol, iters, g);
     // the two-level preconditioner: with a constraint projection (SQP, adjoint)
     // the correction is projected too, so the preconditioner stays SPD on the
     // free subspace (the coarse matrix itself is built without the projection)
-    h->tl_active = h->s.two_level && h->cargs.nc > 0;
+    h->tl_active = h->s.two_level && h->cargs.nc > 0 && h->batch.nmem <= 1;
     bool refreshed = false;
     if (h->tl_active && !h->tl_ready) {
         const int nc = h->cargs.nc;
@@ -2379,6 +2449,53 @@ int sors_set_assembly_variant(SorsHandle* h, int32_t variant) {
 }
 
 int64_t sors_assembly_chunks(SorsHandle* h) { return h ? (int64_t)h->chunks.nchunks : 0; }
+
+int sors_set_members(SorsHandle* h, const int32_t* node_offsets, int32_t n_members) {
+    if (!h || (n_members > 0 && !node_offsets)) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    if (n_members <= 1) {
+        h->batch.nmem = 0;
+        return SORS_OK;
+    }
+    if (node_offsets[0] != 0 || node_offsets[n_members] != h->N)
+        return fail(SORS_ERR_ARG, "member node offsets must run from 0 to the node count");
+    for (int k = 0; k < n_members; k++)
+        if (node_offsets[k + 1] <= node_offsets[k]) return fail(SORS_ERR_ARG, "member node offsets must increase");
+    // no element may couple two members
+    std::vector<int> conn((size_t)h->E * h->nv);
+    if (!conn.empty()) CK(d2h(h, conn.data(), h->conn, sizeof(int) * conn.size()));
+    std::vector<int> mem_of(h->N);
+    for (int k = 0; k < n_members; k++)
+        for (int i = node_offsets[k]; i < node_offsets[k + 1]; i++) mem_of[i] = k;
+    for (int e = 0; e < h->E; e++)
+        for (int v = 1; v < h->nv; v++)
+            if (mem_of[conn[(size_t)e * h->nv + v]] != mem_of[conn[(size_t)e * h->nv]])
+                return fail(SORS_ERR_ARG, "an element joins two members");
+    std::vector<int> blk0(n_members + 1, 0), blk_mem;
+    for (int k = 0; k < n_members; k++) {
+        const int nb = (node_offsets[k + 1] - node_offsets[k] + kBatchThreads - 1) / kBatchThreads;
+        blk0[k + 1] = blk0[k] + nb;
+        for (int b = 0; b < nb; b++) blk_mem.push_back(k);
+    }
+    BatchArgs& b = h->batch;
+    int *d_node0 = nullptr, *d_blk0 = nullptr, *d_blkmem = nullptr;
+    if ((st = upload(h, &d_node0, node_offsets, (size_t)n_members + 1))) return st;
+    if ((st = upload(h, &d_blk0, blk0.data(), blk0.size()))) return st;
+    if ((st = upload(h, &d_blkmem, blk_mem.data(), blk_mem.size()))) return st;
+    MemberScalars* d_ms = nullptr;
+    double* d_part = nullptr;
+    if ((st = dalloc_t(h, &d_ms, (size_t)n_members))) return st;
+    CK(dzero(h, d_ms, sizeof(MemberScalars) * n_members));
+    if ((st = dalloc_t(h, &d_part, (size_t)2 * blk_mem.size()))) return st;
+    b.mem_node0 = d_node0; b.mem_blk0 = d_blk0; b.blk_mem = d_blkmem; b.ms = d_ms; b.partials = d_part;
+    b.nblocks = (int)blk_mem.size();
+    b.nmem = n_members;
+    h->mem_node0_h.assign(node_offsets, node_offsets + n_members + 1);
+    h->ms_h.assign(n_members, MemberScalars{});
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
 
 int sors_last_step_curvature(SorsHandle* h, double* min_rayleigh, int32_t* indefinite_solves) {
     if (!h || !min_rayleigh || !indefinite_solves) return fail(SORS_ERR_ARG, "NULL argument");

@@ -134,6 +134,32 @@ struct PressureArgs {
     double* f_ext;              // 3N (written for surface nodes)
 };
 
+// Member-segmented PCG (batched.cu): a handle holding several independent
+// meshes runs one preconditioned CG per member in the same launches.  Thread
+// blocks of kBatchThreads nodes never straddle members.
+constexpr int kBatchThreads = 256;
+struct MemberScalars {
+    double rz, rr, pq, alpha, beta, tol2, bnorm2, abs2;
+    int it, done, breakdown, maxit;
+    unsigned counter[4];
+};
+struct BatchArgs {
+    int nmem = 0, nblocks = 0;
+    const int* mem_node0 = nullptr;   // nmem + 1: first node of each member
+    const int* mem_blk0 = nullptr;    // nmem + 1: first thread block of each member
+    const int* blk_mem = nullptr;     // nblocks: member of each thread block
+    MemberScalars* ms = nullptr;      // nmem
+    double* partials = nullptr;       // 2 per thread block
+};
+template <typename VT>
+void launch_bpcg_init(const BatchArgs& b, const double* g, const VT* Minv, VT* x, VT* r, VT* z, VT* p0, double eta2,
+                      double abs_tol2, int tol_mode, int maxit, const uint8_t* pflag, const double4* pn,
+                      cudaStream_t st);
+template <typename HT, typename VT>
+void launch_bpcg_iter(const BatchArgs& b, const int* row_ptr, const int* col, const HT* H, const VT* Minv,
+                      const VT* z_in, const VT* p_old, VT* p_new, VT* qv, VT* x, VT* r, VT* z,
+                      const uint8_t* pflag, const double4* pn, cudaStream_t st);
+
 // Caps the grid of every kernel launched from this thread (kernels.cu).
 void set_grid_cap(int blocks);
 

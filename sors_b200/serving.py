@@ -15,7 +15,13 @@ and one captured CUDA graph per chunk then serve all of them at once (each
 kernel launch does the work of the whole batch).  Each rollout keeps its own
 disk indenter (an independent disk contact group).  Results are sliced back
 per request; they equal the rollout run alone up to the solver tolerances
-(the Krylov iterates of the union differ from those of each mesh alone).
+(the union's Newton / SQP iterations continue until every member has
+converged, and its dot products are summed in a different order).
+
+Inside a union every linear solve runs one preconditioned CG per member
+(sors_set_members): the members share each kernel launch but keep their own
+step lengths, tolerances and convergence, so a union's solves take as many
+iterations as its slowest member alone, not those of the joined system.
 
 Every admitted batch keeps its union mesh, state and Hessian pattern resident
 in its own handle (one CUDA stream) and is stepped by a worker thread, so the
@@ -336,6 +342,11 @@ def build_union(batch, device: int = 0, max_blocks: int = 0):
         _lib.check(_lib.load().sors_set_disk_contact_groups(en._h, dp(cen), dp(nrm), dp(rad), len(disks), ip(dsurf),
                                                             ip(ptr)))
         en._constraints = list(en._constraints) + ["diskContact"]
+    if len(batch) > 1:
+        # one PCG per member inside the shared launches (batched.cu)
+        node_offsets = np.ascontiguousarray(offs, dtype=np.int32)
+        _lib.check(_lib.load().sors_set_members(en._h, node_offsets.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                len(batch)))
     slices = [(3 * offs[k], 3 * offs[k + 1]) for k in range(len(batch))]
     return en, sol, slices, disks
 

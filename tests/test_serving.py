@@ -100,3 +100,46 @@ def test_batched_equals_alone(precision):
         err = np.abs(res.final - alone[tag]).max()
         # FP64: within the SQP stopping tolerance ||dx|| < 1e-9 m; mixed: 1e-6 of the displacement
         assert err <= (1e-9 if precision == "fp64" else 1e-6 * disp), (tag, err, disp)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_member_segmented_pcg_equals_alone(precision):
+    # three cantilevers of different lengths in one handle, declared as three
+    # members: each member's trajectory equals its run alone
+    import ctypes as C
+
+    from sors_b200 import _lib, meshes
+    from tests.helpers import make_pair
+    parts = [meshes.cantilever_tets(n, 2, 2, (0.005 * n, 0.01, 0.01)) for n in (4, 8, 12)]
+    alone = []
+    for X, T in parts:
+        en, sol, _, _ = make_pair(X, T, dt=1e-3, precision=precision, res_tol=1e-8)
+        q = X.ravel().copy()
+        for _ in range(5):
+            q = sol.step(q, en)
+        alone.append(q)
+    offs = np.cumsum([0] + [X.shape[0] for X, _ in parts]).astype(np.int32)
+    Xu = np.vstack([X for X, _ in parts])
+    Tu = np.vstack([T + offs[k] for k, (_, T) in enumerate(parts)]).astype(np.int32)
+    en, sol, _, _ = make_pair(Xu, Tu, dt=1e-3, precision=precision, res_tol=1e-8)
+    _lib.check(_lib.load().sors_set_members(en.handle(), offs.ctypes.data_as(C.POINTER(C.c_int32)), len(parts)))
+    q = Xu.ravel().copy()
+    for _ in range(5):
+        q = sol.step(q, en)
+    for k, (X, _) in enumerate(parts):
+        qk = q[3 * offs[k]:3 * offs[k + 1]]
+        disp = np.abs(alone[k] - X.ravel()).max()
+        err = np.abs(qk - alone[k]).max()
+        assert err <= (1e-9 if precision == "fp64" else 1e-6 * disp), (k, err, disp)
+
+
+def test_members_reject_a_coupling_element():
+    import ctypes as C
+
+    from sors_b200 import _lib, meshes
+    from tests.helpers import make_pair
+    X, T = meshes.cantilever_tets(4, 2, 2, (0.02, 0.01, 0.01))
+    en, _, _, _ = make_pair(X, T, dt=1e-3)
+    offs = np.array([0, 10, X.shape[0]], np.int32)  # cuts through the beam
+    st = _lib.load().sors_set_members(en.handle(), offs.ctypes.data_as(C.POINTER(C.c_int32)), 2)
+    assert st == 1 and "joins two members" in _lib.last_error()
