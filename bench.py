@@ -612,7 +612,7 @@ def run_serve(args):
         r = np.random.default_rng(11)
         out = []
         for i in range(args.rollouts):
-            tets = float(np.exp(r.uniform(np.log(5e3), np.log(2.5e5))))
+            tets = float(np.exp(r.uniform(np.log(5e3), np.log(args.tets_max))))
             n = max(2, int(round((tets / 6.0) ** (1.0 / 3.0))))
             out.append(serving.poke_cube_request(r, n, tag=i, steps=args.rollout_steps, dt=1e-2, precision=precision))
         return out
@@ -662,7 +662,8 @@ def run_serve(args):
                  max(np.abs(final_p[r.tag] - by_tag[r.tag].vertices.ravel()).max(), 1e-30))
            for r in res_m if r.final is not None and r.tag in final_p]
     print(json.dumps({"workload": f"poke sweep: {args.rollouts} rollouts x {args.rollout_steps} steps, "
-                                  f"Poisson arrivals at {args.rate}/s, 6-tet cubes 5k-250k tets on z=0 "
+                                  f"Poisson arrivals at {args.rate}/s, 6-tet cubes 5k-{args.tets_max / 1e3:.0f}k "
+                                  f"tets (log-uniform) on z=0 "
                                   f"pressed by a 10 mm disk moving 10 mm down (minimize_SQP contact)",
                       "slots": args.slots, "batch_max": args.batch, "served_mixed": served,
                       "plain_fp64_sequential": plain,
@@ -714,6 +715,7 @@ def main():
     ap.add_argument("--rollouts", type=int, default=512)
     ap.add_argument("--rollout-steps", type=int, default=100)
     ap.add_argument("--rate", type=float, default=2.0, help="serve: Poisson arrival rate (rollouts/s)")
+    ap.add_argument("--tets-max", type=float, default=2.5e5, help="serve: upper end of the log-uniform tet counts")
     ap.add_argument("--slots", type=int, default=16, help="serve: concurrent handles")
     ap.add_argument("--batch", type=int, default=1, help="serve: rollouts packed into one union handle (1: none; unions measured slower on the poke mix)")
     ap.add_argument("--baseline-sample", type=int, default=64,
