@@ -628,7 +628,7 @@ def run_serve(args):
                 "step_latency_p99_ms": 1e3 * serving.percentile(steps, 99),
                 "rollout_latency_p50_s": serving.percentile(lat, 50),
                 "rollout_latency_p99_s": serving.percentile(lat, 99),
-                "tets_total": int(sum(q.elements.shape[0] for q in reqs))}
+                "tets_total": int(sum(q.elements.shape[0] for q in reqs.values()))}
 
     rng = np.random.default_rng(7)
     gaps = rng.exponential(1.0 / args.rate, size=args.rollouts)

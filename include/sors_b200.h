@@ -271,6 +271,8 @@ typedef struct SorsKernelProfile {
     double tl_restrict_ms, tl_coarse_z_ms, tl_restrict_bytes, tl_coarse_z_bytes;
     /* p = z + beta p_old, formed before the SpMV (padded, 4 values per node) */
     double form_p_ms, form_p_bytes;
+    /* the assembly launch without the Hessian (gradient rows only) */
+    double assemble_grad_ms;
 } SorsKernelProfile;
 int sors_profile_kernels(SorsHandle* h, int32_t iters, SorsKernelProfile* out);
 

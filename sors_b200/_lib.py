@@ -54,7 +54,7 @@ class SorsKernelProfile(C.Structure):
     _fields_ = [(n, C.c_double) for n in ("assemble_ms", "spmv_ms", "pcg_update_ms", "energy_ms", "assemble_bytes",
                                           "spmv_bytes", "pcg_update_bytes", "energy_bytes", "tl_restrict_ms",
                                           "tl_coarse_z_ms", "tl_restrict_bytes", "tl_coarse_z_bytes",
-                                          "form_p_ms", "form_p_bytes")]
+                                          "form_p_ms", "form_p_bytes", "assemble_grad_ms")]
 
 
 # (name, restype, argtypes) of every exported symbol declared in include/sors_b200.h

@@ -2532,6 +2532,16 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
     CK(cudaEventSynchronize(b));
     CK(cudaEventElapsedTime(&ms, a, b));
     out->assemble_ms = ms / iters;
+    {
+        AsmArgs<HT> ag = aa;
+        ag.want_hess = 0;
+        CK(cudaEventRecord(a, h->stream));
+        for (int i = 0; i < iters; i++) launch_assemble<HT>(ag, h->max_pairs, h->stream);
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        CK(cudaEventElapsedTime(&ms, a, b));
+        out->assemble_grad_ms = ms / iters;
+    }
     if (aa.ch.nchunks > 0 && nv == 4 && !aa.project && !aa.mus.group) {
         // chunked element-owner kernel, each compulsory input and output once:
         // conn, shape gradients + volume, (mu, lambda); q, mask, mass; chunk rows

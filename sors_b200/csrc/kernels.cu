@@ -697,12 +697,7 @@ ChunkLimits chunk_limits(int hsize, int material) {
 size_t chunk_region_bytes(int hsize, int material, int max_pairs) {
     (void)max_pairs;
     const ChunkLimits l = chunk_limits(hsize, material);
-    // gradient pairs, later the chunk's item codes (4 per pair) and the item
-    // offset of each block (a row has at most one block per incident pair
-    // vertex, at most 3 pairs + 1 blocks per pair)
-    const size_t grad = (size_t)l.pairs * 3 * sizeof(double);
-    const size_t items = (size_t)l.pairs * 4 * sizeof(uint16_t) + ((size_t)l.pairs * 3 + l.rows + 1) * sizeof(uint16_t);
-    return ((grad > items ? grad : items) + 15) / 16 * 16;
+    return ((size_t)l.pairs * 3 * sizeof(double) + 15) / 16 * 16;
 }
 
 size_t chunk_smem_bytes(int hsize, int material, int max_pairs) {
@@ -877,24 +872,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
         a.g_int[3 * (size_t)row + 2] = g2;
     }
     if (!a.want_hess) return;
-    // the chunk's item codes and each block's first item, chunk-local, into the
-    // gradient pairs' memory (rows' items are contiguous in slot order)
-    __syncthreads();
-    uint16_t* sitem = reinterpret_cast<uint16_t*>(smem_raw);
-    uint16_t* sbi = sitem + 4 * (size_t)a.ch.pairs_max;
-    {
-        const int warp = threadIdx.x >> 5;
-        for (int p = warp; p < nr; p += blockDim.x >> 5) {
-            const int b0 = srp0[p], nb = sblk0[p + 1] - sblk0[p];
-            const int base = __ldg(a.slot_item_ptr + b0);
-            const int nit = 4 * (spair0[p + 1] - spair0[p]);
-            const int l0 = 4 * spair0[p];
-            for (int it = lane; it < nit; it += 32) sitem[l0 + it] = __ldg(a.ch.items + base + it);
-            for (int k = lane; k < nb; k += 32) sbi[sblk0[p] + k] = (uint16_t)(l0 + __ldg(a.slot_item_ptr + b0 + k) - base);
-        }
-        if (threadIdx.x == 0) sbi[sblk0[nr]] = (uint16_t)(4 * spair0[nr]);
-    }
-    __syncthreads();
     // B. Hessian blocks, one thread per block, the chunk's diagonal blocks
     // first: a diagonal block sums one item per incident pair (about four
     // times an off-diagonal block's), so grouping them keeps warps balanced.
@@ -921,13 +898,13 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             bg = srp0[pos] + kb;
         }
         const int row = srow[pos];
-        const int i0 = sbi[sblk0[pos] + kb], i1 = sbi[sblk0[pos] + kb + 1];
+        const int i0 = __ldg(a.slot_item_ptr + bg), i1 = __ldg(a.slot_item_ptr + bg + 1);
         HT acc[9];
 #pragma unroll
         for (int k = 0; k < 9; k++) acc[k] = HT(0);
         if (diag) {
             for (int it = i0; it < i1; ++it) {
-                const unsigned item = sitem[it];
+                const unsigned item = __ldg(a.ch.items + it);
                 const int es = (int)(item >> 4), v = (item >> 2) & 3;
                 const HT hmu = gen[0 * EM + es], c1 = gen[1 * EM + es] - gen[2 * EM + es];
                 const HT dd = gen[(G::kDD + dd_index(v, v)) * EM + es];
@@ -953,7 +930,7 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             acc[3] = acc[1]; acc[6] = acc[2]; acc[7] = acc[5];
         } else {
             for (int it = i0; it < i1; ++it) {
-                const unsigned item = sitem[it];
+                const unsigned item = __ldg(a.ch.items + it);
                 const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
                 const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
                 const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
