@@ -243,12 +243,18 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+_asm_variant = 0
+
+
 def build_energy(precision, X, T, E, mask, val, device):
+    from sors_b200 import _lib
     from sors_b200 import py_sors as ps
     s = make_settings(precision)
     s.device = device
     en = ps.EnergyTet.from_arrays(X, T, s, np.array([0.0, 0.0, -9.81]), 0.0, density=1070.0, youngsModulus=E,
                                   poissonsRatio=0.45, neumannBCmask=mask, neumannBCvalue=val)
+    if _asm_variant:
+        _lib.check(_lib.load().sors_set_assembly_variant(en.handle(), _asm_variant))
     return en, ps.Solver(s)
 
 
@@ -390,6 +396,7 @@ def run_gpu(args, rank, world, local_rank):
                    "hessian_projection": _projection,
                    "preconditioner": "two-level" if _two_level else "block Jacobi",
                    "numbering": "random permutation" if _shuffle else "grid order (x fastest)",
+                   "assembly": ["chunked element-owner", "row-owner", "chunked, two passes"][_asm_variant],
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "inputs larger than L2 (assembled system ~1 GB resident), no flush"},
         "newton_steps_per_s": world * args.steps / (ms / 1e3),
@@ -705,6 +712,8 @@ def main():
                     help="SPD projection of the element Hessians: always, never, or only where PCG meets "
                          "negative curvature")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--assembly", type=int, default=0, choices=[0, 1, 2],
+                    help="assembly kernel: 0 chunked element-owner, 1 row-owner, 2 chunked in two passes")
     ap.add_argument("--shuffle", action="store_true",
                     help="renumber the block's nodes and elements by a seeded random permutation")
     ap.add_argument("--no-phases", action="store_true",
@@ -730,7 +739,8 @@ def main():
                     help="assemble once at rest and launch each hot kernel 3 times (short ncu capture target)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    global _projection, _two_level, _shuffle
+    global _projection, _two_level, _shuffle, _asm_variant
+    _asm_variant = args.assembly
     _projection = args.projection
     _two_level = args.two_level
     _shuffle = args.shuffle

@@ -289,8 +289,11 @@ int64_t sors_evaluation_count(SorsHandle* h, int32_t with_hessian);
  * 0 (default) the element-owner kernel over node chunks wherever it applies
  * (exact Neo-Hookean or stable Neo-Hookean tets without fibre terms; the
  * projected Hessian, fibres, the quartic test element and hexes always use
- * the row-owner kernel), 1 the row-owner kernel everywhere.  Both give the
- * same Hessian values; no counterpart in the reference.  Diagnostic only. */
+ * the row-owner kernel), 1 the row-owner kernel everywhere, 2 the chunked
+ * kernel in two passes (every element evaluated once into records in device
+ * memory, which the chunks then load; allocates those records on first use).
+ * All give the same Hessian values to rounding; no counterpart in the
+ * reference.  Diagnostic only. */
 int sors_set_assembly_variant(SorsHandle* h, int32_t variant);
 
 /* Node chunks of the element-owner assembly (0: the mesh uses the row-owner

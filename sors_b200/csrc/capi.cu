@@ -84,7 +84,9 @@ struct SorsHandle {
     // element-owner tet assembly: node chunks (build_tet_chunks)
     ChunkArgs chunks;
     long long chunk_elem_total = 0;  // sum over chunks of their element counts
-    int asm_variant = 0;  // 0: chunked element-owner where it applies, 1: row-owner
+    int asm_variant = 0;  // 0: chunked element-owner where it applies, 1: row-owner, 2: two-pass chunked
+    void* chunk_gen = nullptr;        // two-pass variant: element generator records
+    double* chunk_gradg = nullptr;    // two-pass variant: element gradient rows
     uint8_t* node_mask = nullptr;
     std::vector<uint8_t> mask_h;
     std::vector<int> row_ptr_h, col_h;
@@ -608,7 +610,7 @@ enum AsmMode { kAsmStep = 0, kAsmMaskedIdentity = 1, kAsmFull = 2 };
 template <typename HT>
 AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int project) {
     AsmArgs<HT> a;
-    a.N = h->N; a.nv = h->nv; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
+    a.N = h->N; a.nv = h->nv; a.E = h->E; a.X = h->X; a.q = h->q; a.conn = h->conn; a.mat = h->mat; a.mus = muscles(h);
     a.tshape = h->tshape;
     a.pair_ptr = h->pair_ptr; a.pair_ev = h->pair_ev; a.row_ptr = h->row_ptr; a.col = h->col;
     a.diag_slot = h->diag_slot;
@@ -622,7 +624,11 @@ AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int
     a.want_hess = want_hess ? 1 : 0;
     a.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0;
     a.inertia_coef = inertia_coef(h, dt);
-    if (h->asm_variant == 0) a.ch = h->chunks;
+    if (h->asm_variant == 0 || h->asm_variant == 2) a.ch = h->chunks;
+    if (h->asm_variant == 2) {
+        a.ch.gen = h->chunk_gen;
+        a.ch.gradg = h->chunk_gradg;
+    }
     return a;
 }
 
@@ -2443,7 +2449,14 @@ int64_t sors_kernel_launch_count(void) { return (int64_t)g_kernel_launches.load(
 
 int sors_set_assembly_variant(SorsHandle* h, int32_t variant) {
     if (!h) return fail(SORS_ERR_ARG, "NULL handle");
-    if (variant != 0 && variant != 1) return fail(SORS_ERR_ARG, "assembly variant must be 0 or 1");
+    if (variant < 0 || variant > 2) return fail(SORS_ERR_ARG, "assembly variant must be 0, 1 or 2");
+    if (variant == 2 && h->chunks.nchunks > 0 && !h->chunk_gen) {
+        int st;
+        if ((st = set_device(h))) return st;
+        const size_t rec = h->s.material == 2 ? 40 : 28;  // generator fields padded to 16 bytes
+        if ((st = dalloc(h, &h->chunk_gen, (size_t)h->E * rec * hsize(h)))) return st;
+        if ((st = dalloc_t(h, &h->chunk_gradg, (size_t)h->E * 12))) return st;
+    }
     h->asm_variant = variant;
     return SORS_OK;
 }

@@ -707,7 +707,148 @@ size_t chunk_smem_bytes(int hsize, int material, int max_pairs) {
            (size_t)(5 * l.rows + 2) * sizeof(int);
 }
 
+// Hessian generator and gradient rows of one tet (the element math of the
+// chunked assembly): out.grad(v, r, x) receives V (P d_v)_r for the vertices
+// out.wants(v), out.gen(f, x) generator field f.  Returns false for an
+// inverted element (J <= 0; J == 0 for stable Neo-Hookean), whose generator is
+// zero.
+template <typename HT, bool SNH, typename Sink>
+__device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, bool want_hess, Sink& out) {
+    using G = ChunkGen<SNH>;
+    const double2* ts = reinterpret_cast<const double2*>(a.tshape + (size_t)e * 10);
+    double t[10];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const double2 u = __ldg(ts + k);
+        t[2 * k] = u.x; t[2 * k + 1] = u.y;
+    }
+    const int4 cn = __ldg(reinterpret_cast<const int4*>(a.conn) + e);
+    const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
+    double d[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        d[0][c] = t[c]; d[1][c] = t[3 + c]; d[2][c] = t[6 + c];
+        d[3][c] = -(t[c] + t[3 + c] + t[6 + c]);
+    }
+    const double V = t[9];
+    double F[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) F[k] = 0.0;
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            const double xr = a.q[3 * (size_t)nodes[w] + r];
+#pragma unroll
+            for (int c = 0; c < 3; c++) F[r * 3 + c] += xr * d[w][c];
+        }
+    }
+    const double2 m = __ldg(a.mat + e);
+    double C[9];
+    cof3(F, C);
+    const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+    const double iJ = 1.0 / J;
+    double IC = 0.0;
+    if (SNH) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+    }
+    const double alpha = SNH ? 1.0 + 0.75 * m.x / m.y : 0.0;
+    const double logJ = SNH ? 0.0 : log(J);
+    const double pa = SNH ? m.x * (1.0 - 1.0 / (IC + 1.0)) : m.x;
+    const double pb = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
+    double P[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) P[k] = pa * F[k] + pb * C[k] * iJ;
+#pragma unroll
+    for (int v = 0; v < 4; v++) {
+        if (!out.wants(v)) continue;
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+            double pr = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; c++) pr += P[r * 3 + c] * d[v][c];
+            out.grad(v, r, V * pr);
+        }
+    }
+    const bool eok = SNH ? (J != 0.0) : (J > 0.0);
+    if (!want_hess) return eok;
+    if (!eok) {
+#pragma unroll
+        for (int f = 0; f < G::kFields; f++) out.gen(f, HT(0));
+        return false;
+    }
+    HT Gh[9], dh[4][3];
+#pragma unroll
+    for (int k = 0; k < 9; k++) Gh[k] = (HT)(C[k] * iJ);
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) dh[v][c] = (HT)d[v][c];
+    out.gen(0, (HT)(V * pa));
+    out.gen(1, (HT)(SNH ? V * m.y * (2.0 * J - alpha) * J : V * m.y));
+    out.gen(2, (HT)(V * pb));
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+            out.gen((G::kA + v * 3 + r), Gh[r * 3 + 0] * dh[v][0] + Gh[r * 3 + 1] * dh[v][1] + Gh[r * 3 + 2] * dh[v][2]);
+#pragma unroll
+    for (int v = 0; v < 4; v++)
+#pragma unroll
+        for (int w = v; w < 4; w++)
+            out.gen((G::kDD + dd_index(v, w)), dh[v][0] * dh[w][0] + dh[v][1] * dh[w][1] + dh[v][2] * dh[w][2]);
+    if (SNH) {
+        out.gen(G::kH4, (HT)(V * 2.0 * m.x / ((IC + 1.0) * (IC + 1.0))));
+        HT Fh[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
+#pragma unroll
+        for (int v = 0; v < 4; v++)
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+                out.gen((G::kF + v * 3 + r), Fh[r * 3 + 0] * dh[v][0] + Fh[r * 3 + 1] * dh[v][1] + Fh[r * 3 + 2] * dh[v][2]);
+    }
+    return true;
+}
+
+template <typename HT>
+struct SmemGenSink {
+    HT* g;
+    int EM, s;
+    double* gslot;
+    unsigned short slots[4];
+    __device__ __forceinline__ bool wants(int v) const { return slots[v] != 0xffff; }
+    __device__ __forceinline__ void grad(int v, int r, double x) { gslot[3 * slots[v] + r] = x; }
+    __device__ __forceinline__ void gen(int f, HT x) { g[f * EM + s] = x; }
+};
+
+template <typename HT>
+struct GlobalGenSink {
+    HT* rec;
+    double* gr;
+    __device__ __forceinline__ bool wants(int) const { return true; }
+    __device__ __forceinline__ void grad(int v, int r, double x) { gr[3 * v + r] = x; }
+    __device__ __forceinline__ void gen(int f, HT x) { rec[f] = x; }
+};
+
+// Record stride of the element generators in memory (fields padded to 16 bytes).
 template <typename HT, bool SNH>
+__host__ __device__ constexpr int chunk_gen_stride() {
+    return (ChunkGen<SNH>::kFields * (int)sizeof(HT) + 15) / 16 * 16 / (int)sizeof(HT);
+}
+
+// Pass 1 of the two-pass chunked assembly: every tet once, one thread each.
+template <typename HT, bool SNH>
+__global__ void __launch_bounds__(128) k_tet_gen(AsmArgs<HT> a, int E) {
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= E) return;
+    GlobalGenSink<HT> sink{reinterpret_cast<HT*>(a.ch.gen) + (size_t)e * chunk_gen_stride<HT, SNH>(),
+                           a.ch.gradg + (size_t)e * 12};
+    if (!tet_generator<HT, SNH>(a, e, a.want_hess != 0, sink)) atomicOr(a.status, kFlagInverted);
+}
+
+template <typename HT, bool SNH, bool FROMGEN>
 __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT> a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using G = ChunkGen<SNH>;
@@ -750,106 +891,28 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
         }
         if (lane == 0) { spair0[nr] = pacc; sblk0[nr] = bacc; }
     }
-    // A. element generators and gradient pairs
+    // A. element generators and gradient pairs (evaluated here, or loaded
+    // from the records of k_tet_gen)
     bool ok = true;
     for (int s = threadIdx.x; s < ne; s += blockDim.x) {
         const int e = __ldg(a.ch.ch_elems + e0 + s);
         const ushort4 sl = a.ch.ch_eslot[e0 + s];
-        const double2* ts = reinterpret_cast<const double2*>(a.tshape + (size_t)e * 10);
-        double t[10];
-#pragma unroll
-        for (int k = 0; k < 5; k++) {
-            const double2 u = __ldg(ts + k);
-            t[2 * k] = u.x; t[2 * k + 1] = u.y;
-        }
-        const int4 cn = __ldg(reinterpret_cast<const int4*>(a.conn) + e);
-        const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
-        double d[4][3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            d[0][c] = t[c]; d[1][c] = t[3 + c]; d[2][c] = t[6 + c];
-            d[3][c] = -(t[c] + t[3 + c] + t[6 + c]);
-        }
-        const double V = t[9];
-        double F[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) F[k] = 0.0;
-#pragma unroll
-        for (int w = 0; w < 4; w++) {
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-                const double xr = a.q[3 * (size_t)nodes[w] + r];
-#pragma unroll
-                for (int c = 0; c < 3; c++) F[r * 3 + c] += xr * d[w][c];
-            }
-        }
-        const double2 m = __ldg(a.mat + e);
-        double C[9];
-        cof3(F, C);
-        const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
-        const double iJ = 1.0 / J;
-        double IC = 0.0;
-        if (SNH) {
-#pragma unroll
-            for (int k = 0; k < 9; k++) IC += F[k] * F[k];
-        }
-        const double alpha = SNH ? 1.0 + 0.75 * m.x / m.y : 0.0;
-        const double logJ = SNH ? 0.0 : log(J);
-        const double pa = SNH ? m.x * (1.0 - 1.0 / (IC + 1.0)) : m.x;
-        const double pb = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
-        double P[9];
-#pragma unroll
-        for (int k = 0; k < 9; k++) P[k] = pa * F[k] + pb * C[k] * iJ;
         const unsigned short slots[4] = {sl.x, sl.y, sl.z, sl.w};
+        if (FROMGEN) {
+            const HT* rec = reinterpret_cast<const HT*>(a.ch.gen) + (size_t)e * chunk_gen_stride<HT, SNH>();
+            const double* gr = a.ch.gradg + (size_t)e * 12;
 #pragma unroll
-        for (int v = 0; v < 4; v++) {
-            if (slots[v] == 0xffff) continue;
+            for (int v = 0; v < 4; v++) {
+                if (slots[v] == 0xffff) continue;
 #pragma unroll
-            for (int r = 0; r < 3; r++) {
-                double pr = 0.0;
-#pragma unroll
-                for (int c = 0; c < 3; c++) pr += P[r * 3 + c] * d[v][c];
-                gslot[3 * slots[v] + r] = V * pr;
+                for (int r = 0; r < 3; r++) gslot[3 * slots[v] + r] = __ldg(gr + 3 * v + r);
             }
-        }
-        const bool eok = SNH ? (J != 0.0) : (J > 0.0);
-        ok &= eok;
-        if (!a.want_hess) continue;
-        if (!eok) {
+            if (a.want_hess)
 #pragma unroll
-            for (int f = 0; f < G::kFields; f++) gen[f * EM + s] = HT(0);
-            continue;
-        }
-        HT Gh[9], dh[4][3];
-#pragma unroll
-        for (int k = 0; k < 9; k++) Gh[k] = (HT)(C[k] * iJ);
-#pragma unroll
-        for (int v = 0; v < 4; v++)
-#pragma unroll
-            for (int c = 0; c < 3; c++) dh[v][c] = (HT)d[v][c];
-        gen[0 * EM + s] = (HT)(V * pa);
-        gen[1 * EM + s] = (HT)(SNH ? V * m.y * (2.0 * J - alpha) * J : V * m.y);
-        gen[2 * EM + s] = (HT)(V * pb);
-#pragma unroll
-        for (int v = 0; v < 4; v++)
-#pragma unroll
-            for (int r = 0; r < 3; r++)
-                gen[(G::kA + v * 3 + r) * EM + s] = Gh[r * 3 + 0] * dh[v][0] + Gh[r * 3 + 1] * dh[v][1] + Gh[r * 3 + 2] * dh[v][2];
-#pragma unroll
-        for (int v = 0; v < 4; v++)
-#pragma unroll
-            for (int w = v; w < 4; w++)
-                gen[(G::kDD + dd_index(v, w)) * EM + s] = dh[v][0] * dh[w][0] + dh[v][1] * dh[w][1] + dh[v][2] * dh[w][2];
-        if (SNH) {
-            gen[G::kH4 * EM + s] = (HT)(V * 2.0 * m.x / ((IC + 1.0) * (IC + 1.0)));
-            HT Fh[9];
-#pragma unroll
-            for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
-#pragma unroll
-            for (int v = 0; v < 4; v++)
-#pragma unroll
-                for (int r = 0; r < 3; r++)
-                    gen[(G::kF + v * 3 + r) * EM + s] = Fh[r * 3 + 0] * dh[v][0] + Fh[r * 3 + 1] * dh[v][1] + Fh[r * 3 + 2] * dh[v][2];
+                for (int f = 0; f < G::kFields; f++) gen[f * EM + s] = __ldg(rec + f);
+        } else {
+            SmemGenSink<HT> sink{gen, EM, s, gslot, {slots[0], slots[1], slots[2], slots[3]}};
+            ok &= tet_generator<HT, SNH>(a, e, a.want_hess != 0, sink);
         }
     }
     if (!ok) atomicOr(a.status, kFlagInverted);
@@ -993,12 +1056,21 @@ static void set_smem_limit(K kernel, size_t smem, std::atomic<int>* done) {
 
 template <typename HT, bool SNH>
 static void launch_assemble_chunk(const AsmArgs<HT>& a, cudaStream_t st) {
-    static std::atomic<int> limit[kMaxDevices];
-    auto k = k_assemble_chunk<HT, SNH>;
+    static std::atomic<int> limit[2][kMaxDevices];
     const size_t smem = a.ch.smem_bytes;
-    set_smem_limit(k, smem, limit);
-    k<<<a.ch.nchunks, kChunkThreads, smem, st>>>(a);
-    counted();
+    if (a.ch.gen) {
+        // two passes: every element once, then the chunks load its records
+        k_tet_gen<HT, SNH><<<(a.E + 127) / 128, 128, 0, st>>>(a, a.E);
+        auto k = k_assemble_chunk<HT, SNH, true>;
+        set_smem_limit(k, smem, limit[1]);
+        k<<<a.ch.nchunks, kChunkThreads, smem, st>>>(a);
+        counted(2);
+    } else {
+        auto k = k_assemble_chunk<HT, SNH, false>;
+        set_smem_limit(k, smem, limit[0]);
+        k<<<a.ch.nchunks, kChunkThreads, smem, st>>>(a);
+        counted();
+    }
 }
 
 template <typename HT>

@@ -76,6 +76,8 @@ struct ChunkArgs {
     int rows_max = 0, elems_max = 0, pairs_max = 0;
     int region_bytes = 0;       // gradient pairs
     int smem_bytes = 0;         // dynamic shared memory of one chunk block
+    void* gen = nullptr;        // two-pass variant: generator records (HT, padded), E of them
+    double* gradg = nullptr;    // two-pass variant: V P d_v of every element vertex, 12 per element
 };
 
 // Chunk limits and shared-memory size of the chunked assembly for a Hessian
@@ -90,7 +92,7 @@ size_t chunk_smem_bytes(int hsize, int material, int max_pairs);
 // Row-owner assembly arguments (tet or hex).
 template <typename HT>
 struct AsmArgs {
-    int N, nv;
+    int N, nv, E;
     const double* X;        // 3N undeformed
     const double* q;        // 3N current
     const int* conn;        // E*nv

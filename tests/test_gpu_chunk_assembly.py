@@ -97,3 +97,27 @@ def test_inverted_element_reported(oracle):
     q[[a, b]] = q[[b, a]]  # swapping two vertices of one tet inverts it
     with pytest.raises(RuntimeError, match="Inverted Elements"):
         en.compute_hessian(q.ravel(), 5e-3)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("energy", ["neohookean", "stableneohookean"])
+def test_two_pass_chunked_matches_one_pass(oracle, precision, energy):
+    # variant 2: every element evaluated once into device records, then the
+    # chunks load them; the same generators, so the same sums
+    from sors_b200 import _lib
+    L = _lib.load()
+    X, T, E = _block(True)
+    rng = np.random.default_rng(14)
+    en, _, o, _ = make_pair(X, T, E=E, dt=5e-3, project=False, precision=precision, energy=energy)
+    q = deform(X, rng, amp=0.04)
+    g1 = en.compute_gradient(q, 5e-3)
+    H1 = en.compute_hessian(q, 5e-3)
+    _lib.check(L.sors_set_assembly_variant(en.handle(), 2))
+    g2 = en.compute_gradient(q, 5e-3)
+    H2 = en.compute_hessian(q, 5e-3)
+    _lib.check(L.sors_set_assembly_variant(en.handle(), 0))
+    assert np.abs((H2 - H1).data).max(initial=0.0) <= 1e-6 * np.abs(H1.data).max()
+    assert rel_err(g2, g1) < 1e-14
+    if precision == "fp64":
+        Ho, _ = o.hessian_csr(q, 5e-3)
+        assert np.abs((H2 - Ho).data).max(initial=0.0) <= ELEM_TOL * np.abs(Ho.data).max()
