@@ -629,6 +629,7 @@ def run_serve(args):
         lat = [r.latency for r in res]
         failed = sorted((r.tag, r.error) for r in res if r.error)
         return {"rollouts": len(res), "rollouts_per_s": len(res) / wall, "makespan_s": wall,
+                "mean_batch": float(np.mean([r.batch for r in res])) if res else 0.0,
                 "failures": len(failed), "failed": [{"tag": t, "tets": int(reqs[t].elements.shape[0]), "error": e}
                                                     for t, e in failed],
                 "step_latency_p50_ms": 1e3 * serving.percentile(steps, 50),
