@@ -425,7 +425,7 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     if (chunk_smem_bytes(hsz, h->s.material, h->max_pairs) > 113 * 1024) return SORS_OK;
     for (int i = 0; i < N; i++) {
         const int np = ph.pair_ptr[i + 1] - ph.pair_ptr[i];
-        if (np > lim.pairs || np > lim.elems || 3 * np + 1 > lim.nodes) return SORS_OK;
+        if (np > lim.pairs || np > lim.elems) return SORS_OK;
     }
     // Morton order of the undeformed positions (21 bits per axis)
     double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
@@ -461,31 +461,18 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     std::vector<int> ch_ptr{0}, ch_rows, ch_eptr{0}, ch_elems;
     ch_rows.reserve(N);
     ch_elems.reserve((size_t)E * 3 / 2);
-    std::vector<int> mark(E, -1), nmark(N, -1);
-    int cur = 0, nr = 0, ne = 0, np = 0, nn = 0;
-    std::vector<int> fresh_nodes;
+    std::vector<int> mark(E, -1);
+    int cur = 0, nr = 0, ne = 0, np = 0;
     for (int o = 0; o < N; o++) {
         const int i = key[o].second;
         const int p0 = ph.pair_ptr[i], p1 = ph.pair_ptr[i + 1];
         int fresh = 0;
-        fresh_nodes.clear();
-        for (int t = p0; t < p1; t++) {
-            const int e = ph.pair_ev[t] >> 3;
-            if (mark[e] == cur) continue;
-            fresh++;
-            for (int w = 0; w < 4; w++) {
-                const int v = conn[(size_t)e * 4 + w];
-                if (nmark[v] != cur) fresh_nodes.push_back(v);
-            }
-        }
-        std::sort(fresh_nodes.begin(), fresh_nodes.end());
-        const int nfresh = (int)(std::unique(fresh_nodes.begin(), fresh_nodes.end()) - fresh_nodes.begin());
-        if (nr > 0 && (nr + 1 > lim.rows || ne + fresh > lim.elems || np + (p1 - p0) > lim.pairs ||
-                       nn + nfresh > lim.nodes)) {
+        for (int t = p0; t < p1; t++) fresh += mark[ph.pair_ev[t] >> 3] != cur;
+        if (nr > 0 && (nr + 1 > lim.rows || ne + fresh > lim.elems || np + (p1 - p0) > lim.pairs)) {
             cur++;
             ch_ptr.push_back((int)ch_rows.size());
             ch_eptr.push_back((int)ch_elems.size());
-            nr = ne = np = nn = 0;
+            nr = ne = np = 0;
         }
         ch_rows.push_back(i);
         nr++;
@@ -496,38 +483,12 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
                 mark[e] = cur;
                 ch_elems.push_back(e);
                 ne++;
-                for (int w = 0; w < 4; w++) {
-                    const int v = conn[(size_t)e * 4 + w];
-                    if (nmark[v] != cur) { nmark[v] = cur; nn++; }
-                }
             }
         }
     }
     ch_ptr.push_back((int)ch_rows.size());
     ch_eptr.push_back((int)ch_elems.size());
     const int nch = (int)ch_ptr.size() - 1;
-    // per chunk: the distinct nodes of its elements (ascending) and each
-    // element's vertices as indices into that list
-    std::vector<int> ch_nptr(nch + 1, 0);
-    std::vector<std::vector<int>> cnodes(nch);
-    std::vector<uint16_t> lconn(ch_elems.size() * 4);
-    parallel_for(nch, [&](int a, int b) {
-        for (int c = a; c < b; c++) {
-            std::vector<int>& L = cnodes[c];
-            for (int k = ch_eptr[c]; k < ch_eptr[c + 1]; k++)
-                for (int w = 0; w < 4; w++) L.push_back(conn[(size_t)ch_elems[k] * 4 + w]);
-            std::sort(L.begin(), L.end());
-            L.erase(std::unique(L.begin(), L.end()), L.end());
-            for (int k = ch_eptr[c]; k < ch_eptr[c + 1]; k++)
-                for (int w = 0; w < 4; w++)
-                    lconn[(size_t)k * 4 + w] = (uint16_t)(std::lower_bound(L.begin(), L.end(),
-                                                                           conn[(size_t)ch_elems[k] * 4 + w]) - L.begin());
-        }
-    });
-    for (int c = 0; c < nch; c++) ch_nptr[c + 1] = ch_nptr[c] + (int)cnodes[c].size();
-    std::vector<int> ch_nodes((size_t)ch_nptr[nch]);
-    for (int c = 0; c < nch; c++) std::copy(cnodes[c].begin(), cnodes[c].end(), ch_nodes.begin() + ch_nptr[c]);
-    cnodes.clear();
     // per chunk: pair slots of owned vertices, and the (element, v) of every pair
     std::vector<uint16_t> eslot(ch_elems.size() * 4, 0xffff);
     std::vector<uint32_t> pair_sv(ph.pair_ev.size());
@@ -583,10 +544,6 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
             owned++;
         }
         if (owned != npc) return fail(SORS_ERR_ARG, "internal: chunk pair slots incomplete");
-        const int nnc = ch_nptr[c + 1] - ch_nptr[c];
-        if (nnc > lim.nodes) return fail(SORS_ERR_ARG, "internal: node chunk exceeds its node limit");
-        for (size_t k = (size_t)ch_eptr[c] * 4; k < (size_t)ch_eptr[c + 1] * 4; k++)
-            if (lconn[k] >= nnc) return fail(SORS_ERR_ARG, "internal: chunk-local vertex out of range");
     }
     for (int r = 0; r < N; r++) {
         if (chunk_of_row[r] < 0) return fail(SORS_ERR_ARG, "internal: node missing from the chunks");
@@ -598,12 +555,8 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     if ((long long)nch > 0x7fffffffLL) return fail(SORS_ERR_ARG, "internal: too many node chunks");
     int st;
     ChunkArgs& c = h->chunks;
-    int *d_ptr = nullptr, *d_rows = nullptr, *d_eptr = nullptr, *d_elems = nullptr, *d_nptr = nullptr,
-        *d_nodes = nullptr;
-    uint16_t *d_eslot = nullptr, *d_items = nullptr, *d_lconn = nullptr;
-    if ((st = upload(h, &d_nptr, ch_nptr.data(), ch_nptr.size()))) return st;
-    if ((st = upload(h, &d_nodes, ch_nodes.data(), std::max<size_t>(1, ch_nodes.size())))) return st;
-    if ((st = upload(h, &d_lconn, lconn.data(), lconn.size()))) return st;
+    int *d_ptr = nullptr, *d_rows = nullptr, *d_eptr = nullptr, *d_elems = nullptr;
+    uint16_t *d_eslot = nullptr, *d_items = nullptr;
     if ((st = upload(h, &d_ptr, ch_ptr.data(), ch_ptr.size()))) return st;
     if ((st = upload(h, &d_rows, ch_rows.data(), ch_rows.size()))) return st;
     if ((st = upload(h, &d_eptr, ch_eptr.data(), ch_eptr.size()))) return st;
@@ -612,9 +565,6 @@ int build_tet_chunks(SorsHandle* h, const int32_t* conn, const double* X, const 
     if ((st = upload(h, &d_items, items.data(), items.size()))) return st;
     c.ch_ptr = d_ptr; c.ch_rows = d_rows; c.ch_eptr = d_eptr; c.ch_elems = d_elems;
     c.ch_eslot = reinterpret_cast<const ushort4*>(d_eslot);
-    c.ch_nptr = d_nptr; c.ch_nodes = d_nodes;
-    c.ch_lconn = reinterpret_cast<const ushort4*>(d_lconn);
-    c.nodes_max = lim.nodes;
     c.items = d_items;
     c.rows_max = lim.rows; c.elems_max = lim.elems; c.pairs_max = lim.pairs;
     c.region_bytes = (int)chunk_region_bytes(hsz, h->s.material, h->max_pairs);

@@ -688,8 +688,8 @@ __device__ __forceinline__ int dd_index(int v, int w) {
 
 ChunkLimits chunk_limits(int hsize, int material) {
     const bool snh = material == 2;
-    if (hsize == 4) return snh ? ChunkLimits{64, 384, 1152, 384} : ChunkLimits{64, 512, 1536, 384};
-    return snh ? ChunkLimits{32, 192, 576, 192} : ChunkLimits{32, 256, 768, 192};
+    if (hsize == 4) return snh ? ChunkLimits{64, 384, 1152} : ChunkLimits{64, 512, 1536};
+    return snh ? ChunkLimits{32, 192, 576} : ChunkLimits{32, 256, 768};
 }
 
 // Shared memory of one chunk block: the gradient pairs (3 doubles per pair),
@@ -700,94 +700,12 @@ size_t chunk_region_bytes(int hsize, int material, int max_pairs) {
     return ((size_t)l.pairs * 3 * sizeof(double) + 15) / 16 * 16;
 }
 
-// Bytes of one element's generator in shared memory: FP32 generators are
-// records of 16-byte slots (an odd count, so that the records of different
-// elements start in different bank groups), FP64 ones one array per field.
-static size_t chunk_gen_bytes(int hsize, int material) {
-    const bool snh = material == 2;
-    if (hsize == 4) return (size_t)(snh ? 11 : 7) * 16;
-    return (size_t)(snh ? ChunkGen<true>::kFields : ChunkGen<false>::kFields) * hsize;
-}
-
 size_t chunk_smem_bytes(int hsize, int material, int max_pairs) {
     const ChunkLimits l = chunk_limits(hsize, material);
-    return chunk_region_bytes(hsize, material, max_pairs) + chunk_gen_bytes(hsize, material) * l.elems +
-           (size_t)l.nodes * 3 * sizeof(double) + (size_t)(5 * l.rows + 2) * sizeof(int);
+    const int nf = material == 2 ? ChunkGen<true>::kFields : ChunkGen<false>::kFields;
+    return chunk_region_bytes(hsize, material, max_pairs) + (size_t)nf * l.elems * hsize +
+           (size_t)(5 * l.rows + 2) * sizeof(int);
 }
-
-// Generator access.  Fields: hmu, h1, h2 and h4 (stable Neo-Hookean); a_v =
-// F^-T d_v; d_v . d_w; f_v = F d_v (stable Neo-Hookean).
-template <typename HT>
-struct GenQuad {
-    HT x, y, z, w;
-};
-
-template <typename HT, bool SNH>
-struct GenView;
-
-// FP32: per element the slots (hmu, h1, h2, h4), (a_v, d_v . d_v) for v = 0..3,
-// (d01, d02, d03, d12), (d13, d23, -, -) and, stable Neo-Hookean, (f_v, -).
-template <bool SNH>
-struct GenView<float, SNH> {
-    static constexpr int kSlots = SNH ? 11 : 7;
-    float4* g;
-    // slot * 4 + component of generator field f (ChunkGen numbering)
-    __device__ static constexpr int place(int f) {
-        return f < 3 ? f
-             : f < ChunkGen<SNH>::kDD ? (1 + (f - 3) / 3) * 4 + (f - 3) % 3
-             : f < ChunkGen<SNH>::kH4 ? dd_place(f - ChunkGen<SNH>::kDD)
-             : f == ChunkGen<SNH>::kH4 ? 3
-             : (7 + (f - ChunkGen<SNH>::kF) / 3) * 4 + (f - ChunkGen<SNH>::kF) % 3;
-    }
-    __device__ static constexpr int dd_place(int i) {
-        // dd_index order: 00 01 02 03 11 12 13 22 23 33
-        return i == 0 ? 7 : i == 1 ? 20 : i == 2 ? 21 : i == 3 ? 22 : i == 4 ? 11 : i == 5 ? 23 : i == 6 ? 24
-             : i == 7 ? 15 : i == 8 ? 25 : 19;
-    }
-    __device__ __forceinline__ void put(int s, int f, float x) const {
-        reinterpret_cast<float*>(g + (size_t)s * kSlots)[place(f)] = x;
-    }
-    __device__ __forceinline__ GenQuad<float> h(int s) const {
-        const float4 u = g[(size_t)s * kSlots];
-        return {u.x, u.y, u.z, u.w};
-    }
-    __device__ __forceinline__ GenQuad<float> a(int s, int v) const {  // a_v and d_v . d_v
-        const float4 u = g[(size_t)s * kSlots + 1 + v];
-        return {u.x, u.y, u.z, u.w};
-    }
-    __device__ __forceinline__ float dd(int s, int v, int w) const {  // v != w
-        const int lo = v < w ? v : w, hi = v < w ? w : v;
-        return reinterpret_cast<const float*>(g + (size_t)s * kSlots)[dd_place(dd_index(lo, hi))];
-    }
-    __device__ __forceinline__ GenQuad<float> f(int s, int v) const {
-        const float4 u = g[(size_t)s * kSlots + 7 + v];
-        return {u.x, u.y, u.z, u.w};
-    }
-};
-
-// FP64: one array of elems_max values per field.
-template <bool SNH>
-struct GenView<double, SNH> {
-    using G = ChunkGen<SNH>;
-    double* g;
-    int EM;
-    __device__ __forceinline__ void put(int s, int f, double x) const { g[(size_t)f * EM + s] = x; }
-    __device__ __forceinline__ GenQuad<double> h(int s) const {
-        return {g[s], g[(size_t)EM + s], g[2 * (size_t)EM + s], SNH ? g[(size_t)G::kH4 * EM + s] : 0.0};
-    }
-    __device__ __forceinline__ GenQuad<double> a(int s, int v) const {
-        return {g[(size_t)(G::kA + 3 * v) * EM + s], g[(size_t)(G::kA + 3 * v + 1) * EM + s],
-                g[(size_t)(G::kA + 3 * v + 2) * EM + s], g[(size_t)(G::kDD + dd_index(v, v)) * EM + s]};
-    }
-    __device__ __forceinline__ double dd(int s, int v, int w) const {
-        const int lo = v < w ? v : w, hi = v < w ? w : v;
-        return g[(size_t)(G::kDD + dd_index(lo, hi)) * EM + s];
-    }
-    __device__ __forceinline__ GenQuad<double> f(int s, int v) const {
-        return {g[(size_t)(G::kF + 3 * v) * EM + s], g[(size_t)(G::kF + 3 * v + 1) * EM + s],
-                g[(size_t)(G::kF + 3 * v + 2) * EM + s], 0.0};
-    }
-};
 
 // Hessian generator and gradient rows of one tet (the element math of the
 // chunked assembly): out.grad(v, r, x) receives V (P d_v)_r for the vertices
@@ -795,8 +713,7 @@ struct GenView<double, SNH> {
 // inverted element (J <= 0; J == 0 for stable Neo-Hookean), whose generator is
 // zero.
 template <typename HT, bool SNH, typename Sink>
-__device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, const double (&x)[4][3], bool want_hess,
-                                              Sink& out) {
+__device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, bool want_hess, Sink& out) {
     using G = ChunkGen<SNH>;
     const double2* ts = reinterpret_cast<const double2*>(a.tshape + (size_t)e * 10);
     double t[10];
@@ -805,6 +722,8 @@ __device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, const
         const double2 u = __ldg(ts + k);
         t[2 * k] = u.x; t[2 * k + 1] = u.y;
     }
+    const int4 cn = __ldg(reinterpret_cast<const int4*>(a.conn) + e);
+    const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
     double d[4][3];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
@@ -819,8 +738,9 @@ __device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, const
     for (int w = 0; w < 4; w++) {
 #pragma unroll
         for (int r = 0; r < 3; r++) {
+            const double xr = a.q[3 * (size_t)nodes[w] + r];
 #pragma unroll
-            for (int c = 0; c < 3; c++) F[r * 3 + c] += x[w][r] * d[w][c];
+            for (int c = 0; c < 3; c++) F[r * 3 + c] += xr * d[w][c];
         }
     }
     const double2 m = __ldg(a.mat + e);
@@ -892,15 +812,15 @@ __device__ __forceinline__ bool tet_generator(const AsmArgs<HT>& a, int e, const
     return true;
 }
 
-template <typename HT, bool SNH>
+template <typename HT>
 struct SmemGenSink {
-    GenView<HT, SNH> view;
-    int s;
+    HT* g;
+    int EM, s;
     double* gslot;
     unsigned short slots[4];
     __device__ __forceinline__ bool wants(int v) const { return slots[v] != 0xffff; }
     __device__ __forceinline__ void grad(int v, int r, double x) { gslot[3 * slots[v] + r] = x; }
-    __device__ __forceinline__ void gen(int f, HT x) { view.put(s, f, x); }
+    __device__ __forceinline__ void gen(int f, HT x) { g[f * EM + s] = x; }
 };
 
 template <typename HT>
@@ -925,14 +845,7 @@ __global__ void __launch_bounds__(128) k_tet_gen(AsmArgs<HT> a, int E) {
     if (e >= E) return;
     GlobalGenSink<HT> sink{reinterpret_cast<HT*>(a.ch.gen) + (size_t)e * chunk_gen_stride<HT, SNH>(),
                            a.ch.gradg + (size_t)e * 12};
-    const int4 cn = __ldg(reinterpret_cast<const int4*>(a.conn) + e);
-    const int nodes[4] = {cn.x, cn.y, cn.z, cn.w};
-    double x[4][3];
-#pragma unroll
-    for (int w = 0; w < 4; w++)
-#pragma unroll
-        for (int r = 0; r < 3; r++) x[w][r] = a.q[3 * (size_t)nodes[w] + r];
-    if (!tet_generator<HT, SNH>(a, e, x, a.want_hess != 0, sink)) atomicOr(a.status, kFlagInverted);
+    if (!tet_generator<HT, SNH>(a, e, a.want_hess != 0, sink)) atomicOr(a.status, kFlagInverted);
 }
 
 template <typename HT, bool SNH, bool FROMGEN>
@@ -941,19 +854,8 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
     using G = ChunkGen<SNH>;
     const int EM = a.ch.elems_max;
     double* gslot = reinterpret_cast<double*>(smem_raw);
-    unsigned char* gen_raw = smem_raw + a.ch.region_bytes;
-    GenView<HT, SNH> view;
-    size_t gen_bytes;
-    if constexpr (sizeof(HT) == 4) {
-        view.g = reinterpret_cast<float4*>(gen_raw);
-        gen_bytes = (size_t)GenView<float, SNH>::kSlots * 16 * EM;
-    } else {
-        view.g = reinterpret_cast<double*>(gen_raw);
-        view.EM = EM;
-        gen_bytes = (size_t)G::kFields * sizeof(double) * EM;
-    }
-    double* spos = reinterpret_cast<double*>(gen_raw + gen_bytes);  // chunk node positions
-    int* srow = reinterpret_cast<int*>(spos + 3 * (size_t)a.ch.nodes_max);
+    HT* gen = reinterpret_cast<HT*>(smem_raw + a.ch.region_bytes);
+    int* srow = reinterpret_cast<int*>(gen + (size_t)G::kFields * EM);
     int* srp0 = srow + a.ch.rows_max;
     int* spair0 = srp0 + a.ch.rows_max;
     int* sblk0 = spair0 + a.ch.rows_max + 1;
@@ -989,15 +891,6 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
         }
         if (lane == 0) { spair0[nr] = pacc; sblk0[nr] = bacc; }
     }
-    // the positions of the chunk's nodes, once each
-    if (!FROMGEN) {
-        const int n0 = __ldg(a.ch.ch_nptr + chunk), nn = __ldg(a.ch.ch_nptr + chunk + 1) - n0;
-        for (int k = threadIdx.x; k < 3 * nn; k += blockDim.x) {
-            const int node = __ldg(a.ch.ch_nodes + n0 + k / 3);
-            spos[k] = a.q[3 * (size_t)node + k % 3];
-        }
-        __syncthreads();
-    }
     // A. element generators and gradient pairs (evaluated here, or loaded
     // from the records of k_tet_gen)
     bool ok = true;
@@ -1016,17 +909,10 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             }
             if (a.want_hess)
 #pragma unroll
-                for (int f = 0; f < G::kFields; f++) view.put(s, f, __ldg(rec + f));
+                for (int f = 0; f < G::kFields; f++) gen[f * EM + s] = __ldg(rec + f);
         } else {
-            const ushort4 lc = a.ch.ch_lconn[e0 + s];
-            const int ln[4] = {lc.x, lc.y, lc.z, lc.w};
-            double x[4][3];
-#pragma unroll
-            for (int w = 0; w < 4; w++)
-#pragma unroll
-                for (int r = 0; r < 3; r++) x[w][r] = spos[3 * ln[w] + r];
-            SmemGenSink<HT, SNH> sink{view, s, gslot, {slots[0], slots[1], slots[2], slots[3]}};
-            ok &= tet_generator<HT, SNH>(a, e, x, a.want_hess != 0, sink);
+            SmemGenSink<HT> sink{gen, EM, s, gslot, {slots[0], slots[1], slots[2], slots[3]}};
+            ok &= tet_generator<HT, SNH>(a, e, a.want_hess != 0, sink);
         }
     }
     if (!ok) atomicOr(a.status, kFlagInverted);
@@ -1083,14 +969,16 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             for (int it = i0; it < i1; ++it) {
                 const unsigned item = __ldg(a.ch.items + it);
                 const int es = (int)(item >> 4), v = (item >> 2) & 3;
-                const GenQuad<HT> hq = view.h(es), aq = view.a(es, v);
-                const HT hmu = hq.x, c1 = hq.y - hq.z, dd = aq.w;
-                const HT av[3] = {aq.x, aq.y, aq.z};
-                HT fv[3] = {HT(0), HT(0), HT(0)};
-                const HT h4 = SNH ? hq.w : HT(0);
+                const HT hmu = gen[0 * EM + es], c1 = gen[1 * EM + es] - gen[2 * EM + es];
+                const HT dd = gen[(G::kDD + dd_index(v, v)) * EM + es];
+                HT av[3], fv[3] = {HT(0), HT(0), HT(0)};
+#pragma unroll
+                for (int k = 0; k < 3; k++) av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                HT h4 = HT(0);
                 if (SNH) {
-                    const GenQuad<HT> fq = view.f(es, v);
-                    fv[0] = fq.x; fv[1] = fq.y; fv[2] = fq.z;
+                    h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
                 }
 #pragma unroll
                 for (int k = 0; k < 3; k++)
@@ -1107,15 +995,22 @@ __global__ void __launch_bounds__(kChunkThreads, 2) k_assemble_chunk(AsmArgs<HT>
             for (int it = i0; it < i1; ++it) {
                 const unsigned item = __ldg(a.ch.items + it);
                 const int es = (int)(item >> 4), v = (item >> 2) & 3, w = item & 3;
-                const GenQuad<HT> hq = view.h(es), aq = view.a(es, v), bq = view.a(es, w);
-                const HT hmu = hq.x, h1 = hq.y, h2 = hq.z, dd = view.dd(es, v, w);
-                const HT av[3] = {aq.x, aq.y, aq.z}, aw[3] = {bq.x, bq.y, bq.z};
-                const HT h4 = SNH ? hq.w : HT(0);
-                HT fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
+                const HT hmu = gen[0 * EM + es], h1 = gen[1 * EM + es], h2 = gen[2 * EM + es];
+                const HT dd = gen[(G::kDD + (v <= w ? dd_index(v, w) : dd_index(w, v))) * EM + es];
+                HT av[3], aw[3];
+#pragma unroll
+                for (int k = 0; k < 3; k++) {
+                    av[k] = gen[(G::kA + v * 3 + k) * EM + es];
+                    aw[k] = gen[(G::kA + w * 3 + k) * EM + es];
+                }
+                HT h4 = HT(0), fv[3] = {HT(0), HT(0), HT(0)}, fw[3] = {HT(0), HT(0), HT(0)};
                 if (SNH) {
-                    const GenQuad<HT> fq = view.f(es, v), gq = view.f(es, w);
-                    fv[0] = fq.x; fv[1] = fq.y; fv[2] = fq.z;
-                    fw[0] = gq.x; fw[1] = gq.y; fw[2] = gq.z;
+                    h4 = gen[G::kH4 * EM + es];
+#pragma unroll
+                    for (int k = 0; k < 3; k++) {
+                        fv[k] = gen[(G::kF + v * 3 + k) * EM + es];
+                        fw[k] = gen[(G::kF + w * 3 + k) * EM + es];
+                    }
                 }
 #pragma unroll
                 for (int k = 0; k < 3; k++)

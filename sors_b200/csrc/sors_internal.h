@@ -73,10 +73,7 @@ struct ChunkArgs {
     const int* ch_elems = nullptr;      // element ids, chunk by chunk
     const ushort4* ch_eslot = nullptr;  // chunk-local pair slot of local vertex v (0xffff: not owned)
     const uint16_t* items = nullptr;    // one per slot item, same order as slot_items
-    const int* ch_nptr = nullptr;       // nchunks+1: positions in ch_nodes
-    const int* ch_nodes = nullptr;      // the distinct nodes of each chunk's elements, ascending
-    const ushort4* ch_lconn = nullptr;  // per chunk element: its vertices as indices into the chunk's nodes
-    int rows_max = 0, elems_max = 0, pairs_max = 0, nodes_max = 0;
+    int rows_max = 0, elems_max = 0, pairs_max = 0;
     int region_bytes = 0;       // gradient pairs
     int smem_bytes = 0;         // dynamic shared memory of one chunk block
     void* gen = nullptr;        // two-pass variant: generator records (HT, padded), E of them
@@ -86,7 +83,7 @@ struct ChunkArgs {
 // Chunk limits and shared-memory size of the chunked assembly for a Hessian
 // type size (4 or 8 bytes) and material (0 Neo-Hookean, 2 stable Neo-Hookean).
 struct ChunkLimits {
-    int rows, elems, pairs, nodes;
+    int rows, elems, pairs;
 };
 ChunkLimits chunk_limits(int hsize, int material);
 size_t chunk_region_bytes(int hsize, int material, int max_pairs);
