@@ -10,6 +10,7 @@
 // synchronisation per Newton iteration and one per PCG chunk.
 #include <cuda_runtime.h>
 #include <math.h>
+#include <tuple>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -81,6 +82,13 @@ struct SorsHandle {
     int *row_ptr = nullptr, *col = nullptr, *diag_slot = nullptr, *pair_ptr = nullptr, *pair_ev = nullptr,
         *slot_item_ptr = nullptr;
     uint16_t* slot_items = nullptr;
+    // node numbering: internal node i is the caller's node n2o[i] (identity
+    // when renum is false); every entry point converts at the boundary
+    bool renum = false;
+    std::vector<int> n2o, o2n;
+    int *n2o_d = nullptr, *o2n_d = nullptr;
+    double* perm_tmp = nullptr;           // 3N staging for device-side conversions
+    std::vector<int> caller_row_ptr, caller_col, caller_blk;  // sors_hessian_bsr in caller numbering
     // element-owner tet assembly: node chunks (build_tet_chunks)
     ChunkArgs chunks;
     long long chunk_elem_total = 0;  // sum over chunks of their element counts
@@ -1851,6 +1859,94 @@ int set_device(SorsHandle* h) {
     return SORS_OK;
 }
 
+// Locality order of the nodes: connected components in the order of their
+// lowest caller index (so that the meshes of a union keep their node ranges),
+// and within each the Morton order of the undeformed positions (21 bits per
+// axis over the bounding box).  Element order is not changed.  SORS_NO_RENUMBER=1
+// keeps the caller's numbering (for comparison).
+void locality_order(int N, int E, int nv, const double* X, const int32_t* conn, std::vector<int>& n2o) {
+    std::vector<int> parent(N);
+    for (int i = 0; i < N; i++) parent[i] = i;
+    auto find = [&](int a) {
+        while (parent[a] != a) a = parent[a] = parent[parent[a]];
+        return a;
+    };
+    for (int e = 0; e < E; e++)
+        for (int v = 1; v < nv; v++) {
+            int a = find(conn[(size_t)e * nv]), b = find(conn[(size_t)e * nv + v]);
+            if (a != b) parent[std::max(a, b)] = std::min(a, b);
+        }
+    std::vector<int> root(N);
+    for (int i = 0; i < N; i++) root[i] = find(i);  // the component's lowest index
+    double lo[3] = {X[0], X[1], X[2]}, hi[3] = {X[0], X[1], X[2]};
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < 3; k++) {
+            lo[k] = std::min(lo[k], X[3 * (size_t)i + k]);
+            hi[k] = std::max(hi[k], X[3 * (size_t)i + k]);
+        }
+    auto spread = [](uint64_t v) {
+        v &= 0x1fffff;
+        v = (v | v << 32) & 0x1f00000000ffffULL;
+        v = (v | v << 16) & 0x1f0000ff0000ffULL;
+        v = (v | v << 8) & 0x100f00f00f00f00fULL;
+        v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+        v = (v | v << 2) & 0x1249249249249249ULL;
+        return v;
+    };
+    std::vector<std::tuple<int, uint64_t, int>> key(N);
+    for (int i = 0; i < N; i++) {
+        uint64_t code = 0;
+        for (int k = 0; k < 3; k++) {
+            const double ext = hi[k] - lo[k];
+            const double u = ext > 0 ? (X[3 * (size_t)i + k] - lo[k]) / ext : 0.0;
+            code |= spread((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << k;
+        }
+        key[i] = std::make_tuple(root[i], code, i);
+    }
+    std::sort(key.begin(), key.end());
+    n2o.resize(N);
+    for (int i = 0; i < N; i++) n2o[i] = std::get<2>(key[i]);
+}
+
+// Caller-numbered DOF vector (host or device) -> internal device vector.
+int dof_in(SorsHandle* h, double* dst, const double* src, cudaMemcpyKind kind) {
+    const size_t bytes = sizeof(double) * h->ndof;
+    if (!h->renum) {
+        CK(cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+        return SORS_OK;
+    }
+    CK(cudaMemcpyAsync(h->perm_tmp, src, bytes, kind, h->stream));
+    launch_gather_dofs(h->N, h->perm_tmp, h->n2o_d, dst, h->stream);
+    return SORS_OK;
+}
+
+// Internal device vector -> caller-numbered DOF vector (host or device); the
+// caller synchronises before reading a host destination.
+int dof_out(SorsHandle* h, double* dst, const double* src, cudaMemcpyKind kind) {
+    const size_t bytes = sizeof(double) * h->ndof;
+    if (!h->renum) {
+        CK(cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+        return SORS_OK;
+    }
+    launch_gather_dofs(h->N, src, h->o2n_d, h->perm_tmp, h->stream);
+    CK(cudaMemcpyAsync(dst, h->perm_tmp, bytes, kind, h->stream));
+    return SORS_OK;
+}
+
+// Host-side conversions (set-up and diagnostic calls).
+std::vector<double> dofs_to_internal(const SorsHandle* h, const double* src) {
+    std::vector<double> out((size_t)h->ndof);
+    for (int i = 0; i < h->N; i++)
+        for (int k = 0; k < 3; k++) out[3 * (size_t)i + k] = src[3 * (size_t)(h->renum ? h->n2o[i] : i) + k];
+    return out;
+}
+void dofs_to_caller(const SorsHandle* h, const double* src, double* dst) {
+    for (int i = 0; i < h->N; i++)
+        for (int k = 0; k < 3; k++) dst[3 * (size_t)(h->renum ? h->n2o[i] : i) + k] = src[3 * (size_t)i + k];
+}
+inline int node_in(const SorsHandle* h, int v) { return h->renum ? h->o2n[v] : v; }
+inline int node_out(const SorsHandle* h, int v) { return h->renum ? h->n2o[v] : v; }
+
 }  // namespace
 
 // ===========================================================================
@@ -1910,6 +2006,34 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess)
         return bail(fail(SORS_ERR_CUDA, "stream creation failed"));
     const int N = n_nodes, E = n_elems, nv = nodes_per_elem;
+    // the handle's node numbering (locality order); the rest of the set-up
+    // reads the renumbered positions and connectivity
+    std::vector<double> X_int;
+    std::vector<int32_t> conn_int;
+    {
+        const char* env = getenv("SORS_NO_RENUMBER");
+        const bool off = env && *env && *env != '0';
+        if (!off) locality_order(N, E, nv, X, conn, h->n2o);
+        h->renum = false;
+        if (!off)
+            for (int i = 0; i < N && !h->renum; i++) h->renum = h->n2o[i] != i;
+        if (h->renum) {
+            h->o2n.assign(N, 0);
+            for (int i = 0; i < N; i++) h->o2n[h->n2o[i]] = i;
+            X_int.resize((size_t)3 * N);
+            for (int i = 0; i < N; i++)
+                for (int k = 0; k < 3; k++) X_int[3 * (size_t)i + k] = X[3 * (size_t)h->n2o[i] + k];
+            conn_int.resize((size_t)E * nv);
+            for (size_t t = 0; t < conn_int.size(); t++) conn_int[t] = h->o2n[conn[t]];
+            X = X_int.data();
+            conn = conn_int.data();
+            if ((st = upload(h, &h->n2o_d, h->n2o.data(), (size_t)N))) return bail(st);
+            if ((st = upload(h, &h->o2n_d, h->o2n.data(), (size_t)N))) return bail(st);
+            if ((st = dalloc_t(h, &h->perm_tmp, (size_t)3 * N))) return bail(st);
+        } else {
+            h->n2o.clear();
+        }
+    }
     // per-element Lame parameters (neoHookean.cpp:10-11) and lumped mass (energy.cpp:176-189)
     std::vector<double2> mat(E > 0 ? E : 1);
     std::vector<double> mass(N, 0.0);
@@ -1996,12 +2120,16 @@ int sors_set_neumann(SorsHandle* h, const int32_t* mask, const double* value) {
     if ((st = set_device(h))) return st;
     for (int i = 0; i < h->N; i++) {
         uint8_t m = 0;
+        const int o = node_out(h, i);
         for (int k = 0; k < 3; k++)
-            if (mask[3 * i + k] == 1) m |= (uint8_t)(1u << k);
+            if (mask[3 * o + k] == 1) m |= (uint8_t)(1u << k);
         h->mask_h[i] = m;
     }
     CK(h2d(h, h->node_mask, h->mask_h.data(), h->N));
-    CK(h2d(h, h->mval, value, sizeof(double) * h->ndof));
+    {
+        const std::vector<double> vi = dofs_to_internal(h, value);
+        CK(h2d(h, h->mval, vi.data(), sizeof(double) * h->ndof));
+    }
     h->has_neumann = true;
     h->tl_ready = false;  // the coarse space drops held DOFs
     return SORS_OK;
@@ -2019,6 +2147,9 @@ int sors_set_pressure_faces(SorsHandle* h, const int32_t* faces, int32_t n_faces
         if (faces[t] < 0 || faces[t] >= h->N) return fail(SORS_ERR_ARG, "face vertex out of range");
     for (int f = 0; f < n_faces; f++)
         if (groups[f] < 0 || groups[f] >= n_groups) return fail(SORS_ERR_ARG, "face group out of range");
+    std::vector<int32_t> faces_int((size_t)n_faces * verts_per_face);
+    for (size_t t = 0; t < faces_int.size(); t++) faces_int[t] = node_in(h, faces[t]);
+    faces = faces_int.data();
     // surface rows: node -> (face, local index)
     std::vector<std::vector<int>> inc(h->N);
     for (int f = 0; f < n_faces; f++)
@@ -2061,7 +2192,8 @@ int sors_set_actuation(SorsHandle* h, const char* name, const double* values, in
     }
     if (nm == "vertexForce") {
         if (n != h->ndof) return fail(SORS_ERR_ARG, "vertexForce actuation must have 3N entries");
-        CK(h2d(h, h->vforce, values, sizeof(double) * h->ndof));
+        if ((st = dof_in(h, h->vforce, values, cudaMemcpyHostToDevice))) return st;
+        CK(cudaStreamSynchronize(h->stream));
         return SORS_OK;
     }
     if (nm == "softconMuscle") {
@@ -2106,7 +2238,8 @@ int sors_set_initial_deformation(SorsHandle* h, const double* q) {
     if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(h2d(h, h->qPrev, q, sizeof(double) * h->ndof));
+    if ((st = dof_in(h, h->qPrev, q, cudaMemcpyHostToDevice))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
 
@@ -2114,7 +2247,8 @@ int sors_set_initial_velocity(SorsHandle* h, const double* v) {
     if (!h || !v) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(h2d(h, h->vPrev, v, sizeof(double) * h->ndof));
+    if ((st = dof_in(h, h->vPrev, v, cudaMemcpyHostToDevice))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
 
@@ -2122,9 +2256,10 @@ int sors_get_state(SorsHandle* h, double* q_prev, double* v_prev) {
     if (!h) return fail(SORS_ERR_ARG, "NULL handle");
     int st;
     if ((st = set_device(h))) return st;
+    if (q_prev && (st = dof_out(h, q_prev, h->qPrev, cudaMemcpyDeviceToHost))) return st;
     CK(cudaStreamSynchronize(h->stream));
-    if (q_prev) CK(d2h(h, q_prev, h->qPrev, sizeof(double) * h->ndof));
-    if (v_prev) CK(d2h(h, v_prev, h->vPrev, sizeof(double) * h->ndof));
+    if (v_prev && (st = dof_out(h, v_prev, h->vPrev, cudaMemcpyDeviceToHost))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
 
@@ -2132,7 +2267,7 @@ int sors_energy(SorsHandle* h, const double* q, double dt, double* out) {
     if (!h || !q || !out) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q, cudaMemcpyHostToDevice))) return st;
     return eval_energy(h, dt, out);
 }
 
@@ -2140,10 +2275,10 @@ int sors_gradient(SorsHandle* h, const double* q, double dt, double* g) {
     if (!h || !q || !g) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q, cudaMemcpyHostToDevice))) return st;
     st = mixed(h) ? eval_system<float>(h, dt, false) : eval_system<double>(h, dt, false);
     if (st) return st;
-    CK(cudaMemcpyAsync(g, h->g, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    if ((st = dof_out(h, g, h->g, cudaMemcpyDeviceToHost))) return st;
     CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
@@ -2155,11 +2290,34 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
     if (!row_ptr && !col && !val) return SORS_OK;
     int st;
     if ((st = set_device(h))) return st;
-    if (row_ptr) memcpy(row_ptr, h->row_ptr_h.data(), sizeof(int) * (h->N + 1));
-    if (col) memcpy(col, h->col_h.data(), sizeof(int) * h->nnzb);
+    if (h->renum && h->caller_blk.empty()) {
+        // the pattern in the caller's numbering: caller row o is internal row
+        // o2n[o]; its blocks sorted by caller column
+        const int N = h->N;
+        h->caller_row_ptr.assign(N + 1, 0);
+        h->caller_col.resize(h->nnzb);
+        h->caller_blk.resize(h->nnzb);
+        std::vector<std::pair<int, int>> tmp;
+        for (int o = 0; o < N; o++) {
+            const int i = h->o2n[o];
+            tmp.clear();
+            for (int b = h->row_ptr_h[i]; b < h->row_ptr_h[i + 1]; b++) tmp.push_back({h->n2o[h->col_h[b]], b});
+            std::sort(tmp.begin(), tmp.end());
+            const int b0 = h->caller_row_ptr[o];
+            for (size_t k = 0; k < tmp.size(); k++) {
+                h->caller_col[b0 + k] = tmp[k].first;
+                h->caller_blk[b0 + k] = tmp[k].second;
+            }
+            h->caller_row_ptr[o + 1] = b0 + (int)tmp.size();
+        }
+    }
+    const int* rp_out = h->renum ? h->caller_row_ptr.data() : h->row_ptr_h.data();
+    const int* col_out = h->renum ? h->caller_col.data() : h->col_h.data();
+    if (row_ptr) memcpy(row_ptr, rp_out, sizeof(int) * (h->N + 1));
+    if (col) memcpy(col, col_out, sizeof(int) * h->nnzb);
     if (!val) return SORS_OK;
     if (!q) return fail(SORS_ERR_ARG, "q is NULL");
-    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q, cudaMemcpyHostToDevice))) return st;
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
     st = mixed(h) ? eval_system<float>(h, dt, true) : eval_system<double>(h, dt, true);
     if (st) return st;
@@ -2176,8 +2334,10 @@ int sors_hessian_bsr(SorsHandle* h, const double* q, double dt, int32_t* row_ptr
     }
     // the ABI returns each block's 9 values contiguously, row-major
     const size_t nb = (size_t)h->nnzb;
-    for (size_t b = 0; b < nb; b++)
-        for (int rc = 0; rc < 9; rc++) val[b * 9 + rc] = raw[hval(b, rc, nb)];
+    for (size_t b = 0; b < nb; b++) {
+        const size_t bi = h->renum ? (size_t)h->caller_blk[b] : b;
+        for (int rc = 0; rc < 9; rc++) val[b * 9 + rc] = raw[hval(bi, rc, nb)];
+    }
     int flag = 0;
     CK(d2h(h, &flag, h->status, sizeof(int)));
     if (flag & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
@@ -2194,7 +2354,7 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
     if (psi && cudaMalloc(&dpsi, sizeof(double) * std::max(1, h->E)) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
     if (grad && cudaMalloc(&dgrad, sizeof(double) * (size_t)std::max(1, h->E) * n) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
     if (hess && cudaMalloc(&dhess, sizeof(double) * (size_t)std::max(1, h->E) * n * n) != cudaSuccess) { cleanup(); return fail(SORS_ERR_OOM, "alloc"); }
-    cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream);
+    if ((st = dof_in(h, h->q, q, cudaMemcpyHostToDevice))) { cleanup(); return st; }
     cudaMemsetAsync(h->status, 0, sizeof(int), h->stream);
     if (mixed(h))
         launch_elem_rows<float>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->tshape, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
@@ -2227,7 +2387,8 @@ int sors_set_plane_contact(SorsHandle* h, const double* points, const double* no
     }
     for (int i = 0; i < n_surface; i++)
         if (surface_vertices[i] < 0 || surface_vertices[i] >= h->N) return fail(SORS_ERR_ARG, "surface vertex out of range");
-    h->plane_surf.assign(surface_vertices, surface_vertices + n_surface);
+    h->plane_surf.resize(n_surface);
+    for (int i = 0; i < n_surface; i++) h->plane_surf[i] = node_in(h, surface_vertices[i]);
     h->plane_mask.assign(n_surface, -1);
     return SORS_OK;
 }
@@ -2252,7 +2413,8 @@ int sors_set_disk_contact(SorsHandle* h, const double* centers, const double* no
     h->disk_groups.assign(1, SorsHandle::DiskGroup{});
     auto& G = h->disk_groups[0];
     for (int k = 0; k < n_disks; k++) G.disks.push_back(k);
-    G.surf.assign(surface_vertices, surface_vertices + n_surface);
+    G.surf.resize(n_surface);
+    for (int i = 0; i < n_surface; i++) G.surf[i] = node_in(h, surface_vertices[i]);
     G.mask.assign(n_surface, -1);
     return SORS_OK;
 }
@@ -2270,7 +2432,8 @@ int sors_set_disk_contact_groups(SorsHandle* h, const double* centers, const dou
     for (int k = 0; k < n_disks; k++) {
         auto& G = h->disk_groups[k];
         G.disks = {k};
-        G.surf.assign(surface_vertices + surface_ptr[k], surface_vertices + surface_ptr[k + 1]);
+        G.surf.clear();
+        for (int i = surface_ptr[k]; i < surface_ptr[k + 1]; i++) G.surf.push_back(node_in(h, surface_vertices[i]));
         G.mask.assign(G.surf.size(), -1);
     }
     return SORS_OK;
@@ -2296,13 +2459,14 @@ int sors_set_max_distance(SorsHandle* h, const int32_t* vertex1, const int32_t* 
             return fail(SORS_ERR_ARG, "max-distance vertex out of range");
     int st;
     if ((st = ensure_pair_buffers(h, n_pairs))) return st;
-    h->md_i.assign(vertex1, vertex1 + n_pairs);
-    h->md_j.assign(vertex2, vertex2 + n_pairs);
+    h->md_i.resize(n_pairs);
+    h->md_j.resize(n_pairs);
+    for (int k = 0; k < n_pairs; k++) { h->md_i[k] = node_in(h, vertex1[k]); h->md_j[k] = node_in(h, vertex2[k]); }
     h->md_d.assign(max_distance, max_distance + n_pairs);
     h->md_work.assign(n_pairs, 0);
     h->held_pairs.clear();
     std::vector<int> nodes(2 * (size_t)n_pairs);
-    for (int k = 0; k < n_pairs; k++) { nodes[2 * k] = vertex1[k]; nodes[2 * k + 1] = vertex2[k]; }
+    for (int k = 0; k < n_pairs; k++) { nodes[2 * k] = h->md_i[k]; nodes[2 * k + 1] = h->md_j[k]; }
     if (n_pairs) CK(h2d(h, h->md_nodes_d, nodes.data(), sizeof(int) * nodes.size()));
     return SORS_OK;
 }
@@ -2333,7 +2497,7 @@ int32_t sors_held_contacts(SorsHandle* h, int32_t* nodes, double* normals, int32
     if (!h) return 0;
     const int k = (int)h->held_nodes.size();
     for (int c = 0; c < k && c < cap; c++) {
-        if (nodes) nodes[c] = h->held_nodes[c];
+        if (nodes) nodes[c] = node_out(h, h->held_nodes[c]);
         if (normals)
             for (int j = 0; j < 3; j++) normals[3 * c + j] = h->held_normals[3 * (size_t)c + j];
     }
@@ -2393,20 +2557,38 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
     if (h->s.material == 1) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
     if (stats) *stats = SorsStepStats{};
-    return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
-                                                 dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats)
-                    : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
-                                                   dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats);
+    if (!h->renum)
+        return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
+                                                     dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats)
+                        : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
+                                                       dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann,
+                                                       stats);
+    // the handle's numbering inside, the caller's at the boundary
+    const std::vector<double> qn = dofs_to_internal(h, q_next), bq = dofs_to_internal(h, dL_dq_next);
+    std::vector<int32_t> hn(n_held);
+    for (int c = 0; c < n_held; c++) hn[c] = node_in(h, held_nodes[c]);
+    std::vector<double> oq(dL_dq_prev ? h->ndof : 0), ov(dL_dv_prev ? h->ndof : 0), on(dL_dneumann ? h->ndof : 0);
+    st = mixed(h) ? adjoint_impl<float, float>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
+                                               dL_dq_prev ? oq.data() : nullptr, dL_dv_prev ? ov.data() : nullptr,
+                                               dL_dyoungs, dL_dact, dL_dneumann ? on.data() : nullptr, stats)
+                  : adjoint_impl<double, double>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
+                                                 dL_dq_prev ? oq.data() : nullptr, dL_dv_prev ? ov.data() : nullptr,
+                                                 dL_dyoungs, dL_dact, dL_dneumann ? on.data() : nullptr, stats);
+    if (st) return st;
+    if (dL_dq_prev) dofs_to_caller(h, oq.data(), dL_dq_prev);
+    if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
+    if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
+    return SORS_OK;
 }
 
 int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32_t substeps, SorsStepStats* stats) {
     if (!h || !q_in || !q_out) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpyAsync(h->q, q_in, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q_in, cudaMemcpyHostToDevice))) return st;
     st = step_resident(h, dt, substeps, stats);
     if (st) return st;
-    CK(cudaMemcpyAsync(q_out, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToHost, h->stream));
+    if ((st = dof_out(h, q_out, h->q, cudaMemcpyDeviceToHost))) return st;
     CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
@@ -2415,10 +2597,10 @@ int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substep
     if (!h || !q_device) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpyAsync(h->q, q_device, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q_device, cudaMemcpyDeviceToDevice))) return st;
     st = step_resident(h, dt, substeps, stats);
     if (st) return st;
-    CK(cudaMemcpyAsync(q_device, h->q, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
+    if ((st = dof_out(h, q_device, h->q, cudaMemcpyDeviceToDevice))) return st;
     CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
@@ -2427,7 +2609,7 @@ int sors_update_state(SorsHandle* h, const double* q, double dt) {
     if (!h || !q) return fail(SORS_ERR_ARG, "NULL argument");
     int st;
     if ((st = set_device(h))) return st;
-    CK(cudaMemcpyAsync(h->q, q, sizeof(double) * h->ndof, cudaMemcpyHostToDevice, h->stream));
+    if ((st = dof_in(h, h->q, q, cudaMemcpyHostToDevice))) return st;
     launch_update_state(h->ndof, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, dt, h->s.time_stepping, h->stream);
     CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
@@ -2475,6 +2657,13 @@ int sors_set_members(SorsHandle* h, const int32_t* node_offsets, int32_t n_membe
         return fail(SORS_ERR_ARG, "member node offsets must run from 0 to the node count");
     for (int k = 0; k < n_members; k++)
         if (node_offsets[k + 1] <= node_offsets[k]) return fail(SORS_ERR_ARG, "member node offsets must increase");
+    // the handle orders nodes by connected component (lowest caller index
+    // first), so independent meshes keep their caller node ranges
+    if (h->renum)
+        for (int k = 0; k < n_members; k++)
+            for (int i = node_offsets[k]; i < node_offsets[k + 1]; i++)
+                if (h->n2o[i] < node_offsets[k] || h->n2o[i] >= node_offsets[k + 1])
+                    return fail(SORS_ERR_ARG, "an element joins two members");
     // no element may couple two members
     std::vector<int> conn((size_t)h->E * h->nv);
     if (!conn.empty()) CK(d2h(h, conn.data(), h->conn, sizeof(int) * conn.size()));

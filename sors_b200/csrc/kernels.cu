@@ -1861,6 +1861,22 @@ void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const do
     counted();
 }
 
+// dst[3i + k] = src[3 idx[i] + k]: DOF vectors between the caller's node
+// numbering and the handle's (idx is the permutation in one direction or the other)
+__global__ void k_gather_dofs(int N, const double* __restrict__ src, const int* __restrict__ idx,
+                              double* __restrict__ dst) {
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < 3 * N; t += gridDim.x * blockDim.x) {
+        const int i = t / 3, k = t - 3 * i;
+        dst[t] = src[3 * (size_t)__ldg(idx + i) + k];
+    }
+}
+
+void launch_gather_dofs(int N, const double* src, const int* idx, double* dst, cudaStream_t st) {
+    if (N == 0) return;
+    k_gather_dofs<<<red_grid(3LL * N), kRedThreads, 0, st>>>(N, src, idx, dst);
+    counted();
+}
+
 __global__ void k_predict(int n, double* q, const double* vPrev, double dt) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) q[i] += dt * vPrev[i];

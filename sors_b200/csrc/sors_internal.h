@@ -257,6 +257,7 @@ void launch_dot_gdx(int n, const double* g, const VT* dx, double* partials, DevS
 void launch_update_state(int n, const double* q, double* qPrev, double* vPrev, double* gPrev,
                          const double* gPrevTmp, double dt, int scheme, cudaStream_t st);
 void launch_predict(int n, double* q, const double* vPrev, double dt, cudaStream_t st);
+void launch_gather_dofs(int N, const double* src, const int* idx, double* dst, cudaStream_t st);
 void launch_cfl(int E, int nv, const double* q, const int* conn, int n, const double* vPrev, double* partials,
                 DevScalars* sc, cudaStream_t st);
 template <typename HT>
