@@ -93,6 +93,8 @@ struct SorsHandle {
     ChunkArgs chunks;
     long long chunk_elem_total = 0;  // sum over chunks of their element counts
     int asm_variant = 0;  // 0: chunked element-owner where it applies, 1: row-owner, 2: two-pass chunked
+    void* hex_tile = nullptr;         // hexes: element tiles of the element-owner assembly
+    double* hex_gtile = nullptr;
     void* chunk_gen = nullptr;        // two-pass variant: element generator records
     double* chunk_gradg = nullptr;    // two-pass variant: element gradient rows
     uint8_t* node_mask = nullptr;
@@ -632,7 +634,11 @@ AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int
     a.want_hess = want_hess ? 1 : 0;
     a.hscale = (h->s.time_stepping == 1 && dt != 0.0) ? 0.5 : 1.0;
     a.inertia_coef = inertia_coef(h, dt);
-    if (h->asm_variant == 0 || h->asm_variant == 2) a.ch = h->chunks;
+    if (h->asm_variant == 0 || h->asm_variant == 2) {
+        a.ch = h->chunks;
+        a.hex_tile = h->hex_tile;
+        a.hex_gtile = h->hex_gtile;
+    }
     if (h->asm_variant == 2) {
         a.ch.gen = h->chunk_gen;
         a.ch.gradg = h->chunk_gradg;
@@ -2058,6 +2064,11 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
         PatternHost ph;
         if ((st = build_pattern(h, conn, &ph))) return bail(st);
         if ((st = build_tet_chunks(h, conn, X, ph))) return bail(st);
+    }
+    if (nv == 8 && E > 0 && (h->s.material == 0 || h->s.material == 2)) {
+        // element tiles of the element-owner hex assembly
+        if ((st = dalloc(h, &h->hex_tile, (size_t)E * 36 * 9 * hsize(h)))) return bail(st);
+        if ((st = dalloc_t(h, &h->hex_gtile, (size_t)E * 24))) return bail(st);
     }
     const size_t nd = (size_t)3 * N;
     double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,

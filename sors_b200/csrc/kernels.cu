@@ -1073,6 +1073,290 @@ static void launch_assemble_chunk(const AsmArgs<HT>& a, cudaStream_t st) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Element-owner hex assembly in two passes.
+// Pass 1 (k_hex_tiles): one warp per hex.  Lanes 0-7 take one Gauss point
+// each: shape gradients d_s (hexahedron.cpp:170-207), F, P and the 9x9
+// dP/dF as an explicit matrix A_s (exact Neo-Hookean or stable Neo-Hookean
+// terms hmu I + h1 g g^T - h2 G_rc' G_r'c [+ h4 f f^T], the SPD projection's
+// corrections -lambda_m vec(Q_m) vec(Q_m)^T for the negative modes of the
+// analytic eigensystem, and the fibre term), in shared memory.  Then every
+// lane reads the same A_s entries (broadcast) to form the hex's 36 upper
+// 3x3 blocks, block(v,w) = sum_s wV d_sv^T A_s d_sw, and 24 lanes its
+// gradient rows; both are written as the element's tile.
+// Pass 2 (k_hex_gather): one warp per row, a lane per CSR block, sums the
+// block's items from the tiles (transposed for v > w) in slot order.
+// ---------------------------------------------------------------------------
+constexpr int kHexWarps = 4;
+
+__device__ __forceinline__ int hex_upper(int v, int w) {  // v <= w
+    return v * 8 - (v * (v - 1)) / 2 + (w - v);
+}
+
+template <typename HT, bool SNH, bool PROJ>
+__global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int E) {
+    struct WarpMem {
+        double X[8][3], x[8][3];
+        double d[8][8][3];
+        double P[8][9];
+        HT A[8][81];
+        double wV;
+    };
+    __shared__ WarpMem wm[kHexWarps];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    WarpMem& W = wm[warp];
+    bool ok = true;
+    for (int e = blockIdx.x * kHexWarps + warp; e < E; e += gridDim.x * kHexWarps) {
+        if (lane < 24) {
+            const int v = lane / 3, r = lane - 3 * (lane / 3);
+            const int n = __ldg(a.conn + (size_t)e * 8 + v);
+            W.X[v][r] = __ldg(a.X + 3 * (size_t)n + r);
+            W.x[v][r] = a.q[3 * (size_t)n + r];
+        }
+        __syncwarp();
+        if (lane < 8) {
+            const int s = lane;
+            if (s == 0) W.wV = hex_volume((const double(*)[3])W.X) * 0.125;
+            double d[8][3];
+            hex_shape((const double(*)[3])W.X, s, d);
+            double F[9];
+#pragma unroll
+            for (int r = 0; r < 3; r++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) {
+                    double acc = 0.0;
+#pragma unroll
+                    for (int w = 0; w < 8; w++) acc += W.x[w][r] * d[w][c];
+                    F[r * 3 + c] = acc;
+                }
+#pragma unroll
+            for (int w = 0; w < 8; w++)
+#pragma unroll
+                for (int c = 0; c < 3; c++) W.d[s][w][c] = d[w][c];
+            const double2 m = __ldg(a.mat + e);
+            double C[9];
+            cof3(F, C);
+            const double J = F[0] * C[0] + F[1] * C[1] + F[2] * C[2];
+            const double iJ = 1.0 / J;
+            double G[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) G[k] = C[k] * iJ;
+            double IC = 0.0;
+            if (SNH)
+#pragma unroll
+                for (int k = 0; k < 9; k++) IC += F[k] * F[k];
+            const double alpha = SNH ? 1.0 + 0.75 * m.x / m.y : 0.0;
+            const double logJ = SNH ? 0.0 : log(J);
+            const double hmu = SNH ? m.x * (1.0 - 1.0 / (IC + 1.0)) : m.x;
+            const double h2 = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
+            const double h1 = SNH ? m.y * (2.0 * J - alpha) * J : m.y;
+            const double h4 = SNH ? 2.0 * m.x / ((IC + 1.0) * (IC + 1.0)) : 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; k++) W.P[s][k] = hmu * F[k] + h2 * G[k];
+            const bool qok = SNH ? (J != 0.0) : (J > 0.0);
+            ok &= qok;
+            if (a.want_hess) {
+                // exact dP/dF; rows (r, c), columns (r', c')
+                for (int i = 0; i < 9; i++) {
+                    const int r = i / 3, c = i - 3 * (i / 3);
+#pragma unroll
+                    for (int j = 0; j < 9; j++) {
+                        const int rp = j / 3, cp = j - 3 * (j / 3);
+                        double val = h1 * G[i] * G[j] - h2 * G[r * 3 + cp] * G[rp * 3 + c];
+                        if (SNH) val += h4 * F[i] * F[j];
+                        if (i == j) val += hmu;
+                        W.A[s][i * 9 + j] = qok ? (HT)val : HT(0);
+                    }
+                }
+                if (PROJ && qok) {
+                    HT Fh[9];
+#pragma unroll
+                    for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
+                    NhModes<HT> pm;
+                    if (SNH) snh_modes<HT>(Fh, (HT)J, (HT)IC, (HT)m.x, (HT)m.y, (HT)alpha, pm);
+                    else nh_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)m.x, (HT)m.y, pm);
+                    if (pm.any) {
+                        const HT r2 = HT(0.70710678118654752440);
+                        HT Q[9];
+                        auto add_mode = [&](HT lam_m) {
+                            for (int i = 0; i < 9; i++)
+                                for (int j = 0; j < 9; j++) W.A[s][i * 9 + j] += -lam_m * Q[i] * Q[j];
+                        };
+                        const int pI[3] = {0, 0, 1}, pJ[3] = {1, 2, 2};
+                        for (int mm = 0; mm < 3; mm++) {
+                            const int I = pI[mm], JJ = pJ[mm];
+                            for (int sg = 0; sg < 2; sg++) {
+                                const HT lam_m = sg == 0 ? pm.lt[mm] : pm.lf[mm];
+                                if (!(lam_m < HT(0))) continue;
+                                const HT sign = sg == 0 ? HT(-1) : HT(1);
+                                for (int r = 0; r < 3; r++)
+                                    for (int c = 0; c < 3; c++)
+                                        Q[r * 3 + c] = (pm.U[r * 3 + I] * pm.V[c * 3 + JJ] +
+                                                        sign * pm.U[r * 3 + JJ] * pm.V[c * 3 + I]) * r2;
+                                add_mode(lam_m);
+                            }
+                        }
+                        for (int mm = 0; mm < 3; mm++) {
+                            if (!(pm.ls[mm] < HT(0))) continue;
+                            for (int r = 0; r < 3; r++)
+                                for (int c = 0; c < 3; c++) {
+                                    HT acc = HT(0);
+                                    for (int k = 0; k < 3; k++)
+                                        acc += pm.U[r * 3 + k] * pm.Y[k * 3 + mm] * pm.V[c * 3 + k];
+                                    Q[r * 3 + c] = acc;
+                                }
+                            add_mode(pm.ls[mm]);
+                        }
+                    }
+                }
+            }
+            // fibre term (softconMuscle.cpp, in its consistent squared form)
+            const int grp = a.mus.group ? __ldg(a.mus.group + e) : -1;
+            if (grp >= 0) {
+                const double4 mp = a.mus.param[e];
+                const double eact = __ldg(a.mus.act + grp);
+                double u[3];
+#pragma unroll
+                for (int r = 0; r < 3; r++) u[r] = F[r * 3 + 0] * mp.x + F[r * 3 + 1] * mp.y + F[r * 3 + 2] * mp.z;
+                const double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+                const double rr = (1.0 - eact) / l;
+                const double mv[3] = {mp.x, mp.y, mp.z};
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) W.P[s][r * 3 + c] += mp.w * (1.0 - rr) * u[r] * mv[c];
+                if (a.want_hess) {
+                    double cf = 1.0 - rr;
+                    if (PROJ && cf < 0.0) cf = 0.0;
+                    const double il2 = 1.0 / (l * l);
+                    for (int i = 0; i < 9; i++) {
+                        const int r = i / 3, c = i - 3 * (i / 3);
+#pragma unroll
+                        for (int j = 0; j < 9; j++) {
+                            const int rp = j / 3, cp = j - 3 * (j / 3);
+                            const double M = (1.0 - cf) * u[r] * u[rp] * il2 + (r == rp ? cf : 0.0);
+                            W.A[s][i * 9 + j] += (HT)(mp.w * mv[c] * mv[cp] * M);
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const double wV = W.wV;
+        // gradient rows: g_v = sum_s wV P_s d_sv
+        if (lane < 24) {
+            const int v = lane / 3, r = lane - 3 * (lane / 3);
+            double acc = 0.0;
+            for (int s = 0; s < 8; s++)
+                acc += wV * (W.P[s][r * 3 + 0] * W.d[s][v][0] + W.P[s][r * 3 + 1] * W.d[s][v][1] +
+                             W.P[s][r * 3 + 2] * W.d[s][v][2]);
+            a.hex_gtile[(size_t)e * 24 + lane] = acc;
+        }
+        if (a.want_hess) {
+            HT* tile = reinterpret_cast<HT*>(a.hex_tile) + (size_t)e * 36 * 9;
+            for (int b = lane; b < 36; b += 32) {
+                int v = 0, rem = b;
+                while (rem >= 8 - v) { rem -= 8 - v; v++; }
+                const int w = v + rem;
+                HT acc[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) acc[k] = HT(0);
+                for (int s = 0; s < 8; s++) {
+                    const HT dv[3] = {(HT)W.d[s][v][0], (HT)W.d[s][v][1], (HT)W.d[s][v][2]};
+                    const HT dw[3] = {(HT)W.d[s][w][0], (HT)W.d[s][w][1], (HT)W.d[s][w][2]};
+                    const HT* A = W.A[s];
+#pragma unroll
+                    for (int k = 0; k < 3; k++)
+#pragma unroll
+                        for (int l = 0; l < 3; l++) {
+                            HT t = HT(0);
+#pragma unroll
+                            for (int i = 0; i < 3; i++)
+#pragma unroll
+                                for (int j = 0; j < 3; j++) t += dv[i] * A[(k * 3 + i) * 9 + l * 3 + j] * dw[j];
+                            acc[k * 3 + l] += (HT)wV * t;
+                        }
+                }
+#pragma unroll
+                for (int k = 0; k < 9; k++) tile[b * 9 + k] = acc[k];
+            }
+        }
+        __syncwarp();
+    }
+    if (!ok) atomicOr(a.status, kFlagInverted);
+}
+
+template <typename HT>
+__global__ void __launch_bounds__(256) k_hex_gather(AsmArgs<HT> a) {
+    const int lane = threadIdx.x & 31;
+    const int wpb = blockDim.x >> 5;
+    const HT* tiles = reinterpret_cast<const HT*>(a.hex_tile);
+    for (int row = blockIdx.x * wpb + (threadIdx.x >> 5); row < a.N; row += gridDim.x * wpb) {
+        const int p0 = __ldg(a.pair_ptr + row);
+        const unsigned mrow = a.node_mask[row];
+        if (lane < 3) {
+            double g = 0.0;
+            for (int p = p0; p < __ldg(a.pair_ptr + row + 1); p++) {
+                const int ev = __ldg(a.pair_ev + p);
+                g += a.hex_gtile[(size_t)(ev >> 3) * 24 + (ev & 7) * 3 + lane];
+            }
+            if (a.apply_mask && ((mrow >> lane) & 1u)) g = 0.0;
+            a.g_int[3 * (size_t)row + lane] = g;
+        }
+        if (!a.want_hess) continue;
+        const int b0 = __ldg(a.row_ptr + row), nb = __ldg(a.row_ptr + row + 1) - b0;
+        const double md = a.inertia_coef * a.mass[row];
+        for (int k = lane; k < nb; k += 32) {
+            const int bg = b0 + k;
+            HT acc[9];
+#pragma unroll
+            for (int t = 0; t < 9; t++) acc[t] = HT(0);
+            for (int it = __ldg(a.slot_item_ptr + bg); it < __ldg(a.slot_item_ptr + bg + 1); ++it) {
+                const int item = __ldg(a.slot_items + it);
+                const int kp = item >> 3, w = item & 7;
+                const int ev = __ldg(a.pair_ev + p0 + kp);
+                const int e = ev >> 3, v = ev & 7;
+                const HT* T = tiles + ((size_t)e * 36 + (v <= w ? hex_upper(v, w) : hex_upper(w, v))) * 9;
+                if (v <= w) {
+#pragma unroll
+                    for (int t = 0; t < 9; t++) acc[t] += T[t];
+                } else {
+#pragma unroll
+                    for (int r = 0; r < 3; r++)
+#pragma unroll
+                        for (int c = 0; c < 3; c++) acc[r * 3 + c] += T[c * 3 + r];
+                }
+            }
+            const int j = __ldg(a.col + bg);
+            const unsigned mcol = a.node_mask[j];
+#pragma unroll
+            for (int rc = 0; rc < 9; rc++) {
+                const int r = rc / 3, c = rc - 3 * (rc / 3);
+                const bool rmask = (mrow >> r) & 1u;
+                double val = (double)acc[rc] * a.hscale;
+                if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
+                if (j == row && r == c) {
+                    val += md;
+                    if (a.neumann_override && rmask) val = 1.0;
+                }
+                a.H[hval(bg, rc, a.nnzb)] = (HT)val;
+            }
+        }
+    }
+}
+
+template <typename HT>
+static void launch_hex_tiles(const AsmArgs<HT>& a, cudaStream_t st) {
+    const bool snh = a.material == 2, proj = a.project != 0;
+    const long long hb = cap_grid(((long long)a.E + kHexWarps - 1) / kHexWarps);
+    auto k = snh ? (proj ? k_hex_tiles<HT, true, true> : k_hex_tiles<HT, true, false>)
+                 : (proj ? k_hex_tiles<HT, false, true> : k_hex_tiles<HT, false, false>);
+    if (a.E > 0) k<<<(int)hb, 32 * kHexWarps, 0, st>>>(a, a.E);
+    const long long gb = cap_grid(((long long)a.N + 7) / 8);
+    k_hex_gather<HT><<<(int)gb, 256, 0, st>>>(a);
+    counted(2);
+}
+
 template <typename HT>
 void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     if (a.N == 0) return;
@@ -1090,6 +1374,10 @@ void launch_assemble(const AsmArgs<HT>& a, int max_pairs, cudaStream_t st) {
     if (nv == 4 && a.ch.nchunks > 0 && !a.project && !a.mus.group && (a.material == 0 || snh)) {
         if (snh) launch_assemble_chunk<HT, true>(a, st);
         else launch_assemble_chunk<HT, false>(a, st);
+        return;
+    }
+    if (nv == 8 && a.hex_tile && (a.material == 0 || snh)) {
+        launch_hex_tiles<HT>(a, st);
         return;
     }
     if (nv == 4) {

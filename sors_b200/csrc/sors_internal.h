@@ -121,6 +121,8 @@ struct AsmArgs {
     double hscale;          // 0.5 for Crank-Nicolson with dt != 0
     double inertia_coef;    // diag m * coef
     ChunkArgs ch;           // element-owner tet assembly (used when ch.nchunks > 0)
+    void* hex_tile = nullptr;      // hexes: 36 upper 3x3 blocks (HT) per element, written by k_hex_tiles
+    double* hex_gtile = nullptr;   // hexes: 8 gradient rows per element
 };
 
 struct PressureArgs {
