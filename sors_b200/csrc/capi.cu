@@ -86,6 +86,9 @@ struct SorsHandle {
     // when renum is false); every entry point converts at the boundary
     bool renum = false;
     std::vector<int> n2o, o2n;
+    // element order: internal element e is the caller's element e2o[e]
+    bool renum_e = false;
+    std::vector<int> e2o;
     int *n2o_d = nullptr, *o2n_d = nullptr;
     double* perm_tmp = nullptr;           // 3N staging for device-side conversions
     std::vector<int> caller_row_ptr, caller_col, caller_blk;  // sors_hessian_bsr in caller numbering
@@ -1951,6 +1954,7 @@ void dofs_to_caller(const SorsHandle* h, const double* src, double* dst) {
         for (int k = 0; k < 3; k++) dst[3 * (size_t)(h->renum ? h->n2o[i] : i) + k] = src[3 * (size_t)i + k];
 }
 inline int node_in(const SorsHandle* h, int v) { return h->renum ? h->o2n[v] : v; }
+inline int elem_out(const SorsHandle* h, int e) { return h->renum_e ? h->e2o[e] : e; }
 inline int node_out(const SorsHandle* h, int v) { return h->renum ? h->n2o[v] : v; }
 
 }  // namespace
@@ -2014,7 +2018,7 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
     const int N = n_nodes, E = n_elems, nv = nodes_per_elem;
     // the handle's node numbering (locality order); the rest of the set-up
     // reads the renumbered positions and connectivity
-    std::vector<double> X_int;
+    std::vector<double> X_int, rho_int, youngs_int, poisson_int;
     std::vector<int32_t> conn_int;
     {
         const char* env = getenv("SORS_NO_RENUMBER");
@@ -2029,10 +2033,34 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
             X_int.resize((size_t)3 * N);
             for (int i = 0; i < N; i++)
                 for (int k = 0; k < 3; k++) X_int[3 * (size_t)i + k] = X[3 * (size_t)h->n2o[i] + k];
+            // elements in the order of their lowest internal vertex
+            std::vector<std::pair<int, int>> ek((size_t)E);
+            for (int e = 0; e < E; e++) {
+                int mn = N;
+                for (int v = 0; v < nv; v++) mn = std::min(mn, h->o2n[conn[(size_t)e * nv + v]]);
+                ek[e] = {mn, e};
+            }
+            std::sort(ek.begin(), ek.end());
+            h->e2o.resize(E);
+            for (int e = 0; e < E; e++) {
+                h->e2o[e] = ek[e].second;
+                h->renum_e |= h->e2o[e] != e;
+            }
             conn_int.resize((size_t)E * nv);
-            for (size_t t = 0; t < conn_int.size(); t++) conn_int[t] = h->o2n[conn[t]];
+            for (int e = 0; e < E; e++)
+                for (int v = 0; v < nv; v++)
+                    conn_int[(size_t)e * nv + v] = h->o2n[conn[(size_t)h->e2o[e] * nv + v]];
             X = X_int.data();
             conn = conn_int.data();
+            if (h->renum_e) {
+                rho_int.resize(E); youngs_int.resize(E); poisson_int.resize(E);
+                for (int e = 0; e < E; e++) {
+                    rho_int[e] = density[h->e2o[e]];
+                    youngs_int[e] = youngs[h->e2o[e]];
+                    poisson_int[e] = poisson[h->e2o[e]];
+                }
+                density = rho_int.data(); youngs = youngs_int.data(); poisson = poisson_int.data();
+            }
             if ((st = upload(h, &h->n2o_d, h->n2o.data(), (size_t)N))) return bail(st);
             if ((st = upload(h, &h->o2n_d, h->o2n.data(), (size_t)N))) return bail(st);
             if ((st = dalloc_t(h, &h->perm_tmp, (size_t)3 * N))) return bail(st);
@@ -2223,11 +2251,15 @@ int sors_set_muscles(SorsHandle* h, const int32_t* group, const double* stiffnes
     int st;
     if ((st = set_device(h))) return st;
     std::vector<double4> prm((size_t)std::max(1, h->E));
+    std::vector<int32_t> grp_int((size_t)std::max(1, h->E));
     for (int e = 0; e < h->E; e++) {
-        if (group[e] >= n_groups || group[e] < -1) return fail(SORS_ERR_ARG, "muscle group out of range");
-        prm[e] = make_double4(direction[3 * (size_t)e], direction[3 * (size_t)e + 1], direction[3 * (size_t)e + 2],
-                              stiffness[e]);
+        const int o = elem_out(h, e);
+        if (group[o] >= n_groups || group[o] < -1) return fail(SORS_ERR_ARG, "muscle group out of range");
+        prm[e] = make_double4(direction[3 * (size_t)o], direction[3 * (size_t)o + 1], direction[3 * (size_t)o + 2],
+                              stiffness[o]);
+        grp_int[e] = group[o];
     }
+    group = grp_int.data();
     if (!h->mgroup) {
         if ((st = dalloc_t(h, &h->mgroup, (size_t)std::max(1, h->E)))) return st;
         if ((st = dalloc_t(h, &h->mparam, (size_t)std::max(1, h->E)))) return st;
@@ -2374,9 +2406,18 @@ int sors_elem_eval(SorsHandle* h, const double* q, int32_t project, double* psi,
         launch_elem_rows<double>(h->E, h->nv, h->X, h->q, h->conn, h->mat, h->tshape, muscles(h), h->s.material, project, dpsi, dgrad, dhess,
                                  h->status, h->stream);
     cudaError_t e = cudaStreamSynchronize(h->stream);
-    if (e == cudaSuccess && psi) e = d2h(h, psi, dpsi, sizeof(double) * h->E);
-    if (e == cudaSuccess && grad) e = d2h(h, grad, dgrad, sizeof(double) * (size_t)h->E * n);
-    if (e == cudaSuccess && hess) e = d2h(h, hess, dhess, sizeof(double) * (size_t)h->E * n * n);
+    // per-element outputs in the caller's element order
+    auto fetch = [&](double* dst, const double* src, size_t per) {
+        if (!h->renum_e) return d2h(h, dst, src, sizeof(double) * (size_t)h->E * per);
+        std::vector<double> tmp((size_t)h->E * per);
+        cudaError_t r = d2h(h, tmp.data(), src, sizeof(double) * tmp.size());
+        for (int el = 0; el < h->E && r == cudaSuccess; el++)
+            memcpy(dst + (size_t)h->e2o[el] * per, tmp.data() + (size_t)el * per, sizeof(double) * per);
+        return r;
+    };
+    if (e == cudaSuccess && psi) e = fetch(psi, dpsi, 1);
+    if (e == cudaSuccess && grad) e = fetch(grad, dgrad, (size_t)n);
+    if (e == cudaSuccess && hess) e = fetch(hess, dhess, (size_t)n * n);
     int flag = 0;
     if (e == cudaSuccess) e = d2h(h, &flag, h->status, sizeof(int));
     cleanup();
@@ -2547,9 +2588,14 @@ int sors_set_material(SorsHandle* h, const double* youngs, const double* poisson
     int st;
     if ((st = set_device(h))) return st;
     std::vector<double2> mat((size_t)std::max(1, h->E));
-    for (int e = 0; e < h->E; e++) mat[e] = lame_params(youngs[e], poisson[e], h->s.material);
-    h->youngs_h.assign(youngs, youngs + h->E);
-    h->poisson_h.assign(poisson, poisson + h->E);
+    h->youngs_h.resize(h->E);
+    h->poisson_h.resize(h->E);
+    for (int e = 0; e < h->E; e++) {
+        const int o = elem_out(h, e);
+        mat[e] = lame_params(youngs[o], poisson[o], h->s.material);
+        h->youngs_h[e] = youngs[o];
+        h->poisson_h[e] = poisson[o];
+    }
     if (h->E) CK(h2d(h, h->mat, mat.data(), sizeof(double2) * h->E));
     return SORS_OK;
 }
@@ -2568,7 +2614,7 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
     if (h->s.material == 1) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
     if (stats) *stats = SorsStepStats{};
-    if (!h->renum)
+    if (!h->renum && !h->renum_e)
         return mixed(h) ? adjoint_impl<float, float>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
                                                      dL_dq_prev, dL_dv_prev, dL_dyoungs, dL_dact, dL_dneumann, stats)
                         : adjoint_impl<double, double>(h, q_next, dt, dL_dq_next, held_nodes, held_normals, n_held,
@@ -2579,13 +2625,18 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     std::vector<int32_t> hn(n_held);
     for (int c = 0; c < n_held; c++) hn[c] = node_in(h, held_nodes[c]);
     std::vector<double> oq(dL_dq_prev ? h->ndof : 0), ov(dL_dv_prev ? h->ndof : 0), on(dL_dneumann ? h->ndof : 0);
+    std::vector<double> oe(dL_dyoungs ? h->E : 0);
     st = mixed(h) ? adjoint_impl<float, float>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
                                                dL_dq_prev ? oq.data() : nullptr, dL_dv_prev ? ov.data() : nullptr,
-                                               dL_dyoungs, dL_dact, dL_dneumann ? on.data() : nullptr, stats)
+                                               dL_dyoungs ? oe.data() : nullptr, dL_dact,
+                                               dL_dneumann ? on.data() : nullptr, stats)
                   : adjoint_impl<double, double>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
                                                  dL_dq_prev ? oq.data() : nullptr, dL_dv_prev ? ov.data() : nullptr,
-                                                 dL_dyoungs, dL_dact, dL_dneumann ? on.data() : nullptr, stats);
+                                                 dL_dyoungs ? oe.data() : nullptr, dL_dact,
+                                                 dL_dneumann ? on.data() : nullptr, stats);
     if (st) return st;
+    if (dL_dyoungs)
+        for (int e = 0; e < h->E; e++) dL_dyoungs[elem_out(h, e)] = oe[e];
     if (dL_dq_prev) dofs_to_caller(h, oq.data(), dL_dq_prev);
     if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
     if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
