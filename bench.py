@@ -454,6 +454,28 @@ def run_c3(args):
     faces = np.concatenate(groups)
     gid = np.concatenate([np.full(len(g), k) for k, g in enumerate(groups)])
     mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
+    if args.profile_only:
+        # the hex kernels at rest, 5 launches each (short ncu capture target)
+        import ctypes
+        from sors_b200 import _lib
+        L = _lib.load()
+        for precision in ("mixed", "fp64"):
+            s = ps.SimulationSettings()
+            s.meshType = "Hexahedron"; s.dt = 0.0; s.precision = precision
+            s.hessianProjection = PROJECTION[args.c3_projection]
+            fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
+            en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
+                                          poissonsRatio=0.48, neumannBCmask=mask,
+                                          neumannBCvalue=np.zeros(mask.size), forceTypesList=["pressure"],
+                                          forceParameterList=fp)
+            prof = _lib.SorsKernelProfile()
+            _lib.check(L.sors_profile_kernels(en.handle(), 5, ctypes.byref(prof)))
+            print(json.dumps({"workload": "c3 hex assembly at rest", "precision": precision,
+                              "hessian_projection": args.c3_projection, "hexes": int(H.shape[0]),
+                              "assemble_ms": prof.assemble_ms, "assemble_grad_ms": prof.assemble_grad_ms}),
+                  flush=True)
+            del en
+        return
     for case, chambers in (("one chamber", [0]), ("all three chambers", list(range(len(groups))))):
         for precision in ("mixed", "fp64"):
             s = ps.SimulationSettings()
