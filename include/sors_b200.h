@@ -72,6 +72,13 @@ typedef struct SorsSettings {
                                 rigid-body modes (no reference counterpart);
                                 0: block Jacobi; 2 (default): 1 for meshes of
                                 20,000 nodes or more                              */
+    int32_t linear_solver;   /* Newton systems of "minimize_newton": 0 (default)
+                                PCG; 1 MINRES, which takes the Newton step of an
+                                indefinite exact Hessian as the reference's LDL^T
+                                does (cpp/src/solver.cpp:65-84), preconditioned
+                                by block Jacobi on |D_ii| and the coarse
+                                correction of the projected Hessian.  Contact
+                                QPs, adjoints and unions use PCG.              */
 } SorsSettings;
 
 typedef struct SorsStepStats {

@@ -37,6 +37,7 @@ class SorsSettings(C.Structure):
         ("max_blocks", C.c_int32),
         ("newton_safeguard", C.c_int32),
         ("two_level", C.c_int32),
+        ("linear_solver", C.c_int32),
     ]
 
 

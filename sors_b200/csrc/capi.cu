@@ -174,6 +174,7 @@ struct SorsHandle {
     // two-level preconditioner (settings.two_level): node aggregates, the
     // Galerkin coarse matrix and its inverse (refreshed when PCG slows down)
     bool tl_ready = false, tl_active = false;
+    bool tl_proj = false;             // the coarse operator came from the projected Hessian
     double tl_ref_rate = 0.0;
     CoarseArgs cargs;
     int tl_npairs = 0;
@@ -207,6 +208,13 @@ struct SorsHandle {
     // project_spd == 2: the exact Hessian first, the projected one for this
     // iteration after PCG met negative curvature
     bool proj_fallback = false;
+    // >= 0: the projection of the next assemblies regardless of the settings
+    // (the MINRES coarse operator is built from the projected Hessian)
+    int force_project = -1;
+    // MINRES (settings.linear_solver 1): the two update-direction buffers,
+    // and whether the chunk graph runs MINRES iterations
+    void* mr_w[2] = {nullptr, nullptr};
+    bool mr_active = false;
 };
 
 namespace {
@@ -654,7 +662,8 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
     int st = compute_external(h);
     if (st) return st;
     (want_hess ? h->n_hess_evals : h->n_grad_evals)++;
-    const int project = h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd;
+    const int project = h->force_project >= 0 ? h->force_project
+                        : (h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd);
     AsmArgs<HT> a = asm_args<HT>(h, dt, want_hess, mode, project);
     launch_assemble<HT>(a, h->max_pairs, h->stream);
     if (want_hess && h->has_pressure && method(h) == 0) {
@@ -684,9 +693,40 @@ int eval_energy(SorsHandle* h, double dt, double* out) {
     return SORS_OK;
 }
 
+template <typename VT>
+MinresBufs<VT> minres_bufs(SorsHandle* h) {
+    MinresBufs<VT> b;
+    b.Z[1] = (VT*)h->p0;
+    b.Z[0] = (VT*)h->p1;
+    b.V[1] = (VT*)h->r;
+    b.V[0] = (VT*)h->z;
+    b.W[0] = (VT*)h->mr_w[0];
+    b.W[1] = (VT*)h->mr_w[1];
+    b.x = (VT*)h->x;
+    b.q = (VT*)h->qv;
+    b.Minv = (const VT*)h->Minv;
+    return b;
+}
+
 template <typename HT, typename VT>
 void pcg_iter_pair(SorsHandle* h) {
     VT* z = (VT*)h->z;
+    if (h->mr_active) {
+        // two MINRES iterations, j odd then j even (a chunk starts at an odd j)
+        const MinresBufs<VT> b = minres_bufs<VT>(h);
+        for (int par = 1; par >= 0; par--) {
+            launch_minres_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, b, par,
+                                       h->partials, h->sc, h->stream);
+            if (h->tl_active) {
+                launch_minres_lanczos_restrict<VT>(h->cargs, b, par, h->tl_yc, h->sc, h->stream);
+                launch_minres_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, b, par ^ 1, 0, 0.0,
+                                           0.0, 0, h->partials, h->sc, h->stream);
+            } else {
+                launch_minres_lanczos<VT>(h->N, b, par, h->partials, h->sc, h->stream);
+            }
+        }
+        return;
+    }
     if (h->batch.nmem > 1) {
         for (int half = 0; half < 2; half++) {
             VT* pin = (VT*)(half ? h->p1 : h->p0);
@@ -724,7 +764,8 @@ void pcg_iter_pair(SorsHandle* h) {
 
 template <typename HT, typename VT>
 int pcg_chunk(SorsHandle* h) {
-    const int mode = (h->proj_flag ? 1 : 0) + (h->tl_active ? 2 : 0) + (h->batch.nmem > 1 ? 4 : 0);
+    const int mode = (h->proj_flag ? 1 : 0) + (h->tl_active ? 2 : 0) + (h->batch.nmem > 1 ? 4 : 0) +
+                     (h->mr_active ? 8 : 0);
     if (h->pcg_exec && h->pcg_exec_mode != mode) {
         // the captured launches carry the projection pointers: capture again
         cudaGraphExecDestroy(h->pcg_exec);
@@ -836,6 +877,37 @@ int pcg_solve_members(SorsHandle* h, double eta, double abs_tol, int* iters, con
     return SORS_OK;
 }
 
+// The coarse operator P^T H P of the Hessian in h->H, inverted in place.
+template <typename HT, typename VT>
+int build_coarse(SorsHandle* h) {
+    const int nc = h->cargs.nc;
+    CK(cudaMemsetAsync(h->tl_Ac, 0, sizeof(double) * (size_t)nc * nc, h->stream));
+    if (sizeof(HT) == 4)
+        launch_coarse_galerkin_f(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col, (const float*)h->H,
+                                 h->nnzb, h->cargs, h->tl_Ac, h->stream);
+    else
+        launch_coarse_galerkin_d(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col, (const double*)h->H,
+                                 h->nnzb, h->cargs, h->tl_Ac, h->stream);
+    launch_coarse_invert(nc, h->tl_Ac, h->tl_rowk, h->tl_colk, h->stream);
+    launch_to_vt_pad<VT>(nc, h->tl_ld, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
+    h->tl_ready = true;
+    h->tl_refreshes++;
+    return SORS_OK;
+}
+
+// Rebuilds the coarse operator when the iterations per decade of residual
+// reduction of a solve of two decades or more doubled against the first such
+// solve after the last rebuild.
+void coarse_rate_check(SorsHandle* h, bool refreshed) {
+    if (refreshed) h->tl_ref_rate = -1.0;
+    const DevScalars& sh = *h->sc_host;
+    if (h->tl_active && sh.it >= 8 && sh.rr > 0.0 && sh.bnorm2 >= 1e4 * sh.rr) {
+        const double rate = sh.it / (0.5 * log10(sh.bnorm2 / sh.rr));
+        if (h->tl_ref_rate <= 0.0) h->tl_ref_rate = rate;
+        else if (rate > 2.0 * h->tl_ref_rate) h->tl_ready = false;
+    }
+}
+
 template <typename HT, typename VT>
 int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const double* g = nullptr) {
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
@@ -846,18 +918,9 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
     h->tl_active = h->s.two_level && h->cargs.nc > 0 && h->batch.nmem <= 1;
     bool refreshed = false;
     if (h->tl_active && !h->tl_ready) {
-        const int nc = h->cargs.nc;
-        CK(cudaMemsetAsync(h->tl_Ac, 0, sizeof(double) * (size_t)nc * nc, h->stream));
-        if (sizeof(HT) == 4)
-            launch_coarse_galerkin_f(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col, (const float*)h->H,
-                                     h->nnzb, h->cargs, h->tl_Ac, h->stream);
-        else
-            launch_coarse_galerkin_d(h->tl_npairs, h->tl_pair_ptr, h->tl_items, h->tl_ab, h->col,
-                                     (const double*)h->H, h->nnzb, h->cargs, h->tl_Ac, h->stream);
-        launch_coarse_invert(nc, h->tl_Ac, h->tl_rowk, h->tl_colk, h->stream);
-        launch_to_vt_pad<VT>(nc, h->tl_ld, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
-        h->tl_ready = true;
-        h->tl_refreshes++;
+        int st = build_coarse<HT, VT>(h);
+        if (st) return st;
+        h->tl_proj = false;
         refreshed = true;
     }
     launch_pcg_init<HT, VT>(h->N, g ? g : h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0,
@@ -882,19 +945,119 @@ int pcg_solve(SorsHandle* h, double eta, double abs_tol, int* iters, const doubl
         int st = record_curvature<VT>(h);
         if (st) return st;
     }
-    if (refreshed) h->tl_ref_rate = -1.0;
-    if (h->tl_active && h->sc_host->it >= 8 && h->sc_host->rr > 0.0 && h->sc_host->bnorm2 >= 1e4 * h->sc_host->rr) {
-        // iterations per decade of residual reduction, over solves of two
-        // decades or more (loose solves converge faster per decade and would
-        // skew it): the coarse operator is rebuilt when that doubles against
-        // the first such solve after the last rebuild
-        const double rate = h->sc_host->it / (0.5 * log10(h->sc_host->bnorm2 / h->sc_host->rr));
-        if (h->tl_ref_rate <= 0.0) h->tl_ref_rate = rate;
-        else if (rate > 2.0 * h->tl_ref_rate) h->tl_ready = false;
-    }
+    // loose solves converge faster per decade and are not counted
+    coarse_rate_check(h, refreshed);
     if (h->sc_host->breakdown && h->sc_host->it == 0 && !(h->s.project_spd == 2 && !h->proj_fallback))
         return fail(SORS_ERR_PCG_BREAKDOWN, "PCG breakdown: the Hessian is not positive definite");
     return SORS_OK;
+}
+
+// Solves H dx = -g (dx in h->x) by preconditioned MINRES: the Newton step of
+// a symmetric indefinite Hessian, which the reference takes with LDL^T
+// (cpp/src/solver.cpp:65-84).  Preconditioner: block Jacobi on |D_ii| and,
+// with the two-level setting, the coarse correction of the SPD-projected
+// Hessian (assembled at the current state when the coarse operator is
+// rebuilt; the exact Hessian is then assembled again).  Tolerances as
+// pcg_solve's, on the preconditioned residual norm.
+// MINRES forcing cap: inexact Newton steps of an indefinite system stall at
+// loose forcing (a bar compressed 10 %: 15 Newton iterations at 3e-2, 10 at
+// 1e-2, 7 at 1e-3, 6 exact).
+constexpr double kMinresEtaMax = 1e-3;
+
+template <typename HT, typename VT>
+int minres_solve(SorsHandle* h, double dt, double eta, double abs_tol, int* iters) {
+    eta = std::min(eta, kMinresEtaMax);
+    for (int k = 0; k < 2; k++)
+        if (!h->mr_w[k]) {
+            int st = dalloc(h, &h->mr_w[k], sizeof(VT) * 3 * (size_t)h->N);
+            if (st) return st;
+        }
+    h->tl_active = h->s.two_level && h->cargs.nc > 0;
+    bool refreshed = false;
+    if (h->tl_active && (!h->tl_ready || !h->tl_proj)) {
+        // the preconditioner must be SPD: the coarse operator of the projected Hessian
+        int st;
+        h->force_project = 1;
+        st = eval_system<HT>(h, dt, true);
+        h->force_project = -1;
+        if (st) return st;
+        if ((st = build_coarse<HT, VT>(h))) return st;
+        h->tl_proj = true;
+        if ((st = eval_system<HT>(h, dt, true))) return st;
+        refreshed = true;
+    }
+    launch_block_jacobi_abs<HT, VT>(h->N, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
+    const MinresBufs<VT> b = minres_bufs<VT>(h);
+    const double eta2 = eta * eta, abs2 = abs_tol * abs_tol;
+    launch_minres_init<VT>(h->N, h->g, b, !h->tl_active, eta2, abs2, h->s.pcg_max_iter, h->partials, h->sc,
+                           h->stream);
+    if (h->tl_active) {
+        launch_coarse_restrict<VT>(h->cargs, b.V[1], h->tl_yc, h->stream);
+        launch_minres_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, b, 1, 1, eta2, abs2,
+                                   h->s.pcg_max_iter, h->partials, h->sc, h->stream);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    h->mr_active = true;
+    const int maxchunks = (h->s.pcg_max_iter + kPcgChunk - 1) / kPcgChunk + 1;
+    for (int c = 0; c < maxchunks && !h->sc_host->done; c++) {
+        int st = pcg_chunk<HT, VT>(h);
+        if (st) { h->mr_active = false; return st; }
+        CK(cudaMemcpyAsync(h->sc_host, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
+    h->mr_active = false;
+    const int J = h->sc_host->it;
+    if (h->sc_host->mr_pending) launch_minres_finish<VT>(h->N, b, (J + 1) & 1, h->sc, h->stream);
+    CK(cudaGetLastError());
+    *iters = J;
+    if (verbose()) {
+        // true residual ||H x + g|| of the returned solution (host copies)
+        const size_t n = 3 * (size_t)h->N;
+        std::vector<VT> xv(n);
+        std::vector<HT> Hv(9 * (size_t)h->nnzb);
+        std::vector<int> rp(h->N + 1), cl(h->nnzb);
+        std::vector<double> gv(n);
+        CK(cudaMemcpyAsync(xv.data(), h->x, sizeof(VT) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(Hv.data(), h->H, sizeof(HT) * Hv.size(), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(rp.data(), h->row_ptr, sizeof(int) * rp.size(), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(cl.data(), h->col, sizeof(int) * cl.size(), cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemcpyAsync(gv.data(), h->g, sizeof(double) * n, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        double rr = 0.0, gg = 0.0, xx = 0.0;
+        for (int i = 0; i < h->N; i++)
+            for (int r = 0; r < 3; r++) {
+                double acc = gv[3 * (size_t)i + r];
+                for (int k = rp[i]; k < rp[i + 1]; k++)
+                    for (int c = 0; c < 3; c++) {
+                        // the lower triangle defines the operator
+                        const int j = cl[k];
+                        double a = (double)Hv[9 * (size_t)k + r * 3 + c];
+                        if (j == i && c > r) a = (double)Hv[9 * (size_t)k + c * 3 + r];
+                        acc += a * (double)xv[3 * (size_t)j + c];
+                    }
+                rr += acc * acc;
+                gg += gv[3 * (size_t)i + r] * gv[3 * (size_t)i + r];
+                xx += (double)xv[3 * (size_t)i + r] * (double)xv[3 * (size_t)i + r];
+            }
+        fprintf(stderr, "[sors] minres it=%d eta=%.2e |eta_M|/|b_M|=%.2e ||Hx+g||/||g||=%.2e |x|=%.3e bad=%d brk=%d\n",
+                J, eta, sqrt(h->sc_host->rr / (h->sc_host->bnorm2 > 0 ? h->sc_host->bnorm2 : 1.0)),
+                sqrt(rr / (gg > 0 ? gg : 1.0)), sqrt(xx), h->sc_host->mr_bad, h->sc_host->breakdown);
+    }
+    if (h->sc_host->mr_bad)
+        return fail(SORS_ERR_PCG_BREAKDOWN, "MINRES breakdown: the preconditioner is not positive definite");
+    coarse_rate_check(h, refreshed);
+    return SORS_OK;
+}
+
+// The Newton system's solver of the settings: MINRES (linear_solver 1) for a
+// plain Newton solve on one mesh, PCG otherwise.
+template <typename HT, typename VT>
+int newton_solve(SorsHandle* h, double dt, double eta, double abs_tol, int* iters) {
+    if (h->s.linear_solver == 1 && h->batch.nmem <= 1 && !h->proj_flag)
+        return minres_solve<HT, VT>(h, dt, eta, abs_tol, iters);
+    return pcg_solve<HT, VT>(h, eta, abs_tol, iters);
 }
 
 int ensure_sqp_buffers(SorsHandle* h, int m);
@@ -1056,7 +1219,7 @@ int minimize(SorsHandle* h, double dt, SorsStepStats* stats) {
         prev_g = gn;
         prev_eta = eta;
         int pit = 0;
-        if ((st = pcg_solve<HT, VT>(h, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
+        if ((st = newton_solve<HT, VT>(h, dt, eta, res_tol > 0.0 ? 0.1 * res_tol : 0.0, &pit))) return st;
         if (stats) stats->pcg_iters += pit;
         if (h->s.project_spd == 2 && !h->proj_fallback && h->sc_host->breakdown) {
             // negative curvature in the exact Hessian: solve this iteration with the projected one
@@ -1985,6 +2148,7 @@ void sors_default_settings(SorsSettings* s) {
     s->max_blocks = 0;
     s->newton_safeguard = 0;
     s->two_level = 2;
+    s->linear_solver = 0;
 }
 
 int sors_last_error(char* buf, size_t n) {

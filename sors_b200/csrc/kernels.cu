@@ -1075,15 +1075,20 @@ static void launch_assemble_chunk(const AsmArgs<HT>& a, cudaStream_t st) {
 
 // ---------------------------------------------------------------------------
 // Element-owner hex assembly in two passes.
-// Pass 1 (k_hex_tiles): one warp per hex.  Lanes 0-7 take one Gauss point
-// each: shape gradients d_s (hexahedron.cpp:170-207), F, P and the 9x9
-// dP/dF as an explicit matrix A_s (exact Neo-Hookean or stable Neo-Hookean
-// terms hmu I + h1 g g^T - h2 G_rc' G_r'c [+ h4 f f^T], the SPD projection's
-// corrections -lambda_m vec(Q_m) vec(Q_m)^T for the negative modes of the
-// analytic eigensystem, and the fibre term), in shared memory.  Then every
-// lane reads the same A_s entries (broadcast) to form the hex's 36 upper
-// 3x3 blocks, block(v,w) = sum_s wV d_sv^T A_s d_sw, and 24 lanes its
-// gradient rows; both are written as the element's tile.
+// Pass 1 (k_hex_tiles): one warp per hex, four lanes per Gauss point s (all
+// 32 lanes busy).  The four lanes of s each compute the shape gradients d_s
+// (hexahedron.cpp:170-207), F and the scalar terms; each then writes its own
+// rows i = part, part + 4, part + 8 of P_s and of the 9x9 dP/dF A_s (exact
+// Neo-Hookean or stable Neo-Hookean terms hmu I + h1 g g^T - h2 G_rc' G_r'c
+// [+ h4 f f^T], the SPD projection's corrections -lambda_m vec(Q_m) vec(Q_m)^T
+// for the negative modes of the analytic eigensystem, and the fibre term)
+// into shared memory.  The 36 upper 3x3 blocks block(v,w) = sum_s wV d_sv^T
+// A_s d_sw are then formed through T_sw = A_s (I x d_sw) (27 values per
+// (s, w), 216 per s on the 32 lanes): block(v,w)[k][l] = sum_s wV sum_i
+// d_sv[i] T_sw[k,i][l], 108 (block, k) rows on the 32 lanes, accumulated in
+// registers over s.  That is 13k multiply-adds per hex instead of the 47k of
+// d_v^T A_s d_w per block.  24 lanes write the gradient rows; both go to the
+// element's tile.
 // Pass 2 (k_hex_gather): one warp per row, a lane per CSR block, sums the
 // block's items from the tiles (transposed for v > w) in slot order.
 // ---------------------------------------------------------------------------
@@ -1093,18 +1098,48 @@ __device__ __forceinline__ int hex_upper(int v, int w) {  // v <= w
     return v * 8 - (v * (v - 1)) / 2 + (w - v);
 }
 
+// v[i] for a lane-dependent i in [0, 9) without local memory
+template <typename T>
+__device__ __forceinline__ T pick9(const T (&v)[9], int i) {
+    T r = v[0];
+#pragma unroll
+    for (int k = 1; k < 9; k++) r = (i == k) ? v[k] : r;
+    return r;
+}
+
+template <typename HT>
+struct HexWarpMem {
+    double X[8][3], x[8][3];
+    double d[8][8][3];
+    double P[8][9];
+    HT A[8][81];
+    HT T[2][216];                            // T_sw, double-buffered over s
+    float dh[sizeof(HT) == 4 ? 8 : 1][8][3]; // FP32 copy of d for the block phase (FP32 tiles only)
+    double wV;
+};
+
+template <typename HT>
+__device__ __forceinline__ HT hex_d(const HexWarpMem<HT>& W, int s, int w, int j) {
+    if constexpr (sizeof(HT) == 4) return W.dh[s][w][j];
+    else return W.d[s][w][j];
+}
+
 template <typename HT, bool SNH, bool PROJ>
 __global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int E) {
-    struct WarpMem {
-        double X[8][3], x[8][3];
-        double d[8][8][3];
-        double P[8][9];
-        HT A[8][81];
-        double wV;
-    };
-    __shared__ WarpMem wm[kHexWarps];
+    __shared__ HexWarpMem<HT> wm[kHexWarps];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    WarpMem& W = wm[warp];
+    HexWarpMem<HT>& W = wm[warp];
+    const int s = lane >> 2, part = lane & 3;
+    // this lane's (block, k) rows of the block phase: t = lane + 32 u < 108
+    int bv[4], bw[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int t = lane + 32 * u;
+        int v = 0, rem = t < 108 ? t / 3 : 0;
+        while (rem >= 8 - v) { rem -= 8 - v; v++; }
+        bv[u] = v;
+        bw[u] = v + rem;
+    }
     bool ok = true;
     for (int e = blockIdx.x * kHexWarps + warp; e < E; e += gridDim.x * kHexWarps) {
         if (lane < 24) {
@@ -1114,9 +1149,8 @@ __global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int
             W.x[v][r] = a.q[3 * (size_t)n + r];
         }
         __syncwarp();
-        if (lane < 8) {
-            const int s = lane;
-            if (s == 0) W.wV = hex_volume((const double(*)[3])W.X) * 0.125;
+        {
+            if (lane == 0) W.wV = hex_volume((const double(*)[3])W.X) * 0.125;
             double d[8][3];
             hex_shape((const double(*)[3])W.X, s, d);
             double F[9];
@@ -1129,10 +1163,15 @@ __global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int
                     for (int w = 0; w < 8; w++) acc += W.x[w][r] * d[w][c];
                     F[r * 3 + c] = acc;
                 }
+            // this lane stores d_s of vertices 2 part and 2 part + 1
 #pragma unroll
             for (int w = 0; w < 8; w++)
+                if ((w >> 1) == part)
 #pragma unroll
-                for (int c = 0; c < 3; c++) W.d[s][w][c] = d[w][c];
+                    for (int c = 0; c < 3; c++) {
+                        W.d[s][w][c] = d[w][c];
+                        if constexpr (sizeof(HT) == 4) W.dh[s][w][c] = (float)d[w][c];
+                    }
             const double2 m = __ldg(a.mat + e);
             double C[9];
             cof3(F, C);
@@ -1151,92 +1190,109 @@ __global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int
             const double h2 = SNH ? m.y * (J - alpha) * J : (m.y * logJ - m.x);
             const double h1 = SNH ? m.y * (2.0 * J - alpha) * J : m.y;
             const double h4 = SNH ? 2.0 * m.x / ((IC + 1.0) * (IC + 1.0)) : 0.0;
-#pragma unroll
-            for (int k = 0; k < 9; k++) W.P[s][k] = hmu * F[k] + h2 * G[k];
             const bool qok = SNH ? (J != 0.0) : (J > 0.0);
             ok &= qok;
-            if (a.want_hess) {
-                // exact dP/dF; rows (r, c), columns (r', c')
-                for (int i = 0; i < 9; i++) {
-                    const int r = i / 3, c = i - 3 * (i / 3);
-#pragma unroll
-                    for (int j = 0; j < 9; j++) {
-                        const int rp = j / 3, cp = j - 3 * (j / 3);
-                        double val = h1 * G[i] * G[j] - h2 * G[r * 3 + cp] * G[rp * 3 + c];
-                        if (SNH) val += h4 * F[i] * F[j];
-                        if (i == j) val += hmu;
-                        W.A[s][i * 9 + j] = qok ? (HT)val : HT(0);
-                    }
-                }
-                if (PROJ && qok) {
-                    HT Fh[9];
-#pragma unroll
-                    for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
-                    NhModes<HT> pm;
-                    if (SNH) snh_modes<HT>(Fh, (HT)J, (HT)IC, (HT)m.x, (HT)m.y, (HT)alpha, pm);
-                    else nh_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)m.x, (HT)m.y, pm);
-                    if (pm.any) {
-                        const HT r2 = HT(0.70710678118654752440);
-                        HT Q[9];
-                        auto add_mode = [&](HT lam_m) {
-                            for (int i = 0; i < 9; i++)
-                                for (int j = 0; j < 9; j++) W.A[s][i * 9 + j] += -lam_m * Q[i] * Q[j];
-                        };
-                        const int pI[3] = {0, 0, 1}, pJ[3] = {1, 2, 2};
-                        for (int mm = 0; mm < 3; mm++) {
-                            const int I = pI[mm], JJ = pJ[mm];
-                            for (int sg = 0; sg < 2; sg++) {
-                                const HT lam_m = sg == 0 ? pm.lt[mm] : pm.lf[mm];
-                                if (!(lam_m < HT(0))) continue;
-                                const HT sign = sg == 0 ? HT(-1) : HT(1);
-                                for (int r = 0; r < 3; r++)
-                                    for (int c = 0; c < 3; c++)
-                                        Q[r * 3 + c] = (pm.U[r * 3 + I] * pm.V[c * 3 + JJ] +
-                                                        sign * pm.U[r * 3 + JJ] * pm.V[c * 3 + I]) * r2;
-                                add_mode(lam_m);
-                            }
-                        }
-                        for (int mm = 0; mm < 3; mm++) {
-                            if (!(pm.ls[mm] < HT(0))) continue;
-                            for (int r = 0; r < 3; r++)
-                                for (int c = 0; c < 3; c++) {
-                                    HT acc = HT(0);
-                                    for (int k = 0; k < 3; k++)
-                                        acc += pm.U[r * 3 + k] * pm.Y[k * 3 + mm] * pm.V[c * 3 + k];
-                                    Q[r * 3 + c] = acc;
-                                }
-                            add_mode(pm.ls[mm]);
-                        }
-                    }
-                }
-            }
             // fibre term (softconMuscle.cpp, in its consistent squared form)
             const int grp = a.mus.group ? __ldg(a.mus.group + e) : -1;
+            double4 mp = make_double4(0.0, 0.0, 0.0, 0.0);
+            double u[3] = {0.0, 0.0, 0.0}, rr = 0.0, il2 = 0.0;
             if (grp >= 0) {
-                const double4 mp = a.mus.param[e];
+                mp = a.mus.param[e];
                 const double eact = __ldg(a.mus.act + grp);
-                double u[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++) u[r] = F[r * 3 + 0] * mp.x + F[r * 3 + 1] * mp.y + F[r * 3 + 2] * mp.z;
                 const double l = sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-                const double rr = (1.0 - eact) / l;
-                const double mv[3] = {mp.x, mp.y, mp.z};
+                rr = (1.0 - eact) / l;
+                il2 = 1.0 / (l * l);
+            }
+            const double mv[3] = {mp.x, mp.y, mp.z};
+            // rows i = part, part + 4, part + 8 of P_s and A_s
 #pragma unroll
-                for (int r = 0; r < 3; r++)
+            for (int ii = 0; ii < 3; ii++) {
+                const int i = part + 4 * ii;
+                if (i >= 9) break;
+                const int r = i / 3, c = i - 3 * (i / 3);
+                const double Gi = pick9(G, i), Fi = pick9(F, i);
+                double Pi = hmu * Fi + h2 * Gi;
+                const double ur = r == 0 ? u[0] : (r == 1 ? u[1] : u[2]);
+                const double mc = c == 0 ? mv[0] : (c == 1 ? mv[1] : mv[2]);
+                if (grp >= 0) Pi += mp.w * (1.0 - rr) * ur * mc;
+                W.P[s][i] = Pi;
+                if (!a.want_hess) continue;
+                // G[r*3+cp] and G[rp*3+c] for the nine columns (rp, cp)
+                double Gr[3], Gc[3];
 #pragma unroll
-                    for (int c = 0; c < 3; c++) W.P[s][r * 3 + c] += mp.w * (1.0 - rr) * u[r] * mv[c];
-                if (a.want_hess) {
-                    double cf = 1.0 - rr;
-                    if (PROJ && cf < 0.0) cf = 0.0;
-                    const double il2 = 1.0 / (l * l);
-                    for (int i = 0; i < 9; i++) {
-                        const int r = i / 3, c = i - 3 * (i / 3);
+                for (int k = 0; k < 3; k++) {
+                    Gr[k] = pick9(G, r * 3 + k);
+                    Gc[k] = pick9(G, k * 3 + c);
+                }
+                double cf = 1.0 - rr;
+                if (PROJ && cf < 0.0) cf = 0.0;
 #pragma unroll
-                        for (int j = 0; j < 9; j++) {
-                            const int rp = j / 3, cp = j - 3 * (j / 3);
-                            const double M = (1.0 - cf) * u[r] * u[rp] * il2 + (r == rp ? cf : 0.0);
-                            W.A[s][i * 9 + j] += (HT)(mp.w * mv[c] * mv[cp] * M);
+                for (int j = 0; j < 9; j++) {
+                    const int rp = j / 3, cp = j - 3 * (j / 3);
+                    double val = h1 * Gi * G[j] - h2 * Gr[cp] * Gc[rp];
+                    if (SNH) val += h4 * Fi * F[j];
+                    if (i == j) val += hmu;
+                    if (!qok) val = 0.0;
+                    if (grp >= 0) {
+                        const double M = (1.0 - cf) * ur * u[rp] * il2 + (r == rp ? cf : 0.0);
+                        val += mp.w * mc * mv[cp] * M;
+                    }
+                    W.A[s][i * 9 + j] = (HT)val;
+                }
+            }
+            if (a.want_hess && PROJ && qok) {
+                HT Fh[9];
+#pragma unroll
+                for (int k = 0; k < 9; k++) Fh[k] = (HT)F[k];
+                NhModes<HT> pm;
+                if (SNH) snh_modes<HT>(Fh, (HT)J, (HT)IC, (HT)m.x, (HT)m.y, (HT)alpha, pm);
+                else nh_modes<HT>(Fh, (HT)J, (HT)logJ, (HT)m.x, (HT)m.y, pm);
+                if (pm.any) {
+                    const HT r2 = HT(0.70710678118654752440);
+                    HT Q[9];
+                    auto add_mode = [&](HT lam_m) {
+#pragma unroll
+                        for (int ii = 0; ii < 3; ii++) {
+                            const int i = part + 4 * ii;
+                            if (i >= 9) break;
+                            const HT Qi = pick9(Q, i);
+#pragma unroll
+                            for (int j = 0; j < 9; j++) W.A[s][i * 9 + j] += -lam_m * Qi * Q[j];
                         }
+                    };
+#pragma unroll
+                    for (int mm = 0; mm < 3; mm++) {
+                        const int I = mm == 2 ? 1 : 0, JJ = mm == 0 ? 1 : 2;
+#pragma unroll
+                        for (int sg = 0; sg < 2; sg++) {
+                            const HT lam_m = sg == 0 ? pm.lt[mm] : pm.lf[mm];
+                            if (!(lam_m < HT(0))) continue;
+                            const HT sign = sg == 0 ? HT(-1) : HT(1);
+#pragma unroll
+                            for (int r = 0; r < 3; r++)
+#pragma unroll
+                                for (int c = 0; c < 3; c++)
+                                    Q[r * 3 + c] = (pm.U[r * 3 + I] * pm.V[c * 3 + JJ] +
+                                                    sign * pm.U[r * 3 + JJ] * pm.V[c * 3 + I]) * r2;
+                            add_mode(lam_m);
+                        }
+                    }
+#pragma unroll
+                    for (int mm = 0; mm < 3; mm++) {
+                        if (!(pm.ls[mm] < HT(0))) continue;
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+#pragma unroll
+                            for (int c = 0; c < 3; c++) {
+                                HT acc = HT(0);
+#pragma unroll
+                                for (int k = 0; k < 3; k++)
+                                    acc += pm.U[r * 3 + k] * pm.Y[k * 3 + mm] * pm.V[c * 3 + k];
+                                Q[r * 3 + c] = acc;
+                            }
+                        add_mode(pm.ls[mm]);
                     }
                 }
             }
@@ -1247,38 +1303,48 @@ __global__ void __launch_bounds__(32 * kHexWarps) k_hex_tiles(AsmArgs<HT> a, int
         if (lane < 24) {
             const int v = lane / 3, r = lane - 3 * (lane / 3);
             double acc = 0.0;
-            for (int s = 0; s < 8; s++)
-                acc += wV * (W.P[s][r * 3 + 0] * W.d[s][v][0] + W.P[s][r * 3 + 1] * W.d[s][v][1] +
-                             W.P[s][r * 3 + 2] * W.d[s][v][2]);
+            for (int s2 = 0; s2 < 8; s2++)
+                acc += wV * (W.P[s2][r * 3 + 0] * W.d[s2][v][0] + W.P[s2][r * 3 + 1] * W.d[s2][v][1] +
+                             W.P[s2][r * 3 + 2] * W.d[s2][v][2]);
             a.hex_gtile[(size_t)e * 24 + lane] = acc;
         }
         if (a.want_hess) {
-            HT* tile = reinterpret_cast<HT*>(a.hex_tile) + (size_t)e * 36 * 9;
-            for (int b = lane; b < 36; b += 32) {
-                int v = 0, rem = b;
-                while (rem >= 8 - v) { rem -= 8 - v; v++; }
-                const int w = v + rem;
-                HT acc[9];
+            HT acc[4][3];
 #pragma unroll
-                for (int k = 0; k < 9; k++) acc[k] = HT(0);
-                for (int s = 0; s < 8; s++) {
-                    const HT dv[3] = {(HT)W.d[s][v][0], (HT)W.d[s][v][1], (HT)W.d[s][v][2]};
-                    const HT dw[3] = {(HT)W.d[s][w][0], (HT)W.d[s][w][1], (HT)W.d[s][w][2]};
-                    const HT* A = W.A[s];
+            for (int u = 0; u < 4; u++)
 #pragma unroll
-                    for (int k = 0; k < 3; k++)
+                for (int l = 0; l < 3; l++) acc[u][l] = HT(0);
+            for (int s2 = 0; s2 < 8; s2++) {
+                HT* Tb = W.T[s2 & 1];
+                const HT* A = W.A[s2];
+                // T_sw[k,i][l] = sum_j A_s[(k,i),(l,j)] d_sw[j], index w*27 + (k*3+i)*3 + l
 #pragma unroll
-                        for (int l = 0; l < 3; l++) {
-                            HT t = HT(0);
-#pragma unroll
-                            for (int i = 0; i < 3; i++)
-#pragma unroll
-                                for (int j = 0; j < 3; j++) t += dv[i] * A[(k * 3 + i) * 9 + l * 3 + j] * dw[j];
-                            acc[k * 3 + l] += (HT)wV * t;
-                        }
+                for (int t2 = lane; t2 < 216; t2 += 32) {
+                    const int w = t2 / 27, rem = t2 - 27 * (t2 / 27);
+                    const int ki = rem / 3, l = rem - 3 * (rem / 3);
+                    const HT* Ar = A + ki * 9 + l * 3;
+                    Tb[t2] = Ar[0] * hex_d(W, s2, w, 0) + Ar[1] * hex_d(W, s2, w, 1) + Ar[2] * hex_d(W, s2, w, 2);
                 }
+                __syncwarp();
 #pragma unroll
-                for (int k = 0; k < 9; k++) tile[b * 9 + k] = acc[k];
+                for (int u = 0; u < 4; u++) {
+                    const int t = lane + 32 * u;
+                    if (t >= 108) break;
+                    const int k = t - 3 * (t / 3);
+                    const HT dv0 = hex_d(W, s2, bv[u], 0), dv1 = hex_d(W, s2, bv[u], 1), dv2 = hex_d(W, s2, bv[u], 2);
+                    const HT* Tr = Tb + bw[u] * 27 + k * 9;
+#pragma unroll
+                    for (int l = 0; l < 3; l++) acc[u][l] += dv0 * Tr[l] + dv1 * Tr[3 + l] + dv2 * Tr[6 + l];
+                }
+            }
+            HT* tile = reinterpret_cast<HT*>(a.hex_tile) + (size_t)e * 36 * 9;
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int t = lane + 32 * u;
+                if (t >= 108) break;
+                const int b = t / 3, k = t - 3 * (t / 3);
+#pragma unroll
+                for (int l = 0; l < 3; l++) tile[b * 9 + k * 3 + l] = (HT)wV * acc[u][l];
             }
         }
         __syncwarp();
@@ -1882,12 +1948,43 @@ __device__ __forceinline__ void load_group(const HT* __restrict__ H, int gi, HT 
 // loads per two FP64 blocks): against one block per lane (nine 4-byte loads)
 // 77.5 -> 64.4 us FP32 and 150 -> 123 us FP64; G = 4 (16-byte FP32 loads)
 // needs 36 value registers a lane and measured 87-99 us.
-template <typename HT, typename VT, int LPR, int G>
+// MODE 1 is the MINRES SpMV (minres section below): p4 holds the unnormalised
+// z_j, the dot gives delta_j = z_j.A z_j / gamma_j^2 (no curvature test), and
+// the lanes that store row i of q also apply the previous iteration's pending
+// solution update to row i (MinresUpd).
+template <typename VT>
+struct MinresUpd {
+    const VT* zprev = nullptr;  // z_{j-1}, padded
+    const VT* wread = nullptr;  // w_{j-1}
+    VT* wrw = nullptr;          // w_{j-2} in, w_j out
+    VT* x = nullptr;
+};
+
+template <typename VT>
+__device__ __forceinline__ void minres_row_update(const MinresUpd<VT>& u, size_t row, int d, VT ig, VT a1i, VT a2,
+                                                  VT a3, VT ceta) {
+    const size_t k = 3 * row + d;
+    const VT wn = (u.zprev[4 * row + d] * ig - a3 * u.wrw[k] - a2 * u.wread[k]) * a1i;
+    u.wrw[k] = wn;
+    u.x[k] += ceta * wn;
+}
+
+template <typename HT, typename VT, int LPR, int G, int MODE = 0>
 __global__ void __launch_bounds__(kRedThreads, sizeof(HT) == 4 ? 8 : 4) k_pcg_spmv(
     int N, const int* __restrict__ row_ptr, const int* __restrict__ col, const HT* __restrict__ H, long long nnzb,
-    const VT* __restrict__ p4, VT* __restrict__ qv, double* partials, DevScalars* sc) {
+    const VT* __restrict__ p4, VT* __restrict__ qv, double* partials, DevScalars* sc, MinresUpd<VT> mu) {
     (void)nnzb;
     if (*(volatile int*)&sc->done) return;
+    // (named apart from the row sums a0..a2 below)
+    bool pend = false;
+    VT u_ig = VT(0), u_a1i = VT(0), u_a2 = VT(0), u_a3 = VT(0), u_ceta = VT(0);
+    if constexpr (MODE == 1) {
+        pend = *(volatile int*)&sc->mr_pending != 0;
+        if (pend) {
+            u_ig = (VT)sc->mr_ig; u_a1i = (VT)(1.0 / sc->mr_a1); u_a2 = (VT)sc->mr_a2; u_a3 = (VT)sc->mr_a3;
+            u_ceta = (VT)sc->mr_ceta;
+        }
+    }
     const int lane = threadIdx.x & 31;
     const int sub = lane / LPR, sl = lane % LPR;
     constexpr int RPW = 32 / LPR;
@@ -1937,10 +2034,17 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(HT) == 4 ? 8 : 4) k_pcg_sp
             const VT qi = sl == 0 ? a0 : (sl == 1 ? a1 : a2);
             qv[3 * (size_t)row + sl] = qi;
             acc[0] += (double)p4[4 * (size_t)row + sl] * (double)qi;
+            if constexpr (MODE == 1)
+                if (pend) minres_row_update<VT>(mu, (size_t)row, sl, u_ig, u_a1i, u_a2, u_a3, u_ceta);
         }
     }
     double tot[1];
     if (reduce_grid<1>(acc, partials, &sc->counters[4], tot) && threadIdx.x == 0) {
+        if constexpr (MODE == 1) {
+            sc->pq = tot[0];
+            sc->mr_delta = tot[0] / (sc->mr_g * sc->mr_g);
+            return;
+        }
         sc->pq = tot[0];
         if (!(tot[0] > 0.0)) {
             sc->breakdown = 1;
@@ -1952,9 +2056,10 @@ __global__ void __launch_bounds__(kRedThreads, sizeof(HT) == 4 ? 8 : 4) k_pcg_sp
     }
 }
 
-template <typename HT, typename VT, int G>
+template <typename HT, typename VT, int G, int MODE = 0>
 static void launch_spmv_g(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H,
-                          long long nnzb, const VT* p4, VT* qv, double* partials, DevScalars* sc, cudaStream_t st) {
+                          long long nnzb, const VT* p4, VT* qv, double* partials, DevScalars* sc, cudaStream_t st,
+                          MinresUpd<VT> mu = MinresUpd<VT>()) {
     // groups a row of max_row_blocks blocks can span, rounded up to a power of two
     const int groups = G == 1 ? max_row_blocks : (max_row_blocks + 2 * G - 2) / G;
     const int lpr = groups <= 2 ? 2 : (groups <= 4 ? 4 : (groups <= 8 ? 8 : (groups <= 16 ? 16 : 32)));
@@ -1964,11 +2069,11 @@ static void launch_spmv_g(int N, int max_row_blocks, const int* row_ptr, const i
     if (blocks < 1) blocks = 1;
     blocks = cap_grid(blocks);
     switch (lpr) {
-        case 2: k_pcg_spmv<HT, VT, 2, G><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
-        case 4: k_pcg_spmv<HT, VT, 4, G><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
-        case 8: k_pcg_spmv<HT, VT, 8, G><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
-        case 16: k_pcg_spmv<HT, VT, 16, G><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
-        default: k_pcg_spmv<HT, VT, 32, G><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc); break;
+        case 2: k_pcg_spmv<HT, VT, 2, G, MODE><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc, mu); break;
+        case 4: k_pcg_spmv<HT, VT, 4, G, MODE><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc, mu); break;
+        case 8: k_pcg_spmv<HT, VT, 8, G, MODE><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc, mu); break;
+        case 16: k_pcg_spmv<HT, VT, 16, G, MODE><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc, mu); break;
+        default: k_pcg_spmv<HT, VT, 32, G, MODE><<<(int)blocks, kRedThreads, 0, st>>>(N, row_ptr, col, H, nnzb, p4, qv, partials, sc, mu); break;
     }
     counted();
 }
@@ -2759,5 +2864,384 @@ template void launch_spmv_plain<double>(int, const int*, const int*, const doubl
                                         double*, cudaStream_t);
 template void launch_spmv_plain<float>(int, const int*, const int*, const float*, long long, const double*, double*,
                                        cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// MINRES for the symmetric indefinite Newton systems of the exact Hessian
+// (Paige & Saunders 1975, preconditioned form as in Elman, Silvester &
+// Wathen, "Finite Elements and Fast Iterative Solvers", 2nd ed., Alg. 4.1).
+// The reference factors such systems with LDL^T (cpp/src/solver.cpp:65-84);
+// CG cannot take them.  The preconditioner must be SPD: block Jacobi on
+// |D_ii| (each diagonal block with its eigenvalues replaced by their absolute
+// values), plus the two-level coarse correction built from the SPD-projected
+// Hessian.  Iteration j (1-based): the SpMV q = A z_j on the unnormalised
+// z_j (MODE 1 of k_pcg_spmv, which also applies iteration j-1's pending
+// solution update row by row), then the Lanczos step
+//   v_{j+1} = q / g_j - (delta_j / g_j) v_j - (g_j / g_{j-1}) v_{j-1}
+// fused with z_{j+1} = M^-1 v_{j+1} and the dot g_{j+1}^2 = v_{j+1}.z_{j+1},
+// whose last block advances the Givens QR (minres_advance).  Buffers
+// alternate by parity: Z[j & 1] (padded), V[j & 1], W[j & 1]; the Lanczos
+// step writes v_{j+1} and z_{j+1} over v_{j-1} and z_{j-1}, the update writes
+// w_{j+1} over w_{j-1}.  After the last iteration the host applies its
+// pending update with k_minres_finish.
+// ---------------------------------------------------------------------------
+template <typename HT, typename VT>
+__global__ void k_block_jacobi_abs(int N, const int* diag_slot, const HT* H, long long nnzb, VT* Minv) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const size_t d = (size_t)diag_slot[i];
+    double a[9], w[3], Y[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) a[k] = (double)H[hval(d, k, nnzb)];
+    // symmetric part: the lower triangle defines the operator
+    a[1] = a[3]; a[2] = a[6]; a[5] = a[7];
+    sym3_eig(a, w, Y);
+    double amax = 0.0;
+#pragma unroll
+    for (int k = 0; k < 3; k++) amax = fmax(amax, fabs(w[k]));
+    double iw[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const double aw = fabs(w[k]);
+        iw[k] = (aw > 1e-12 * amax && aw == aw) ? 1.0 / aw : (amax > 0.0 ? 1.0 / amax : 1.0);
+    }
+    VT* o = Minv + (size_t)i * 9;
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            o[r * 3 + c] = (VT)(Y[r * 3 + 0] * iw[0] * Y[c * 3 + 0] + Y[r * 3 + 1] * iw[1] * Y[c * 3 + 1] +
+                                Y[r * 3 + 2] * iw[2] * Y[c * 3 + 2]);
+}
+
+template <typename HT, typename VT>
+void launch_block_jacobi_abs(int N, const int* diag_slot, const HT* H, long long nnzb, VT* Minv, cudaStream_t st) {
+    if (N == 0) return;
+    k_block_jacobi_abs<HT, VT><<<(N + 127) / 128, 128, 0, st>>>(N, diag_slot, H, nnzb, Minv);
+    counted();
+}
+
+// First Lanczos vector: v_1 = b = -g (gamma_1 = ||b||_{M^-1} = eta_0).
+__device__ void minres_start(DevScalars* sc, double vz, double vv, double eta2, double abs_tol2, int maxit) {
+    sc->it = 0;
+    sc->maxit = maxit;
+    sc->breakdown = 0;
+    sc->mr_bad = (vz >= 0.0) ? 0 : 1;
+    const double g = vz > 0.0 ? sqrt(vz) : 0.0;
+    sc->mr_g = g;
+    sc->mr_gprev = 1.0;
+    sc->mr_delta = 0.0;
+    sc->mr_c = sc->mr_cprev = 1.0;
+    sc->mr_s = sc->mr_sprev = 0.0;
+    sc->mr_eta = g;
+    sc->mr_pending = 0;
+    sc->bnorm2 = vz;
+    sc->rr = vz;
+    // the absolute target is a 2-norm; scaled to the M^-1 norm by their ratio at b
+    const double t1 = eta2 * vz, t2 = vv > 0.0 ? abs_tol2 * vz / vv : 0.0;
+    sc->tol2 = t1 > t2 ? t1 : t2;
+    sc->counters[4] = 0u;
+    sc->counters[12] = 0u;
+    sc->done = (vz <= sc->tol2 || maxit <= 0 || g == 0.0 || sc->mr_bad) ? 1 : 0;
+}
+
+// Givens step of iteration j from g_{j+1}^2 = vz: leaves the solution update
+// w_{j+1} = (z_j / g_j - a3 w_{j-1} - a2 w_j) / a1, x += c_{j+1} eta_j w_{j+1}
+// pending, and |eta_{j+1}| = ||r_j||_{M^-1}.
+__device__ void minres_advance(DevScalars* sc, double vz) {
+    const double g = sc->mr_g, d = sc->mr_delta;
+    if (!(vz >= 0.0)) sc->mr_bad = 1;
+    const double gn = vz > 0.0 ? sqrt(vz) : 0.0;
+    const double a0 = sc->mr_c * d - sc->mr_cprev * sc->mr_s * g;
+    const double a1 = sqrt(a0 * a0 + gn * gn);
+    const double a2 = sc->mr_s * d + sc->mr_cprev * sc->mr_c * g;
+    const double a3 = sc->mr_sprev * g;
+    sc->it += 1;
+    if (!(a1 > 0.0) || !(d == d)) {
+        sc->breakdown = 1;
+        sc->mr_pending = 0;
+        sc->done = 1;
+        return;
+    }
+    const double cn = a0 / a1, sn = gn / a1;
+    sc->mr_a1 = a1;
+    sc->mr_a2 = a2;
+    sc->mr_a3 = a3;
+    sc->mr_ceta = cn * sc->mr_eta;
+    sc->mr_ig = 1.0 / g;
+    sc->mr_pending = 1;
+    sc->mr_eta = -sn * sc->mr_eta;
+    sc->mr_cprev = sc->mr_c;
+    sc->mr_c = cn;
+    sc->mr_sprev = sc->mr_s;
+    sc->mr_s = sn;
+    sc->mr_gprev = g;
+    sc->mr_g = gn;
+    sc->rr = sc->mr_eta * sc->mr_eta;
+    if (sc->rr <= sc->tol2 || sc->it >= sc->maxit || gn == 0.0 || sc->mr_bad) sc->done = 1;
+}
+
+template <typename VT>
+__device__ __forceinline__ void st_pad(VT* z4, size_t i, const VT (&z)[3]) {
+    if constexpr (sizeof(VT) == 4) {
+        reinterpret_cast<float4*>(z4)[i] = make_float4(z[0], z[1], z[2], 0.0f);
+    } else {
+        double2* d = reinterpret_cast<double2*>(z4) + 2 * i;
+        d[0] = make_double2(z[0], z[1]);
+        d[1] = make_double2(z[2], 0.0);
+    }
+}
+
+// v_1 = -g into V[1], v_0 = 0, w_0 = w_1 = 0, x = 0; with the block-Jacobi
+// preconditioner also z_1 = M^-1 v_1 into Z[1] and the start of the recurrence.
+template <typename VT, bool WITHZ>
+__global__ void __launch_bounds__(kRedThreads) k_minres_init(int N, const double* __restrict__ g, MinresBufs<VT> b,
+                                                              double eta2, double abs_tol2, int maxit,
+                                                              double* partials, DevScalars* sc) {
+    double acc[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT v[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const size_t ii = 3 * (size_t)i + k;
+            v[k] = (VT)(-g[ii]);
+            b.V[1][ii] = v[k];
+            b.V[0][ii] = VT(0);
+            b.W[0][ii] = VT(0);
+            b.W[1][ii] = VT(0);
+            b.x[ii] = VT(0);
+        }
+        if (WITHZ) {
+            const VT* M = b.Minv + (size_t)i * 9;
+            VT z[3];
+#pragma unroll
+            for (int k = 0; k < 3; k++) z[k] = M[k * 3 + 0] * v[0] + M[k * 3 + 1] * v[1] + M[k * 3 + 2] * v[2];
+            st_pad<VT>(b.Z[1], (size_t)i, z);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                acc[0] += (double)v[k] * (double)z[k];
+                acc[1] += (double)v[k] * (double)v[k];
+            }
+        }
+    }
+    if (!WITHZ) return;
+    double tot[2];
+    if (reduce_grid<2>(acc, partials, &sc->counters[11], tot) && threadIdx.x == 0)
+        minres_start(sc, tot[0], tot[1], eta2, abs_tol2, maxit);
+}
+
+template <typename VT>
+void launch_minres_init(int N, const double* g, const MinresBufs<VT>& b, bool with_z, double eta2, double abs_tol2,
+                        int maxit, double* partials, DevScalars* sc, cudaStream_t st) {
+    if (with_z)
+        k_minres_init<VT, true><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, b, eta2, abs_tol2, maxit, partials, sc);
+    else
+        k_minres_init<VT, false><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, g, b, eta2, abs_tol2, maxit, partials, sc);
+    counted();
+}
+
+// Iteration j's SpMV (par = j & 1).
+template <typename HT, typename VT>
+void launch_minres_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
+                        const MinresBufs<VT>& b, int par, double* partials, DevScalars* sc, cudaStream_t st) {
+    MinresUpd<VT> u;
+    u.zprev = b.Z[par ^ 1];
+    u.wread = b.W[par ^ 1];
+    u.wrw = b.W[par];
+    u.x = b.x;
+    launch_spmv_g<HT, VT, 2, 1>(N, max_row_blocks, row_ptr, col, H, nnzb, b.Z[par], b.q, partials, sc, st, u);
+}
+
+// The Lanczos vector of iteration j (par = j & 1) at node i, written over v_{j-1}.
+template <typename VT>
+__device__ __forceinline__ void minres_lanczos_node(const MinresBufs<VT>& b, int par, size_t i, VT ig, VT dg, VT gg,
+                                                    VT (&v)[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const size_t ii = 3 * i + k;
+        v[k] = b.q[ii] * ig - dg * b.V[par][ii] - gg * b.V[par ^ 1][ii];
+        b.V[par ^ 1][ii] = v[k];
+    }
+}
+
+// Block-Jacobi variant: Lanczos step, z_{j+1} = M^-1 v_{j+1}, the Givens step.
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_minres_lanczos(int N, MinresBufs<VT> b, int par, double* partials,
+                                                                 DevScalars* sc) {
+    if (*(volatile int*)&sc->done) return;
+    const double g = sc->mr_g;
+    const VT ig = (VT)(1.0 / g), dg = (VT)(sc->mr_delta / g), gg = (VT)(g / sc->mr_gprev);
+    double acc[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+        VT v[3];
+        minres_lanczos_node<VT>(b, par, (size_t)i, ig, dg, gg, v);
+        const VT* M = b.Minv + (size_t)i * 9;
+        VT z[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) z[k] = M[k * 3 + 0] * v[0] + M[k * 3 + 1] * v[1] + M[k * 3 + 2] * v[2];
+        st_pad<VT>(b.Z[par ^ 1], (size_t)i, z);
+#pragma unroll
+        for (int k = 0; k < 3; k++) acc[0] += (double)v[k] * (double)z[k];
+    }
+    double tot[1];
+    if (reduce_grid<1>(acc, partials, &sc->counters[12], tot) && threadIdx.x == 0) minres_advance(sc, tot[0]);
+}
+
+template <typename VT>
+void launch_minres_lanczos(int N, const MinresBufs<VT>& b, int par, double* partials, DevScalars* sc,
+                           cudaStream_t st) {
+    k_minres_lanczos<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, b, par, partials, sc);
+    counted();
+}
+
+// Two-level variant, first half: the Lanczos step on each aggregate's nodes
+// and yc = P^T v_{j+1} (one block per aggregate, fixed-order sums).
+template <typename VT>
+__global__ void __launch_bounds__(kAggThreads) k_minres_lanczos_restrict(CoarseArgs c, MinresBufs<VT> b, int par,
+                                                                          double* __restrict__ yc,
+                                                                          const DevScalars* sc) {
+    if (*(volatile const int*)&sc->done) return;
+    __shared__ double sh[32][6];
+    const int a = blockIdx.x;
+    const double g = sc->mr_g;
+    const VT ig = (VT)(1.0 / g), dg = (VT)(sc->mr_delta / g), gg = (VT)(g / sc->mr_gprev);
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
+        const int i = c.agg_nodes[k];
+        VT v[3];
+        minres_lanczos_node<VT>(b, par, (size_t)i, ig, dg, gg, v);
+        const double vd[3] = {(double)v[0], (double)v[1], (double)v[2]};
+        double y[6];
+        coarse_restrict_node(c, i, vd, y);
+#pragma unroll
+        for (int m = 0; m < 6; m++) acc[m] += y[m];
+    }
+    block_sum<6>(acc, sh);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int m = 0; m < 6; m++) yc[6 * a + m] = acc[m];
+}
+
+template <typename VT>
+void launch_minres_lanczos_restrict(const CoarseArgs& c, const MinresBufs<VT>& b, int par, double* yc,
+                                    const DevScalars* sc, cudaStream_t st) {
+    k_minres_lanczos_restrict<VT><<<c.nagg, kAggThreads, 0, st>>>(c, b, par, yc, sc);
+    counted();
+}
+
+// Two-level variant, second half: z = M^-1 v + P Ainv yc for the Lanczos
+// vector in V[vpar] into Z[vpar], with v.z (and v.v); init = 1 starts the
+// recurrence (vpar = 1), init = 0 takes the Givens step.  The coarse rows are
+// formed as in k_tl_coarse_z.
+template <typename VT>
+__global__ void __launch_bounds__(kAggThreads, 4) k_minres_coarse_z(CoarseArgs c, int ld, const VT* __restrict__ Ainv,
+                                                                 const double* __restrict__ yc, MinresBufs<VT> b,
+                                                                 int vpar, int init, double eta2, double abs_tol2,
+                                                                 int maxit, double* partials, DevScalars* sc) {
+    if (!init && *(volatile int*)&sc->done) return;
+    __shared__ double sh[32][6];
+    constexpr int W = 16 / sizeof(VT);
+    const int a = blockIdx.x;
+    double zc[6] = {0, 0, 0, 0, 0, 0};
+    const VT* A = Ainv + (size_t)(6 * a) * ld;
+    for (int j = threadIdx.x * W; j < ld; j += blockDim.x * W) {
+        double y[W];
+#pragma unroll
+        for (int w = 0; w < W; w++) y[w] = yc[j + w];
+#pragma unroll
+        for (int m = 0; m < 6; m++) {
+            VT v[W];
+            load16<VT>(A + (size_t)m * ld + j, v);
+#pragma unroll
+            for (int w = 0; w < W; w++) zc[m] += (double)v[w] * y[w];
+        }
+    }
+    block_sum<6>(zc, sh);
+    const VT t0 = (VT)zc[0], t1 = (VT)zc[1], t2 = (VT)zc[2];
+    const VT w0 = (VT)zc[3], w1 = (VT)zc[4], w2 = (VT)zc[5];
+    const VT* vin = b.V[vpar];
+    double acc[2] = {0.0, 0.0};
+    for (int k = c.agg_ptr[a] + threadIdx.x; k < c.agg_ptr[a + 1]; k += blockDim.x) {
+        const int i = __ldg(c.agg_nodes + k);
+        const size_t bi = 3 * (size_t)i;
+        const VT v[3] = {vin[bi], vin[bi + 1], vin[bi + 2]};
+        const VT* M = b.Minv + 9 * (size_t)i;
+        VT z[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) z[d] = M[d * 3 + 0] * v[0] + M[d * 3 + 1] * v[1] + M[d * 3 + 2] * v[2];
+        const float4 o = __ldg(c.off + i);
+        const unsigned f = c.fixed ? (unsigned)__ldg(c.fixed + i) : 0u;
+        const VT ox = (VT)o.x, oy = (VT)o.y, oz = (VT)o.z;
+        VT add[3] = {t0 + w1 * oz - w2 * oy, t1 - w0 * oz + w2 * ox, t2 + w0 * oy - w1 * ox};
+        if (f & 1u) add[0] = VT(0);
+        if (f & 2u) add[1] = VT(0);
+        if (f & 4u) add[2] = VT(0);
+#pragma unroll
+        for (int d = 0; d < 3; d++) z[d] += add[d];
+        st_pad<VT>(b.Z[vpar], (size_t)i, z);
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            acc[0] += (double)v[d] * (double)z[d];
+            acc[1] += (double)v[d] * (double)v[d];
+        }
+    }
+    double tot[2];
+    if (reduce_grid<2>(acc, partials, &sc->counters[init ? 11 : 12], tot) && threadIdx.x == 0) {
+        if (init) minres_start(sc, tot[0], tot[1], eta2, abs_tol2, maxit);
+        else minres_advance(sc, tot[0]);
+    }
+}
+
+template <typename VT>
+void launch_minres_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const MinresBufs<VT>& b,
+                            int vpar, int init, double eta2, double abs_tol2, int maxit, double* partials,
+                            DevScalars* sc, cudaStream_t st) {
+    k_minres_coarse_z<VT><<<c.nagg, kAggThreads, 0, st>>>(c, ld, Ainv, yc, b, vpar, init, eta2, abs_tol2, maxit,
+                                                           partials, sc);
+    counted();
+}
+
+// The last iteration's pending solution update (par = (J + 1) & 1 for the
+// last iteration J, as the SpMV of iteration J + 1 would have applied it).
+template <typename VT>
+__global__ void __launch_bounds__(kRedThreads) k_minres_finish(int N, MinresBufs<VT> b, int par, const DevScalars* sc) {
+    if (!sc->mr_pending) return;
+    MinresUpd<VT> u;
+    u.zprev = b.Z[par ^ 1];
+    u.wread = b.W[par ^ 1];
+    u.wrw = b.W[par];
+    u.x = b.x;
+    const VT ig = (VT)sc->mr_ig, a1i = (VT)(1.0 / sc->mr_a1), a2 = (VT)sc->mr_a2, a3 = (VT)sc->mr_a3;
+    const VT ceta = (VT)sc->mr_ceta;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x)
+#pragma unroll
+        for (int d = 0; d < 3; d++) minres_row_update<VT>(u, (size_t)i, d, ig, a1i, a2, a3, ceta);
+}
+
+template <typename VT>
+void launch_minres_finish(int N, const MinresBufs<VT>& b, int par, const DevScalars* sc, cudaStream_t st) {
+    k_minres_finish<VT><<<red_grid(N, 2), kRedThreads, 0, st>>>(N, b, par, sc);
+    counted();
+}
+
+#define SORS_MINRES_INST(HT, VT)                                                                                   \
+    template void launch_block_jacobi_abs<HT, VT>(int, const int*, const HT*, long long, VT*, cudaStream_t);     \
+    template void launch_minres_spmv<HT, VT>(int, int, const int*, const int*, const HT*, long long,              \
+                                             const MinresBufs<VT>&, int, double*, DevScalars*, cudaStream_t);
+SORS_MINRES_INST(double, double)
+SORS_MINRES_INST(float, float)
+#undef SORS_MINRES_INST
+#define SORS_MINRES_INST_V(VT)                                                                                      \
+    template void launch_minres_init<VT>(int, const double*, const MinresBufs<VT>&, bool, double, double, int,     \
+                                         double*, DevScalars*, cudaStream_t);                                      \
+    template void launch_minres_lanczos<VT>(int, const MinresBufs<VT>&, int, double*, DevScalars*, cudaStream_t);  \
+    template void launch_minres_lanczos_restrict<VT>(const CoarseArgs&, const MinresBufs<VT>&, int, double*,       \
+                                                     const DevScalars*, cudaStream_t);                             \
+    template void launch_minres_coarse_z<VT>(const CoarseArgs&, int, const VT*, const double*,                     \
+                                             const MinresBufs<VT>&, int, int, double, double, int, double*,         \
+                                             DevScalars*, cudaStream_t);                                            \
+    template void launch_minres_finish<VT>(int, const MinresBufs<VT>&, int, const DevScalars*, cudaStream_t);
+SORS_MINRES_INST_V(double)
+SORS_MINRES_INST_V(float)
+#undef SORS_MINRES_INST_V
 
 }  // namespace sors

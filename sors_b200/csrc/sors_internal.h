@@ -35,6 +35,13 @@ struct DevScalars {
     // PCG
     double rz, pq, alpha, beta, rr, tol2, bnorm2;
     int it, done, maxit, breakdown;
+    // MINRES (Lanczos vectors with Givens QR, minres.cu): gamma_{j-1},
+    // gamma_j, delta_j, c_{j-1}, c_j, s_{j-1}, s_j and eta (the preconditioned
+    // residual norm, signed); the solution update the last iteration left
+    // pending (alpha1, alpha2, alpha3, c_{j+1} eta_j, 1 / gamma_j)
+    double mr_gprev, mr_g, mr_delta, mr_cprev, mr_c, mr_sprev, mr_s, mr_eta;
+    double mr_a1, mr_a2, mr_a3, mr_ceta, mr_ig;
+    int mr_pending, mr_bad;
     int status;          // kFlag* bits
     unsigned counters[16];
 };
@@ -197,6 +204,40 @@ template <typename VT>
 void launch_tl_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const VT* r, const VT* Minv,
                         VT* z, int init, const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc,
                         cudaStream_t st);
+
+// MINRES work vectors (kernels.cu, minres section), by the parity of the
+// iteration j: Z[j & 1] padded z_j (four values per node), V[j & 1] the
+// Lanczos vector v_j, W[j & 1] the update direction w_j; x the solution, q
+// the SpMV output, Minv the SPD block-Jacobi inverse.
+template <typename VT>
+struct MinresBufs {
+    VT* Z[2] = {nullptr, nullptr};
+    VT* V[2] = {nullptr, nullptr};
+    VT* W[2] = {nullptr, nullptr};
+    VT* x = nullptr;
+    VT* q = nullptr;
+    const VT* Minv = nullptr;
+};
+template <typename HT, typename VT>
+void launch_block_jacobi_abs(int N, const int* diag_slot, const HT* H, long long nnzb, VT* Minv, cudaStream_t st);
+template <typename VT>
+void launch_minres_init(int N, const double* g, const MinresBufs<VT>& b, bool with_z, double eta2, double abs_tol2,
+                        int maxit, double* partials, DevScalars* sc, cudaStream_t st);
+template <typename HT, typename VT>
+void launch_minres_spmv(int N, int max_row_blocks, const int* row_ptr, const int* col, const HT* H, long long nnzb,
+                        const MinresBufs<VT>& b, int par, double* partials, DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_minres_lanczos(int N, const MinresBufs<VT>& b, int par, double* partials, DevScalars* sc,
+                           cudaStream_t st);
+template <typename VT>
+void launch_minres_lanczos_restrict(const CoarseArgs& c, const MinresBufs<VT>& b, int par, double* yc,
+                                    const DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_minres_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const MinresBufs<VT>& b,
+                            int vpar, int init, double eta2, double abs_tol2, int maxit, double* partials,
+                            DevScalars* sc, cudaStream_t st);
+template <typename VT>
+void launch_minres_finish(int N, const MinresBufs<VT>& b, int par, const DevScalars* sc, cudaStream_t st);
 
 // Sets the message returned by sors_last_error on this thread (capi.cu).
 void set_last_error(const std::string& msg);

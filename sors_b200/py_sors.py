@@ -62,6 +62,9 @@ class SimulationSettings:
         # block Jacobi + coarse rigid-body correction: True, False or "auto"
         # (on for meshes of 20,000 nodes or more)
         self.twoLevelPreconditioner = "auto"
+        # Newton linear solver of "minimize_newton": "pcg", or "minres" for the
+        # exact Newton step of an indefinite Hessian (the reference's LDL^T step)
+        self.linearSolver = "pcg"
         self.newtonResidualTol = 0.0       # absolute ||gradient|| stop; 0 = reference dx test only
         self.newtonDxTol = 1e-9            # reference DX_TOL (cpp/headers/common.h:25)
         self.newtonMaxIter = 100           # reference MAX_ITER (cpp/headers/common.h:21)
@@ -290,6 +293,10 @@ class _EnergyBase:
         s.newton_safeguard = int(bool(getattr(settings, "newtonSafeguard", False)))
         tl = getattr(settings, "twoLevelPreconditioner", "auto")
         s.two_level = 2 if (isinstance(tl, str) and tl == "auto") else int(bool(tl))
+        ls = getattr(settings, "linearSolver", "pcg")
+        if ls not in ("pcg", "minres"):
+            raise ValueError(f"linearSolver must be 'pcg' or 'minres', not {ls!r}")
+        s.linear_solver = 1 if ls == "minres" else 0
         self._settings_c = s
         h = C.c_void_p()
         _lib.check(L.sors_create(_p(X, C.c_double), X.shape[0], _p(T, C.c_int32), ne, self.NV, _p(rho, C.c_double),
