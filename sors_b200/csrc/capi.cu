@@ -1373,23 +1373,45 @@ void update_disk_contacts(SorsHandle* h, const double* q) {
 // unknowns are its 3 translations and 3 rotations about its centroid, the
 // rotations scaled by 1 / (box size).  The Galerkin matrix P^T H P is summed
 // per aggregate pair over a fixed list of Hessian blocks (deterministic).
+// Two-level aggregates: a grid of about N / 1000 (at most 512) near-cubic
+// boxes over the bounding box of the undeformed positions.  The locality
+// order numbers the nodes box by box, so that each aggregate is a contiguous
+// node range.
+struct AggBins {
+    double lo[3], L[3], hb;
+    int dim[3];
+    void cell(const double* x, int (&c)[3]) const {
+        for (int k = 0; k < 3; k++) c[k] = std::max(0, std::min(dim[k] - 1, (int)((x[k] - lo[k]) / L[k] * dim[k])));
+    }
+};
+AggBins agg_bins(int N, const double* X) {
+    AggBins b;
+    double hi[3] = {-1e300, -1e300, -1e300};
+    for (int k = 0; k < 3; k++) b.lo[k] = 1e300;
+    for (int i = 0; i < N; i++)
+        for (int k = 0; k < 3; k++) {
+            b.lo[k] = std::min(b.lo[k], X[3 * (size_t)i + k]);
+            hi[k] = std::max(hi[k], X[3 * (size_t)i + k]);
+        }
+    const int target = std::max(1, std::min(512, N / 1000));
+    double vol = 1.0;
+    for (int k = 0; k < 3; k++) b.L[k] = std::max(hi[k] - b.lo[k], 1e-12);
+    const double lmax = std::max(b.L[0], std::max(b.L[1], b.L[2]));
+    for (int k = 0; k < 3; k++) vol *= std::max(b.L[k], 1e-3 * lmax);
+    b.hb = cbrt(vol / target);
+    for (int k = 0; k < 3; k++) b.dim[k] = std::max(1, (int)llround(b.L[k] / b.hb));
+    return b;
+}
+
 int setup_two_level(SorsHandle* h, const double* X) {
     const int N = h->N;
-    double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-    for (int i = 0; i < N; i++)
-        for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], X[3 * i + k]); hi[k] = std::max(hi[k], X[3 * i + k]); }
-    const int target = std::max(1, std::min(512, N / 1000));
-    double L[3], vol = 1.0;
-    for (int k = 0; k < 3; k++) { L[k] = std::max(hi[k] - lo[k], 1e-12); }
-    double lmax = std::max(L[0], std::max(L[1], L[2]));
-    for (int k = 0; k < 3; k++) vol *= std::max(L[k], 1e-3 * lmax);
-    const double hb = cbrt(vol / target);
-    int dim[3];
-    for (int k = 0; k < 3; k++) dim[k] = std::max(1, (int)llround(L[k] / hb));
+    AggBins ab = agg_bins(N, X);
+    const double hb = ab.hb;
+    const int* dim = ab.dim;
     std::vector<int> bin(N), remap((size_t)dim[0] * dim[1] * dim[2], -1);
     for (int i = 0; i < N; i++) {
         int c[3];
-        for (int k = 0; k < 3; k++) c[k] = std::min(dim[k] - 1, (int)((X[3 * i + k] - lo[k]) / L[k] * dim[k]));
+        ab.cell(X + 3 * (size_t)i, c);
         bin[i] = c[0] + dim[0] * (c[1] + dim[1] * c[2]);
     }
     int nagg = 0;
@@ -2033,9 +2055,10 @@ int set_device(SorsHandle* h) {
 
 // Locality order of the nodes: connected components in the order of their
 // lowest caller index (so that the meshes of a union keep their node ranges),
-// and within each the Morton order of the undeformed positions (21 bits per
-// axis over the bounding box).  Element order is not changed.  SORS_NO_RENUMBER=1
-// keeps the caller's numbering (for comparison).
+// within each the two-level aggregate boxes (agg_bins) in Morton order, and
+// within a box the Morton order of the undeformed positions (21 bits per axis,
+// one scale for all axes), so that every aggregate is a contiguous node range.
+// SORS_NO_RENUMBER=1 keeps the caller's numbering (for comparison).
 void locality_order(int N, int E, int nv, const double* X, const int32_t* conn, std::vector<int>& n2o) {
     std::vector<int> parent(N);
     for (int i = 0; i < N; i++) parent[i] = i;
@@ -2065,19 +2088,23 @@ void locality_order(int N, int E, int nv, const double* X, const int32_t* conn, 
         v = (v | v << 2) & 0x1249249249249249ULL;
         return v;
     };
-    std::vector<std::tuple<int, uint64_t, int>> key(N);
+    const double ext = std::max(hi[0] - lo[0], std::max(hi[1] - lo[1], hi[2] - lo[2]));
+    const AggBins ab = agg_bins(N, X);
+    std::vector<std::tuple<int, uint64_t, uint64_t, int>> key(N);
     for (int i = 0; i < N; i++) {
-        uint64_t code = 0;
+        uint64_t code = 0, box = 0;
+        int c[3];
+        ab.cell(X + 3 * (size_t)i, c);
         for (int k = 0; k < 3; k++) {
-            const double ext = hi[k] - lo[k];
             const double u = ext > 0 ? (X[3 * (size_t)i + k] - lo[k]) / ext : 0.0;
             code |= spread((uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0))) << k;
+            box |= spread((uint64_t)c[k]) << k;
         }
-        key[i] = std::make_tuple(root[i], code, i);
+        key[i] = std::make_tuple(root[i], box, code, i);
     }
     std::sort(key.begin(), key.end());
     n2o.resize(N);
-    for (int i = 0; i < N; i++) n2o[i] = std::get<2>(key[i]);
+    for (int i = 0; i < N; i++) n2o[i] = std::get<3>(key[i]);
 }
 
 // Caller-numbered DOF vector (host or device) -> internal device vector.
