@@ -470,9 +470,10 @@ def run_c3(args):
                                           forceParameterList=fp)
             prof = _lib.SorsKernelProfile()
             _lib.check(L.sors_profile_kernels(en.handle(), 5, ctypes.byref(prof)))
-            print(json.dumps({"workload": "c3 hex assembly at rest", "precision": precision,
+            print(json.dumps({"workload": "c3 kernels at rest", "precision": precision,
                               "hessian_projection": args.c3_projection, "hexes": int(H.shape[0]),
-                              "assemble_ms": prof.assemble_ms, "assemble_grad_ms": prof.assemble_grad_ms}),
+                              **{k: getattr(prof, k) for k, _ in _lib.SorsKernelProfile._fields_
+                                 if k.endswith("_ms")}}),
                   flush=True)
             del en
         return

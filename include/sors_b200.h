@@ -245,12 +245,22 @@ int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32
  *   dL/dact (one per muscle group, "softconMuscle" activations),
  *   dL/dneumann (3N)             the Neumann velocities, nonzero on fixed DOFs.
  * Any dependence of the loss on v_next = (q_next - q_n)/dt is the caller's to
- * add to dL/dq_next (and subtract from dL/dq_n).  Pressure loads and
- * Crank-Nicolson steps return SORS_ERR_UNSUPPORTED.  dt = 0 takes settings.dt. */
+ * add to dL/dq_next (and subtract from dL/dq_n).  With pressure loads the
+ * transpose system uses the exact derivative of the follower load (not the
+ * Newton matrix's symmetrised one; see sors_adjoint_pressure_grad); pressure
+ * loads with held max-distance pairs, and Crank-Nicolson steps, return
+ * SORS_ERR_UNSUPPORTED.  dt = 0 takes settings.dt. */
 int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
                       const int32_t* held_nodes, const double* held_normals, int32_t n_held, double* dL_dq_prev,
                       double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
                       SorsStepStats* stats);
+
+/* dL/d(pressure of each group) of the last sors_adjoint_step on this handle
+ * (no reference counterpart), for PressureForce's per-group "pressure"
+ * actuation (cpp/src/forces/pressureForce.cpp:12-56): lam . f_g with lam the
+ * step's adjoint and f_g the follower load of group g at unit pressure on
+ * q_next.  n_groups must equal the groups given to sors_set_pressure_faces. */
+int sors_adjoint_pressure_grad(SorsHandle* h, double* dL_dpressure, int32_t n_groups);
 
 /* Same step on a device-resident FP64 solution vector (in place). */
 int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substeps,

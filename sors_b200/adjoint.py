@@ -19,7 +19,9 @@ curvature (the multiplier times the Hessian of |x_i - x_j|) in the transpose
 system.
 
 `rollout(...)` is the torch entry point: a torch.autograd.Function whose inputs
-are float64 tensors E (E,) and act (T, G).
+are float64 tensors E (E,) and act (T, G).  Follower-load pressures per step
+(`RolloutAdjoint.forward(..., pressure=...)`) are differentiated too
+(`grad_pressure` after `backward`).
 """
 from __future__ import annotations
 
@@ -56,6 +58,8 @@ class RolloutAdjoint:
         self._cstate0 = None
         self._E = None
         self._act = None
+        self._pressure = None
+        self.grad_pressure = None  # dL/d pressure (T, groups) after backward, with a pressure schedule
         self.last_pcg_iters = 0
 
     # -- helpers --------------------------------------------------------------
@@ -69,6 +73,12 @@ class RolloutAdjoint:
             return
         a = np.ascontiguousarray(a, dtype=np.float64)
         _lib.check(_lib.load().sors_set_actuation(self.en._h, b"softconMuscle", _p(a), a.size))
+
+    def _set_pressure(self, p):
+        if p is None or p.size == 0:
+            return
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        _lib.check(_lib.load().sors_set_actuation(self.en._h, b"pressure", _p(p), p.size))
 
     def _contact_state(self):
         L = _lib.load()
@@ -98,15 +108,18 @@ class RolloutAdjoint:
         if self.before_step is not None:
             self.before_step(t)
         self._set_act(None if self._act is None else self._act[t])
+        self._set_pressure(None if self._pressure is None else self._pressure[t])
         qn = self.sol.step(q, self.en, None, self.dt)
         self._held[t] = self._held_now()
         return qn
 
     # -- forward ----------------------------------------------------------------
-    def forward(self, E, act=None):
-        """Runs the rollout; returns q_T.  E: (E,), act: (T, G) or None."""
+    def forward(self, E, act=None, pressure=None):
+        """Runs the rollout; returns q_T.  E: (E,), act: (T, G) or None,
+        pressure: (T, pressure groups) follower-load pressures per step or None."""
         self._E = np.array(E, dtype=np.float64)
         self._act = None if act is None else np.array(act, dtype=np.float64).reshape(self.steps, -1)
+        self._pressure = None if pressure is None else np.array(pressure, dtype=np.float64).reshape(self.steps, -1)
         self._set_material(self._E)
         self._restore(self.q0, self.v0, self._contact_state() if self._cstate0 is None else self._cstate0)
         if self._cstate0 is None:
@@ -135,6 +148,9 @@ class RolloutAdjoint:
         gE = np.zeros(ne)
         gA = None if self._act is None else np.zeros_like(self._act)
         dq = np.zeros(n); dv = np.zeros(n); dE = np.zeros(ne); dA = np.zeros(max(G, 1))
+        P = 0 if self._pressure is None else self._pressure.shape[1]
+        self.grad_pressure = None if P == 0 else np.zeros_like(self._pressure)
+        dP = np.zeros(max(P, 1))
         stats = _lib.SorsStepStats()
         self.last_pcg_iters = 0
         self._set_material(self._E)
@@ -148,6 +164,7 @@ class RolloutAdjoint:
                 qs.append(self._step(qs[-1], t))
             for t in range(e - 1, s - 1, -1):
                 self._set_act(None if self._act is None else self._act[t])
+                self._set_pressure(None if self._pressure is None else self._pressure[t])
                 b = Qb + Vb / self.dt
                 hn, hv, hp, hmu = self._held[t]
                 hv = np.ascontiguousarray(hv)
@@ -161,6 +178,9 @@ class RolloutAdjoint:
                 gE += dE
                 if G:
                     gA[t] = dA[:G]
+                if P:
+                    _lib.check(L.sors_adjoint_pressure_grad(self.en._h, _p(dP), P))
+                    self.grad_pressure[t] = dP[:P]
                 Qb = dq - Vb / self.dt
                 Vb = dv.copy()
         return gE, gA, Qb, Vb

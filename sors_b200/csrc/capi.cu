@@ -123,6 +123,8 @@ struct SorsHandle {
     std::vector<double> youngs_h, poisson_h, mass_h;
     std::vector<int> mgroup_h;
     double *adj_l = nullptr, *adj_y = nullptr, *adj_e = nullptr;
+    double *adj_q = nullptr, *adj_pg = nullptr;  // q_next of the last adjoint step; group pressures scratch
+    bool adj_ready = false;                      // adj_l and adj_q hold the last adjoint step
 
     // SoftCon fibre terms
     int* mgroup = nullptr;
@@ -604,6 +606,14 @@ double inertia_coef(const SorsHandle* h, double dt) {
 
 int method(const SorsHandle* h) { return h->s.solver_method; }
 
+PressureArgs pressure_args(SorsHandle* h) {
+    PressureArgs p;
+    p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
+    p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
+    p.f_ext = h->f_ext;
+    return p;
+}
+
 // f_ext = vertexForce + pressure forces at h->q
 int compute_external(SorsHandle* h) {
     if (!(h->has_vforce || h->has_pressure)) return SORS_OK;
@@ -611,13 +621,7 @@ int compute_external(SorsHandle* h) {
         CK(cudaMemcpyAsync(h->f_ext, h->vforce, sizeof(double) * h->ndof, cudaMemcpyDeviceToDevice, h->stream));
     else
         CK(cudaMemsetAsync(h->f_ext, 0, sizeof(double) * h->ndof, h->stream));
-    if (h->has_pressure) {
-        PressureArgs p;
-        p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
-        p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
-        p.f_ext = h->f_ext;
-        launch_pressure_force(p, h->stream);
-    }
+    if (h->has_pressure) launch_pressure_force(pressure_args(h), h->stream);
     return SORS_OK;
 }
 
@@ -666,13 +670,9 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
                         : (h->s.project_spd == 2 ? (h->proj_fallback ? 1 : 0) : h->s.project_spd);
     AsmArgs<HT> a = asm_args<HT>(h, dt, want_hess, mode, project);
     launch_assemble<HT>(a, h->max_pairs, h->stream);
-    if (want_hess && h->has_pressure && method(h) == 0) {
-        PressureArgs p;
-        p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
-        p.faces = h->faces; p.face_group = h->face_group; p.fnv = h->fnv; p.pressure = h->pressure_d; p.q = h->q;
-        p.f_ext = h->f_ext;
-        launch_pressure_jac<HT>(p, h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->nnzb, h->stream);
-    }
+    if (want_hess && h->has_pressure && method(h) == 0)
+        launch_pressure_jac<HT>(pressure_args(h), h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->nnzb,
+                                h->stream);
     launch_finalize_grad(h->N, h->g_int, h->f_ext, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, h->mass,
                          h->node_mask, h->mval, dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav,
                          a.neumann_override, (h->has_vforce || h->has_pressure) ? 1 : 0, h->g, h->partials, h->sc,
@@ -1073,6 +1073,8 @@ int adjoint_pairs(SorsHandle* h, double eta, std::vector<double>& lam, std::vect
 // lam = Z (Z^T H Z)^-1 Z^T b is a projected solve with the exact Hessian, and
 //   dL/dtheta = -lam^T dg/dtheta  for the material, activations and old state,
 //   r = b - H lam                 carries dL through the fixed DOFs' targets.
+constexpr int kAdjointPressureIters = 200;
+
 template <typename HT, typename VT>
 int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b, const int* held_nodes,
                  const double* held_normals, int n_held, double* dq, double* dv, double* dE, double* dact,
@@ -1083,7 +1085,9 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         if ((st = dalloc_t(h, &h->adj_l, (size_t)n))) return st;
         if ((st = dalloc_t(h, &h->adj_y, (size_t)n))) return st;
         if ((st = dalloc_t(h, &h->adj_e, (size_t)2 * std::max(1, E)))) return st;
+        if ((st = dalloc_t(h, &h->adj_q, (size_t)n))) return st;
     }
+    h->adj_ready = false;
     if ((st = ensure_sqp_buffers(h, 0))) return st;
     CK(h2d(h, h->q, q_next, sizeof(double) * n));
     CK(cudaMemsetAsync(h->status, 0, sizeof(int), h->stream));
@@ -1108,27 +1112,61 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     }
     CK(h2d(h, h->pflag_d, h->pflag_h.data(), (size_t)N));
     CK(h2d(h, h->pn_d, h->pn_h.data(), sizeof(double4) * N));
-    std::vector<double> lam(n);
-    for (int i = 0; i < n; i++) lam[i] = -b[i];  // pcg_solve solves H x = -g
-    CK(h2d(h, h->qp_g2, lam.data(), sizeof(double) * n));
+    std::vector<double> lam(n), rhs(b, b + n);
     const double eta = mixed(h) ? 1e-6 : std::max(1e-12, 0.01 * h->s.pcg_rel_tol);
-    int pit = 0;
-    h->proj_flag = h->pflag_d;
-    h->proj_n = h->pn_d;
-    st = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
-    h->proj_flag = nullptr;
-    h->proj_n = nullptr;
-    if (st) return st;
-    if (h->sc_host->status & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
-    if (stats) { stats->pcg_iters += pit; stats->residual_norm = sqrt(h->sc_host->rr); }
-    if (sizeof(VT) == sizeof(double)) {
-        CK(d2h(h, lam.data(), h->x, sizeof(double) * n));
-    } else {
-        std::vector<float> lf(n);
-        CK(d2h(h, lf.data(), h->x, sizeof(float) * n));
-        for (int i = 0; i < n; i++) lam[i] = lf[i];
+    // lam = H^-1 rhs on the free subspace (H symmetric)
+    auto solve = [&](const std::vector<double>& r) -> int {
+        std::vector<double> g(n);
+        for (int i = 0; i < n; i++) g[i] = -r[i];  // pcg_solve solves H x = -g
+        CK(h2d(h, h->qp_g2, g.data(), sizeof(double) * n));
+        int pit = 0;
+        h->proj_flag = h->pflag_d;
+        h->proj_n = h->pn_d;
+        int s2 = pcg_solve<HT, VT>(h, eta, 0.0, &pit, h->qp_g2);
+        h->proj_flag = nullptr;
+        h->proj_n = nullptr;
+        if (s2) return s2;
+        if (h->sc_host->status & kFlagInverted) return fail(SORS_ERR_INVERTED, "Inverted Elements");
+        if (stats) { stats->pcg_iters += pit; stats->residual_norm = sqrt(h->sc_host->rr); }
+        if (sizeof(VT) == sizeof(double)) {
+            CK(d2h(h, lam.data(), h->x, sizeof(double) * n));
+        } else {
+            std::vector<float> lf(n);
+            CK(d2h(h, lf.data(), h->x, sizeof(float) * n));
+            for (int i = 0; i < n; i++) lam[i] = lf[i];
+        }
+        CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
+        return SORS_OK;
+    };
+    if ((st = solve(rhs))) return st;
+    // Follower load: the residual's exact Jacobian K + T is not symmetric and
+    // the Newton matrix holds K + S instead (k_pressure_adj_corr).  The
+    // transpose system (K + T)^T lam = b is solved by the fixed point
+    // lam <- H^-1 (b - (T^T - S) lam), which contracts when the load term is
+    // small against stiffness and inertia.
+    std::vector<double> corr;  // (T^T - S) lam at the final lam
+    if (h->has_pressure) {
+        const double tol = mixed(h) ? 1e-6 : 1e-11;
+        corr.assign(n, 0.0);
+        bool conv = false;
+        for (int k = 0; k < kAdjointPressureIters && !conv; k++) {
+            CK(cudaMemsetAsync(h->adj_y, 0, sizeof(double) * n, h->stream));
+            launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? 1 : 0, h->adj_l, h->adj_y,
+                                     h->stream);
+            CK(d2h(h, corr.data(), h->adj_y, sizeof(double) * n));
+            const std::vector<double> prev = lam;
+            for (int i = 0; i < n; i++) rhs[i] = b[i] - corr[i];
+            if ((st = solve(rhs))) return st;
+            double dd = 0.0, ll = 0.0;
+            for (int i = 0; i < n; i++) { dd += (lam[i] - prev[i]) * (lam[i] - prev[i]); ll += lam[i] * lam[i]; }
+            conv = dd <= tol * tol * ll;
+        }
+        if (!conv) return fail(SORS_ERR_NOT_CONVERGED, "the pressure-load adjoint fixed point did not converge");
+        CK(cudaMemsetAsync(h->adj_y, 0, sizeof(double) * n, h->stream));
+        launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? 1 : 0, h->adj_l, h->adj_y,
+                                 h->stream);
+        CK(d2h(h, corr.data(), h->adj_y, sizeof(double) * n));
     }
-    CK(h2d(h, h->adj_l, lam.data(), sizeof(double) * n));
     std::vector<double> extra;  // forces of the held pairs' columns (empty: none)
     if (!h->adj_pairs.empty()) {
         int pp = 0;
@@ -1144,7 +1182,8 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     if (h->has_neumann) {
         launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->adj_l, h->adj_y, h->stream);
         CK(d2h(h, r.data(), h->adj_y, sizeof(double) * n));
-        for (int i = 0; i < n; i++) r[i] = b[i] - r[i] + (extra.empty() ? 0.0 : extra[i]);
+        for (int i = 0; i < n; i++)
+            r[i] = b[i] - r[i] + (extra.empty() ? 0.0 : extra[i]) - (corr.empty() ? 0.0 : corr[i]);
     }
     const double a = h->s.damping_alpha;
     for (int i = 0; i < n; i++) {
@@ -1155,6 +1194,8 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         if (dv) dv[i] = dt != 0.0 ? lam[i] * m / dt : 0.0;
         if (dneu) dneu[i] = f ? r[i] * dt : 0.0;
     }
+    CK(cudaMemcpyAsync(h->adj_q, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
+    h->adj_ready = true;
     if (dE)
         for (int e = 0; e < E; e++) dE[e] = h->youngs_h[e] != 0.0 ? -ge[e] / h->youngs_h[e] : 0.0;
     if (dact) {
@@ -2802,7 +2843,8 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (dt == 0.0) dt = h->s.dt;
     if (h->s.time_stepping != 0 && dt != 0.0)
         return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for backward Euler steps");
-    if (h->has_pressure) return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not differentiate pressure loads");
+    if (h->has_pressure && !h->adj_pairs.empty())
+        return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not combine pressure loads with held max-distance pairs");
     if (h->s.material == 1) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
     if (stats) *stats = SorsStepStats{};
     if (!h->renum && !h->renum_e)
@@ -2831,6 +2873,37 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (dL_dq_prev) dofs_to_caller(h, oq.data(), dL_dq_prev);
     if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
     if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
+    return SORS_OK;
+}
+
+int sors_adjoint_pressure_grad(SorsHandle* h, double* dL_dpressure, int32_t n_groups) {
+    if (!h || !dL_dpressure) return fail(SORS_ERR_ARG, "NULL argument");
+    if (!h->has_pressure || n_groups != h->n_groups)
+        return fail(SORS_ERR_ARG, "n_groups must equal the number of pressure groups");
+    if (!h->adj_ready) return fail(SORS_ERR_ARG, "no adjoint step to differentiate");
+    int st;
+    if ((st = set_device(h))) return st;
+    const int n = h->ndof;
+    if (!h->adj_pg && (st = dalloc_t(h, &h->adj_pg, (size_t)std::max(1, n_groups)))) return st;
+    std::vector<double> lam(n), f(n), e(n_groups);
+    CK(d2h(h, lam.data(), h->adj_l, sizeof(double) * n));
+    // dL/dp_g = -lam . dg/dp_g = lam . f_g, f_g the follower load of group g at unit pressure
+    for (int g = 0; g < n_groups; g++) {
+        std::fill(e.begin(), e.end(), 0.0);
+        e[g] = 1.0;
+        CK(h2d(h, h->adj_pg, e.data(), sizeof(double) * n_groups));
+        CK(cudaMemsetAsync(h->adj_y, 0, sizeof(double) * n, h->stream));
+        PressureArgs p = pressure_args(h);
+        p.pressure = h->adj_pg;
+        p.q = h->adj_q;
+        p.f_ext = h->adj_y;
+        launch_pressure_force(p, h->stream);
+        CK(cudaGetLastError());
+        CK(d2h(h, f.data(), h->adj_y, sizeof(double) * n));
+        double acc = 0.0;
+        for (int i = 0; i < n; i++) acc += lam[i] * f[i];
+        dL_dpressure[g] = acc;
+    }
     return SORS_OK;
 }
 

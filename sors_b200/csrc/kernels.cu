@@ -1659,6 +1659,59 @@ void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* c
     counted();
 }
 
+// Adjoint correction of the follower load, y = (T^T - S) lam on the surface
+// rows (y is zero elsewhere and must be cleared by the caller):
+//   T: the exact derivative of the residual's pressure term,
+//      d g_j / d x_k = p / (2 fnv) * 2 dA/dx_k for every vertex j of the face
+//      (face_hess gives 2 dA/dx_k; p/6 for triangles, p/8 for quads);
+//   S: what k_pressure_jac adds to the Newton matrix (with_s), the reference's
+//      coefficient p/6 for both face types, lower triangle mirrored, held
+//      DOFs skipped.
+// The Newton matrix H = K + S is symmetric; the adjoint needs (K + T)^T =
+// H + (T^T - S).
+__global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, int with_s, const double* lam,
+                                    double* y) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= p.nsurf) return;
+    int i = p.surf_nodes[s];
+    unsigned mi = node_mask[i];
+    double acc[3] = {0.0, 0.0, 0.0};
+    for (int t = p.sface_ptr[s]; t < p.sface_ptr[s + 1]; t++) {
+        int fl = p.sface_fl[t];
+        int face = fl >> 2, ki = fl & 3;
+        const int* fv = p.faces + (size_t)face * p.fnv;
+        double h[4][9];
+        face_hess(fv, p.fnv, p.q, h);
+        const double pr = p.pressure[p.face_group[face]];
+        const double c_true = pr / (2.0 * p.fnv), c_ref = pr / 6.0;
+        for (int kj = 0; kj < p.fnv; kj++) {
+            int j = fv[kj];
+            unsigned mj = node_mask[j];
+            for (int l = 0; l < 3; l++) {
+                for (int m = 0; m < 3; m++) {
+                    const double lb = lam[3 * (size_t)j + m];
+                    // (T^T lam)_a: T[b][a] = c_true h[ki](m, l), a = 3i+l, b = 3j+m
+                    double v = c_true * h[ki][m * 3 + l];
+                    if (with_s && !((mi >> l) & 1u) && !((mj >> m) & 1u)) {
+                        const long long a = 3LL * i + l, b = 3LL * j + m;
+                        if (a > b) v -= c_ref * h[kj][l * 3 + m];
+                        else if (a < b) v -= c_ref * h[ki][m * 3 + l];
+                    }
+                    acc[l] += v * lb;
+                }
+            }
+        }
+    }
+    for (int l = 0; l < 3; l++) y[3 * (size_t)i + l] = acc[l];
+}
+
+void launch_pressure_adj_corr(const PressureArgs& p, const uint8_t* node_mask, int with_s, const double* lam,
+                              double* y, cudaStream_t st) {
+    if (p.nsurf == 0) return;
+    k_pressure_adj_corr<<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, node_mask, with_s, lam, y);
+    counted();
+}
+
 // ---------------------------------------------------------------------------
 // gradient finalisation: external forces, integrator, Neumann rows
 // (energy.cpp:282-306, integrator.cpp:45-84)
