@@ -3084,10 +3084,20 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
         out->assemble_bytes = E * nv * 4 + E * 16 + N * 24 * 2 + N * 1 + N * 8 + (N + 1) * 4 + E * nv * 4 +
                               (nnzb + 1) * 4 + E * nv * nv * 2 + (N + 1) * 4 + nnzb * 4 + nnzb * 9 * hs + N * 24;
     }
-    // PCG kernels on the assembled system
+    // PCG kernels on the assembled system, on nonzero vectors (p = r = 1) so
+    // that no launch meets a zero curvature or a converged residual and exits early
     launch_block_jacobi<HT, VT>(h->N, h->row_ptr, h->diag_slot, (const HT*)h->H, h->nnzb, (VT*)h->Minv, h->stream);
     launch_pcg_init<HT, VT>(h->N, h->g, (const VT*)h->Minv, (VT*)h->x, (VT*)h->r, (VT*)h->z, (VT*)h->p0, 0.0, 0.0,
                             1 << 30, nullptr, nullptr, h->partials, h->sc, h->stream);
+    {
+        std::vector<VT> ones(4 * (size_t)h->N, VT(1));
+        for (size_t i = 3; i < ones.size(); i += 4) ones[i] = VT(0);
+        CK(cudaMemcpyAsync(h->p0, ones.data(), sizeof(VT) * ones.size(), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->p1, ones.data(), sizeof(VT) * ones.size(), cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->r, ones.data(), sizeof(VT) * 3 * (size_t)h->N, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaMemcpyAsync(h->z, ones.data(), sizeof(VT) * 3 * (size_t)h->N, cudaMemcpyHostToDevice, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+    }
     CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
     CK(cudaEventRecord(a, h->stream));
     for (int i = 0; i < iters; i++)
