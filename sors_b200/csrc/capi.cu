@@ -179,6 +179,7 @@ struct SorsHandle {
     bool tl_proj = false;             // the coarse operator came from the projected Hessian
     double tl_ref_rate = 0.0;
     CoarseArgs cargs;
+    CoarseRuns cruns;                 // nruns > 0: aggregates are contiguous node ranges
     int tl_npairs = 0;
     int *tl_pair_ptr = nullptr;
     int2 *tl_items = nullptr, *tl_ab = nullptr;
@@ -743,8 +744,12 @@ void pcg_iter_pair(SorsHandle* h) {
             launch_form_p<VT>(h->N, z, pin, pout, h->sc, h->stream);
             launch_pcg_spmv<HT, VT>(h->N, h->max_row_blocks, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, pout,
                                     (VT*)h->qv, h->partials, h->sc, h->stream);
-            launch_tl_update_restrict<VT>(h->cargs, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag,
-                                          h->proj_n, h->tl_yc, h->sc, h->stream);
+            if (h->cruns.nruns > 0)
+                launch_tl_update_restrict_runs<VT>(h->cargs, h->cruns, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r,
+                                                   h->proj_flag, h->proj_n, h->tl_yc, h->sc, h->stream);
+            else
+                launch_tl_update_restrict<VT>(h->cargs, pout, (VT*)h->qv, (VT*)h->x, (VT*)h->r, h->proj_flag,
+                                              h->proj_n, h->tl_yc, h->sc, h->stream);
             launch_tl_coarse_z<VT>(h->cargs, h->tl_ld, (const VT*)h->tl_Ainv, h->tl_yc, (VT*)h->r,
                                    (const VT*)h->Minv, z, 0, h->proj_flag, h->proj_n, h->partials, h->sc, h->stream);
         }
@@ -1455,11 +1460,10 @@ int setup_two_level(SorsHandle* h, const double* X) {
         ab.cell(X + 3 * (size_t)i, c);
         bin[i] = c[0] + dim[0] * (c[1] + dim[1] * c[2]);
     }
+    // aggregates numbered in the order of their lowest node
     int nagg = 0;
     for (int i = 0; i < N; i++)
-        if (remap[bin[i]] < 0) remap[bin[i]] = 0;
-    for (auto& r : remap)
-        if (r == 0) r = nagg++;
+        if (remap[bin[i]] < 0) remap[bin[i]] = nagg++;
     std::vector<int> aid(N), cnt(nagg + 1, 0);
     for (int i = 0; i < N; i++) { aid[i] = remap[bin[i]]; cnt[aid[i] + 1]++; }
     for (int a = 0; a < nagg; a++) cnt[a + 1] += cnt[a];
@@ -1524,6 +1528,34 @@ int setup_two_level(SorsHandle* h, const double* X) {
     if ((st = dalloc_t(h, &h->tl_rowk, (size_t)nc))) return st;
     if ((st = dalloc_t(h, &h->tl_colk, (size_t)nc))) return st;
     if ((st = dalloc(h, &h->tl_Ainv, (size_t)nc * h->tl_ld * hsize(h)))) return st;
+    // contiguous aggregates (aid non-decreasing in node order): the runs of the
+    // node-parallel restriction
+    bool contiguous = true;
+    for (int i = 1; i < N && contiguous; i++) contiguous = aid[i] >= aid[i - 1];
+    if (contiguous && N > 0) {
+        constexpr int kB = 256;  // kRunThreads
+        const int nblk = (N + kB - 1) / kB;
+        std::vector<int> run_start, block_ptr(nblk + 1, 0), agg_begin(nagg + 1, 0);
+        for (int b = 0; b < nblk; b++) {
+            block_ptr[b] = (int)run_start.size();
+            const int i1 = std::min(N, (b + 1) * kB);
+            for (int i = b * kB; i < i1; i++)
+                if (i == b * kB || aid[i] != aid[i - 1]) run_start.push_back(i);
+        }
+        block_ptr[nblk] = (int)run_start.size();
+        const int nruns = (int)run_start.size();
+        for (int k = nruns - 1; k >= 0; k--) agg_begin[aid[run_start[k]]] = k;
+        agg_begin[nagg] = nruns;
+        run_start.push_back(N);
+        int *rs_d = nullptr, *bp_d = nullptr, *ab_d = nullptr;
+        double* part_d = nullptr;
+        if ((st = upload(h, &rs_d, run_start.data(), run_start.size()))) return st;
+        if ((st = upload(h, &bp_d, block_ptr.data(), block_ptr.size()))) return st;
+        if ((st = upload(h, &ab_d, agg_begin.data(), agg_begin.size()))) return st;
+        if ((st = dalloc_t(h, &part_d, (size_t)6 * nruns))) return st;
+        h->cruns.run_start = rs_d; h->cruns.block_run_ptr = bp_d; h->cruns.agg_run_begin = ab_d;
+        h->cruns.partial = part_d; h->cruns.nruns = nruns;
+    }
     h->cargs.N = N; h->cargs.nagg = nagg; h->cargs.nc = nc;
     h->cargs.aid = aid_d; h->cargs.agg_c = cen_d; h->cargs.agg_ptr = aggptr_d; h->cargs.agg_nodes = nodes_d;
     h->cargs.fixed = h->node_mask; h->cargs.off = off_d;
@@ -3135,14 +3167,20 @@ int profile_impl(SorsHandle* h, int iters, SorsKernelProfile* out) {
         // two-level iteration kernels (their values are not used: timing only)
         CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
         CK(cudaEventRecord(a, h->stream));
-        for (int i = 0; i < iters; i++)
-            launch_tl_update_restrict<VT>(h->cargs, (VT*)h->p1, (VT*)h->qv, (VT*)h->x, (VT*)h->r, nullptr, nullptr,
-                                          h->tl_yc, h->sc, h->stream);
+        for (int i = 0; i < iters; i++) {
+            if (h->cruns.nruns > 0)
+                launch_tl_update_restrict_runs<VT>(h->cargs, h->cruns, (VT*)h->p1, (VT*)h->qv, (VT*)h->x,
+                                                   (VT*)h->r, nullptr, nullptr, h->tl_yc, h->sc, h->stream);
+            else
+                launch_tl_update_restrict<VT>(h->cargs, (VT*)h->p1, (VT*)h->qv, (VT*)h->x, (VT*)h->r, nullptr,
+                                              nullptr, h->tl_yc, h->sc, h->stream);
+        }
         CK(cudaEventRecord(b, h->stream));
         CK(cudaEventSynchronize(b));
         CK(cudaEventElapsedTime(&ms, a, b));
         out->tl_restrict_ms = ms / iters;
-        // p, q, x, r read; x, r written; offsets (16 B) and node list (4 B) per node
+        // p, q, x, r read; x, r written; offsets (16 B) and the node list or
+        // the aggregate id (4 B) per node
         out->tl_restrict_bytes = 18 * N * vs + 20 * N;
         CK(cudaMemsetAsync(&h->sc->done, 0, sizeof(int), h->stream));
         CK(cudaEventRecord(a, h->stream));

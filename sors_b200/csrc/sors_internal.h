@@ -200,6 +200,21 @@ void launch_coarse_restrict(const CoarseArgs& c, const VT* r, double* yc, cudaSt
 template <typename VT>
 void launch_tl_update_restrict(const CoarseArgs& c, const VT* p, const VT* qv, VT* x, VT* r, const uint8_t* pflag,
                                const double4* pn, double* yc, DevScalars* sc, cudaStream_t st);
+// Runs of the restriction over contiguous aggregates (k_tl_update_restrict_runs):
+// node blocks of 256 cut into runs of one aggregate; run k covers nodes
+// [run_start[k], run_start[k+1]); block b holds runs [block_run_ptr[b],
+// block_run_ptr[b+1]); aggregate a's runs are [agg_run_begin[a], agg_run_begin[a+1]).
+struct CoarseRuns {
+    const int* run_start = nullptr;      // nruns + 1
+    const int* block_run_ptr = nullptr;  // node blocks + 1
+    const int* agg_run_begin = nullptr;  // nagg + 1 (aggregates in run order)
+    double* partial = nullptr;           // 6 per run
+    int nruns = 0;
+};
+template <typename VT>
+void launch_tl_update_restrict_runs(const CoarseArgs& c, const CoarseRuns& ru, const VT* p, const VT* qv, VT* x,
+                                    VT* r, const uint8_t* pflag, const double4* pn, double* yc, DevScalars* sc,
+                                    cudaStream_t st);
 template <typename VT>
 void launch_tl_coarse_z(const CoarseArgs& c, int ld, const VT* Ainv, const double* yc, const VT* r, const VT* Minv,
                         VT* z, int init, const uint8_t* pflag, const double4* pn, double* partials, DevScalars* sc,
