@@ -191,6 +191,85 @@ __global__ void __launch_bounds__(kBT) k_bspmv(BatchArgs b, const int* __restric
     }
 }
 
+// q = A p for a block's nodes with LPR lanes per row, in passes of kBT / LPR
+// rows: each lane takes groups of two consecutive blocks of the row (nine
+// 8-byte FP32 / 16-byte FP64 loads for 18 values, both columns in one load,
+// one 16-byte gather of p per block), the row's lanes are summed with
+// shuffles, and the member's p.q is reduced as in k_bspmv.
+template <typename HT, typename VT, int LPR>
+__global__ void __launch_bounds__(kBT) k_bspmv_g(BatchArgs b, const int* __restrict__ row_ptr,
+                                                 const int* __restrict__ col, const HT* __restrict__ H,
+                                                 const VT* __restrict__ p, VT* __restrict__ qv) {
+    const int m = __ldg(b.blk_mem + blockIdx.x);
+    const int first = __ldg(b.mem_node0 + m) + (blockIdx.x - __ldg(b.mem_blk0 + m)) * kBT;
+    const int last = min(first + kBT, __ldg(b.mem_node0 + m + 1));
+    MemberScalars& ms = b.ms[m];
+    if (*(volatile int*)&ms.done) return;
+    constexpr int RPP = kBT / LPR;
+    const int sub = threadIdx.x / LPR, sl = threadIdx.x % LPR;
+    double acc[1] = {0.0};
+    for (int r0 = first; r0 < last; r0 += RPP) {
+        const int row = r0 + sub;
+        VT a0 = VT(0), a1 = VT(0), a2 = VT(0);
+        if (row < last) {
+            const int b0 = __ldg(row_ptr + row), b1 = __ldg(row_ptr + row + 1);
+            for (int gi = b0 / 2 + sl; gi <= (b1 - 1) / 2; gi += LPR) {
+                HT hv[18];
+                if constexpr (sizeof(HT) == 4) {
+                    const float2* src = reinterpret_cast<const float2*>(H) + 9 * (size_t)gi;
+#pragma unroll
+                    for (int k = 0; k < 9; k++) {
+                        const float2 t = __ldg(src + k);
+                        hv[2 * k] = t.x;
+                        hv[2 * k + 1] = t.y;
+                    }
+                } else {
+                    const double2* src = reinterpret_cast<const double2*>(H) + 9 * (size_t)gi;
+#pragma unroll
+                    for (int k = 0; k < 9; k++) {
+                        const double2 t = __ldg(src + k);
+                        hv[2 * k] = t.x;
+                        hv[2 * k + 1] = t.y;
+                    }
+                }
+                const int2 c2 = __ldg(reinterpret_cast<const int2*>(col) + gi);
+#pragma unroll
+                for (int u = 0; u < 2; u++) {
+                    const int bk = 2 * gi + u;
+                    if (bk < b0 || bk >= b1) continue;
+                    const int j = u == 0 ? c2.x : c2.y;
+                    const VT x0 = p[4 * (size_t)j], x1 = p[4 * (size_t)j + 1], x2 = p[4 * (size_t)j + 2];
+                    a0 += (VT)hv[9 * u] * x0 + (VT)hv[9 * u + 1] * x1 + (VT)hv[9 * u + 2] * x2;
+                    a1 += (VT)hv[9 * u + 3] * x0 + (VT)hv[9 * u + 4] * x1 + (VT)hv[9 * u + 5] * x2;
+                    a2 += (VT)hv[9 * u + 6] * x0 + (VT)hv[9 * u + 7] * x1 + (VT)hv[9 * u + 8] * x2;
+                }
+            }
+        }
+#pragma unroll
+        for (int o = LPR / 2; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (row < last && sl < 3) {
+            const VT qi = sl == 0 ? a0 : (sl == 1 ? a1 : a2);
+            qv[3 * (size_t)row + sl] = qi;
+            acc[0] += (double)p[4 * (size_t)row + sl] * (double)qi;
+        }
+    }
+    double tot[1];
+    if (member_reduce<1>(b, m, acc, 1, tot)) {
+        ms.pq = tot[0];
+        if (!(tot[0] > 0.0)) {
+            ms.breakdown = 1;
+            ms.done = 1;
+            ms.alpha = 0.0;
+        } else {
+            ms.alpha = ms.rz / tot[0];
+        }
+    }
+}
+
 template <typename VT>
 __global__ void __launch_bounds__(kBT) k_bupdate(BatchArgs b, const VT* __restrict__ p, const VT* __restrict__ qv,
                                                  const VT* __restrict__ Minv, VT* __restrict__ x, VT* __restrict__ r,
@@ -252,7 +331,13 @@ void launch_bpcg_iter(const BatchArgs& b, const int* row_ptr, const int* col, co
                       const VT* z_in, const VT* p_old, VT* p_new, VT* qv, VT* x, VT* r, VT* z,
                       const uint8_t* pflag, const double4* pn, cudaStream_t st) {
     k_bform_p<VT><<<b.nblocks, kBT, 0, st>>>(b, z_in, p_old, p_new);
-    k_bspmv<HT, VT><<<b.nblocks, kBT, 0, st>>>(b, row_ptr, col, H, p_new, qv);
+    const int groups = (b.max_row_blocks + 2) / 2;
+    if (groups <= 4)
+        k_bspmv_g<HT, VT, 4><<<b.nblocks, kBT, 0, st>>>(b, row_ptr, col, H, p_new, qv);
+    else if (groups <= 8)
+        k_bspmv_g<HT, VT, 8><<<b.nblocks, kBT, 0, st>>>(b, row_ptr, col, H, p_new, qv);
+    else
+        k_bspmv_g<HT, VT, 16><<<b.nblocks, kBT, 0, st>>>(b, row_ptr, col, H, p_new, qv);
     k_bupdate<VT><<<b.nblocks, kBT, 0, st>>>(b, p_new, qv, Minv, x, r, z, pflag, pn);
     g_kernel_launches.fetch_add(3, std::memory_order_relaxed);
 }

@@ -3051,6 +3051,7 @@ int sors_set_members(SorsHandle* h, const int32_t* node_offsets, int32_t n_membe
     b.mem_node0 = d_node0; b.mem_blk0 = d_blk0; b.blk_mem = d_blkmem; b.ms = d_ms; b.partials = d_part;
     b.nblocks = (int)blk_mem.size();
     b.nmem = n_members;
+    b.max_row_blocks = h->max_row_blocks;
     h->mem_node0_h.assign(node_offsets, node_offsets + n_members + 1);
     h->ms_h.assign(n_members, MemberScalars{});
     CK(cudaStreamSynchronize(h->stream));

@@ -156,6 +156,7 @@ struct MemberScalars {
 };
 struct BatchArgs {
     int nmem = 0, nblocks = 0;
+    int max_row_blocks = 0;           // longest block row (the SpMV's lanes per row)
     const int* mem_node0 = nullptr;   // nmem + 1: first node of each member
     const int* mem_blk0 = nullptr;    // nmem + 1: first thread block of each member
     const int* blk_mem = nullptr;     // nblocks: member of each thread block
