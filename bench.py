@@ -484,6 +484,7 @@ def run_c3(args):
             s.precision = precision; s.newtonResidualTol = 1e-8
             s.hessianProjection = PROJECTION[args.c3_projection]
             s.linearSolver = args.c3_solver
+            s.pressureJacobian = args.c3_pressure_jac
             fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
             en = ps.EnergyHex.from_arrays(X, H, s, np.zeros(3), 0.0, density=1070.0, youngsModulus=3e5,
                                           poissonsRatio=0.48, neumannBCmask=mask,
@@ -505,7 +506,7 @@ def run_c3(args):
             wall = time.perf_counter() - t0
             print(json.dumps({"workload": f"c3 pressure-actuated hex arm, static 10-level ramp to 50 kPa ({case})",
                               "precision": precision, "hessian_projection": args.c3_projection,
-                              "linear_solver": args.c3_solver,
+                              "linear_solver": args.c3_solver, "pressure_jacobian": args.c3_pressure_jac,
                               "hexes": int(H.shape[0]), "nodes": int(X.shape[0]), "chambers": len(groups),
                               "s_per_load_level": wall / levels, "newton_iters_per_level": newton / levels,
                               "pcg_iters_per_level": pcg / levels, "error": err,
@@ -755,6 +756,8 @@ def main():
     ap.add_argument("--batch", type=int, default=1, help="serve: rollouts packed into one union handle (1: none; unions measured slower on the poke mix)")
     ap.add_argument("--baseline-sample", type=int, default=64,
                     help="serve: measure the sequential FP64 baseline on every (rollouts / K)-th request")
+    ap.add_argument("--c3-pressure-jac", default="reference", choices=["reference", "exact"],
+                    help="c3: follower-load coefficient of the Newton matrix for quads (p/6 as the reference, or p/8)")
     ap.add_argument("--c3-solver", default="pcg", choices=["pcg", "minres"],
                     help="c3: Newton linear solver (minres takes the exact-Hessian step, with --c3-projection false)")
     ap.add_argument("--c3-projection", default="true", choices=sorted(PROJECTION),

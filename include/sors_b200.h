@@ -79,6 +79,12 @@ typedef struct SorsSettings {
                                 by block Jacobi on |D_ii| and the coarse
                                 correction of the projected Hessian.  Contact
                                 QPs, adjoints and unions use PCG.              */
+    int32_t pressure_jac_exact; /* 1: the Newton matrix takes the exact follower
+                                load coefficient for quads (p/8, the derivative of
+                                the quad force -p A / 4) instead of the reference's
+                                p/6 (pressureForce.cpp:105,174); the solution is
+                                the same, only the Newton iterates change.
+                                0 (default): the reference's                   */
 } SorsSettings;
 
 typedef struct SorsStepStats {

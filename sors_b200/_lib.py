@@ -38,6 +38,7 @@ class SorsSettings(C.Structure):
         ("newton_safeguard", C.c_int32),
         ("two_level", C.c_int32),
         ("linear_solver", C.c_int32),
+        ("pressure_jac_exact", C.c_int32),
     ]
 
 

@@ -607,6 +607,11 @@ double inertia_coef(const SorsHandle* h, double dt) {
 
 int method(const SorsHandle* h) { return h->s.solver_method; }
 
+// The Newton matrix's follower-load coefficient relative to the reference's
+// p/6: 1, or with settings.pressure_jac_exact the exact derivative of the quad
+// force -p A / 4 (p/8, 0.75 of p/6; triangles are exact at p/6).
+double pressure_jac_scale(const SorsHandle* h) { return (h->s.pressure_jac_exact && h->fnv == 4) ? 0.75 : 1.0; }
+
 PressureArgs pressure_args(SorsHandle* h) {
     PressureArgs p;
     p.nsurf = h->nsurf; p.surf_nodes = h->surf_nodes; p.sface_ptr = h->sface_ptr; p.sface_fl = h->sface_fl;
@@ -672,8 +677,8 @@ int eval_system(SorsHandle* h, double dt, bool want_hess, AsmMode mode = kAsmSte
     AsmArgs<HT> a = asm_args<HT>(h, dt, want_hess, mode, project);
     launch_assemble<HT>(a, h->max_pairs, h->stream);
     if (want_hess && h->has_pressure && method(h) == 0)
-        launch_pressure_jac<HT>(pressure_args(h), h->row_ptr, h->col, h->node_mask, a.hscale, (HT*)h->H, h->nnzb,
-                                h->stream);
+        launch_pressure_jac<HT>(pressure_args(h), h->row_ptr, h->col, h->node_mask, a.hscale * pressure_jac_scale(h),
+                                (HT*)h->H, h->nnzb, h->stream);
     launch_finalize_grad(h->N, h->g_int, h->f_ext, h->q, h->qPrev, h->vPrev, h->gPrev, h->gPrevTmp, h->mass,
                          h->node_mask, h->mval, dt, h->s.time_stepping, h->s.damping_alpha, h->s.grav,
                          a.neumann_override, (h->has_vforce || h->has_pressure) ? 1 : 0, h->g, h->partials, h->sc,
@@ -1156,7 +1161,7 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         bool conv = false;
         for (int k = 0; k < kAdjointPressureIters && !conv; k++) {
             CK(cudaMemsetAsync(h->adj_y, 0, sizeof(double) * n, h->stream));
-            launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? 1 : 0, h->adj_l, h->adj_y,
+            launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? pressure_jac_scale(h) : 0.0, h->adj_l, h->adj_y,
                                      h->stream);
             CK(d2h(h, corr.data(), h->adj_y, sizeof(double) * n));
             const std::vector<double> prev = lam;
@@ -1168,7 +1173,7 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         }
         if (!conv) return fail(SORS_ERR_NOT_CONVERGED, "the pressure-load adjoint fixed point did not converge");
         CK(cudaMemsetAsync(h->adj_y, 0, sizeof(double) * n, h->stream));
-        launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? 1 : 0, h->adj_l, h->adj_y,
+        launch_pressure_adj_corr(pressure_args(h), h->node_mask, method(h) == 0 ? pressure_jac_scale(h) : 0.0, h->adj_l, h->adj_y,
                                  h->stream);
         CK(d2h(h, corr.data(), h->adj_y, sizeof(double) * n));
     }
@@ -2249,6 +2254,7 @@ void sors_default_settings(SorsSettings* s) {
     s->newton_safeguard = 0;
     s->two_level = 2;
     s->linear_solver = 0;
+    s->pressure_jac_exact = 0;
 }
 
 int sors_last_error(char* buf, size_t n) {

@@ -1664,12 +1664,12 @@ void launch_pressure_jac(const PressureArgs& p, const int* row_ptr, const int* c
 //   T: the exact derivative of the residual's pressure term,
 //      d g_j / d x_k = p / (2 fnv) * 2 dA/dx_k for every vertex j of the face
 //      (face_hess gives 2 dA/dx_k; p/6 for triangles, p/8 for quads);
-//   S: what k_pressure_jac adds to the Newton matrix (with_s), the reference's
-//      coefficient p/6 for both face types, lower triangle mirrored, held
-//      DOFs skipped.
+//   S: what k_pressure_jac adds to the Newton matrix, s_scale times the
+//      reference's coefficient p/6 for both face types (0: none), lower
+//      triangle mirrored, held DOFs skipped.
 // The Newton matrix H = K + S is symmetric; the adjoint needs (K + T)^T =
 // H + (T^T - S).
-__global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, int with_s, const double* lam,
+__global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, double s_scale, const double* lam,
                                     double* y) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= p.nsurf) return;
@@ -1683,7 +1683,7 @@ __global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, in
         double h[4][9];
         face_hess(fv, p.fnv, p.q, h);
         const double pr = p.pressure[p.face_group[face]];
-        const double c_true = pr / (2.0 * p.fnv), c_ref = pr / 6.0;
+        const double c_true = pr / (2.0 * p.fnv), c_ref = s_scale * pr / 6.0;
         for (int kj = 0; kj < p.fnv; kj++) {
             int j = fv[kj];
             unsigned mj = node_mask[j];
@@ -1692,7 +1692,7 @@ __global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, in
                     const double lb = lam[3 * (size_t)j + m];
                     // (T^T lam)_a: T[b][a] = c_true h[ki](m, l), a = 3i+l, b = 3j+m
                     double v = c_true * h[ki][m * 3 + l];
-                    if (with_s && !((mi >> l) & 1u) && !((mj >> m) & 1u)) {
+                    if (s_scale != 0.0 && !((mi >> l) & 1u) && !((mj >> m) & 1u)) {
                         const long long a = 3LL * i + l, b = 3LL * j + m;
                         if (a > b) v -= c_ref * h[kj][l * 3 + m];
                         else if (a < b) v -= c_ref * h[ki][m * 3 + l];
@@ -1705,10 +1705,10 @@ __global__ void k_pressure_adj_corr(PressureArgs p, const uint8_t* node_mask, in
     for (int l = 0; l < 3; l++) y[3 * (size_t)i + l] = acc[l];
 }
 
-void launch_pressure_adj_corr(const PressureArgs& p, const uint8_t* node_mask, int with_s, const double* lam,
+void launch_pressure_adj_corr(const PressureArgs& p, const uint8_t* node_mask, double s_scale, const double* lam,
                               double* y, cudaStream_t st) {
     if (p.nsurf == 0) return;
-    k_pressure_adj_corr<<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, node_mask, with_s, lam, y);
+    k_pressure_adj_corr<<<(p.nsurf + 127) / 128, 128, 0, st>>>(p, node_mask, s_scale, lam, y);
     counted();
 }
 

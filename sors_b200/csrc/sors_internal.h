@@ -268,7 +268,7 @@ void launch_elem_rows(int E, int nv, const double* X, const double* q, const int
 void launch_elem_energy(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,
                         const MuscleArgs& mus, int material, double* partials, DevScalars* sc, cudaStream_t st);
 void launch_pressure_force(const PressureArgs& p, cudaStream_t st);
-void launch_pressure_adj_corr(const PressureArgs& p, const uint8_t* node_mask, int with_s, const double* lam,
+void launch_pressure_adj_corr(const PressureArgs& p, const uint8_t* node_mask, double s_scale, const double* lam,
                               double* y, cudaStream_t st);
 void launch_tet_shapes(int E, const double* X, const int* conn, double* out, cudaStream_t st);
 void launch_adjoint_elem(int E, int nv, const double* X, const double* q, const int* conn, const double2* mat,

@@ -65,6 +65,9 @@ class SimulationSettings:
         # Newton linear solver of "minimize_newton": "pcg", or "minres" for the
         # exact Newton step of an indefinite Hessian (the reference's LDL^T step)
         self.linearSolver = "pcg"
+        # follower-load coefficient of the Newton matrix for quads: "reference"
+        # (p/6, as pressureForce.cpp) or "exact" (p/8); the solution is the same
+        self.pressureJacobian = "reference"
         self.newtonResidualTol = 0.0       # absolute ||gradient|| stop; 0 = reference dx test only
         self.newtonDxTol = 1e-9            # reference DX_TOL (cpp/headers/common.h:25)
         self.newtonMaxIter = 100           # reference MAX_ITER (cpp/headers/common.h:21)
@@ -297,6 +300,10 @@ class _EnergyBase:
         if ls not in ("pcg", "minres"):
             raise ValueError(f"linearSolver must be 'pcg' or 'minres', not {ls!r}")
         s.linear_solver = 1 if ls == "minres" else 0
+        pj = getattr(settings, "pressureJacobian", "reference")
+        if pj not in ("reference", "exact"):
+            raise ValueError(f"pressureJacobian must be 'reference' or 'exact', not {pj!r}")
+        s.pressure_jac_exact = 1 if pj == "exact" else 0
         self._settings_c = s
         h = C.c_void_p()
         _lib.check(L.sors_create(_p(X, C.c_double), X.shape[0], _p(T, C.c_int32), ne, self.NV, _p(rho, C.c_double),

@@ -110,3 +110,35 @@ def test_linear_solver_setting_is_checked():
     params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [1000.0, 1e5, 0.45])] * ne
     with pytest.raises(ValueError):
         ps.Energy(X, T, s, np.zeros(3), 0.0, [{"neohookean"}] * ne, params, [], ps.Params(), [], ps.Params())
+
+
+def test_exact_quad_pressure_jacobian_same_solution(oracle):
+    """pressureJacobian = "exact" (p/8 for quads in the Newton matrix) changes
+    the Newton iterates, not the solution: the chamber cylinder ends where the
+    oracle's LDL^T Newton with the reference's p/6 ends."""
+    from sors_b200 import py_sors as ps
+    X, H = meshes.voxel_cylinder(length=0.015, h=2.5e-3, cap_layers=2)
+    groups, _ = meshes.extract_surfaces(X, H)
+    faces = np.concatenate(groups)
+    gid = np.concatenate([np.full(len(g), k) for k, g in enumerate(groups)])
+    ng = len(groups)
+    mask = np.repeat((np.abs(X[:, 2]) < 1e-12).astype(np.int32), 3)
+    o = oracle.System(X, H, rho=1070.0, youngs=3e5, nu=0.48, grav=(0, 0, 0), dt=0.0)
+    o.set_neumann(mask, np.zeros(mask.size)); o.set_pressure(faces, gid)
+    s = ps.SimulationSettings()
+    s.meshType = "Hexahedron"; s.dt = 0.0; s.timeSteppingScheme = "backward_euler"
+    s.precision = "fp64"; s.newtonResidualTol = 1e-10; s.pressureJacobian = "exact"
+    ne = H.shape[0]
+    params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [1070.0, 3e5, 0.48])] * ne
+    cp = ps.Params(["neumannBCmask", "neumannBCvalue"], [mask.astype(float), np.zeros(mask.size)])
+    fp = ps.Params(["surfaceVertexIdx", "surfaceGroups"], [faces.astype(float), gid.astype(float)])
+    en = ps.Energy(X, H, s, np.zeros(3), 0.0, [{"neohookean"}] * ne, params, ["neumannBC"], cp, ["pressure"], fp)
+    sol = ps.Solver(s)
+    q, qo = X.ravel().copy(), X.ravel().copy()
+    for level in (1, 2, 3):
+        pr = np.zeros(ng); pr[1] = 5e3 * level
+        qo, st = o.step(qo, dt=0.0, pressure=pr)
+        assert st == 0
+        q = sol.step(q, en, ps.Params(["pressure"], [pr.reshape(-1, 1)]), 0.0)
+    assert np.abs(qo - X.ravel()).max() > 1e-5
+    assert np.abs(q - qo).max() < 1e-8, np.abs(q - qo).max()
