@@ -2734,7 +2734,7 @@ __global__ void __launch_bounds__(kRunThreads) k_tl_update_restrict_runs(CoarseA
                                                                         VT* __restrict__ r,
                                                                         const uint8_t* __restrict__ pflag,
                                                                         const double4* __restrict__ pn,
-                                                                        double* __restrict__ yc, DevScalars* sc) {
+                                                                        const DevScalars* sc) {
     if (*(volatile const int*)&sc->done) return;
     __shared__ double ys[kRunThreads][6];
     const int i = blockIdx.x * kRunThreads + threadIdx.x;
@@ -2801,7 +2801,7 @@ void launch_tl_update_restrict_runs(const CoarseArgs& c, const CoarseRuns& ru, c
         return;
     }
     const int blocks = (c.N + kRunThreads - 1) / kRunThreads;
-    k_tl_update_restrict_runs<VT><<<blocks, kRunThreads, 0, st>>>(c, ru, p, qv, x, r, pflag, pn, yc, sc);
+    k_tl_update_restrict_runs<VT><<<blocks, kRunThreads, 0, st>>>(c, ru, p, qv, x, r, pflag, pn, sc);
     k_tl_restrict_finalize<<<(6 * c.nagg + 255) / 256, 256, 0, st>>>(c.nagg, ru, yc, sc);
     counted(2);
 }
