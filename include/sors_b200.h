@@ -210,6 +210,12 @@ int sors_set_initial_velocity(SorsHandle* h, const double* v);
 /* TimeIntegrator::get_qPrev / get_vPrev (cpp/headers/integrator.h:100-101). */
 int sors_get_state(SorsHandle* h, double* q_prev, double* v_prev);
 
+/* The Crank-Nicolson state's previous-step force gPrev_ (3N; cpp/headers/
+ * integrator.h:82, zero at construction), read and restored with q_prev and
+ * v_prev when a rollout is checkpointed. */
+int sors_get_prev_force(SorsHandle* h, double* g_prev);
+int sors_set_prev_force(SorsHandle* h, const double* g_prev);
+
 /* Energy::compute_energy (cpp/src/energy.cpp:208-248). */
 int sors_energy(SorsHandle* h, const double* q, double dt, double* out);
 
@@ -254,8 +260,9 @@ int sors_step(SorsHandle* h, const double* q_in, double* q_out, double dt, int32
  * add to dL/dq_next (and subtract from dL/dq_n).  With pressure loads the
  * transpose system uses the exact derivative of the follower load (not the
  * Newton matrix's symmetrised one; see sors_adjoint_pressure_grad); pressure
- * loads with held max-distance pairs, and Crank-Nicolson steps, return
- * SORS_ERR_UNSUPPORTED.  dt = 0 takes settings.dt. */
+ * loads with held max-distance pairs return SORS_ERR_UNSUPPORTED, and
+ * Crank-Nicolson steps are differentiated by sors_adjoint_step_cn.  dt = 0
+ * takes settings.dt. */
 int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
                       const int32_t* held_nodes, const double* held_normals, int32_t n_held, double* dL_dq_prev,
                       double* dL_dv_prev, double* dL_dyoungs, double* dL_dact, double* dL_dneumann,
@@ -267,6 +274,20 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
  * step's adjoint and f_g the follower load of group g at unit pressure on
  * q_next.  n_groups must equal the groups given to sors_set_pressure_faces. */
 int sors_adjoint_pressure_grad(SorsHandle* h, double* dL_dpressure, int32_t n_groups);
+
+/* Adjoint of one Crank-Nicolson step (no reference counterpart; the residual
+ * of cpp/src/integrator.cpp:72-78).  As sors_adjoint_step, plus the state's
+ * previous-step force: the step's residual holds 0.5 gPrev, and the next
+ * step's gPrev is this step's internal force at q_next.  dL_dgprev_next (3N,
+ * NULL = zero) is the cotangent of the next step's gPrev (the
+ * dL_dgprev_prev that the next step's call wrote); dL_dgprev_prev receives
+ * this step's.  The velocity of the state is v_next = 2 (q_next - q_n) / dt
+ * - v_n; the caller chains it as it chains v for backward Euler.  Pressure
+ * loads and held max-distance pairs return SORS_ERR_UNSUPPORTED. */
+int sors_adjoint_step_cn(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
+                         const double* dL_dgprev_next, const int32_t* held_nodes, const double* held_normals,
+                         int32_t n_held, double* dL_dq_prev, double* dL_dv_prev, double* dL_dgprev_prev,
+                         double* dL_dyoungs, double* dL_dact, double* dL_dneumann, SorsStepStats* stats);
 
 /* Same step on a device-resident FP64 solution vector (in place). */
 int sors_step_device(SorsHandle* h, double* q_device, double dt, int32_t substeps,

@@ -89,6 +89,10 @@ SIGNATURES = [
     ("sors_adjoint_step", C.c_int, [_h, _dp, C.c_double, _dp, _ip, _dp, C.c_int32, _dp, _dp, _dp, _dp, _dp,
                                     C.POINTER(SorsStepStats)]),
     ("sors_adjoint_pressure_grad", C.c_int, [_h, _dp, C.c_int32]),
+    ("sors_adjoint_step_cn", C.c_int, [_h, _dp, C.c_double, _dp, _dp, _ip, _dp, C.c_int32, _dp, _dp, _dp, _dp, _dp,
+                                       _dp, C.POINTER(SorsStepStats)]),
+    ("sors_get_prev_force", C.c_int, [_h, _dp]),
+    ("sors_set_prev_force", C.c_int, [_h, _dp]),
     ("sors_set_actuation", C.c_int, [_h, C.c_char_p, _dp, C.c_int64]),
     ("sors_set_initial_deformation", C.c_int, [_h, _dp]),
     ("sors_set_initial_velocity", C.c_int, [_h, _dp]),

@@ -18,6 +18,10 @@ held maxDistance pairs enter as equalities too, with their constraint
 curvature (the multiplier times the Hessian of |x_i - x_j|) in the transpose
 system.
 
+Crank-Nicolson rollouts (`timeSteppingScheme = "crank_nicolson"`) chain the
+state's previous-step force as well (`sors_adjoint_step_cn`; checkpoints keep
+it).
+
 `rollout(...)` is the torch entry point: a torch.autograd.Function whose inputs
 are float64 tensors E (E,) and act (T, G).  Follower-load pressures per step
 (`RolloutAdjoint.forward(..., pressure=...)`) are differentiated too
@@ -61,6 +65,9 @@ class RolloutAdjoint:
         self._pressure = None
         self.grad_pressure = None  # dL/d pressure (T, groups) after backward, with a pressure schedule
         self.last_pcg_iters = 0
+        # Crank-Nicolson: the state carries the previous step's internal force
+        # (zero at the start), and v_{t+1} = 2 (q_{t+1} - q_t) / dt - v_t
+        self.cn = int(energy._settings_c.time_stepping) == 1
 
     # -- helpers --------------------------------------------------------------
     def _set_material(self, E):
@@ -87,10 +94,20 @@ class RolloutAdjoint:
         L.sors_get_contact_state(self.en._h, _p(st, C.c_int32), k)
         return st
 
-    def _restore(self, q, v, cstate):
+    def _restore(self, q, v, cstate, g=None):
         self.en.set_initial_deformation(q)
         self.en.set_initial_velocity(v)
+        if self.cn:
+            g = np.zeros(self.en.ndof) if g is None else np.ascontiguousarray(g, dtype=np.float64)
+            _lib.check(_lib.load().sors_set_prev_force(self.en._h, _p(g)))
         _lib.check(_lib.load().sors_set_contact_state(self.en._h, _p(cstate, C.c_int32), cstate.size))
+
+    def _prev_force(self):
+        if not self.cn:
+            return None
+        g = np.zeros(self.en.ndof)
+        _lib.check(_lib.load().sors_get_prev_force(self.en._h, _p(g)))
+        return g
 
     def _held_now(self):
         L = _lib.load()
@@ -130,9 +147,9 @@ class RolloutAdjoint:
         self._held = {}
         for t in range(self.steps):
             if t % self.k == 0:
-                self._ckpt[t] = (q.copy(), v.copy(), self._contact_state())
+                self._ckpt[t] = (q.copy(), v.copy(), self._contact_state(), self._prev_force())
             qn = self._step(q, t)
-            v = (qn - q) / self.dt
+            v = 2.0 * (qn - q) / self.dt - v if self.cn else (qn - q) / self.dt
             q = qn
         return q
 
@@ -148,6 +165,7 @@ class RolloutAdjoint:
         gE = np.zeros(ne)
         gA = None if self._act is None else np.zeros_like(self._act)
         dq = np.zeros(n); dv = np.zeros(n); dE = np.zeros(ne); dA = np.zeros(max(G, 1))
+        Gb = np.zeros(n); dG = np.zeros(n)  # Crank-Nicolson: cotangent of the state's previous-step force
         P = 0 if self._pressure is None else self._pressure.shape[1]
         self.grad_pressure = None if P == 0 else np.zeros_like(self._pressure)
         dP = np.zeros(max(P, 1))
@@ -157,23 +175,32 @@ class RolloutAdjoint:
         starts = sorted(self._ckpt)
         for s in reversed(starts):
             e = min(s + self.k, self.steps)
-            q, v, cst = self._ckpt[s]
-            self._restore(q, v, cst)
+            q, v, cst, g = self._ckpt[s]
+            self._restore(q, v, cst, g)
             qs = [q.copy()]
             for t in range(s, e):
                 qs.append(self._step(qs[-1], t))
             for t in range(e - 1, s - 1, -1):
                 self._set_act(None if self._act is None else self._act[t])
                 self._set_pressure(None if self._pressure is None else self._pressure[t])
-                b = Qb + Vb / self.dt
+                # v_{t+1} = (q_{t+1} - q_t) / dt, or 2 (q_{t+1} - q_t) / dt - v_t (Crank-Nicolson)
+                cv = 2.0 / self.dt if self.cn else 1.0 / self.dt
+                b = Qb + cv * Vb
                 hn, hv, hp, hmu = self._held[t]
                 hv = np.ascontiguousarray(hv)
                 _lib.check(L.sors_adjoint_set_pairs(self.en._h, _p(hp, C.c_int32) if hp.size else None,
                                                     _p(hmu) if hp.size else None, hp.size))
-                _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b),
-                                               _p(hn, C.c_int32) if hn.size else None, _p(hv) if hn.size else None,
-                                               hn.size, _p(dq), _p(dv), _p(dE), _p(dA) if G else None, None,
-                                               C.byref(stats)))
+                if self.cn:
+                    _lib.check(L.sors_adjoint_step_cn(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b), _p(Gb),
+                                                      _p(hn, C.c_int32) if hn.size else None,
+                                                      _p(hv) if hn.size else None, hn.size, _p(dq), _p(dv), _p(dG),
+                                                      _p(dE), _p(dA) if G else None, None, C.byref(stats)))
+                    Gb = dG.copy()
+                else:
+                    _lib.check(L.sors_adjoint_step(self.en._h, _p(qs[t + 1 - s]), self.dt, _p(b),
+                                                   _p(hn, C.c_int32) if hn.size else None,
+                                                   _p(hv) if hn.size else None, hn.size, _p(dq), _p(dv), _p(dE),
+                                                   _p(dA) if G else None, None, C.byref(stats)))
                 self.last_pcg_iters += stats.pcg_iters
                 gE += dE
                 if G:
@@ -181,8 +208,8 @@ class RolloutAdjoint:
                 if P:
                     _lib.check(L.sors_adjoint_pressure_grad(self.en._h, _p(dP), P))
                     self.grad_pressure[t] = dP[:P]
-                Qb = dq - Vb / self.dt
-                Vb = dv.copy()
+                Qb = dq - cv * Vb
+                Vb = dv - Vb if self.cn else dv.copy()
         return gE, gA, Qb, Vb
 
 

@@ -1088,7 +1088,7 @@ constexpr int kAdjointPressureIters = 200;
 template <typename HT, typename VT>
 int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b, const int* held_nodes,
                  const double* held_normals, int n_held, double* dq, double* dv, double* dE, double* dact,
-                 double* dneu, SorsStepStats* stats) {
+                 double* dneu, SorsStepStats* stats, const double* bg_in = nullptr, double* bg_out = nullptr) {
     const int n = h->ndof, N = h->N, E = h->E;
     int st;
     if (!h->adj_l) {
@@ -1124,6 +1124,22 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
     CK(h2d(h, h->pn_d, h->pn_h.data(), sizeof(double4) * N));
     std::vector<double> lam(n), rhs(b, b + n);
     const double eta = mixed(h) ? 1e-6 : std::max(1e-12, 0.01 * h->s.pcg_rel_tol);
+    // Crank-Nicolson: the next step's residual holds 0.5 gi(q_next), gi the
+    // internal force (gPrev), so its cotangent bg_in adds K^T bg_in to the
+    // right-hand side; K = 2 (H - c M) with H the step's matrix (inertia c M
+    // plus 0.5 K), evaluated by the SpMV of H.
+    const bool cn = h->s.time_stepping == 1 && dt != 0.0;
+    const double c_in = inertia_coef(h, dt);
+    std::vector<double> bg;
+    if (cn && bg_in) bg.assign(bg_in, bg_in + n);
+    if (!bg.empty()) {
+        CK(h2d(h, h->qp_dx, bg.data(), sizeof(double) * n));
+        launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->qp_dx, h->adj_y, h->stream);
+        std::vector<double> hb(n);
+        CK(d2h(h, hb.data(), h->adj_y, sizeof(double) * n));
+        for (int i = 0; i < n; i++) rhs[i] += 2.0 * (hb[i] - c_in * h->mass_h[i / 3] * bg[i]);
+    }
+    const std::vector<double> rhs0 = rhs;
     // lam = H^-1 rhs on the free subspace (H symmetric)
     auto solve = [&](const std::vector<double>& r) -> int {
         std::vector<double> g(n);
@@ -1165,7 +1181,7 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
                                      h->stream);
             CK(d2h(h, corr.data(), h->adj_y, sizeof(double) * n));
             const std::vector<double> prev = lam;
-            for (int i = 0; i < n; i++) rhs[i] = b[i] - corr[i];
+            for (int i = 0; i < n; i++) rhs[i] = rhs0[i] - corr[i];
             if ((st = solve(rhs))) return st;
             double dd = 0.0, ll = 0.0;
             for (int i = 0; i < n; i++) { dd += (lam[i] - prev[i]) * (lam[i] - prev[i]); ll += lam[i] * lam[i]; }
@@ -1183,8 +1199,17 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         if ((st = adjoint_pairs<HT, VT>(h, eta, lam, extra, &pp))) return st;
         if (stats) stats->pcg_iters += pp;
     }
-    // element contractions with lam (zero on fixed DOFs and along held normals)
-    launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, h->adj_l, h->adj_e,
+    // element contractions with lam (zero on fixed DOFs and along held normals);
+    // Crank-Nicolson: the step's 0.5 gi(q_next) and the next step's gPrev =
+    // gi(q_next), i.e. with 0.5 lam - bg_in
+    const double* lam_elem = h->adj_l;
+    if (cn) {
+        std::vector<double> le(n);
+        for (int i = 0; i < n; i++) le[i] = 0.5 * lam[i] - (bg.empty() ? 0.0 : bg[i]);
+        CK(h2d(h, h->qp_dx, le.data(), sizeof(double) * n));
+        lam_elem = h->qp_dx;
+    }
+    launch_adjoint_elem(E, h->nv, h->X, h->q, h->conn, h->mat, muscles(h), h->s.material, lam_elem, h->adj_e,
                         h->stream);
     std::vector<double> ge((size_t)2 * std::max(1, E));
     CK(d2h(h, ge.data(), h->adj_e, sizeof(double) * 2 * (size_t)E));
@@ -1193,16 +1218,19 @@ int adjoint_impl(SorsHandle* h, const double* q_next, double dt, const double* b
         launch_spmv_plain<HT>(N, h->row_ptr, h->col, (const HT*)h->H, h->nnzb, h->adj_l, h->adj_y, h->stream);
         CK(d2h(h, r.data(), h->adj_y, sizeof(double) * n));
         for (int i = 0; i < n; i++)
-            r[i] = b[i] - r[i] + (extra.empty() ? 0.0 : extra[i]) - (corr.empty() ? 0.0 : corr[i]);
+            r[i] = rhs0[i] - r[i] + (extra.empty() ? 0.0 : extra[i]) - (corr.empty() ? 0.0 : corr[i]);
     }
     const double a = h->s.damping_alpha;
     for (int i = 0; i < n; i++) {
         const double m = h->mass_h[i / 3];
         const bool f = fixed(i);
-        const double inert = dt != 0.0 ? lam[i] * (m / (dt * dt) + a * m / dt) : 0.0;
+        // d g / d q_n = -c M; d g / d v_n = -M / dt (backward Euler), -(2 / dt + alpha) M (Crank-Nicolson)
+        const double inert = dt != 0.0 ? lam[i] * m * c_in : 0.0;
         if (dq) dq[i] = f ? r[i] : inert;
-        if (dv) dv[i] = dt != 0.0 ? lam[i] * m / dt : 0.0;
+        if (dv) dv[i] = dt != 0.0 ? lam[i] * m * (cn ? 2.0 / dt + a : 1.0 / dt) : 0.0;
         if (dneu) dneu[i] = f ? r[i] * dt : 0.0;
+        // the step's residual holds 0.5 gPrev
+        if (bg_out) bg_out[i] = cn ? -0.5 * lam[i] : 0.0;
     }
     CK(cudaMemcpyAsync(h->adj_q, h->q, sizeof(double) * n, cudaMemcpyDeviceToDevice, h->stream));
     h->adj_ready = true;
@@ -2880,7 +2908,7 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if ((st = set_device(h))) return st;
     if (dt == 0.0) dt = h->s.dt;
     if (h->s.time_stepping != 0 && dt != 0.0)
-        return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for backward Euler steps");
+        return fail(SORS_ERR_UNSUPPORTED, "Crank-Nicolson steps are differentiated by sors_adjoint_step_cn");
     if (h->has_pressure && !h->adj_pairs.empty())
         return fail(SORS_ERR_UNSUPPORTED, "the adjoint does not combine pressure loads with held max-distance pairs");
     if (h->s.material == 1) return fail(SORS_ERR_UNSUPPORTED, "the adjoint is built for Neo-Hookean elements");
@@ -2911,6 +2939,63 @@ int sors_adjoint_step(SorsHandle* h, const double* q_next, double dt, const doub
     if (dL_dq_prev) dofs_to_caller(h, oq.data(), dL_dq_prev);
     if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
     if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
+    return SORS_OK;
+}
+
+int sors_adjoint_step_cn(SorsHandle* h, const double* q_next, double dt, const double* dL_dq_next,
+                         const double* dL_dgprev_next, const int32_t* held_nodes, const double* held_normals,
+                         int32_t n_held, double* dL_dq_prev, double* dL_dv_prev, double* dL_dgprev_prev,
+                         double* dL_dyoungs, double* dL_dact, double* dL_dneumann, SorsStepStats* stats) {
+    if (!h || !q_next || !dL_dq_next) return fail(SORS_ERR_ARG, "NULL argument");
+    if (n_held < 0 || (n_held > 0 && (!held_nodes || !held_normals))) return fail(SORS_ERR_ARG, "held contacts");
+    int st;
+    if ((st = set_device(h))) return st;
+    if (dt == 0.0) dt = h->s.dt;
+    if (h->s.time_stepping != 1 || dt == 0.0)
+        return fail(SORS_ERR_ARG, "sors_adjoint_step_cn differentiates Crank-Nicolson steps (dt > 0)");
+    if (h->has_pressure || !h->adj_pairs.empty() || h->s.material == 1)
+        return fail(SORS_ERR_UNSUPPORTED,
+                    "the Crank-Nicolson adjoint is built for Neo-Hookean elements without pressure loads or held pairs");
+    if (stats) *stats = SorsStepStats{};
+    const int n = h->ndof;
+    const std::vector<double> qn = dofs_to_internal(h, q_next), bq = dofs_to_internal(h, dL_dq_next);
+    std::vector<double> bgi;
+    if (dL_dgprev_next) bgi = dofs_to_internal(h, dL_dgprev_next);
+    std::vector<int32_t> hn(n_held);
+    for (int c = 0; c < n_held; c++) hn[c] = node_in(h, held_nodes[c]);
+    std::vector<double> oq(n), ov(n), og(n), on(n), oe(h->E);
+    st = mixed(h) ? adjoint_impl<float, float>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
+                                               oq.data(), ov.data(), oe.data(), dL_dact, on.data(), stats,
+                                               bgi.empty() ? nullptr : bgi.data(), og.data())
+                  : adjoint_impl<double, double>(h, qn.data(), dt, bq.data(), hn.data(), held_normals, n_held,
+                                                 oq.data(), ov.data(), oe.data(), dL_dact, on.data(), stats,
+                                                 bgi.empty() ? nullptr : bgi.data(), og.data());
+    if (st) return st;
+    if (dL_dyoungs)
+        for (int e = 0; e < h->E; e++) dL_dyoungs[elem_out(h, e)] = oe[e];
+    if (dL_dq_prev) dofs_to_caller(h, oq.data(), dL_dq_prev);
+    if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
+    if (dL_dgprev_prev) dofs_to_caller(h, og.data(), dL_dgprev_prev);
+    if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
+    (void)n;
+    return SORS_OK;
+}
+
+int sors_get_prev_force(SorsHandle* h, double* g_prev) {
+    if (!h || !g_prev) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    if ((st = dof_out(h, g_prev, h->gPrev, cudaMemcpyDeviceToHost))) return st;
+    CK(cudaStreamSynchronize(h->stream));
+    return SORS_OK;
+}
+
+int sors_set_prev_force(SorsHandle* h, const double* g_prev) {
+    if (!h || !g_prev) return fail(SORS_ERR_ARG, "NULL argument");
+    int st;
+    if ((st = set_device(h))) return st;
+    if ((st = dof_in(h, h->gPrev, g_prev, cudaMemcpyHostToDevice))) return st;
+    CK(cudaStreamSynchronize(h->stream));
     return SORS_OK;
 }
 
