@@ -177,6 +177,7 @@ struct SorsHandle {
     // Galerkin coarse matrix and its inverse (refreshed when PCG slows down)
     bool tl_ready = false, tl_active = false;
     bool tl_proj = false;             // the coarse operator came from the projected Hessian
+    size_t l2_window_bytes = 0;       // coarse inverse marked persisting in L2 (keep_coarse_in_l2)
     double tl_ref_rate = 0.0;
     CoarseArgs cargs;
     CoarseRuns cruns;                 // nruns > 0: aggregates are contiguous node ranges
@@ -887,6 +888,46 @@ int pcg_solve_members(SorsHandle* h, double eta, double abs_tol, int* iters, con
     return SORS_OK;
 }
 
+// Keeps the coarse inverse in L2 between PCG iterations: an access-policy
+// window on the handle's stream (captured into the PCG graphs) marks it
+// persisting, within the context's persisting-L2 limit (a per-process
+// setting that ends with the process).  The SpMV streams several times the
+// L2 through between two coarse solves and would evict it otherwise.
+void keep_coarse_in_l2(SorsHandle* h, size_t bytes) {
+    if (h->l2_window_bytes == bytes) return;
+    int dev = 0, maxp = 0, maxw = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&maxp, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess || maxp <= 0 ||
+        maxw <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    size_t limit = 0;
+    cudaDeviceGetLimit(&limit, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min((size_t)maxp, bytes);
+    if (limit < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaStreamAttrValue v = {};
+    v.accessPolicyWindow.base_ptr = h->tl_Ainv;
+    v.accessPolicyWindow.num_bytes = std::min((size_t)maxw, bytes);
+    v.accessPolicyWindow.hitRatio = (float)std::min(1.0, (double)std::max(limit, want) / (double)v.accessPolicyWindow.num_bytes);
+    v.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    v.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    if (cudaStreamSetAttribute(h->stream, cudaStreamAttributeAccessPolicyWindow, &v) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    h->l2_window_bytes = bytes;
+    // graphs captured before carry no window: capture again
+    if (h->pcg_exec) {
+        cudaGraphExecDestroy(h->pcg_exec);
+        h->pcg_exec = nullptr;
+    }
+}
+
 // The coarse operator P^T H P of the Hessian in h->H, inverted in place.
 template <typename HT, typename VT>
 int build_coarse(SorsHandle* h) {
@@ -900,6 +941,7 @@ int build_coarse(SorsHandle* h) {
                                  h->nnzb, h->cargs, h->tl_Ac, h->stream);
     launch_coarse_invert(nc, h->tl_Ac, h->tl_rowk, h->tl_colk, h->stream);
     launch_to_vt_pad<VT>(nc, h->tl_ld, h->tl_Ac, (VT*)h->tl_Ainv, h->stream);
+    keep_coarse_in_l2(h, (size_t)nc * h->tl_ld * sizeof(VT));
     h->tl_ready = true;
     h->tl_refreshes++;
     return SORS_OK;
