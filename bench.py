@@ -534,8 +534,9 @@ def c4_case(seed, steps):
 def c4_energy(X, H, E, surf, precision="fp64", members=1):
     """Energy/Solver of `members` copies of the C4 bar in one handle (a union:
     the copies share no element, so the system, its contacts and its adjoint
-    are the direct sum of the copies'; every kernel launch serves all of them).
-    Each element is its own muscle group."""
+    are the direct sum of the copies'; every kernel launch serves all of them,
+    and each linear solve runs one PCG per copy).  Each element is its own
+    muscle group."""
     from sors_b200 import py_sors as ps
     s = ps.SimulationSettings()
     s.meshType = "Hexahedron"; s.dt = 2e-3; s.timeSteppingScheme = "backward_euler"
@@ -554,6 +555,13 @@ def c4_energy(X, H, E, surf, precision="fp64", members=1):
     cp.set_param("normalVectorListPlanes", np.array([0.0, 0.0, 1.0]))
     cp.set_param("surfaceVerticesIdx", su.astype(float))
     en._setup_constraints_forces(["planeContact"], cp, (), None)
+    if members > 1:
+        # one PCG per copy in shared launches (member-segmented solves)
+        import ctypes
+        from sors_b200 import _lib
+        offs = np.arange(members + 1, dtype=np.int32) * n1
+        _lib.check(_lib.load().sors_set_members(en._h, offs.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                                members))
     return en, ps.Solver(s)
 
 
