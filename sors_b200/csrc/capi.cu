@@ -3002,6 +3002,7 @@ int sors_adjoint_step_cn(SorsHandle* h, const double* q_next, double dt, const d
     const int n = h->ndof;
     const std::vector<double> qn = dofs_to_internal(h, q_next), bq = dofs_to_internal(h, dL_dq_next);
     std::vector<double> bgi;
+    // (every output is computed in the handle's numbering, then converted)
     if (dL_dgprev_next) bgi = dofs_to_internal(h, dL_dgprev_next);
     std::vector<int32_t> hn(n_held);
     for (int c = 0; c < n_held; c++) hn[c] = node_in(h, held_nodes[c]);
@@ -3019,7 +3020,6 @@ int sors_adjoint_step_cn(SorsHandle* h, const double* q_next, double dt, const d
     if (dL_dv_prev) dofs_to_caller(h, ov.data(), dL_dv_prev);
     if (dL_dgprev_prev) dofs_to_caller(h, og.data(), dL_dgprev_prev);
     if (dL_dneumann) dofs_to_caller(h, on.data(), dL_dneumann);
-    (void)n;
     return SORS_OK;
 }
 

@@ -101,17 +101,6 @@ def test_minres_c3_chamber_pressure_matches_oracle(oracle, precision):
     assert np.abs(q - qo).max() < tol, np.abs(q - qo).max()
 
 
-def test_linear_solver_setting_is_checked():
-    from sors_b200 import py_sors as ps
-    X, T, mask, q0 = _compressed_bar()
-    s = ps.SimulationSettings()
-    s.meshType = "Tetrahedron"; s.dt = 1e-2; s.linearSolver = "gmres"
-    ne = T.shape[0]
-    params = [ps.Params(["density", "youngsModulus", "poissonsRatio"], [1000.0, 1e5, 0.45])] * ne
-    with pytest.raises(ValueError):
-        ps.Energy(X, T, s, np.zeros(3), 0.0, [{"neohookean"}] * ne, params, [], ps.Params(), [], ps.Params())
-
-
 def test_exact_quad_pressure_jacobian_same_solution(oracle):
     """pressureJacobian = "exact" (p/8 for quads in the Newton matrix) changes
     the Newton iterates, not the solution: the chamber cylinder ends where the
