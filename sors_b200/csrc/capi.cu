@@ -98,6 +98,7 @@ struct SorsHandle {
     int asm_variant = 0;  // 0: chunked element-owner where it applies, 1: row-owner, 2: two-pass chunked
     void* hex_tile = nullptr;         // hexes: element tiles of the element-owner assembly
     double* hex_gtile = nullptr;
+    int* hex_blk_row = nullptr;       // hexes: the row of each CSR block
     void* chunk_gen = nullptr;        // two-pass variant: element generator records
     double* chunk_gradg = nullptr;    // two-pass variant: element gradient rows
     uint8_t* node_mask = nullptr;
@@ -660,6 +661,7 @@ AsmArgs<HT> asm_args(SorsHandle* h, double dt, bool want_hess, AsmMode mode, int
         a.ch = h->chunks;
         a.hex_tile = h->hex_tile;
         a.hex_gtile = h->hex_gtile;
+        a.hex_blk_row = h->hex_blk_row;
     }
     if (h->asm_variant == 2) {
         a.ch.gen = h->chunk_gen;
@@ -2437,6 +2439,10 @@ int sors_create(const double* X, int32_t n_nodes, const int32_t* conn, int32_t n
         // element tiles of the element-owner hex assembly
         if ((st = dalloc(h, &h->hex_tile, (size_t)E * 36 * 9 * hsize(h)))) return bail(st);
         if ((st = dalloc_t(h, &h->hex_gtile, (size_t)E * 24))) return bail(st);
+        std::vector<int> br((size_t)h->nnzb);
+        for (int i = 0; i < N; i++)
+            for (int b = h->row_ptr_h[i]; b < h->row_ptr_h[i + 1]; b++) br[b] = i;
+        if ((st = upload(h, &h->hex_blk_row, br.data(), br.size()))) return bail(st);
     }
     const size_t nd = (size_t)3 * N;
     double** vecs[] = {&h->q, &h->q0, &h->qPrev, &h->vPrev, &h->gPrev, &h->gPrevTmp, &h->g, &h->g_int, &h->f_ext,

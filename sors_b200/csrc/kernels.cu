@@ -1411,6 +1411,69 @@ __global__ void __launch_bounds__(256) k_hex_gather(AsmArgs<HT> a) {
     }
 }
 
+// Pass 2 with a thread per CSR block (the row from hex_blk_row), so that the
+// lanes of a warp write consecutive blocks, then a thread per gradient entry;
+// each block and each entry sums its items in slot order, as k_hex_gather.
+template <typename HT>
+__global__ void __launch_bounds__(256) k_hex_gather_blocks(AsmArgs<HT> a, long long nblk) {
+    const HT* tiles = reinterpret_cast<const HT*>(a.hex_tile);
+    const long long total = nblk + 3LL * a.N;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        if (t >= nblk) {
+            // gradient entry u of row u / 3
+            const long long u = t - nblk;
+            const int row = (int)(u / 3), lane = (int)(u - 3 * (u / 3));
+            double g = 0.0;
+            for (int p = __ldg(a.pair_ptr + row); p < __ldg(a.pair_ptr + row + 1); p++) {
+                const int ev = __ldg(a.pair_ev + p);
+                g += a.hex_gtile[(size_t)(ev >> 3) * 24 + (ev & 7) * 3 + lane];
+            }
+            if (a.apply_mask && ((a.node_mask[row] >> lane) & 1u)) g = 0.0;
+            a.g_int[3 * (size_t)row + lane] = g;
+            continue;
+        }
+        const int bg = (int)t;
+        const int row = __ldg(a.hex_blk_row + bg);
+        const int p0 = __ldg(a.pair_ptr + row);
+        const unsigned mrow = a.node_mask[row];
+        HT acc[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) acc[k] = HT(0);
+        for (int it = __ldg(a.slot_item_ptr + bg); it < __ldg(a.slot_item_ptr + bg + 1); ++it) {
+            const int item = __ldg(a.slot_items + it);
+            const int kp = item >> 3, w = item & 7;
+            const int ev = __ldg(a.pair_ev + p0 + kp);
+            const int e = ev >> 3, v = ev & 7;
+            const HT* T = tiles + ((size_t)e * 36 + (v <= w ? hex_upper(v, w) : hex_upper(w, v))) * 9;
+            if (v <= w) {
+#pragma unroll
+                for (int k = 0; k < 9; k++) acc[k] += T[k];
+            } else {
+#pragma unroll
+                for (int r = 0; r < 3; r++)
+#pragma unroll
+                    for (int c = 0; c < 3; c++) acc[r * 3 + c] += T[c * 3 + r];
+            }
+        }
+        const int j = __ldg(a.col + bg);
+        const unsigned mcol = a.node_mask[j];
+        const double md = a.inertia_coef * a.mass[row];
+#pragma unroll
+        for (int rc = 0; rc < 9; rc++) {
+            const int r = rc / 3, c = rc - 3 * (rc / 3);
+            const bool rmask = (mrow >> r) & 1u;
+            double val = (double)acc[rc] * a.hscale;
+            if (a.apply_mask && (rmask || ((mcol >> c) & 1u))) val = 0.0;
+            if (j == row && r == c) {
+                val += md;
+                if (a.neumann_override && rmask) val = 1.0;
+            }
+            a.H[hval(bg, rc, a.nnzb)] = (HT)val;
+        }
+    }
+}
+
 template <typename HT>
 static void launch_hex_tiles(const AsmArgs<HT>& a, cudaStream_t st) {
     const bool snh = a.material == 2, proj = a.project != 0;
@@ -1418,8 +1481,15 @@ static void launch_hex_tiles(const AsmArgs<HT>& a, cudaStream_t st) {
     auto k = snh ? (proj ? k_hex_tiles<HT, true, true> : k_hex_tiles<HT, true, false>)
                  : (proj ? k_hex_tiles<HT, false, true> : k_hex_tiles<HT, false, false>);
     if (a.E > 0) k<<<(int)hb, 32 * kHexWarps, 0, st>>>(a, a.E);
-    const long long gb = cap_grid(((long long)a.N + 7) / 8);
-    k_hex_gather<HT><<<(int)gb, 256, 0, st>>>(a);
+    if (a.hex_blk_row) {
+        const long long nblk = a.want_hess ? a.nnzb : 0;
+        const long long total = nblk + 3LL * a.N;
+        const long long gb = cap_grid((total + 255) / 256);
+        k_hex_gather_blocks<HT><<<(int)gb, 256, 0, st>>>(a, nblk);
+    } else {
+        const long long gb = cap_grid(((long long)a.N + 7) / 8);
+        k_hex_gather<HT><<<(int)gb, 256, 0, st>>>(a);
+    }
     counted(2);
 }
 

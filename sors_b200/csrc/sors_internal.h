@@ -130,6 +130,7 @@ struct AsmArgs {
     ChunkArgs ch;           // element-owner tet assembly (used when ch.nchunks > 0)
     void* hex_tile = nullptr;      // hexes: 36 upper 3x3 blocks (HT) per element, written by k_hex_tiles
     double* hex_gtile = nullptr;   // hexes: 8 gradient rows per element
+    const int* hex_blk_row = nullptr;  // hexes: the row of each CSR block (k_hex_gather_blocks)
 };
 
 struct PressureArgs {
